@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Benchmark: solves/s at relative residual 1e-6 on one B200.
+
+Workload (TET10): 1.0 x 0.1 x 0.1 m cantilever,
+200 x 20 x 20 hex cells Kuhn-split into 480,000 TET10 elements / 674,081 nodes
+(2,022,243 DOF); SVK E = 1e7 Pa, nu = 0.3, rho = 1000; nodes at x = 0 clamped;
+a seeded total load (magnitude U[10, 1000] N, seed 0) in -z split over the
+x = 1 face.  A step is one LinearStaticSolver::Solve() from the reference
+configuration: stiffness assembly at the current positions, Dirichlet
+elimination, unpreconditioned FP64 CG to ||r||/||f|| < 1e-6, position update.
+
+The JSON line carries
+  value     solves/s with all inputs resident in HBM (CUDA events on the
+            element's stream, max over ranks; --gpus N runs N replicas);
+  e2e       the same through the public API with host buffers: per step the
+            external force and reference positions go host->device and the
+            solved positions come back;
+  roofline  the dominant kernel of the step (the CG SpMV on 3x3 node blocks);
+  elem_force  the fused element-force kernel (FP32 and FP64) in GB/s of the
+            algorithmic bytes E*(4*NPE + QP*NPE*3*s + QP*s) + N*6*s;
+  cpu_baseline the CPU oracle (C + OpenMP) on a bounded sample.
+Inputs are larger than L2 (K: 1.35 GB, gradient stream: 0.29 / 0.58 GB).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CFG = dict(nx=200, ny=20, nz=20, order=10, lx=1.0, ly=0.1, lz=0.1, E=1e7, nu=0.3, rho=1000.0, tol=1e-6, seed=0)
+METRIC = "solves/s at rel. residual 1e-6 (plain CG linear static, 200x20x20 TET10 beam); elem-force GB/s"
+# CG iterations the CUDA path needs for this workload (used by the CPU legs to
+# turn a bounded sample into solves/s); refreshed from the GPU run when known.
+CG_ITERS_CFG2 = None
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_magnitude(seed):
+    return float(np.random.default_rng(seed).uniform(10.0, 1000.0))
+
+
+def build_mesh(cfg):
+    from tlfea_b200 import mesh as M
+
+    x, y, z, conn = M.box_mesh(cfg["nx"], cfg["ny"], cfg["nz"], cfg["order"], cfg["lx"], cfg["ly"], cfg["lz"])
+    fixed, f, tip = M.cantilever_loads(x, y, z, (0.0, 0.0, -load_magnitude(cfg["seed"])))
+    return x, y, z, conn, fixed, f
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device_index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def elem_force_bytes(E, N, npe, nqp, s):
+    return E * (4 * npe + nqp * npe * 3 * s + nqp * s) + N * 6 * s
+
+
+def spmv_bytes(N, nnzb):
+    # 3x3 blocks: 72 B values + 4 B column per block, row offsets, p read, q write
+    return nnzb * (9 * 8 + 4) + (N + 1) * 4 + 3 * N * 8 * 2
+
+
+def time_stream(torch, stream_ptr, fn, reps):
+    st = torch.cuda.ExternalStream(stream_ptr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(reps):
+        fn()
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def cpu_sample(x, y, z, conn, fixed, f, cfg, iters_per_solve, gpu_K=None, threads=0):
+    """Oracle timing on the host: full stiffness assembly + a few CG
+    iterations, extrapolated to one solve with the CUDA path's iteration count."""
+    from oracle import oracle as O
+
+    if threads:
+        O.set_threads(threads)
+    lam = cfg["E"] * cfg["nu"] / ((1 + cfg["nu"]) * (1 - 2 * cfg["nu"]))
+    mu = cfg["E"] / (2 * (1 + cfg["nu"]))
+    t0 = time.perf_counter()
+    g, dj = O.dndu_pre(x, y, z, conn)
+    t_pre = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    off, cols, vals = O.stiffness(x, y, z, conn, g, dj, lam, mu)
+    kv, fb = O.apply_bcs(off, cols, vals, f, fixed)
+    t_asm = time.perf_counter() - t0
+    m = 5
+    t0 = time.perf_counter()
+    u, it, res, rc = O.cg(off, cols, kv, fb, 0.0, m)
+    t_cg = (time.perf_counter() - t0) / max(it, 1)
+    per_solve = t_asm + iters_per_solve * t_cg
+    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": O.get_threads(), "kind": "port",
+            "sample": (f"oracle (C, OpenMP): full stiffness assembly + BCs ({t_asm:.2f} s) and {it} CG iterations "
+                       f"({t_cg * 1e3:.1f} ms each) timed; one solve = assembly + {iters_per_solve} iterations "
+                       f"(the CUDA path's count); gradient precompute {t_pre:.2f} s not counted")}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = dict(CFG)
+    x, y, z, conn, fixed, f = build_mesh(cfg)
+    iters = CG_ITERS_CFG2 or 3000
+    vals = []
+    for i in range(args.warmup + args.steps):
+        s = cpu_sample(x, y, z, conn, fixed, f, cfg, iters)
+        if i >= args.warmup:
+            vals.append(s["value"])
+    v = float(np.median(vals))
+    s["value"] = v
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "cantilever 200x20x20 TET10 linear static CG to 1e-6", "elements": int(conn.shape[0]),
+                      "nodes": int(len(x)), "parallelism": f"replicas{args.gpus}"},
+           "cpu_baseline": s, "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="tlfea", choices=["tlfea", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--kernel-reps", type=int, default=20)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import tlfea_b200 as T
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    cfg = dict(CFG)
+    x, y, z, conn, fixed, f = build_mesh(cfg)
+    N, E = len(x), conn.shape[0]
+    el = T.GPU_FEAT10_Data(E, N)
+    el.Initialize()
+    el.SetNodalFixed(fixed)
+    el.SetExternalForce(f)
+    el.Setup(*T.Quadrature.t10(), x, y, z, conn)
+    el.SetDensity(cfg["rho"])
+    el.SetDamping(0.0, 0.0)
+    el.SetSVK(cfg["E"], cfg["nu"])
+    el.CalcDnDuPre()
+    el.CalcMassMatrix()
+    solver = T.LinearStaticSolver(el, cfg["tol"], 1000000)
+    stream = el.GetStream()
+
+    def step():
+        el.ResetPositions()
+        solver.Solve()
+
+    for _ in range(args.warmup):
+        step()
+    iters = solver.GetLastIterCount()
+    resid = solver.GetLastResidual()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = T.launch_count()
+    with ClockSampler(local) as clk:
+        ms = time_stream(torch, stream, step, args.steps)
+    launches = T.launch_count() - l0
+    t_total = ms * args.steps / 1e3
+    if dist:
+        tt = torch.tensor([t_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total = float(tt.item())
+    value = world * args.steps / t_total
+
+    # e2e through the public API with host buffers
+    def e2e_step():
+        el.SetExternalForce(f)
+        el.UpdatePositions(x, y, z)
+        solver.Solve()
+        return el.RetrievePositionToCPU()
+
+    e2e_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    t_e2e = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = {"value": world * args.steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": 6 * N * 8,
+           "d2h_bytes_per_step": 3 * N * 8}
+
+    hbm, peak_kind = peaks()
+    # dominant kernel: the CG SpMV (3x3 node blocks), timed back to back on the element stream
+    xin = torch.randn(3 * N, dtype=torch.float64, device="cuda")
+    yout = torch.empty_like(xin)
+    torch.cuda.synchronize()
+    el.SetBlocking(False)
+    for _ in range(3):
+        solver.Apply(xin.data_ptr(), yout.data_ptr())
+    ms_spmv = time_stream(torch, stream, lambda: solver.Apply(xin.data_ptr(), yout.data_ptr()), args.kernel_reps)
+    nnzb = len(el._nnz_cache) if hasattr(el, "_nnz_cache") else None
+    off_m, cols_m, _ = el.RetrieveMassCSRToCPU()
+    nnzb = len(cols_m)
+    b_spmv = spmv_bytes(N, nnzb)
+    ach = b_spmv / (ms_spmv / 1e3) / 1e9
+    roofline = {"kernel": "k_cg_spmv_dot", "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": int(b_spmv),
+                "ms": round(ms_spmv, 4), "traffic": None}
+    # fused element force, FP32 and FP64
+    ef = {}
+    for prec, s in (("fp32", 4), ("fp64", 8)):
+        el.SetForcePrecision(prec)
+        for _ in range(3):
+            el.ComputeInternalForce()
+        ms_f = time_stream(torch, stream, el.ComputeInternalForce, args.kernel_reps)
+        b = elem_force_bytes(E, N, 10, 5, s)
+        a = b / (ms_f / 1e3) / 1e9
+        ef[prec] = {"kernel": "k_tile_force+k_combine", "bound": "hbm", "achieved": round(a, 1), "peak": hbm,
+                    "unit": "GB/s", "frac": round(a / hbm, 4), "algorithmic_bytes": int(b), "ms": round(ms_f, 4)}
+    el.SetForcePrecision("fp64")
+    el.SetBlocking(True)
+
+    out = {"metric": METRIC, "value": round(value, 4), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(t_total * 1e3 / args.steps, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "cantilever 200x20x20 TET10 linear static CG to 1e-6", "elements": E, "nodes": N,
+                      "dof": 3 * N, "cg_iters_per_solve": iters, "final_rel_residual": resid,
+                      "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (K 1.35 GB)"},
+           "e2e": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in e2e.items()},
+           "roofline": roofline, "elem_force": ef, "gpu_launches": int(launches), "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_sample(x, y, z, conn, fixed, f, cfg, iters)
+    if rank == 0:
+        print(json.dumps(out))
+    el.Destroy()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

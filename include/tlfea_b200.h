@@ -1,0 +1,223 @@
+/*
+ * tlfea_b200.h -- C ABI of the B200 (sm_100a) TLFEA hot path.
+ *
+ * Plain pointers, sizes and int status codes: no C++ types, no exceptions.
+ * Each entry point replaces one method of the reference's class API
+ * (Ruochun/TLFEA, paths relative to its src/); the C++ classes in
+ * include/tlfea/ and the Python classes in tlfea_b200/ forward to these.
+ *
+ * Conventions
+ *   - Host arrays are FP64 (Real = double, types.h:19) and int32.
+ *   - Connectivity is column-major E x NPE (Eigen MatrixXi::data(),
+ *     FEAT10Data.cuh:41-43): conn[e + a*E].
+ *   - Nodal vectors are SoA x/y/z (length N); forces and velocities are
+ *     interleaved [3*node + d] (FEAT10Data.cuh:147-177).
+ *   - Every call is synchronous with respect to the host unless noted, like
+ *     the reference (cudaDeviceSynchronize after each launch).  Work runs on
+ *     the handle's stream (default: the legacy default stream).
+ *   - A handle is not thread-safe (the reference is single-threaded, device 0;
+ *     here the device current at create time is used for the handle's life).
+ */
+#ifndef TLFEA_B200_H
+#define TLFEA_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (the reference logs with MOPHI_ERROR and returns,
+ * FEAT10Data.cuh:426-429; here the condition is returned instead). */
+enum {
+    TLFEA_OK = 0,
+    TLFEA_INVALID_ARG = 1,
+    TLFEA_NOT_SETUP = 2,
+    TLFEA_SIZE_MISMATCH = 3,
+    TLFEA_CUDA_ERROR = 4,
+    TLFEA_NO_CONVERGENCE = 5,
+    TLFEA_BUDGET_EXCEEDED = 6,
+    TLFEA_NONFINITE = 7,
+    TLFEA_UNSUPPORTED = 8,
+    TLFEA_ALREADY_SETUP = 9,
+    TLFEA_NO_CUDA_DEVICE = 10
+};
+
+/* ElementType values of ElementBase.h:22 (TYPE_3243, TYPE_3443, TYPE_T10, TYPE_T4). */
+enum { TLFEA_TYPE_T10 = 2, TLFEA_TYPE_T4 = 3 };
+
+/* MaterialModel values of MaterialModel.cuh:16-19. */
+enum { TLFEA_MATERIAL_SVK = 0, TLFEA_MATERIAL_MOONEY_RIVLIN = 1 };
+
+/* Force precision of the fused element kernel (new, no reference counterpart). */
+enum { TLFEA_PRECISION_FP64 = 0, TLFEA_PRECISION_FP32 = 1 };
+
+typedef struct tlfea_element_s* tlfea_element;
+typedef struct tlfea_solver_s* tlfea_solver;
+
+/* Same field order and types as SyncedNesterovParams (SyncedNesterov.cuh:31-35). */
+typedef struct {
+    double alpha, rho, inner_tol, outer_tol;
+    int max_outer, max_inner;
+    double time_step;
+} tlfea_nesterov_params;
+
+/* Same field order and types as SyncedAdamWParams (SyncedAdamW.cuh:32-39);
+ * SyncedAdamWNocoopParams is the same struct (SyncedAdamWNocoop.cuh:23). */
+typedef struct {
+    double lr, beta1, beta2, eps, weight_decay, lr_decay;
+    double inner_tol, outer_tol, rho;
+    int max_outer, max_inner;
+    double time_step;
+    int convergence_check_interval;
+    double inner_rtol;
+} tlfea_adamw_params;
+
+/* Diagnostics of the last Solve() (new). */
+typedef struct {
+    int outer_iters;       /* outer (augmented-Lagrangian) iterations run */
+    int inner_iters_total; /* inner iterations summed over outer iterations */
+    int last_inner_iters;  /* inner iterations of the last outer iteration */
+    int status;            /* TLFEA_OK, TLFEA_NONFINITE, TLFEA_BUDGET_EXCEEDED */
+    double last_norm_g;    /* ||g|| at the last evaluated inner iteration */
+    double kernel_ms;      /* device time of the solve (CUDA events) */
+} tlfea_solve_stats;
+
+/* ------------------------------------------------------------- library */
+
+/* Text of the last error on this thread ("" if none). */
+const char* tlfea_last_error(void);
+/* Kernels launched by this library since load (graph launches count their nodes). */
+long long tlfea_launch_count(void);
+/* Library version string. */
+const char* tlfea_version(void);
+
+/* ------------------------------------------------------------- elements */
+
+/* GPU_FEAT10_Data(E, N) + Initialize()  (FEAT10Data.cuh:354-416);
+ * GPU_FEAT4_Data(E, N) + Initialize()   (FEAT4Data.cuh). type = TLFEA_TYPE_T10/T4. */
+int tlfea_element_create(int type, int n_elem, int n_nodes, tlfea_element* out);
+/* Destroy()  (FEAT10Data.cuh:659-723): frees every device buffer and the handle. */
+int tlfea_element_destroy(tlfea_element h);
+/* Sets / gets the CUDA stream (cudaStream_t) used by this element and the
+ * solvers built on it.  By default each element owns a non-blocking stream
+ * (CUDA graphs cannot be captured on the legacy default stream). */
+int tlfea_element_set_stream(tlfea_element h, void* stream);
+int tlfea_element_get_stream(tlfea_element h, void** stream);
+/* blocking = 1 (default, the reference's behaviour): every compute call
+ * synchronises the stream before returning.  blocking = 0: compute calls
+ * (compute/calc force, calc_p, reset_positions, linear_static_apply) return
+ * after enqueueing; the caller synchronises the stream. */
+int tlfea_element_set_blocking(tlfea_element h, int blocking);
+/* x12 = reference positions captured by the last CalcDnDuPre (device copy). */
+int tlfea_element_reset_positions(tlfea_element h);
+int tlfea_element_get_counts(tlfea_element h, int* n_elem, int* n_nodes, int* n_constraint);
+
+/* Setup(qx, qy, qz, qw, x, y, z, conn)  (FEAT10Data.cuh:418-503).  n_qp must
+ * be 5 (T10) or 1 (T4).  Positions are copied to x12 and to the constraint
+ * targets x12_jac; material scalars reset to zero, SVK selected. */
+int tlfea_element_setup(tlfea_element h, const double* qx, const double* qy, const double* qz, const double* qw,
+                        int n_qp, const double* x, const double* y, const double* z, const int* conn_colmajor);
+/* SetDensity (:508-514), SetDamping (:521-528), SetSVK() (:533-547),
+ * SetSVK(E, nu) (:553-569), SetMooneyRivlin (:576-587). */
+int tlfea_element_set_density(tlfea_element h, double rho0);
+int tlfea_element_set_damping(tlfea_element h, double eta_damp, double lambda_damp);
+int tlfea_element_set_svk_default(tlfea_element h);
+int tlfea_element_set_svk(tlfea_element h, double E, double nu);
+/* Stores the Mooney-Rivlin parameters and selects the model; force, stiffness
+ * and solver calls then return TLFEA_UNSUPPORTED (SVK is the supported law). */
+int tlfea_element_set_mooney_rivlin(tlfea_element h, double mu10, double mu01, double kappa);
+/* SetExternalForce (:589-597); n must be 3*N. */
+int tlfea_element_set_external_force(tlfea_element h, const double* f_ext, int n);
+/* SetNodalFixed (FEAT10Data.cu:650-672) / UpdateNodalFixed (:674-752). */
+int tlfea_element_set_nodal_fixed(tlfea_element h, const int* fixed_nodes, int n_fixed);
+int tlfea_element_update_nodal_fixed(tlfea_element h, const int* fixed_nodes, int n_fixed);
+/* UpdatePositions (FEAT10Data.cuh:628-640), UpdateConstraintTargets (:642-654). */
+int tlfea_element_update_positions(tlfea_element h, const double* x, const double* y, const double* z, int n);
+int tlfea_element_update_constraint_targets(tlfea_element h, const double* x, const double* y, const double* z,
+                                            int n);
+
+/* CalcDnDuPre  (FEAT10Data.cu:277-285; FEAT4Data.cu): reference gradients and
+ * signed detJ at every QP, stored in the tiled layout the force kernel streams. */
+int tlfea_element_calc_dndu_pre(tlfea_element h);
+/* CalcMassMatrix + BuildMassCSRPattern (FEAT10Data.cu:341-417): node-level
+ * consistent mass CSR, deterministic (no atomics). */
+int tlfea_element_calc_mass_matrix(tlfea_element h);
+/* CalcP (FEAT10Data.cu:300-305): P at every QP from the current positions,
+ * no viscous term, stored for RetrievePFromFToCPU and CalcInternalForce. */
+int tlfea_element_calc_p(tlfea_element h);
+/* CalcInternalForce (FEAT10Data.cu:318-323): f_int += forces of the stored P.
+ * Like the reference it does not clear f_int first. */
+int tlfea_element_calc_internal_force(tlfea_element h);
+/* CalcConstraintData (FEAT10Data.cu:325-339). */
+int tlfea_element_calc_constraint_data(tlfea_element h);
+/* ConvertToCSR_ConstraintJacT (FEAT10Data.cu:510-562) and
+ * ConvertToCSR_ConstraintJac (:465-505). */
+int tlfea_element_build_constraint_jact_csr(tlfea_element h);
+int tlfea_element_build_constraint_jac_csr(tlfea_element h);
+
+/* NEW fused hot path: f_int = internal force at the current positions (and
+ * velocities v, interleaved 3N device pointer, or NULL for none), in one
+ * pass over the element stream with a deterministic, atomic-free scatter.
+ * This is compute_p + clear_internal_force + compute_internal_force of the
+ * solver loops (SyncedNesterov.cu:180-207).  v may be NULL. */
+int tlfea_element_compute_internal_force(tlfea_element h, const double* d_v);
+/* Force precision for tlfea_element_compute_internal_force and the solvers. */
+int tlfea_element_set_force_precision(tlfea_element h, int precision);
+
+/* Retrieve*ToCPU (FEAT10Data.cu:564-649, 753-757).  Sizes are in elements of
+ * the output array and must match exactly. */
+int tlfea_element_get_mass_nnz(tlfea_element h, long long* nnz);
+int tlfea_element_retrieve_mass_csr(tlfea_element h, int* offsets, int* columns, double* values);
+int tlfea_element_retrieve_internal_force(tlfea_element h, double* f, int n);
+int tlfea_element_retrieve_external_force(tlfea_element h, double* f, int n);
+int tlfea_element_retrieve_positions(tlfea_element h, double* x, double* y, double* z, int n);
+int tlfea_element_retrieve_p(tlfea_element h, double* P, long long n);        /* E*QP*9 */
+int tlfea_element_retrieve_dndu_pre(tlfea_element h, double* g, long long n); /* E*QP*NPE*3 */
+int tlfea_element_retrieve_detj(tlfea_element h, double* detJ, long long n);  /* E*QP */
+int tlfea_element_retrieve_connectivity(tlfea_element h, int* conn_colmajor, long long n);
+int tlfea_element_retrieve_constraint(tlfea_element h, double* c, int n);
+/* WriteOutputVTK (FEAT10Data.cu:759-794): legacy ASCII VTK of the current mesh. */
+int tlfea_element_write_vtk(tlfea_element h, const char* filename);
+/* Get{X,Y,Z}12DevicePtr, GetExternalForceDevicePtr (FEAT10Data.cuh:599-621). */
+int tlfea_element_device_ptrs(tlfea_element h, double** x, double** y, double** z, double** f_ext, double** f_int);
+
+/* ------------------------------------------------------------- solvers */
+
+/* SyncedNesterovSolver(ElementBase*, n_constraints) (SyncedNesterov.cuh:39-110). */
+int tlfea_nesterov_create(tlfea_element e, int n_constraints, tlfea_solver* out);
+/* SyncedAdamWSolver (SyncedAdamW.cuh:43-) and SyncedAdamWNocoopSolver
+ * (SyncedAdamWNocoop.cuh:25-). */
+int tlfea_adamw_create(tlfea_element e, int n_constraints, tlfea_solver* out);
+int tlfea_adamw_nocoop_create(tlfea_element e, int n_constraints, tlfea_solver* out);
+/* LinearStaticSolver<T>(data, tol, max_iter) (LinearStaticSolver.cuh:56). */
+int tlfea_linear_static_create(tlfea_element e, double tol, int max_iter, tlfea_solver* out);
+/* ~Solver. */
+int tlfea_solver_destroy(tlfea_solver s);
+/* Setup() (SyncedNesterov.cuh:157-179): zeroes every solver vector. */
+int tlfea_solver_setup(tlfea_solver s);
+/* SetParameters(void*) (SyncedNesterov.cuh:139-155, SyncedAdamW.cuh:159-184):
+ * copies the struct and zeroes v_guess, v_prev and the multipliers.  params
+ * points at tlfea_nesterov_params or tlfea_adamw_params as the solver needs;
+ * a no-op for the linear static solver (LinearStaticSolver.cuh:65). */
+int tlfea_solver_set_parameters(tlfea_solver s, const void* params);
+/* Solve() (SyncedNesterov.cuh:266-268, SyncedAdamW.cuh, LinearStaticSolver.cu:590-603). */
+int tlfea_solver_solve(tlfea_solver s);
+/* GetLastIterCount / GetLastResidual (LinearStaticSolver.cuh:68-72). */
+int tlfea_linear_static_last(tlfea_solver s, int* iters, double* rel_residual);
+/* Retrieve the LinearStaticSolver stiffness (BCs applied) as 3N x 3N CSR
+ * (new; the reference keeps K private).  Call with NULL arrays for nnz. */
+int tlfea_linear_static_retrieve_k(tlfea_solver s, long long* nnz, int* offsets, int* columns, double* values);
+/* d_y = K d_x with the stiffness of the last Solve() (device pointers, 3N
+ * each); the SpMV kernel of the CG loop (new). */
+int tlfea_linear_static_apply(tlfea_solver s, const double* d_x, double* d_y);
+/* Velocity state of the first-order solvers (v_guess, v_prev: 3N; lambda: n_c). */
+int tlfea_solver_get_velocity(tlfea_solver s, double* v_guess, double* v_prev, int n);
+int tlfea_solver_set_velocity(tlfea_solver s, const double* v_guess, const double* v_prev, int n);
+int tlfea_solver_get_multipliers(tlfea_solver s, double* lam, int n);
+int tlfea_solver_get_stats(tlfea_solver s, tlfea_solve_stats* st);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,98 @@
+"""GPU parity of LinearStaticSolver: stiffness (BCs applied) vs the oracle,
+CG iterates vs the oracle CG, solution vs a direct solve, positions x += u."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import tlfea_b200 as T
+from oracle import oracle as O
+from tlfea_b200 import mesh as M
+
+from .helpers import box, lame, make_element, rel
+
+pytestmark = pytest.mark.gpu
+LAM, MU = lame()
+
+
+def _problem(order, nx=10, ny=2, nz=2, load=(0.0, 0.0, -100.0)):
+    x, y, z, conn = box(nx, ny, nz, order)
+    fixed, f, tip = M.cantilever_loads(x, y, z, load)
+    el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
+    return el, (x, y, z, conn, fixed, f)
+
+
+def _oracle_system(x, y, z, conn, fixed, f):
+    g, dj = O.dndu_pre(x, y, z, conn)
+    off, cols, vals = O.stiffness(x, y, z, conn, g, dj, LAM, MU)
+    kv, fb = O.apply_bcs(off, cols, vals, f, fixed)
+    return off, cols, kv, fb
+
+
+@pytest.mark.parametrize("order", [10, 4])
+def test_stiffness_and_cg_match_oracle(order):
+    el, (x, y, z, conn, fixed, f) = _problem(order)
+    s = T.LinearStaticSolver(el, 1e-10, 50000)
+    s.Solve()
+    off, cols, kv, fb = _oracle_system(x, y, z, conn, fixed, f)
+    o2, c2, v2 = s.RetrieveStiffnessCSRToCPU()
+    assert np.array_equal(o2, off) and np.array_equal(c2, cols)
+    assert rel(v2, kv) < 1e-12
+    u_ref, it_ref, res_ref, rc = O.cg(off, cols, kv, fb, 1e-10, 50000)
+    assert rc == 0
+    it, res = s.GetLastIterCount(), s.GetLastResidual()
+    assert res < 1e-10
+    assert abs(it - it_ref) <= max(2, 0.02 * it_ref)
+    x2, y2, z2 = el.RetrievePositionToCPU()
+    u = np.stack([x2 - x, y2 - y, z2 - z], 1).ravel()
+    K = sp.csr_matrix((kv, cols, off)).tocsc()
+    u_dir = spla.spsolve(K, fb)
+    assert rel(u, u_dir) < 1e-7
+    assert rel(u, u_ref) < 1e-7
+    el.Destroy()
+
+
+def test_cg_fixed_iteration_count_parity():
+    """At a fixed iteration count the CG iterates agree to rounding."""
+    el, (x, y, z, conn, fixed, f) = _problem(10)
+    s = T.LinearStaticSolver(el, 0.0, 25)  # tol 0: run exactly 25 iterations
+    s.Solve()
+    off, cols, kv, fb = _oracle_system(x, y, z, conn, fixed, f)
+    u_ref, it_ref, res_ref, _ = O.cg(off, cols, kv, fb, 0.0, 25)
+    assert s.GetLastIterCount() == it_ref == 25
+    assert abs(s.GetLastResidual() - res_ref) < 1e-9 * max(res_ref, 1e-300)
+    x2, y2, z2 = el.RetrievePositionToCPU()
+    u = np.stack([x2 - x, y2 - y, z2 - z], 1).ravel()
+    assert rel(u, u_ref) < 1e-10
+    el.Destroy()
+
+
+def test_zero_load_and_zero_iterations():
+    el, (x, y, z, conn, fixed, f) = _problem(10, load=(0.0, 0.0, 0.0))
+    s = T.LinearStaticSolver(el, 1e-10, 100)
+    s.Solve()
+    assert s.GetLastIterCount() == 0 and s.GetLastResidual() == 0.0
+    x2, _, _ = el.RetrievePositionToCPU()
+    assert np.array_equal(x2, x)
+    el.Destroy()
+
+
+def test_beam_fixture_tip_deflection():
+    """beam.vtu (24 TET10, 10x1x1): clamp x=0, load the x=10 face; tip deflection
+    within 30% of Euler-Bernoulli PL^3/(3EI) (the reference's only physics check,
+    examples/beam_linear_static.cc:219-234; a coarse mesh is stiffer)."""
+    from pathlib import Path
+
+    fx = np.load(Path(__file__).parent / "golden" / "beam_t10.npz")
+    x, y, z, conn = fx["x"], fx["y"], fx["z"], fx["conn"]
+    E_mod, P = 2e9, -1000.0
+    fixed, f, tip = M.cantilever_loads(x, y, z, (0.0, 0.0, P))
+    el = make_element(x, y, z, conn, E_mod=E_mod, fixed=fixed, f_ext=f)
+    s = T.LinearStaticSolver(el, 1e-10, 50000)
+    s.Solve()
+    _, _, z2 = el.RetrievePositionToCPU()
+    delta = abs((z2 - z)[tip].min())
+    L, b, h = 10.0, 1.0, 1.0
+    delta_eb = abs(P) * L ** 3 / (3 * E_mod * b * h ** 3 / 12)
+    assert 0.3 < delta / delta_eb < 1.3
+    el.Destroy()

@@ -1,0 +1,137 @@
+"""GPU parity of the first-order solvers (SyncedNesterov, SyncedAdamW,
+SyncedAdamWNocoop) against the oracle restatements, on the cube fixture of
+examples/test_feat10_nesterov.cc and on BASELINE configuration 1 (10x2x2 TET10
+cantilever).  With a zero inner tolerance both sides run the same number of
+iterations, so trajectories compare at rel 1e-10 (FP64 mode)."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import tlfea_b200 as T
+from oracle import oracle as O
+from tlfea_b200 import mesh as M
+
+from .helpers import E_MOD, NU, RHO, box, make_element, rel
+
+pytestmark = pytest.mark.gpu
+
+NESTEROV = (1.0e-8, 1e14, 1.0e-6, 1.0e-6, 5, 300, 1.0e-3)  # test_feat10_nesterov.cc:189
+ADAMW = (2e-4, 0.9, 0.999, 1e-8, 1e-4, 0.995, 1e-1, 1e-6, 1e14, 5, 500, 1e-3, 10, 0.0)  # test_feat10_adamw.cc:189
+
+
+def _cube():
+    fx = np.load(Path(__file__).parent / "golden" / "cube_t10.npz")
+    x, y, z, conn = fx["x"], fx["y"], fx["z"], fx["conn"]
+    fixed = np.nonzero(np.abs(z) < 1e-8)[0].astype(np.int32)
+    f = np.zeros(3 * len(x))
+    f[3 * 6 + 0] = 1000.0  # test_feat10_nesterov.cc:100-104
+    return x, y, z, conn, fixed, f
+
+
+def _cfg1():
+    x, y, z, conn = box(10, 2, 2, 10)
+    fixed, f, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -100.0))
+    return x, y, z, conn, fixed, f
+
+
+def _pair(case, kind, params, steps, prec="fp64"):
+    x, y, z, conn, fixed, f = case()
+    el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
+    if prec != "fp64":
+        el.SetForcePrecision(prec)
+    fea = T.FEASolver()
+    fea.AddElement("body", el)
+    cls = {"nesterov": T.SyncedNesterovSolver, "adamw": T.SyncedAdamWSolver,
+           "nocoop": T.SyncedAdamWNocoopSolver}[kind]
+    solver = cls(el, el.get_n_constraint())
+    fea.AddSolver("s", solver)
+    solver.Setup()
+    if kind == "nesterov":
+        solver.SetParameters(T.SyncedNesterovParams(*params))
+    else:
+        solver.SetParameters(T.SyncedAdamWParams(*params))
+    m = O.OracleModel(x, y, z, conn, E_MOD, NU, RHO, fixed, f)
+    m.set_parameters()
+    gstats, ostats = [], []
+    for _ in range(steps):
+        fea.GetSolver("s").Solve()
+        gstats.append(solver.GetStats())
+        if kind == "nesterov":
+            ostats.append(m.nesterov_solve(*params))
+        elif kind == "adamw":
+            ostats.append(m.adamw_solve(*params))
+        else:
+            ostats.append(m.adamw_nocoop_solve(*params))
+    return el, solver, m, gstats, ostats
+
+
+@pytest.mark.parametrize("case", [_cube, _cfg1])
+def test_nesterov_fixed_iterations(case):
+    params = (1.0e-8, 1e14, 0.0, 0.0, 2, 40, 1.0e-3)
+    el, solver, m, gs, os_ = _pair(case, "nesterov", params, 3)
+    assert [g["inner_iters_total"] for g in gs] == [o["inner_iters_total"] for o in os_] == [80] * 3
+    x, y, z = el.RetrievePositionToCPU()
+    assert rel(np.stack([x, y, z]), np.stack([m.x, m.y, m.z])) < 1e-12
+    vg, vp = solver.GetVelocity()
+    assert rel(vg, m.v_guess) < 1e-10
+    assert rel(solver.GetMultipliers(), m.lam_mult[:solver.n_constraints]) < 1e-10
+    el.Destroy()
+
+
+def test_nesterov_reference_parameters_cube():
+    el, solver, m, gs, os_ = _pair(_cube, "nesterov", NESTEROV, 5)
+    it_g = [g["inner_iters_total"] for g in gs]
+    it_o = [o["inner_iters_total"] for o in os_]
+    assert all(abs(a - b) <= 2 for a, b in zip(it_g, it_o)), (it_g, it_o)
+    x, y, z = el.RetrievePositionToCPU()
+    assert rel(np.stack([x, y, z]), np.stack([m.x, m.y, m.z])) < 1e-9
+    el.Destroy()
+
+
+@pytest.mark.parametrize("kind", ["adamw", "nocoop"])
+def test_adamw_fixed_iterations(kind):
+    params = list(ADAMW)
+    params[6], params[7], params[9], params[10] = 0.0, 0.0, 2, 60  # no early exit
+    el, solver, m, gs, os_ = _pair(_cfg1, kind, tuple(params), 2)
+    assert [g["inner_iters_total"] for g in gs] == [o["inner_iters_total"] for o in os_]
+    x, y, z = el.RetrievePositionToCPU()
+    assert rel(np.stack([x, y, z]), np.stack([m.x, m.y, m.z])) < 1e-12
+    vg, _ = solver.GetVelocity()
+    assert rel(vg, m.v_guess) < 1e-9
+    el.Destroy()
+
+
+@pytest.mark.parametrize("kind", ["adamw", "nocoop"])
+def test_adamw_reference_parameters_cube(kind):
+    el, solver, m, gs, os_ = _pair(_cube, kind, ADAMW, 3)
+    it_g = [g["inner_iters_total"] for g in gs]
+    it_o = [o["inner_iters_total"] for o in os_]
+    assert all(abs(a - b) <= 10 for a, b in zip(it_g, it_o)), (it_g, it_o)
+    x, y, z = el.RetrievePositionToCPU()
+    assert rel(np.stack([x, y, z]), np.stack([m.x, m.y, m.z])) < 1e-8
+    el.Destroy()
+
+
+def test_nesterov_fp32_forces_track_fp64():
+    params = (1.0e-8, 1e14, 0.0, 0.0, 2, 40, 1.0e-3)
+    el, solver, m, gs, os_ = _pair(_cfg1, "nesterov", params, 2, prec="fp32")
+    x, y, z = el.RetrievePositionToCPU()
+    x0, y0, z0, *_ = _cfg1()
+    du = np.stack([x - x0, y - y0, z - z0])
+    du_ref = np.stack([m.x - x0, m.y - y0, m.z - z0])
+    assert rel(du, du_ref) < 1e-4
+    el.Destroy()
+
+
+def test_solver_requires_parameters_and_mass():
+    x, y, z, conn, fixed, f = _cfg1()
+    el = make_element(x, y, z, conn, fixed=fixed, f_ext=f, mass=False)
+    s = T.SyncedNesterovSolver(el, el.get_n_constraint())
+    s.Setup()
+    with pytest.raises(T.TLFEAError):
+        s.Solve()  # no SetParameters
+    s.SetParameters(T.SyncedNesterovParams(*NESTEROV))
+    with pytest.raises(T.TLFEAError):
+        s.Solve()  # no CalcMassMatrix
+    el.Destroy()

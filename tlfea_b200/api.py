@@ -1,0 +1,493 @@
+"""Python mirror of the reference's class API over the C ABI.
+
+Names, argument meaning and call order follow the reference (Ruochun/TLFEA):
+``GPU_FEAT10_Data`` / ``GPU_FEAT4_Data`` (src/elements/FEAT10Data.cuh,
+FEAT4Data.cuh), ``SyncedNesterovSolver`` (src/solvers/SyncedNesterov.cuh),
+``SyncedAdamWSolver`` (SyncedAdamW.cuh), ``SyncedAdamWNocoopSolver``
+(SyncedAdamWNocoop.cuh), ``LinearStaticSolver`` (LinearStaticSolver.cuh) and
+``FEASolver`` (src/FEASolver.h).  Eigen vectors and matrices become numpy
+arrays; ``MatrixXi`` connectivity is an (E, NPE) int array; per-QP matrix
+lists become (E, QP, ...) arrays.  Errors the reference reports with
+MOPHI_ERROR raise ``TLFEAError``; FEASolver raises ValueError / KeyError where
+the reference throws std::invalid_argument / std::out_of_range.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, astuple
+
+import numpy as np
+
+from . import _capi as capi
+from ._capi import TLFEAError
+from . import quadrature as Quadrature
+
+# ElementType (ElementBase.h:22)
+TYPE_3243, TYPE_3443, TYPE_T10, TYPE_T4 = 0, 1, 2, 3
+# MaterialModel (MaterialModel.cuh:16-19)
+MATERIAL_MODEL_SVK, MATERIAL_MODEL_MOONEY_RIVLIN = 0, 1
+
+
+def _f64(a, n=None, name="array"):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+    if n is not None and a.size != n:
+        raise TLFEAError(capi.SIZE_MISMATCH, name, f"expected {n} values, got {a.size}")
+    return a
+
+
+def _i32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32).ravel())
+
+
+class ElementBase:
+    """ElementBase (ElementBase.h:24-48)."""
+
+    type: int = -1
+
+    def get_n_beam(self) -> int:
+        return self.n_elem
+
+    def get_n_coef(self) -> int:
+        return self.n_coef
+
+
+class _TetData(ElementBase):
+    NPE = 10
+    NQP = 5
+    TYPE = TYPE_T10
+
+    def __init__(self, num_elements: int, num_nodes: int):
+        self.n_elem = int(num_elements)
+        self.n_coef = int(num_nodes)
+        self.n_constraint = 0
+        self.type = self.TYPE
+        self._h = None
+        self.d_data = None
+
+    # -- lifecycle ---------------------------------------------------------
+    def Initialize(self):
+        h = C.c_void_p()
+        capi.call("tlfea_element_create", self.TYPE, self.n_elem, self.n_coef, C.byref(h))
+        self._h = h
+        self.d_data = h
+
+    def _handle(self):
+        if self._h is None:
+            raise TLFEAError(capi.NOT_SETUP, type(self).__name__, "Initialize() has not been called")
+        return self._h
+
+    def Destroy(self):
+        if self._h is not None:
+            capi.call("tlfea_element_destroy", self._h)
+            self._h = None
+            self.d_data = None
+
+    def Setup(self, q_x, q_y, q_z, q_w, h_x12, h_y12, h_z12, element_connectivity):
+        conn = np.asarray(element_connectivity, dtype=np.int32)
+        if conn.shape != (self.n_elem, self.NPE):
+            raise TLFEAError(capi.SIZE_MISMATCH, "Setup", f"connectivity must be ({self.n_elem}, {self.NPE})")
+        conn_cm = np.ascontiguousarray(conn.T).ravel()
+        qs = [_f64(q, self.NQP, "quadrature") for q in (q_x, q_y, q_z, q_w)]
+        xs = [_f64(v, self.n_coef, "positions") for v in (h_x12, h_y12, h_z12)]
+        capi.call("tlfea_element_setup", self._handle(), *[capi.dptr(q) for q in qs], self.NQP,
+                  *[capi.dptr(v) for v in xs], capi.iptr(conn_cm))
+
+    # -- material / loads ----------------------------------------------------
+    def SetDensity(self, rho0: float):
+        capi.call("tlfea_element_set_density", self._handle(), float(rho0))
+
+    def SetDamping(self, eta_damp: float, lambda_damp: float):
+        capi.call("tlfea_element_set_damping", self._handle(), float(eta_damp), float(lambda_damp))
+
+    def SetSVK(self, E: float | None = None, nu: float | None = None):
+        if E is None:
+            capi.call("tlfea_element_set_svk_default", self._handle())
+        else:
+            capi.call("tlfea_element_set_svk", self._handle(), float(E), float(nu))
+
+    def SetMooneyRivlin(self, mu10: float, mu01: float, kappa: float):
+        capi.call("tlfea_element_set_mooney_rivlin", self._handle(), float(mu10), float(mu01), float(kappa))
+
+    def SetExternalForce(self, h_f_ext):
+        f = _f64(h_f_ext)
+        capi.call("tlfea_element_set_external_force", self._handle(), capi.dptr(f), int(f.size))
+
+    def SetNodalFixed(self, fixed_nodes):
+        a = _i32(fixed_nodes)
+        capi.call("tlfea_element_set_nodal_fixed", self._handle(), capi.iptr(a), int(a.size))
+        self.n_constraint = 3 * int(a.size)
+
+    def UpdateNodalFixed(self, fixed_nodes):
+        a = _i32(fixed_nodes)
+        capi.call("tlfea_element_update_nodal_fixed", self._handle(), capi.iptr(a), int(a.size))
+        self.n_constraint = 3 * int(a.size)
+
+    def UpdatePositions(self, h_x12, h_y12, h_z12):
+        xs = [_f64(v) for v in (h_x12, h_y12, h_z12)]
+        capi.call("tlfea_element_update_positions", self._handle(), *[capi.dptr(v) for v in xs], int(xs[0].size))
+
+    def UpdateConstraintTargets(self, h_x12, h_y12, h_z12):
+        xs = [_f64(v) for v in (h_x12, h_y12, h_z12)]
+        capi.call("tlfea_element_update_constraint_targets", self._handle(), *[capi.dptr(v) for v in xs],
+                  int(xs[0].size))
+
+    # -- computation -----------------------------------------------------------
+    def CalcDnDuPre(self):
+        capi.call("tlfea_element_calc_dndu_pre", self._handle())
+
+    def CalcMassMatrix(self):
+        capi.call("tlfea_element_calc_mass_matrix", self._handle())
+
+    def BuildMassCSRPattern(self):
+        """The pattern is built by CalcMassMatrix (kept for API compatibility)."""
+
+    def CalcP(self):
+        capi.call("tlfea_element_calc_p", self._handle())
+
+    def CalcInternalForce(self):
+        capi.call("tlfea_element_calc_internal_force", self._handle())
+
+    def CalcConstraintData(self):
+        capi.call("tlfea_element_calc_constraint_data", self._handle())
+
+    def ConvertToCSR_ConstraintJacT(self):
+        capi.call("tlfea_element_build_constraint_jact_csr", self._handle())
+
+    def ConvertToCSR_ConstraintJac(self):
+        capi.call("tlfea_element_build_constraint_jac_csr", self._handle())
+
+    BuildConstraintJacobianTransposeCSR = ConvertToCSR_ConstraintJacT
+    BuildConstraintJacobianCSR = ConvertToCSR_ConstraintJac
+
+    def ComputeInternalForce(self, d_v: int | None = None):
+        """New fused hot path: f_int = internal force at the current positions
+        (one pass, deterministic scatter).  d_v: optional device pointer to 3N
+        interleaved velocities for the Kelvin-Voigt term."""
+        capi.call("tlfea_element_compute_internal_force", self._handle(), C.c_void_p(d_v) if d_v else None)
+
+    def SetForcePrecision(self, precision: str):
+        p = {"fp64": capi.PRECISION_FP64, "fp32": capi.PRECISION_FP32}[precision]
+        capi.call("tlfea_element_set_force_precision", self._handle(), p)
+
+    # -- retrieval ---------------------------------------------------------------
+    def RetrieveMassCSRToCPU(self):
+        nnz = C.c_longlong()
+        capi.call("tlfea_element_get_mass_nnz", self._handle(), C.byref(nnz))
+        off = np.zeros(self.n_coef + 1, np.int32)
+        cols = np.zeros(max(nnz.value, 1), np.int32)
+        vals = np.zeros(max(nnz.value, 1), np.float64)
+        capi.call("tlfea_element_retrieve_mass_csr", self._handle(), capi.iptr(off), capi.iptr(cols), capi.dptr(vals))
+        return off, cols[:nnz.value], vals[:nnz.value]
+
+    def RetrieveInternalForceToCPU(self):
+        f = np.zeros(3 * self.n_coef)
+        capi.call("tlfea_element_retrieve_internal_force", self._handle(), capi.dptr(f), f.size)
+        return f
+
+    def RetrieveExternalForceToCPU(self):
+        f = np.zeros(3 * self.n_coef)
+        capi.call("tlfea_element_retrieve_external_force", self._handle(), capi.dptr(f), f.size)
+        return f
+
+    def RetrievePositionToCPU(self):
+        x, y, z = (np.zeros(self.n_coef) for _ in range(3))
+        capi.call("tlfea_element_retrieve_positions", self._handle(), capi.dptr(x), capi.dptr(y), capi.dptr(z),
+                  self.n_coef)
+        return x, y, z
+
+    def RetrievePFromFToCPU(self):
+        """(E, QP, 3, 3) with P[e, q, i, j]."""
+        P = np.zeros(self.n_elem * self.NQP * 9)
+        capi.call("tlfea_element_retrieve_p", self._handle(), capi.dptr(P), P.size)
+        return P.reshape(self.n_elem, self.NQP, 3, 3).transpose(0, 1, 3, 2).copy()
+
+    def RetrieveDnDuPreToCPU(self):
+        """(E, QP, NPE, 3) with grad_N[e, q, a, j] = dN_a/dx_j."""
+        g = np.zeros(self.n_elem * self.NQP * self.NPE * 3)
+        capi.call("tlfea_element_retrieve_dndu_pre", self._handle(), capi.dptr(g), g.size)
+        return g.reshape(self.n_elem, self.NQP, 3, self.NPE).transpose(0, 1, 3, 2).copy()
+
+    def RetrieveDetJToCPU(self):
+        d = np.zeros(self.n_elem * self.NQP)
+        capi.call("tlfea_element_retrieve_detj", self._handle(), capi.dptr(d), d.size)
+        return d.reshape(self.n_elem, self.NQP)
+
+    def RetrieveConnectivityToCPU(self):
+        c = np.zeros(self.n_elem * self.NPE, np.int32)
+        capi.call("tlfea_element_retrieve_connectivity", self._handle(), capi.iptr(c), c.size)
+        return c.reshape(self.NPE, self.n_elem).T.copy()
+
+    def RetrieveConstraintDataToCPU(self):
+        c = np.zeros(self.n_constraint)
+        if self.n_constraint:
+            capi.call("tlfea_element_retrieve_constraint", self._handle(), capi.dptr(c), c.size)
+        return c
+
+    def WriteOutputVTK(self, filename: str):
+        capi.call("tlfea_element_write_vtk", self._handle(), str(filename).encode())
+
+    def _ptrs(self):
+        ps = [C.c_void_p() for _ in range(5)]
+        capi.call("tlfea_element_device_ptrs", self._handle(), *[C.byref(p) for p in ps])
+        return [p.value for p in ps]
+
+    def GetX12DevicePtr(self):
+        return self._ptrs()[0]
+
+    def GetY12DevicePtr(self):
+        return self._ptrs()[1]
+
+    def GetZ12DevicePtr(self):
+        return self._ptrs()[2]
+
+    def GetExternalForceDevicePtr(self):
+        return self._ptrs()[3]
+
+    def GetInternalForceDevicePtr(self):
+        return self._ptrs()[4]
+
+    def SetBlocking(self, blocking: bool):
+        """New: False makes compute calls return after enqueueing on GetStream()."""
+        capi.call("tlfea_element_set_blocking", self._handle(), 1 if blocking else 0)
+
+    def ResetPositions(self):
+        """New: positions = the reference configuration of the last CalcDnDuPre (device copy)."""
+        capi.call("tlfea_element_reset_positions", self._handle())
+
+    def GetStream(self) -> int:
+        s = C.c_void_p()
+        capi.call("tlfea_element_get_stream", self._handle(), C.byref(s))
+        return s.value or 0
+
+    def get_n_elem(self):
+        return self.n_elem
+
+    def get_n_constraint(self):
+        return self.n_constraint
+
+    def __del__(self):
+        try:
+            self.Destroy()
+        except Exception:
+            pass
+
+
+class GPU_FEAT10_Data(_TetData):
+    """GPU_FEAT10_Data (FEAT10Data.cuh:22-810): 10-node tetrahedra, 5-point rule."""
+    NPE, NQP, TYPE = 10, 5, TYPE_T10
+
+
+class GPU_FEAT4_Data(_TetData):
+    """GPU_FEAT4_Data (FEAT4Data.cuh:22-): 4-node tetrahedra, centroid rule."""
+    NPE, NQP, TYPE = 4, 1, TYPE_T4
+
+
+# ------------------------------------------------------------------- solvers
+
+class SolverBase:
+    """SolverBase (SolverBase.h:18-25)."""
+
+    def Solve(self):
+        raise NotImplementedError
+
+    def SetParameters(self, params):
+        raise NotImplementedError
+
+
+@dataclass
+class SyncedNesterovParams:
+    """SyncedNesterovParams (SyncedNesterov.cuh:31-35), positional like the C++ brace init."""
+    alpha: float
+    rho: float
+    inner_tol: float
+    outer_tol: float
+    max_outer: int
+    max_inner: int
+    time_step: float
+
+
+@dataclass
+class SyncedAdamWParams:
+    """SyncedAdamWParams (SyncedAdamW.cuh:32-39)."""
+    lr: float
+    beta1: float
+    beta2: float
+    eps: float
+    weight_decay: float
+    lr_decay: float
+    inner_tol: float
+    outer_tol: float
+    rho: float
+    max_outer: int
+    max_inner: int
+    time_step: float
+    convergence_check_interval: int
+    inner_rtol: float = 0.0
+
+
+SyncedAdamWNocoopParams = SyncedAdamWParams
+
+
+class _FirstOrder(SolverBase):
+    _CREATE = ""
+
+    def __init__(self, data: _TetData, n_constraints: int):
+        self.data = data
+        self.n_coef = data.n_coef
+        self.n_constraints = int(n_constraints)
+        h = C.c_void_p()
+        capi.call(self._CREATE, data._handle(), self.n_constraints, C.byref(h))
+        self._h = h
+
+    def Setup(self):
+        capi.call("tlfea_solver_setup", self._h)
+
+    def Solve(self):
+        capi.call("tlfea_solver_solve", self._h)
+
+    def GetVelocity(self):
+        vg, vp = np.zeros(3 * self.n_coef), np.zeros(3 * self.n_coef)
+        capi.call("tlfea_solver_get_velocity", self._h, capi.dptr(vg), capi.dptr(vp), vg.size)
+        return vg, vp
+
+    def SetVelocityGuess(self, v_guess, v_prev=None):
+        vg = _f64(v_guess, 3 * self.n_coef)
+        vp = _f64(v_prev, 3 * self.n_coef) if v_prev is not None else None
+        capi.call("tlfea_solver_set_velocity", self._h, capi.dptr(vg), capi.dptr(vp) if vp is not None else None,
+                  vg.size)
+
+    def GetMultipliers(self):
+        lam = np.zeros(self.n_constraints)
+        if self.n_constraints:
+            capi.call("tlfea_solver_get_multipliers", self._h, capi.dptr(lam), lam.size)
+        return lam
+
+    def GetStats(self) -> dict:
+        st = capi.SolveStats()
+        capi.call("tlfea_solver_get_stats", self._h, C.byref(st))
+        return {f: getattr(st, f) for f, _ in st._fields_}
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None) is not None:
+                capi.call("tlfea_solver_destroy", self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+class SyncedNesterovSolver(_FirstOrder):
+    """SyncedNesterovSolver (SyncedNesterov.cuh:39-322)."""
+    _CREATE = "tlfea_nesterov_create"
+
+    def SetParameters(self, params: SyncedNesterovParams):
+        p = capi.NesterovParams(*astuple(params))
+        capi.call("tlfea_solver_set_parameters", self._h, C.cast(C.byref(p), C.c_void_p))
+
+
+class SyncedAdamWSolver(_FirstOrder):
+    """SyncedAdamWSolver (SyncedAdamW.cuh:43-)."""
+    _CREATE = "tlfea_adamw_create"
+
+    def SetParameters(self, params: SyncedAdamWParams):
+        p = capi.AdamWParams(*astuple(params))
+        capi.call("tlfea_solver_set_parameters", self._h, C.cast(C.byref(p), C.c_void_p))
+
+
+class SyncedAdamWNocoopSolver(SyncedAdamWSolver):
+    """SyncedAdamWNocoopSolver (SyncedAdamWNocoop.cuh:25-)."""
+    _CREATE = "tlfea_adamw_nocoop_create"
+
+
+class LinearStaticSolver(SolverBase):
+    """LinearStaticSolver<T>(data, tol, max_iter) (LinearStaticSolver.cuh:44-117)."""
+
+    def __init__(self, data: _TetData, tol: float = 1e-10, max_iter: int = 10000):
+        self.data = data
+        h = C.c_void_p()
+        capi.call("tlfea_linear_static_create", data._handle(), float(tol), int(max_iter), C.byref(h))
+        self._h = h
+
+    def Solve(self):
+        capi.call("tlfea_solver_solve", self._h)
+
+    def SetParameters(self, params=None):
+        """No-op: parameters are set through the constructor."""
+
+    def _last(self):
+        it, res = C.c_int(), C.c_double()
+        capi.call("tlfea_linear_static_last", self._h, C.byref(it), C.byref(res))
+        return it.value, res.value
+
+    def GetLastIterCount(self) -> int:
+        return self._last()[0]
+
+    def GetLastResidual(self) -> float:
+        return self._last()[1]
+
+    def Apply(self, d_x: int, d_y: int):
+        """New: y = K x on device pointers (3N doubles each), the CG's SpMV kernel."""
+        capi.call("tlfea_linear_static_apply", self._h, C.c_void_p(d_x), C.c_void_p(d_y))
+
+    def RetrieveStiffnessCSRToCPU(self):
+        """K (BCs applied) as 3N x 3N CSR (new; the reference keeps K private)."""
+        nnz = C.c_longlong()
+        capi.call("tlfea_linear_static_retrieve_k", self._h, C.byref(nnz), None, None, None)
+        off = np.zeros(3 * self.data.n_coef + 1, np.int32)
+        cols = np.zeros(max(nnz.value, 1), np.int32)
+        vals = np.zeros(max(nnz.value, 1))
+        capi.call("tlfea_linear_static_retrieve_k", self._h, C.byref(nnz), capi.iptr(off), capi.iptr(cols),
+                  capi.dptr(vals))
+        return off, cols[:nnz.value], vals[:nnz.value]
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None) is not None:
+                capi.call("tlfea_solver_destroy", self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+LinearStaticSolverT10 = LinearStaticSolver
+LinearStaticSolverT4 = LinearStaticSolver
+
+
+# -------------------------------------------------------------------- manager
+
+class FEASolver:
+    """FEASolver (FEASolver.h:35-138): name -> non-owning element / solver registry."""
+
+    def __init__(self):
+        self._elements: dict = {}
+        self._solvers: dict = {}
+
+    def AddElement(self, name: str, element):
+        if element is None:
+            raise ValueError("FEASolver::AddElement: element pointer is null")
+        if name in self._elements:
+            raise ValueError(f"FEASolver::AddElement: element '{name}' already registered")
+        self._elements[name] = element
+
+    def GetElement(self, name: str):
+        if name not in self._elements:
+            raise KeyError(f"FEASolver::GetElement: element '{name}' not found")
+        return self._elements[name]
+
+    def GetNumElements(self) -> int:
+        return len(self._elements)
+
+    def AddSolver(self, name: str, solver):
+        if solver is None:
+            raise ValueError("FEASolver::AddSolver: solver pointer is null")
+        if name in self._solvers:
+            raise ValueError(f"FEASolver::AddSolver: solver '{name}' already registered")
+        self._solvers[name] = solver
+
+    def GetSolver(self, name: str):
+        if name not in self._solvers:
+            raise KeyError(f"FEASolver::GetSolver: solver '{name}' not found")
+        return self._solvers[name]
+
+    def GetNumSolvers(self) -> int:
+        return len(self._solvers)

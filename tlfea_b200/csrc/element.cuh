@@ -1,0 +1,463 @@
+// element.cuh -- element state (TET10 / TET4) and the tiled, fused internal-force
+// device code shared by the standalone force kernel and the persistent solvers.
+//
+// HBM layout (all device arrays owned by tlfea_element_s):
+//   positions       x, y, z            FP64 SoA, mesh node order (x12/y12/z12 of
+//                                      FEAT10Data.cuh:756); FP32 mode adds the
+//                                      displacement u = x - X0 as FP32 SoA.
+//   tiles           elements sorted along a Morton curve of their centroids and
+//                   cut into tiles of TILE_ELEMS; each tile owns a sorted table
+//                   of the nodes its elements touch ("local nodes").
+//   grad (per tile) [tile][q][a*3+j][t]   dN_a/dx_j of tile element t at QP q
+//                                      (component-major inside the tile, so a
+//                                      warp's load of one component is one
+//                                      contiguous 128/256-byte segment)
+//   dv   (per tile) [tile][q][t]          detJ(e,q) * w_q
+//   lconn(per tile) [tile][a][t]          uint16 local node of slot a
+//   incidence       per local node, the (slot, element) pairs that touch it,
+//                   in element-slot order: the fixed summation order of the
+//                   deterministic scatter.
+//   boundary        local nodes shared with other tiles write a per-tile
+//                   partial; a second pass sums the partials of each shared
+//                   node in tile order.  Interior nodes are written directly.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace tlfea {
+
+struct Tiling {
+    int te = TILE_ELEMS;
+    int n_tiles = 0;
+    int max_local = 0;
+    long long n_local_total = 0;
+    int n_pslots = 0;
+    int n_bnodes = 0;
+    int n_orphans = 0;  // nodes touched by no element (never written by the scatter)
+    int* node_off = nullptr;        // n_tiles + 1
+    int* ln_gid = nullptr;          // n_local_total
+    int* ln_pslot = nullptr;        // n_local_total, -1 = interior
+    uint16_t* ln_inc_end = nullptr; // n_local_total, end offset in the tile's incidence
+    uint16_t* inc = nullptr;        // n_tiles*te*npe: (slot << TILE_SHIFT) | element
+    uint16_t* lconn = nullptr;      // n_tiles*npe*te
+    int* tile_elem = nullptr;       // n_tiles*te, original element or -1 (padding)
+    int* elem_slot = nullptr;       // E, tile slot of each original element
+    int* bnode_gid = nullptr;       // n_bnodes
+    int* bnode_off = nullptr;       // n_bnodes + 1
+    int* bnode_slots = nullptr;     // n_pslots
+    int* node_bidx = nullptr;       // N, boundary index or -1
+    double* grad64 = nullptr;
+    double* dv64 = nullptr;
+    float* grad32 = nullptr;
+    float* dv32 = nullptr;
+    double* partial64 = nullptr;
+    float* partial32 = nullptr;
+    std::vector<int> h_tile_elem;  // host copy of tile_elem
+};
+
+// Per-call arguments of the tile routine.
+template <typename R>
+struct TileArgs {
+    const int* node_off;
+    const int* ln_gid;
+    const int* ln_pslot;
+    const uint16_t* ln_inc_end;
+    const uint16_t* inc;
+    const uint16_t* lconn;
+    const int* tile_elem;
+    const R* grad;
+    const R* dv;
+    const R* px;  // FP64: positions x; FP32: displacement u = x - X0
+    const R* py;
+    const R* pz;
+    const double* v;  // interleaved velocities for the Kelvin-Voigt term, or null
+    double* Pst;      // stored P in the reference layout (CalcP / CalcInternalForce)
+    R* f_out;         // interleaved 3N
+    R* partial;       // 3 * n_pslots
+    R lambda, mu, eta, lamd;
+    int max_local;
+};
+
+// Tile routine modes.
+enum { TILE_FORCE = 0, TILE_STORE_P = 1, TILE_FORCE_FROM_P = 2 };
+
+template <typename R>
+__device__ __forceinline__ R ld_stream(const R* p) {
+    return __ldcs(p);
+}
+
+// P from F for the SVK law in the reference's form
+// lambda*(tr(F^T F)/2 - 3/2) F + mu (F F^T F - F)  (SVK.cuh:17-39, FEAT10DataFunc.cuh:233-281).
+__device__ __forceinline__ void svk_p_reference(const double F[3][3], double lambda, double mu, double P[3][3]) {
+    double FtF[3][3], FFt[3][3], FFtF[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) s += F[k][i] * F[k][j];
+            FtF[i][j] = s;
+        }
+    const double tr = FtF[0][0] + FtF[1][1] + FtF[2][2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) s += F[i][k] * F[j][k];
+            FFt[i][j] = s;
+        }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) s += FFt[i][k] * F[k][j];
+            FFtF[i][j] = s;
+        }
+    const double lf = lambda * (0.5 * tr - 1.5);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) P[i][j] = lf * F[i][j] + mu * (FFtF[i][j] - F[i][j]);
+}
+
+// Kelvin-Voigt P_vis = F (2 eta Edot + lamd tr(Edot) I), Edot = (Fdot^T F + F^T Fdot)/2
+// (FEAT10DataFunc.cuh:135-222).
+template <typename R>
+__device__ __forceinline__ void kelvin_voigt(const R F[3][3], const R Fd[3][3], R eta, R lamd, R Pv[3][3]) {
+    R Ed[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            R a = R(0), b = R(0);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                a += Fd[k][i] * F[k][j];
+                b += F[k][i] * Fd[k][j];
+            }
+            Ed[i][j] = R(0.5) * (a + b);
+        }
+    const R tr = Ed[0][0] + Ed[1][1] + Ed[2][2];
+    R S[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) S[i][j] = R(2) * eta * Ed[i][j] + lamd * tr * (i == j ? R(1) : R(0));
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            R s = R(0);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) s += F[i][k] * S[k][j];
+            Pv[i][j] = s;
+        }
+}
+
+// One tile: stage the tile's nodes in shared memory, evaluate its elements (one
+// thread per element, QP by QP, gradients streamed from HBM), reduce element
+// forces per node in the fixed incidence order, write interior nodes and
+// boundary partials.  Must be called by all TILE_ELEMS threads of the block.
+//
+// R = double: F = sum_a x_a (x) gradN_a and the reference SVK formula.
+// R = float : the FP32 mode.  F = I + H with H = sum_a u_a (x) gradN_a from
+//             the FP32 displacement, and P = (I + H) S, S = lambda tr(E) I + 2 mu E,
+//             E = (H + H^T + H^T H)/2 -- algebraically the same SVK stress,
+//             without the cancellation of tr(F^T F) - 3 near F = I.
+template <typename R, int NPE, int NQP, int MODE, bool DAMP>
+__device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, unsigned char* smem_raw) {
+    constexpr int TE = TILE_ELEMS;
+    const int t = threadIdx.x;
+    R* xs = reinterpret_cast<R*>(smem_raw);
+    R* ys = xs + A.max_local;
+    R* zs = ys + A.max_local;
+    R* vs = zs + A.max_local;
+    R* fe = DAMP ? vs + 3 * A.max_local : vs;
+
+    const int lb = A.node_off[tile];
+    const int nl = A.node_off[tile + 1] - lb;
+    if (MODE != TILE_FORCE_FROM_P) {
+        for (int ln = t; ln < nl; ln += TE) {
+            const int gid = A.ln_gid[lb + ln];
+            xs[ln] = A.px[gid];
+            ys[ln] = A.py[gid];
+            zs[ln] = A.pz[gid];
+            if (DAMP) {
+                vs[3 * ln + 0] = R(A.v[3 * gid + 0]);
+                vs[3 * ln + 1] = R(A.v[3 * gid + 1]);
+                vs[3 * ln + 2] = R(A.v[3 * gid + 2]);
+            }
+        }
+    }
+    int lc[NPE];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) lc[a] = A.lconn[((size_t)tile * NPE + a) * TE + t];
+    const int eo = (MODE == TILE_FORCE) ? 0 : A.tile_elem[(size_t)tile * TE + t];
+    __syncthreads();
+
+    R f[NPE][3];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
+
+#pragma unroll 1
+    for (int q = 0; q < NQP; ++q) {
+        const R* gp = A.grad + ((size_t)tile * NQP + q) * (NPE * 3) * TE + t;
+        R g[NPE][3];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) g[a][j] = ld_stream(gp + (a * 3 + j) * TE);
+        const R dv = ld_stream(A.dv + ((size_t)tile * NQP + q) * TE + t);
+
+        R P[3][3];
+        if constexpr (MODE == TILE_FORCE_FROM_P) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    P[i][j] = (eo >= 0) ? R(A.Pst[((size_t)eo * NQP + q) * 9 + i + 3 * j]) : R(0);
+        } else if constexpr (sizeof(R) == 8) {
+            double F[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) F[i][j] = 0.0;
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) {
+                const double xa[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) F[i][j] += xa[i] * g[a][j];
+            }
+            svk_p_reference(F, A.lambda, A.mu, P);
+            if (DAMP) {
+                double Fd[3][3], Pv[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) Fd[i][j] = 0.0;
+#pragma unroll
+                for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc[a] + i] * g[a][j];
+                kelvin_voigt<double>(F, Fd, A.eta, A.lamd, Pv);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
+            }
+        } else {
+            R H[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) H[i][j] = R(0);
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) {
+                const R ua[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) H[i][j] += ua[i] * g[a][j];
+            }
+            R Em[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    R s = H[i][j] + H[j][i];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) s += H[k][i] * H[k][j];
+                    Em[i][j] = R(0.5) * s;
+                }
+            const R trE = Em[0][0] + Em[1][1] + Em[2][2];
+            R S[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) S[i][j] = R(2) * A.mu * Em[i][j] + (i == j ? A.lambda * trE : R(0));
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    R s = S[i][j];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) s += H[i][k] * S[k][j];
+                    P[i][j] = s;
+                }
+            if (DAMP) {
+                R F[3][3], Fd[3][3], Pv[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        F[i][j] = H[i][j] + (i == j ? R(1) : R(0));
+                        Fd[i][j] = R(0);
+                    }
+#pragma unroll
+                for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc[a] + i] * g[a][j];
+                kelvin_voigt<R>(F, Fd, A.eta, A.lamd, Pv);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
+            }
+        }
+
+        if constexpr (MODE == TILE_STORE_P) {
+            if (eo >= 0) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) A.Pst[((size_t)eo * NQP + q) * 9 + i + 3 * j] = double(P[i][j]);
+            }
+        } else {
+            // f_a += (P grad_a) dV   (FEAT10DataFunc.cuh:417-449)
+#pragma unroll
+            for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    R fc = R(0);
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) fc += P[i][j] * g[a][j];
+                    f[a][i] += fc * dv;
+                }
+        }
+    }
+    if constexpr (MODE != TILE_STORE_P) {
+
+#pragma unroll
+    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
+    __syncthreads();
+
+    const uint16_t* inc = A.inc + (size_t)tile * TE * NPE;
+    for (int ln = t; ln < nl; ln += TE) {
+        const int beg = ln ? A.ln_inc_end[lb + ln - 1] : 0;
+        const int end = A.ln_inc_end[lb + ln];
+        R s0 = R(0), s1 = R(0), s2 = R(0);
+        for (int k = beg; k < end; ++k) {
+            const int ent = inc[k];
+            const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
+            s0 += fe[base];
+            s1 += fe[base + TE];
+            s2 += fe[base + 2 * TE];
+        }
+        const int ps = A.ln_pslot[lb + ln];
+        if (ps < 0) {
+            const int gid = A.ln_gid[lb + ln];
+            if (MODE == TILE_FORCE_FROM_P) {
+                A.f_out[3 * gid + 0] += s0;
+                A.f_out[3 * gid + 1] += s1;
+                A.f_out[3 * gid + 2] += s2;
+            } else {
+                A.f_out[3 * gid + 0] = s0;
+                A.f_out[3 * gid + 1] = s1;
+                A.f_out[3 * gid + 2] = s2;
+            }
+        } else {
+            A.partial[3 * ps + 0] = s0;
+            A.partial[3 * ps + 1] = s1;
+            A.partial[3 * ps + 2] = s2;
+        }
+    }
+    }  // MODE != TILE_STORE_P
+}
+
+// Shared memory bytes of one tile block.
+template <typename R>
+inline size_t tile_smem_bytes(int npe, int max_local, bool damp) {
+    return sizeof(R) * ((size_t)max_local * (damp ? 6 : 3) + (size_t)3 * npe * TILE_ELEMS);
+}
+
+}  // namespace tlfea
+
+// ---------------------------------------------------------------- element state
+struct tlfea_element_s {
+    int type = TLFEA_TYPE_T10;
+    int npe = tlfea::T10_NPE;
+    int nqp = tlfea::T10_NQP;
+    int E = 0;
+    int N = 0;
+    int device = 0;
+    cudaStream_t stream = 0;
+    bool own_stream = false;
+    bool blocking = true;
+
+    bool is_setup = false;
+    bool precomputed = false;
+    bool constraints_setup = false;
+    bool mass_setup = false;
+    bool jt_setup = false;
+    bool j_setup = false;
+
+    std::vector<int> conn;  // column-major, original element order
+    double qx[5] = {0}, qy[5] = {0}, qz[5] = {0}, qw[5] = {0};
+
+    double rho = 0, E_mod = 0, nu = 0, mu = 0, lambda = 0, eta_d = 0, lambda_d = 0;
+    int material = TLFEA_MATERIAL_SVK;
+    double mu10 = 0, mu01 = 0, kappa = 0;
+    int precision = TLFEA_PRECISION_FP64;
+
+    double *x = nullptr, *y = nullptr, *z = nullptr;
+    double *xj = nullptr, *yj = nullptr, *zj = nullptr;
+    double *X0x = nullptr, *X0y = nullptr, *X0z = nullptr;
+    float *ux = nullptr, *uy = nullptr, *uz = nullptr;
+    bool u_dirty = true;
+    int* d_conn = nullptr;
+    double* f_int = nullptr;
+    double* f_ext = nullptr;
+    float* f_int32 = nullptr;
+    bool f_int_from32 = false;  // last fused evaluation wrote f_int32
+    double* detJ = nullptr;     // reference layout E*nqp
+    double* Pst = nullptr;      // reference layout E*nqp*9 (lazy)
+
+    tlfea::Tiling tl;
+
+    // node -> (element, slot) incidence in element order (cpu_utils.cc:97-109)
+    int* inc_off = nullptr;
+    int* inc_e = nullptr;
+    int* inc_a = nullptr;
+    std::vector<int> h_inc_off, h_inc_e, h_inc_a;
+
+    // node-level pattern, shared by the mass CSR and the 3x3-block stiffness
+    std::vector<int> h_pat_off, h_pat_col;
+    int* pat_off = nullptr;
+    int* pat_col = nullptr;
+    long long pat_nnz = 0;
+    double* m_val = nullptr;
+
+    int n_constraint = 0;
+    std::vector<int> h_fixed;
+    int* fixed = nullptr;
+    double* c = nullptr;
+    int *jt_off = nullptr, *jt_col = nullptr;
+    double* jt_val = nullptr;
+    int *j_off = nullptr, *j_col = nullptr;
+    double* j_val = nullptr;
+
+    // generic scratch for the force evaluation
+    int* d_zero_dummy = nullptr;
+};
+
+namespace tlfea {
+// Implemented in element.cu, used by the solvers.
+int element_build_pattern(tlfea_element_s* h);
+int element_refresh_u32(tlfea_element_s* h);
+int element_force(tlfea_element_s* h, const double* d_v, bool fp32);
+}  // namespace tlfea

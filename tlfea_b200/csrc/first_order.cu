@@ -1,0 +1,525 @@
+// first_order.cu -- SyncedNesterovSolver, SyncedAdamWSolver and
+// SyncedAdamWNocoopSolver (SyncedNesterov.cu:97-414, SyncedAdamW.cu:99-425,
+// SyncedAdamWNocoop.cu:97-458) as one persistent cooperative kernel per Solve().
+//
+// Differences from the reference, none of which changes the iteration:
+//   * every phase is grid-strided, so any mesh size runs (the reference
+//     Nesterov leaves DOFs beyond its co-resident grid un-updated, and its
+//     AdamW refuses such sizes);
+//   * the internal force is the fused tile routine (no F/P round trip through
+//     HBM, no atomics) and the gradient reads it back per node;
+//   * norms are two-level reductions (block shuffles, then every block folds
+//     the per-block partials in block order, so every block takes the same
+//     branch without another barrier) instead of one thread's serial loop;
+//   * about 4 grid barriers per inner iteration instead of 13.
+//   * a non-finite ||g|| ends the solve with TLFEA_NONFINITE.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "solver.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace tlfea {
+
+struct FOArgs {
+    int kind;
+    int N, nc, n_fixed, n_tiles;
+    const int* fixed;
+    double* c;
+    const double *xj, *yj, *zj;
+    double *x, *y, *z;
+    const double *X0x, *X0y, *X0z;
+    float *ux, *uy, *uz;
+    const int* m_off;
+    const int* m_col;
+    const double* m_val;
+    const double* f_ext;
+    double* f_int64;
+    float* f_int32;
+    const int* node_bidx;
+    const int* bnode_off;
+    const int* bnode_slots;
+    const int* jt_off;
+    const int* jt_col;
+    double *vg, *vp, *vk, *vkm1, *g, *lam, *m, *va, *xp, *yp, *zp;
+    double* red;
+    int red_stride;
+    int* stat;          // [outer, inner_total, last_inner, status]
+    double* stat_norm;  // last ||g||
+    // parameters (SyncedNesterovParams / SyncedAdamWParams)
+    double alpha, rho, inner_tol, outer_tol, dt;
+    int max_outer, max_inner;
+    double lr, beta1, beta2, eps, wd, lr_decay, rtol;
+    int check;
+};
+
+// Every block folds the per-block partials of slot `k` in block order.
+__device__ __forceinline__ double fold_partials(const FOArgs& S, int k, double* sh) {
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) s += __ldcg(S.red + (size_t)k * S.red_stride + b);
+        s = warp_sum(s);
+        if (threadIdx.x == 0) *sh = s;
+    }
+    __syncthreads();
+    return *sh;
+}
+
+__device__ __forceinline__ void write_partial(const FOArgs& S, int k, double v, double* red_sh) {
+    const double s = block_sum(v, red_sh);
+    if (threadIdx.x == 0) S.red[(size_t)k * S.red_stride + blockIdx.x] = s;
+}
+
+// x = x_prev + dt * v (and the FP32 displacement when forces run in FP32)
+template <typename R>
+__device__ __forceinline__ void set_node_positions(const FOArgs& S, int i, double v0, double v1, double v2) {
+    const double nx = S.xp[i] + S.dt * v0, ny = S.yp[i] + S.dt * v1, nz = S.zp[i] + S.dt * v2;
+    S.x[i] = nx;
+    S.y[i] = ny;
+    S.z[i] = nz;
+    if (sizeof(R) == 4) {
+        S.ux[i] = (float)(nx - S.X0x[i]);
+        S.uy[i] = (float)(ny - S.X0y[i]);
+        S.uz[i] = (float)(nz - S.X0z[i]);
+    }
+}
+
+// Internal force of node i (boundary nodes: sum of the tile partials in tile
+// order, written back so f_int is complete).
+template <typename R>
+__device__ __forceinline__ void node_force(const FOArgs& S, const TileArgs<R>& A, int i, double f[3]) {
+    const int b = S.node_bidx[i];
+    if (b < 0) {
+        f[0] = (double)A.f_out[3 * i + 0];
+        f[1] = (double)A.f_out[3 * i + 1];
+        f[2] = (double)A.f_out[3 * i + 2];
+    } else {
+        R s0 = R(0), s1 = R(0), s2 = R(0);
+        for (int k = S.bnode_off[b]; k < S.bnode_off[b + 1]; ++k) {
+            const int p = S.bnode_slots[k];
+            s0 += A.partial[3 * p + 0];
+            s1 += A.partial[3 * p + 1];
+            s2 += A.partial[3 * p + 2];
+        }
+        A.f_out[3 * i + 0] = s0;
+        A.f_out[3 * i + 1] = s1;
+        A.f_out[3 * i + 2] = s2;
+        f[0] = (double)s0;
+        f[1] = (double)s1;
+        f[2] = (double)s2;
+    }
+}
+
+// solver_grad_L (SyncedNesterov.cu:32-95) for the 3 DOFs of node i.
+__device__ __forceinline__ void grad_node(const FOArgs& S, int i, const double f[3], double gi[3]) {
+    const double inv_dt = 1.0 / S.dt;
+    double r[3] = {0.0, 0.0, 0.0};
+    for (int k = S.m_off[i]; k < S.m_off[i + 1]; ++k) {
+        const int j = S.m_col[k];
+        const double mij = S.m_val[k];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double vd = S.vg[3 * j + d] - S.vp[3 * j + d];
+            r[d] += mij * vd * inv_dt;
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        r[d] -= (-f[d]);
+        r[d] -= S.f_ext[3 * i + d];
+        if (S.nc > 0) {
+            const int t = 3 * i + d;
+            for (int k = S.jt_off[t]; k < S.jt_off[t + 1]; ++k) {
+                const int ci = S.jt_col[k];
+                r[d] += S.dt * 1.0 * (S.lam[ci] + S.rho * S.c[ci]);
+            }
+        }
+        gi[d] = r[d];
+    }
+}
+
+template <typename R, int NPE, int NQP, bool DAMP>
+__device__ __forceinline__ void force_phase(const FOArgs& S, const TileArgs<R>& A, unsigned char* smem) {
+    for (int tile = blockIdx.x; tile < S.n_tiles; tile += gridDim.x) process_tile<R, NPE, NQP, TILE_FORCE, DAMP>(A, tile, smem);
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    for (int k = gt; k < S.n_fixed; k += gs) {
+        const int n = S.fixed[k];
+        S.c[3 * k + 0] = S.x[n] - S.xj[n];
+        S.c[3 * k + 1] = S.y[n] - S.yj[n];
+        S.c[3 * k + 2] = S.z[n] - S.zj[n];
+    }
+}
+
+template <typename R, int NPE, int NQP, bool DAMP>
+__global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R> A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double red_sh[32];
+    __shared__ double fold_sh;
+    cg::grid_group grid = cg::this_grid();
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    const int N = S.N, n3 = 3 * N;
+    const bool nesterov = (S.kind == KIND_NESTEROV);
+    const bool nocoop = (S.kind == KIND_ADAMW_NOCOOP);
+    const int check = S.check > 0 ? S.check : 1;
+    const int eff_outer = (nocoop && S.nc == 0) ? 1 : S.max_outer;
+
+    for (int i = gt; i < N; i += gs) {
+        S.xp[i] = S.x[i];
+        S.yp[i] = S.y[i];
+        S.zp[i] = S.z[i];
+    }
+    grid.sync();
+
+    int outer_flag = 0, status = 0, n_outer = 0, inner_total = 0, last_inner = 0;
+    double last_norm = 0.0;
+    for (int outer = 0; outer < eff_outer && !outer_flag && !status; ++outer) {
+        ++n_outer;
+        double t = 1.0, prev_norm_g = 0.0, norm_g = 0.0, norm_g0 = -1.0, lr = S.lr;
+        int inner_flag = 0, inner_count = 0;
+        for (int i = gt; i < n3; i += gs) {
+            if (nesterov) {
+                S.vk[i] = S.vg[i];
+                S.vkm1[i] = S.vg[i];
+            } else {
+                S.g[i] = 0.0;
+                S.m[i] = 0.0;
+                S.va[i] = 0.0;
+            }
+        }
+        grid.sync();
+        for (int inner = 0; inner < S.max_inner && !inner_flag; ++inner) {
+            ++inner_count;
+            // ---- P1: new velocity guess and scratch positions
+            if (nesterov) {
+                const double t_next = 0.5 * (1.0 + sqrt(1.0 + 4.0 * t * t));
+                const double beta = (t - 1.0) / t_next;
+                for (int i = gt; i < N; i += gs) {
+                    double v[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const double vk = S.vk[3 * i + d];
+                        v[d] = vk + beta * (vk - S.vkm1[3 * i + d]);
+                        S.vg[3 * i + d] = v[d];
+                    }
+                    set_node_positions<R>(S, i, v[0], v[1], v[2]);
+                }
+                t = t_next;
+            } else {
+                double lr_cur, b1t, b2t;
+                if (nocoop) {
+                    lr_cur = S.lr * pow(S.lr_decay, inner + 1);
+                    const double tc = (double)(inner + 2);
+                    b1t = 1.0 / (1.0 - pow(S.beta1, tc));
+                    b2t = 1.0 / (1.0 - pow(S.beta2, tc));
+                } else {
+                    lr = lr * S.lr_decay;
+                    t += 1;
+                    lr_cur = lr;
+                    b1t = 1 - pow(S.beta1, t);
+                    b2t = 1 - pow(S.beta2, t);
+                }
+                for (int i = gt; i < N; i += gs) {
+                    double v[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const int k = 3 * i + d;
+                        const double gk = S.g[k], vgk = S.vg[k];
+                        const double mt = S.beta1 * S.m[k] + (1 - S.beta1) * gk;
+                        const double vt = S.beta2 * S.va[k] + (1 - S.beta2) * gk * gk;
+                        double mh, vh;
+                        if (nocoop) {
+                            mh = mt * b1t;
+                            vh = vt * b2t;
+                        } else {
+                            mh = mt / b1t;
+                            vh = vt / b2t;
+                        }
+                        v[d] = vgk - lr_cur * (mh / (sqrt(vh) + S.eps) + S.wd * vgk);
+                        S.m[k] = mt;
+                        S.va[k] = vt;
+                        S.vg[k] = v[d];
+                    }
+                    set_node_positions<R>(S, i, v[0], v[1], v[2]);
+                }
+            }
+            grid.sync();
+            // ---- P2: internal force (fused tiles) and constraint values
+            force_phase<R, NPE, NQP, DAMP>(S, A, smem);
+            grid.sync();
+            // ---- P3: gradient per node and the norm partials
+            const bool do_check = nesterov || (inner % check == 0);
+            double sg = 0.0, sv = 0.0;
+            for (int i = gt; i < N; i += gs) {
+                double f[3], gi[3];
+                node_force<R>(S, A, i, f);
+                grad_node(S, i, f, gi);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    S.g[3 * i + d] = gi[d];
+                    sg += gi[d] * gi[d];
+                    if (!nesterov) sv += S.vg[3 * i + d] * S.vg[3 * i + d];
+                }
+            }
+            if (do_check) {
+                write_partial(S, 0, sg, red_sh);
+                if (!nesterov) write_partial(S, 1, sv, red_sh);
+            }
+            grid.sync();
+            if (nesterov) {
+                // ---- P4: ||g|| test, v_next = y - alpha g, norm partials of v_next and v_k
+                norm_g = sqrt(fold_partials(S, 0, &fold_sh));
+                if (!isfinite(norm_g)) status = TLFEA_NONFINITE;
+                if (inner > 0 && fabs(norm_g - prev_norm_g) < S.inner_tol) inner_flag = 1;
+                double snv = 0.0, snk = 0.0;
+                for (int i = gt; i < n3; i += gs) {
+                    const double vn = S.vg[i] - S.alpha * S.g[i];
+                    const double vk = S.vk[i];
+                    snv += vn * vn;
+                    snk += vk * vk;
+                    S.vkm1[i] = vk;
+                    S.vk[i] = vn;
+                    S.vg[i] = vn;
+                }
+                write_partial(S, 1, snv, red_sh);
+                write_partial(S, 2, snk, red_sh);
+                grid.sync();
+                const double nvn = sqrt(fold_partials(S, 1, &fold_sh));
+                const double nvk = sqrt(fold_partials(S, 2, &fold_sh));
+                if (inner > 0 && fabs(nvn - nvk) < S.inner_tol) inner_flag = 1;
+                prev_norm_g = norm_g;
+            } else if (do_check) {
+                norm_g = sqrt(fold_partials(S, 0, &fold_sh));
+                const double nv = sqrt(fold_partials(S, 1, &fold_sh));
+                if (!isfinite(norm_g)) status = TLFEA_NONFINITE;
+                if (norm_g0 < 0.0) norm_g0 = norm_g;
+                const double tol_abs = S.inner_tol * (1.0 + nv);
+                const double tol_rel = (S.rtol > 0.0 && norm_g0 > 0.0) ? (S.rtol * norm_g0) : 0.0;
+                if (norm_g <= tol_abs || (tol_rel > 0.0 && norm_g <= tol_rel)) inner_flag = 1;
+            }
+            if (status) break;
+        }
+        inner_total += inner_count;
+        last_inner = inner_count;
+        last_norm = norm_g;
+        if (status) break;
+        // ---- outer update: v_prev, positions, constraints, multipliers
+        for (int i = gt; i < N; i += gs) {
+            double v[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                v[d] = S.vg[3 * i + d];
+                S.vp[3 * i + d] = v[d];
+            }
+            set_node_positions<R>(S, i, v[0], v[1], v[2]);
+        }
+        grid.sync();
+        double sc = 0.0;
+        for (int k = gt; k < S.n_fixed; k += gs) {
+            const int n = S.fixed[k];
+            const double cc[3] = {S.x[n] - S.xj[n], S.y[n] - S.yj[n], S.z[n] - S.zj[n]};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                S.c[3 * k + d] = cc[d];
+                S.lam[3 * k + d] += S.rho * S.dt * cc[d];
+                sc += cc[d] * cc[d];
+            }
+        }
+        write_partial(S, 3, sc, red_sh);
+        grid.sync();
+        const double norm_c = sqrt(fold_partials(S, 3, &fold_sh));
+        if (nocoop) {
+            if (S.nc > 0 && norm_c < S.outer_tol && inner_flag) outer_flag = 1;
+        } else if (fabs(norm_c) < S.outer_tol) {
+            outer_flag = 1;
+        }
+    }
+    // final positions x = x_prev + dt v
+    for (int i = gt; i < N; i += gs) set_node_positions<R>(S, i, S.vg[3 * i], S.vg[3 * i + 1], S.vg[3 * i + 2]);
+    if (gt == 0) {
+        S.stat[0] = n_outer;
+        S.stat[1] = inner_total;
+        S.stat[2] = last_inner;
+        S.stat[3] = status;
+        *S.stat_norm = last_norm;
+    }
+}
+
+template <typename R, int NPE, int NQP, bool DAMP>
+static int launch_first_order(tlfea_solver_s* s, FOArgs& S, TileArgs<R>& A) {
+    tlfea_element_s* el = s->el;
+    auto kern = k_first_order<R, NPE, NQP, DAMP>;
+    const size_t smem = tile_smem_bytes<R>(NPE, el->tl.max_local, DAMP);
+    if (smem > 48 * 1024) TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, sms = 0;
+    TLFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TILE_ELEMS, smem));
+    TLFEA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, el->device));
+    if (per_sm < 1) {
+        set_error("persistent solver kernel does not fit on an SM");
+        return TLFEA_UNSUPPORTED;
+    }
+    int blocks = std::min(per_sm * sms, s->max_blocks);
+    const int need = std::max((3 * el->N + TILE_ELEMS - 1) / TILE_ELEMS, el->tl.n_tiles);
+    blocks = std::max(1, std::min(blocks, need));
+    void* args[] = {(void*)&S, (void*)&A};
+    TLFEA_CUDA(cudaLaunchCooperativeKernel((const void*)kern, blocks, TILE_ELEMS, args, smem, el->stream));
+    TLFEA_LAUNCHED(1);
+    return TLFEA_OK;
+}
+
+int first_order_alloc(tlfea_solver_s* s) {
+    tlfea_element_s* el = s->el;
+    const size_t n3 = 3 * (size_t)el->N, N = el->N;
+    int st = 0;
+    st |= dalloc(&s->v_guess, n3) | dalloc(&s->v_prev, n3) | dalloc(&s->v_k, n3) | dalloc(&s->v_km1, n3);
+    st |= dalloc(&s->g, n3) | dalloc(&s->m, n3) | dalloc(&s->va, n3);
+    st |= dalloc(&s->lam, (size_t)std::max(s->n_constraints, 1));
+    st |= dalloc(&s->xp, N) | dalloc(&s->yp, N) | dalloc(&s->zp, N);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, el->device);
+    s->max_blocks = std::max(1, sms * 16);
+    st |= dalloc(&s->red, (size_t)4 * s->max_blocks);
+    st |= dalloc(&s->dstat, 8);
+    if (st) return TLFEA_CUDA_ERROR;
+    return TLFEA_OK;
+}
+
+void first_order_free(tlfea_solver_s* s) {
+    dfree(s->v_guess); dfree(s->v_prev); dfree(s->v_k); dfree(s->v_km1);
+    dfree(s->g); dfree(s->m); dfree(s->va); dfree(s->lam);
+    dfree(s->xp); dfree(s->yp); dfree(s->zp);
+    dfree(s->red); dfree(s->dstat);
+}
+
+int first_order_solve(tlfea_solver_s* s) {
+    tlfea_element_s* el = s->el;
+    if (!el->is_setup) {
+        set_error("element must be set up first");
+        return TLFEA_NOT_SETUP;
+    }
+    if (!s->params_set) {
+        set_error("SetParameters must be called before Solve");
+        return TLFEA_NOT_SETUP;
+    }
+    if (!el->mass_setup) {
+        set_error("CalcMassMatrix must be called before Solve");
+        return TLFEA_NOT_SETUP;
+    }
+    if (el->material != TLFEA_MATERIAL_SVK) {
+        set_error("Mooney-Rivlin is not supported");
+        return TLFEA_UNSUPPORTED;
+    }
+    if (s->n_constraints != el->n_constraint) {
+        set_error("solver constraint count differs from the element's");
+        return TLFEA_SIZE_MISMATCH;
+    }
+    int st;
+    if (el->n_constraint > 0 && !el->jt_setup) {
+        if ((st = tlfea_element_build_constraint_jact_csr(el))) return st;
+    }
+    const bool fp32 = (el->precision == TLFEA_PRECISION_FP32);
+    if (fp32 && (st = element_refresh_u32(el))) return st;
+    FOArgs S;
+    memset(&S, 0, sizeof(S));
+    S.kind = s->kind;
+    S.N = el->N;
+    S.nc = el->n_constraint;
+    S.n_fixed = el->n_constraint / 3;
+    S.n_tiles = el->tl.n_tiles;
+    S.fixed = el->fixed;
+    S.c = el->c;
+    S.xj = el->xj; S.yj = el->yj; S.zj = el->zj;
+    S.x = el->x; S.y = el->y; S.z = el->z;
+    S.X0x = el->X0x; S.X0y = el->X0y; S.X0z = el->X0z;
+    S.ux = el->ux; S.uy = el->uy; S.uz = el->uz;
+    S.m_off = el->pat_off; S.m_col = el->pat_col; S.m_val = el->m_val;
+    S.f_ext = el->f_ext;
+    S.f_int64 = el->f_int;
+    S.f_int32 = el->f_int32;
+    S.node_bidx = el->tl.node_bidx;
+    S.bnode_off = el->tl.bnode_off;
+    S.bnode_slots = el->tl.bnode_slots;
+    S.jt_off = el->jt_off;
+    S.jt_col = el->jt_col;
+    S.vg = s->v_guess; S.vp = s->v_prev; S.vk = s->v_k; S.vkm1 = s->v_km1;
+    S.g = s->g; S.lam = s->lam; S.m = s->m; S.va = s->va;
+    S.xp = s->xp; S.yp = s->yp; S.zp = s->zp;
+    S.red = s->red;
+    S.red_stride = s->max_blocks;
+    S.stat = s->dstat;
+    S.stat_norm = (double*)(s->dstat + 4);
+    if (s->kind == KIND_NESTEROV) {
+        S.alpha = s->np.alpha; S.rho = s->np.rho; S.inner_tol = s->np.inner_tol; S.outer_tol = s->np.outer_tol;
+        S.max_outer = s->np.max_outer; S.max_inner = s->np.max_inner; S.dt = s->np.time_step;
+    } else {
+        S.lr = s->ap.lr; S.beta1 = s->ap.beta1; S.beta2 = s->ap.beta2; S.eps = s->ap.eps;
+        S.wd = s->ap.weight_decay; S.lr_decay = s->ap.lr_decay; S.inner_tol = s->ap.inner_tol;
+        S.outer_tol = s->ap.outer_tol; S.rho = s->ap.rho; S.max_outer = s->ap.max_outer;
+        S.max_inner = s->ap.max_inner; S.dt = s->ap.time_step; S.check = s->ap.convergence_check_interval;
+        S.rtol = s->ap.inner_rtol;
+    }
+    const bool damp = (el->eta_d != 0.0 || el->lambda_d != 0.0);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, el->stream);
+    if (fp32) {
+        TileArgs<float> A;
+        memset(&A, 0, sizeof(A));
+        A.node_off = el->tl.node_off; A.ln_gid = el->tl.ln_gid; A.ln_pslot = el->tl.ln_pslot;
+        A.ln_inc_end = el->tl.ln_inc_end; A.inc = el->tl.inc; A.lconn = el->tl.lconn; A.tile_elem = el->tl.tile_elem;
+        A.grad = el->tl.grad32; A.dv = el->tl.dv32; A.px = el->ux; A.py = el->uy; A.pz = el->uz;
+        A.v = s->v_guess; A.f_out = el->f_int32; A.partial = el->tl.partial32;
+        A.lambda = (float)el->lambda; A.mu = (float)el->mu; A.eta = (float)el->eta_d; A.lamd = (float)el->lambda_d;
+        A.max_local = el->tl.max_local;
+        if (el->npe == 10)
+            st = damp ? launch_first_order<float, 10, 5, true>(s, S, A) : launch_first_order<float, 10, 5, false>(s, S, A);
+        else
+            st = damp ? launch_first_order<float, 4, 1, true>(s, S, A) : launch_first_order<float, 4, 1, false>(s, S, A);
+    } else {
+        TileArgs<double> A;
+        memset(&A, 0, sizeof(A));
+        A.node_off = el->tl.node_off; A.ln_gid = el->tl.ln_gid; A.ln_pslot = el->tl.ln_pslot;
+        A.ln_inc_end = el->tl.ln_inc_end; A.inc = el->tl.inc; A.lconn = el->tl.lconn; A.tile_elem = el->tl.tile_elem;
+        A.grad = el->tl.grad64; A.dv = el->tl.dv64; A.px = el->x; A.py = el->y; A.pz = el->z;
+        A.v = s->v_guess; A.f_out = el->f_int; A.partial = el->tl.partial64;
+        A.lambda = el->lambda; A.mu = el->mu; A.eta = el->eta_d; A.lamd = el->lambda_d;
+        A.max_local = el->tl.max_local;
+        if (el->npe == 10)
+            st = damp ? launch_first_order<double, 10, 5, true>(s, S, A) : launch_first_order<double, 10, 5, false>(s, S, A);
+        else
+            st = damp ? launch_first_order<double, 4, 1, true>(s, S, A) : launch_first_order<double, 4, 1, false>(s, S, A);
+    }
+    cudaEventRecord(e1, el->stream);
+    if (st) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return st;
+    }
+    TLFEA_CUDA(cudaStreamSynchronize(el->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int hs[8];
+    TLFEA_CUDA(cudaMemcpy(hs, s->dstat, sizeof(hs), cudaMemcpyDeviceToHost));
+    s->stats.outer_iters = hs[0];
+    s->stats.inner_iters_total = hs[1];
+    s->stats.last_inner_iters = hs[2];
+    s->stats.status = hs[3];
+    memcpy(&s->stats.last_norm_g, hs + 4, sizeof(double));
+    s->stats.kernel_ms = ms;
+    el->f_int_from32 = fp32;
+    el->u_dirty = !fp32;  // the kernel keeps u in step with x in FP32 mode
+    if (s->stats.status == TLFEA_NONFINITE) {
+        set_error("non-finite gradient norm");
+        return TLFEA_NONFINITE;
+    }
+    return TLFEA_OK;
+}
+
+}  // namespace tlfea

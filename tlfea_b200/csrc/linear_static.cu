@@ -1,0 +1,506 @@
+// linear_static.cu -- LinearStaticSolver<T> (LinearStaticSolver.cu:196-603) on
+// sm_100a: deterministic row-wise stiffness assembly into 3x3 node blocks,
+// Dirichlet elimination, and an unpreconditioned FP64 CG whose dot products
+// are fused into the SpMV / axpy kernels and whose scalars never leave the
+// device (CUDA graph of several iterations per host check).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "solver.cuh"
+
+namespace tlfea {
+
+// Stiffness, one thread per node row i.  For every incident (element e, slot a)
+// in element order and every QP: the SVK tangent blocks K_ab of
+// compute_hessian_assemble_csr (FEAT10DataFunc.cuh:512-684; SVK.cuh:41-67) at
+// the current positions, scaled by h, plus the Kelvin-Voigt block C_ab
+// (:686-768) when damping is set.  Block (a,b) is added to row i's block for
+// node conn(e,b).  No atomics: each row is owned by one thread.
+template <int NPE, int NQP>
+__global__ void __launch_bounds__(128) k_stiffness_rows(int N, int E, const int* __restrict__ conn,
+                                                        const double* __restrict__ x, const double* __restrict__ y,
+                                                        const double* __restrict__ z, const int* __restrict__ elem_slot,
+                                                        const double* __restrict__ grad64,
+                                                        const double* __restrict__ dv64,
+                                                        const int* __restrict__ inc_off, const int* __restrict__ inc_e,
+                                                        const int* __restrict__ inc_a, const int* __restrict__ off,
+                                                        const int* __restrict__ col, double* K, double lambda,
+                                                        double mu, double eta_d, double lambda_d, double h) {
+    constexpr int TE = TILE_ELEMS;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int rb = off[i], re = off[i + 1];
+    for (long long k = 9LL * rb; k < 9LL * re; ++k) K[k] = 0.0;
+    const bool visc = (eta_d != 0.0 || lambda_d != 0.0);
+    for (int k = inc_off[i]; k < inc_off[i + 1]; ++k) {
+        const int e = inc_e[k], a = inc_a[k];
+        const int slot = elem_slot[e];
+        const int tile = slot / TE, t = slot % TE;
+        int bpos[NPE];
+        double X[NPE][3];
+        for (int b = 0; b < NPE; ++b) {
+            const int nb = conn[e + (size_t)b * E];
+            X[b][0] = x[nb];
+            X[b][1] = y[nb];
+            X[b][2] = z[nb];
+            int lo = rb, hi = re - 1, pos = -1;
+            while (lo <= hi) {
+                const int mid = lo + ((hi - lo) >> 1);
+                const int v = col[mid];
+                if (v == nb) {
+                    pos = mid;
+                    break;
+                }
+                if (v < nb)
+                    lo = mid + 1;
+                else
+                    hi = mid - 1;
+            }
+            bpos[b] = pos;
+        }
+        for (int q = 0; q < NQP; ++q) {
+            const double* gp = grad64 + ((size_t)tile * NQP + q) * (NPE * 3) * TE + t;
+            double g[NPE][3];
+            for (int b = 0; b < NPE; ++b)
+                for (int j = 0; j < 3; ++j) g[b][j] = gp[(size_t)(b * 3 + j) * TE];
+            const double dV = dv64[((size_t)tile * NQP + q) * TE + t];
+            double F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            for (int b = 0; b < NPE; ++b)
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) F[r][c] += X[b][r] * g[b][c];
+            double C[3][3], FFT[3][3];
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) {
+                    double s = 0.0, s2 = 0.0;
+                    for (int kk = 0; kk < 3; ++kk) {
+                        s += F[kk][r] * F[kk][c];
+                        s2 += F[r][kk] * F[c][kk];
+                    }
+                    C[r][c] = s;
+                    FFT[r][c] = s2;
+                }
+            const double trE = 0.5 * ((C[0][0] + C[1][1] + C[2][2]) - 3.0);
+            double Fha[3];
+            for (int r = 0; r < 3; ++r) {
+                double s = 0.0;
+                for (int c = 0; c < 3; ++c) s += F[r][c] * g[a][c];
+                Fha[r] = s;
+            }
+            for (int b = 0; b < NPE; ++b) {
+                if (bpos[b] < 0) continue;
+                double Fhb[3];
+                for (int r = 0; r < 3; ++r) {
+                    double s = 0.0;
+                    for (int c = 0; c < 3; ++c) s += F[r][c] * g[b][c];
+                    Fhb[r] = s;
+                }
+                const double hij = g[b][0] * g[a][0] + g[b][1] * g[a][1] + g[b][2] * g[a][2];
+                const double fdf = Fhb[0] * Fha[0] + Fhb[1] * Fha[1] + Fhb[2] * Fha[2];
+                double* Kb = K + 9LL * bpos[b];
+                for (int d = 0; d < 3; ++d)
+                    for (int ee = 0; ee < 3; ++ee) {
+                        const double delta = (d == ee) ? 1.0 : 0.0;
+                        const double kv = (lambda * Fha[d] * Fhb[ee] + lambda * trE * hij * delta + mu * fdf * delta +
+                                           mu * Fhb[d] * Fha[ee] + mu * hij * FFT[d][ee] + (-mu * hij * delta)) *
+                                          dV;
+                        Kb[3 * d + ee] += h * kv;
+                    }
+                if (visc) {
+                    const double hd = g[a][0] * g[b][0] + g[a][1] * g[b][1] + g[a][2] * g[b][2];
+                    for (int d = 0; d < 3; ++d)
+                        for (int ee = 0; ee < 3; ++ee)
+                            Kb[3 * d + ee] += (eta_d * (Fhb[d] * Fha[ee]) + eta_d * FFT[d][ee] * hd +
+                                               lambda_d * (Fha[d] * Fhb[ee])) *
+                                              dV;
+                }
+            }
+        }
+    }
+}
+
+// Dirichlet elimination (apply_bcs_kernel, LinearStaticSolver.cu:284-306): a
+// fixed row becomes the identity row with f = 0; free rows drop fixed columns.
+__global__ void k_apply_bcs(int N, const int* __restrict__ off, const int* __restrict__ col,
+                            const unsigned char* __restrict__ fixed, double* K, double* f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    for (int k = off[i]; k < off[i + 1]; ++k) {
+        const int cn = col[k];
+        for (int d = 0; d < 3; ++d) {
+            const int row = 3 * i + d;
+            for (int e = 0; e < 3; ++e) {
+                const int c = 3 * cn + e;
+                if (fixed[row])
+                    K[9LL * k + 3 * d + e] = (c == row) ? 1.0 : 0.0;
+                else if (fixed[c])
+                    K[9LL * k + 3 * d + e] = 0.0;
+            }
+        }
+    }
+    for (int d = 0; d < 3; ++d)
+        if (fixed[3 * i + d]) f[3 * i + d] = 0.0;
+}
+
+__global__ void k_mark_fixed(int nf, const int* __restrict__ nodes, unsigned char* fixed) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nf) return;
+    const int n = nodes[k];
+    fixed[3 * n + 0] = fixed[3 * n + 1] = fixed[3 * n + 2] = 1;
+}
+
+__global__ void k_update_positions(int n, double* x, double* y, double* z, const double* __restrict__ u) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] += u[3 * i + 0];
+    y[i] += u[3 * i + 1];
+    z[i] += u[3 * i + 2];
+}
+
+// Last-block-done reduction of per-block partials in block order (deterministic
+// for a fixed grid).  Returns true in the last block, with the total in `out`
+// (valid in thread 0).
+__device__ __forceinline__ bool last_block_sum(double part, double* partials, unsigned int* ticket, double* out) {
+    __shared__ double red[32];
+    __shared__ bool am_last;
+    const double bs = block_sum(part, red);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = bs;
+        __threadfence();
+        const unsigned int tk = atomicAdd(ticket, 1u);
+        am_last = (tk == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+    double s = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += __ldcg(partials + b);
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) {
+        *out = s;
+        *ticket = 0;
+    }
+    return true;
+}
+
+// u = 0, r = p = f, rr0 = r.r
+__global__ void k_cg_init(int n, const double* __restrict__ f, double* u, double* r, double* p, double* partials,
+                          CgCtl* ctl, int max_iter) {
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double fi = f[i];
+        u[i] = 0.0;
+        r[i] = fi;
+        p[i] = fi;
+        s += fi * fi;
+    }
+    double tot;
+    if (last_block_sum(s, partials, &ctl->ticket, &tot) && threadIdx.x == 0) {
+        ctl->rr0 = tot;
+        ctl->rr = tot;
+        ctl->iters = 0;
+        ctl->status = 0;
+        ctl->rel = 1.0;
+        ctl->done = 0;
+        if (tot == 0.0) {
+            ctl->done = 1;
+            ctl->rel = 0.0;
+        } else if (max_iter <= 0) {
+            ctl->done = 1;
+            ctl->status = 2;
+        }
+    }
+}
+
+// q = K p on 3x3 node blocks (one warp per node row, lanes stride over the
+// row's 9*nb contiguous values) fused with the p.q reduction; the last block
+// sets alpha = rr / p.q (LinearStaticSolver.cu:519-533).
+__global__ void __launch_bounds__(256) k_cg_spmv_dot(int N, const int* __restrict__ off, const int* __restrict__ col,
+                                                     const double* __restrict__ K, const double* __restrict__ p,
+                                                     double* q, double* partials, CgCtl* ctl) {
+    if (ctl->done) return;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    double pq = 0.0;
+    for (int i = warp; i < N; i += nwarps) {
+        const int rb = off[i], nb = off[i + 1] - rb;
+        const double* Kr = K + 9LL * rb;
+        const int* cr = col + rb;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int v = lane; v < 9 * nb; v += 32) {
+            const int kb = v / 9;
+            const int r9 = v - 9 * kb;
+            const int d = r9 / 3;
+            const int e = r9 - 3 * d;
+            const double prod = __ldcs(Kr + v) * p[3 * cr[kb] + e];
+            if (d == 0)
+                a0 += prod;
+            else if (d == 1)
+                a1 += prod;
+            else
+                a2 += prod;
+        }
+        a0 = warp_sum(a0);
+        a1 = warp_sum(a1);
+        a2 = warp_sum(a2);
+        if (lane == 0) {
+            q[3 * i + 0] = a0;
+            q[3 * i + 1] = a1;
+            q[3 * i + 2] = a2;
+            pq += p[3 * i + 0] * a0 + p[3 * i + 1] * a1 + p[3 * i + 2] * a2;
+        }
+    }
+    double tot;
+    if (last_block_sum(pq, partials, &ctl->ticket, &tot) && threadIdx.x == 0) {
+        ctl->pq = tot;
+        if (tot <= 0.0) {
+            ctl->status = 1;
+            ctl->done = 1;
+        } else {
+            ctl->alpha = ctl->rr / tot;
+        }
+    }
+}
+
+// u += alpha p; r -= alpha q; rr_new = r.r; convergence test sqrt(rr_new/rr0) < tol;
+// beta = rr_new / rr (LinearStaticSolver.cu:534-557).
+__global__ void k_cg_axpy_dot(int n, double* u, double* r, const double* __restrict__ p, const double* __restrict__ q,
+                              double* partials, CgCtl* ctl, double tol, int max_iter) {
+    if (ctl->done) return;
+    const double alpha = ctl->alpha;
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        u[i] += alpha * p[i];
+        const double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        s += ri * ri;
+    }
+    double rrn;
+    if (last_block_sum(s, partials, &ctl->ticket, &rrn) && threadIdx.x == 0) {
+        const double rel = (ctl->rr0 > 0.0) ? sqrt(rrn / ctl->rr0) : sqrt(rrn);
+        ctl->iters += 1;
+        if (rel < tol) {
+            ctl->rel = rel;
+            ctl->done = 1;
+        } else {
+            ctl->beta = rrn / ctl->rr;
+            ctl->rr = rrn;
+            if (ctl->iters >= max_iter) {
+                ctl->rel = rel;
+                ctl->status = 2;
+                ctl->done = 1;
+            }
+        }
+    }
+}
+
+// p = r + beta p  (cublasDscal + cublasDaxpy of LinearStaticSolver.cu:554-555)
+__global__ void k_cg_pupdate(int n, const double* __restrict__ r, double* p, const CgCtl* ctl) {
+    if (ctl->done) return;
+    const double beta = ctl->beta;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = r[i] + beta * p[i];
+}
+
+static int cg_grid(const tlfea_solver_s* s) { return s->cg_blocks; }
+
+static int launch_cg_iteration(tlfea_solver_s* s, cudaStream_t st) {
+    tlfea_element_s* el = s->el;
+    const int n = 3 * el->N;
+    const int G = cg_grid(s);
+    k_cg_spmv_dot<<<G, 256, 0, st>>>(el->N, el->pat_off, el->pat_col, s->K, s->p, s->q, s->cg_part, s->ctl);
+    if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+    k_cg_axpy_dot<<<G, 256, 0, st>>>(n, s->u, s->r, s->p, s->q, s->cg_part, s->ctl, s->tol, s->max_iter);
+    if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+    k_cg_pupdate<<<G, 256, 0, st>>>(n, s->r, s->p, s->ctl);
+    if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+    return TLFEA_OK;
+}
+
+// Captures `iters` CG iterations (3 kernels each) in one CUDA graph.
+static int build_cg_graph(tlfea_solver_s* s, int iters) {
+    cudaStream_t st = s->el->stream;
+    if (s->cg_graph) {
+        cudaGraphExecDestroy(s->cg_graph);
+        s->cg_graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    TLFEA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = TLFEA_OK;
+    for (int k = 0; k < iters && rc == TLFEA_OK; ++k) rc = launch_cg_iteration(s, st);
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != TLFEA_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        set_error("CG graph capture failed");
+        return TLFEA_CUDA_ERROR;
+    }
+    e = cudaGraphInstantiate(&s->cg_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+        s->cg_graph = nullptr;
+        return TLFEA_CUDA_ERROR;
+    }
+    s->cg_graph_iters = iters;
+    return TLFEA_OK;
+}
+
+int linear_static_prepare(tlfea_solver_s* s) {
+    tlfea_element_s* el = s->el;
+    int st = element_build_pattern(el);
+    if (st) return st;
+    if (!s->K) {
+        const size_t n3 = 3 * (size_t)el->N;
+        if ((st = dalloc(&s->K, 9 * (size_t)std::max(el->pat_nnz, 1LL)))) return st;
+        if ((st = dalloc(&s->u, n3)) || (st = dalloc(&s->f, n3)) || (st = dalloc(&s->r, n3)) ||
+            (st = dalloc(&s->p, n3)) || (st = dalloc(&s->q, n3)))
+            return st;
+        if ((st = dalloc(&s->is_fixed, n3))) return st;
+        if ((st = dalloc(&s->ctl, 1))) return st;
+        TLFEA_CUDA(cudaMemset(s->ctl, 0, sizeof(CgCtl)));
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int rows_warps = (el->N + 7) / 8;
+        s->cg_blocks = std::max(1, std::min(rows_warps, sms * 8));
+        if ((st = dalloc(&s->cg_part, (size_t)s->cg_blocks))) return st;
+    }
+    return TLFEA_OK;
+}
+
+int linear_static_solve(tlfea_solver_s* s) {
+    tlfea_element_s* el = s->el;
+    if (!el->is_setup) {
+        set_error("element must be set up first");
+        return TLFEA_NOT_SETUP;
+    }
+    if (el->material != TLFEA_MATERIAL_SVK) {
+        set_error("Mooney-Rivlin is not supported");
+        return TLFEA_UNSUPPORTED;
+    }
+    int st = linear_static_prepare(s);
+    if (st) return st;
+    cudaStream_t stream = el->stream;
+    const int N = el->N, n3 = 3 * N;
+    // AssembleLinearStiffness (h = 1)
+    if (el->npe == 10)
+        k_stiffness_rows<10, 5><<<(N + 127) / 128, 128, 0, stream>>>(
+            N, el->E, el->d_conn, el->x, el->y, el->z, el->tl.elem_slot, el->tl.grad64, el->tl.dv64, el->inc_off,
+            el->inc_e, el->inc_a, el->pat_off, el->pat_col, s->K, el->lambda, el->mu, el->eta_d, el->lambda_d, 1.0);
+    else
+        k_stiffness_rows<4, 1><<<(N + 127) / 128, 128, 0, stream>>>(
+            N, el->E, el->d_conn, el->x, el->y, el->z, el->tl.elem_slot, el->tl.grad64, el->tl.dv64, el->inc_off,
+            el->inc_e, el->inc_a, el->pat_off, el->pat_col, s->K, el->lambda, el->mu, el->eta_d, el->lambda_d, 1.0);
+    TLFEA_CHECK_LAUNCH();
+    TLFEA_CUDA(cudaMemcpyAsync(s->f, el->f_ext, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
+    // ApplyDirichletBCs
+    const int nf = el->n_constraint / 3;
+    if (nf > 0) {
+        TLFEA_CUDA(cudaMemsetAsync(s->is_fixed, 0, n3, stream));
+        k_mark_fixed<<<(nf + 255) / 256, 256, 0, stream>>>(nf, el->fixed, s->is_fixed);
+        TLFEA_CHECK_LAUNCH();
+        k_apply_bcs<<<(N + 255) / 256, 256, 0, stream>>>(N, el->pat_off, el->pat_col, s->is_fixed, s->K, s->f);
+        TLFEA_CHECK_LAUNCH();
+    }
+    s->k_built = true;
+    // SolveLinearSystemCG
+    const int G = cg_grid(s);
+    k_cg_init<<<G, 256, 0, stream>>>(n3, s->f, s->u, s->r, s->p, s->cg_part, s->ctl, s->max_iter);
+    TLFEA_CHECK_LAUNCH();
+    int chunk = 8;
+    long long launched = 0;
+    CgCtl h{};
+    for (;;) {
+        TLFEA_CUDA(cudaMemcpyAsync(&h, s->ctl, sizeof(CgCtl), cudaMemcpyDeviceToHost, stream));
+        TLFEA_CUDA(cudaStreamSynchronize(stream));
+        if (h.done || launched >= s->max_iter) break;
+        if (!s->cg_graph || s->cg_graph_iters != chunk) {
+            if ((st = build_cg_graph(s, chunk))) return st;
+        }
+        TLFEA_CUDA(cudaGraphLaunch(s->cg_graph, stream));
+        TLFEA_LAUNCHED(3LL * chunk);
+        launched += chunk;
+        if (chunk < 64) chunk *= 2;
+    }
+    if (h.status == 1) set_error("LinearStaticSolver CG: non-positive p*Kp detected; aborting.");
+    if (h.status == 1) {
+        // the reference leaves last_iter_count = max_iter and residual = 1 on breakdown
+        s->last_iters = s->max_iter;
+        s->last_res = 1.0;
+    } else {
+        s->last_iters = h.iters;
+        s->last_res = h.rel;
+    }
+    // UpdatePositions
+    k_update_positions<<<(N + 255) / 256, 256, 0, stream>>>(N, el->x, el->y, el->z, s->u);
+    TLFEA_CHECK_LAUNCH();
+    el->u_dirty = true;
+    TLFEA_CUDA(cudaStreamSynchronize(stream));
+    return TLFEA_OK;
+}
+
+int linear_static_apply(tlfea_solver_s* s, const double* d_x, double* d_y) {
+    tlfea_element_s* el = s->el;
+    if (!s->k_built) {
+        set_error("LinearStaticSolver::Solve has not assembled K yet");
+        return TLFEA_NOT_SETUP;
+    }
+    if (!s->ctl_apply) {
+        int st = dalloc(&s->ctl_apply, 1);
+        if (st) return st;
+        TLFEA_CUDA(cudaMemsetAsync(s->ctl_apply, 0, sizeof(CgCtl), el->stream));
+    }
+    k_cg_spmv_dot<<<cg_grid(s), 256, 0, el->stream>>>(el->N, el->pat_off, el->pat_col, s->K, d_x, d_y, s->cg_part,
+                                                      s->ctl_apply);
+    TLFEA_CHECK_LAUNCH();
+    if (el->blocking) TLFEA_CUDA(cudaStreamSynchronize(el->stream));
+    return TLFEA_OK;
+}
+
+int linear_static_retrieve_k(tlfea_solver_s* s, long long* nnz, int* offsets, int* columns, double* values) {
+    tlfea_element_s* el = s->el;
+    TLFEA_CUDA(cudaStreamSynchronize(el->stream));
+    if (!s->k_built) {
+        if (nnz) *nnz = 0;
+        return TLFEA_OK;
+    }
+    const int N = el->N;
+    const long long nb = el->pat_nnz;
+    if (nnz) *nnz = 9 * nb;
+    if (!offsets && !columns && !values) return TLFEA_OK;
+    std::vector<double> Kh((size_t)(9 * nb));
+    TLFEA_CUDA(cudaMemcpy(Kh.data(), s->K, sizeof(double) * Kh.size(), cudaMemcpyDeviceToHost));
+    const std::vector<int>& off = el->h_pat_off;
+    const std::vector<int>& col = el->h_pat_col;
+    long long o = 0;
+    for (int i = 0; i < N; ++i)
+        for (int d = 0; d < 3; ++d) {
+            if (offsets) offsets[3 * i + d] = (int)o;
+            for (int k = off[i]; k < off[i + 1]; ++k)
+                for (int e = 0; e < 3; ++e) {
+                    if (columns) columns[o] = 3 * col[k] + e;
+                    if (values) values[o] = Kh[9 * (size_t)k + 3 * d + e];
+                    ++o;
+                }
+        }
+    if (offsets) offsets[3 * N] = (int)o;
+    return TLFEA_OK;
+}
+
+void linear_static_free(tlfea_solver_s* s) {
+    if (s->cg_graph) cudaGraphExecDestroy(s->cg_graph);
+    s->cg_graph = nullptr;
+    dfree(s->K);
+    dfree(s->u);
+    dfree(s->f);
+    dfree(s->r);
+    dfree(s->p);
+    dfree(s->q);
+    dfree(s->is_fixed);
+    dfree(s->ctl);
+    dfree(s->ctl_apply);
+    dfree(s->cg_part);
+}
+
+}  // namespace tlfea

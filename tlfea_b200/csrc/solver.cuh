@@ -1,0 +1,57 @@
+// solver.cuh -- solver state shared by the first-order (Nesterov / AdamW) and the
+// linear static (CG) solvers.
+#pragma once
+
+#include "element.cuh"
+
+namespace tlfea {
+
+enum SolverKind { KIND_NESTEROV = 0, KIND_ADAMW = 1, KIND_ADAMW_NOCOOP = 2, KIND_LINEAR_STATIC = 3 };
+
+// Device-resident scalars of the CG loop (read and written only by kernels
+// between host synchronisations).
+struct CgCtl {
+    unsigned int ticket;  // last-block-done counter, reset by the last block
+    int done;             // 1 once converged, broken down or out of iterations
+    int iters;            // completed iterations
+    int status;           // 0 ok, 1 p.Kp <= 0, 2 max_iter reached
+    double rr0, rr, alpha, beta, rel;
+    double pq;
+};
+
+}  // namespace tlfea
+
+struct tlfea_solver_s {
+    int kind = tlfea::KIND_NESTEROV;
+    tlfea_element_s* el = nullptr;
+    int n_constraints = 0;
+    int device = 0;
+
+    // first-order state (3N / n_c), FP64
+    double *v_guess = nullptr, *v_prev = nullptr, *v_k = nullptr, *v_km1 = nullptr;
+    double *g = nullptr, *lam = nullptr, *m = nullptr, *va = nullptr;
+    double *xp = nullptr, *yp = nullptr, *zp = nullptr;
+    double* red = nullptr;   // per-block partial sums (3 arrays of max_blocks)
+    int max_blocks = 0;
+    int* dstat = nullptr;    // device diagnostics (tlfea_solve_stats fields)
+    tlfea_nesterov_params np{};
+    tlfea_adamw_params ap{};
+    bool params_set = false;
+    tlfea_solve_stats stats{};
+
+    // linear static
+    double tol = 1e-10;
+    int max_iter = 10000;
+    int last_iters = 0;
+    double last_res = 0.0;
+    double* K = nullptr;  // 3x3 blocks on the node pattern, 9 doubles per block
+    double *u = nullptr, *f = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
+    unsigned char* is_fixed = nullptr;  // 3N
+    tlfea::CgCtl* ctl = nullptr;
+    tlfea::CgCtl* ctl_apply = nullptr;  // scratch control block of linear_static_apply
+    double* cg_part = nullptr;  // per-block partials
+    int cg_blocks = 0;
+    cudaGraphExec_t cg_graph = nullptr;
+    int cg_graph_iters = 0;
+    bool k_built = false;
+};
