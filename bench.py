@@ -189,6 +189,49 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def setup_element(T, cfg, x, y, z, conn, fixed, f):
+    el = T.GPU_FEAT10_Data(conn.shape[0], len(x))
+    el.Initialize()
+    el.SetNodalFixed(fixed)
+    el.SetExternalForce(f)
+    el.Setup(*T.Quadrature.t10(), x, y, z, conn)
+    el.SetDensity(cfg["rho"])
+    el.SetDamping(0.0, 0.0)
+    el.SetSVK(cfg["E"], cfg["nu"])
+    el.CalcDnDuPre()
+    return el
+
+
+def kernels_only(args):
+    """Profiling case: the fused element force (2 x FP32 then 2 x FP64) or the CG
+    SpMV (assembly, a 5-iteration solve, then 3 applies) on the --mesh beam."""
+    import torch
+    import tlfea_b200 as T
+
+    torch.cuda.set_device(0)
+    cfg = dict(CFG)
+    x, y, z, conn, fixed, f = build_mesh(cfg)
+    el = setup_element(T, cfg, x, y, z, conn, fixed, f)
+    r = np.random.default_rng(1)
+    el.UpdatePositions(*(v + 1e-4 * r.standard_normal(v.shape) for v in (x, y, z)))
+    if args.kernels_only == "force":
+        for prec in ("fp32", "fp32", "fp64", "fp64"):
+            el.SetForcePrecision(prec)
+            el.ComputeInternalForce()
+    else:
+        s = T.LinearStaticSolver(el, cfg["tol"], 5)
+        s.Solve()
+        xin = torch.randn(3 * len(x), dtype=torch.float64, device="cuda")
+        yout = torch.empty_like(xin)
+        torch.cuda.synchronize()
+        for _ in range(3):
+            s.Apply(xin.data_ptr(), yout.data_ptr())
+        del s
+    torch.cuda.synchronize()
+    print(json.dumps({"kernels_only": args.kernels_only, "elements": int(conn.shape[0]), "nodes": int(len(x))}))
+    el.Destroy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,9 +240,16 @@ def main():
     ap.add_argument("--impl", default="tlfea", choices=["tlfea", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--kernel-reps", type=int, default=20)
+    ap.add_argument("--kernels-only", choices=["force", "spmv"], default=None,
+                    help="profiling case: set up, then launch only the named kernel a few times")
+    ap.add_argument("--mesh", default=None, help="cells NXxNYxNZ (default 200x20x20)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mesh:
+        CFG["nx"], CFG["ny"], CFG["nz"] = (int(v) for v in args.mesh.lower().split("x"))
+    if args.kernels_only:
+        return kernels_only(args)
 
     import torch
     import tlfea_b200 as T
@@ -217,15 +267,7 @@ def main():
     cfg = dict(CFG)
     x, y, z, conn, fixed, f = build_mesh(cfg)
     N, E = len(x), conn.shape[0]
-    el = T.GPU_FEAT10_Data(E, N)
-    el.Initialize()
-    el.SetNodalFixed(fixed)
-    el.SetExternalForce(f)
-    el.Setup(*T.Quadrature.t10(), x, y, z, conn)
-    el.SetDensity(cfg["rho"])
-    el.SetDamping(0.0, 0.0)
-    el.SetSVK(cfg["E"], cfg["nu"])
-    el.CalcDnDuPre()
+    el = setup_element(T, cfg, x, y, z, conn, fixed, f)
     el.CalcMassMatrix()
     solver = T.LinearStaticSolver(el, cfg["tol"], 1000000)
     stream = el.GetStream()
