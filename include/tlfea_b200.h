@@ -164,6 +164,11 @@ int tlfea_element_build_constraint_jac_csr(tlfea_element h);
 int tlfea_element_compute_internal_force(tlfea_element h, const double* d_v);
 /* Force precision for tlfea_element_compute_internal_force and the solvers. */
 int tlfea_element_set_force_precision(tlfea_element h, int precision);
+/* Launch configuration of the fused force kernel (new; the autotuner's knob):
+ * force_kernel 0 = persistent TMA pipeline (default), 1 = one tile per block;
+ * grid_limit caps the pipeline's persistent grid (0 = all resident blocks). */
+int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit);
+
 
 /* Retrieve*ToCPU (FEAT10Data.cu:564-649, 753-757).  Sizes are in elements of
  * the output array and must match exactly. */

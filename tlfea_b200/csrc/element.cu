@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "element.cuh"
+#include "force_pipe.cuh"
 
 namespace tlfea {
 
@@ -593,6 +594,33 @@ static int launch_combine(tlfea_element_s* h, const R* partial, R* f_out) {
     return TLFEA_OK;
 }
 
+// Persistent TMA-fed force kernel: grid = resident CTAs (occupancy) capped by the tile count.
+template <typename R, int NPE, int NQP, bool DAMP>
+static int launch_pipe(tlfea_element_s* h, const TileArgs<R>& A) {
+    auto kern = k_force_pipe<R, NPE, NQP, DAMP>;
+    const size_t smem = pipe_smem_bytes<R, NPE>(h->tl.max_local, DAMP);
+    int& grid = h->pipe_grid[(sizeof(R) == 4 ? 2 : 0) + (DAMP ? 1 : 0)];
+    if (grid == 0) {
+        if (smem > 227 * 1024) {
+            set_error("force pipeline shared memory exceeds 227 KB (tile touches too many nodes)");
+            return TLFEA_UNSUPPORTED;
+        }
+        TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0, sms = 0;
+        TLFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PIPE_THREADS, smem));
+        TLFEA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+        if (per_sm < 1) {
+            set_error("force pipeline does not fit on an SM");
+            return TLFEA_UNSUPPORTED;
+        }
+        grid = std::max(1, std::min(h->tl.n_tiles, per_sm * sms));
+        if (h->pipe_grid_limit > 0) grid = std::min(grid, h->pipe_grid_limit);
+    }
+    kern<<<grid, PIPE_THREADS, smem, h->stream>>>(A, h->tl.n_tiles, h->d_err);
+    TLFEA_CHECK_LAUNCH();
+    return TLFEA_OK;
+}
+
 template <typename R, int NPE, int NQP>
 static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
     TileArgs<R> A = make_args<R>(h, fp32);
@@ -600,7 +628,11 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
     A.v = d_v;
     if (h->tl.n_orphans)
         TLFEA_CUDA(cudaMemsetAsync(A.f_out, 0, sizeof(R) * 3 * (size_t)h->N, h->stream));
-    int st = damp ? launch_tiles<R, NPE, NQP, TILE_FORCE, true>(h, A) : launch_tiles<R, NPE, NQP, TILE_FORCE, false>(h, A);
+    int st;
+    if (h->force_kernel == 1)
+        st = damp ? launch_tiles<R, NPE, NQP, TILE_FORCE, true>(h, A) : launch_tiles<R, NPE, NQP, TILE_FORCE, false>(h, A);
+    else
+        st = damp ? launch_pipe<R, NPE, NQP, true>(h, A) : launch_pipe<R, NPE, NQP, false>(h, A);
     if (st) return st;
     return launch_combine<R, false>(h, A.partial, A.f_out);
 }
@@ -631,6 +663,21 @@ static int sync_f_int64(tlfea_element_s* h) {
     k_f32_to_f64<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(n, h->f_int32, h->f_int);
     TLFEA_CHECK_LAUNCH();
     h->f_int_from32 = false;
+    return TLFEA_OK;
+}
+
+// A kernel's bounded wait ran out: report it once and clear the word.
+static int check_device_error(tlfea_element_s* h) {
+    int e = 0;
+    if (cudaMemcpy(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_error("reading the device error word failed");
+        return TLFEA_CUDA_ERROR;
+    }
+    if (e) {
+        cudaMemset(h->d_err, 0, sizeof(int));
+        set_error("a pipeline wait in the force kernel ran out (code " + std::to_string(e) + ")");
+        return TLFEA_BUDGET_EXCEEDED;
+    }
     return TLFEA_OK;
 }
 
@@ -683,7 +730,11 @@ using namespace tlfea;
 // compute calls honour the non-blocking mode
 #define SYNC_COMPUTE(h)                                            \
     do {                                                           \
-        if ((h)->blocking) TLFEA_CUDA(cudaStreamSynchronize((h)->stream)); \
+        if ((h)->blocking) {                                       \
+            TLFEA_CUDA(cudaStreamSynchronize((h)->stream));        \
+            int st_err_ = check_device_error(h);                   \
+            if (st_err_) return st_err_;                           \
+        }                                                          \
     } while (0)
 // device -> host copy after the element's stream has drained
 #define D2H(dst, src, bytes)                                                      \
@@ -733,6 +784,7 @@ int tlfea_element_create(int type, int n_elem, int n_nodes, tlfea_element* out) 
     st |= dalloc(&h->d_conn, (size_t)n_elem * h->npe);
     st |= dalloc(&h->f_int, 3 * N) | dalloc(&h->f_ext, 3 * N) | dalloc(&h->f_int32, 3 * N);
     st |= dalloc(&h->detJ, (size_t)n_elem * h->nqp);
+    st |= dalloc(&h->d_err, 1);
     if (st) {
         tlfea_element_destroy(h);
         return TLFEA_CUDA_ERROR;
@@ -741,6 +793,7 @@ int tlfea_element_create(int type, int n_elem, int n_nodes, tlfea_element* out) 
     cudaMemsetAsync(h->f_ext, 0, 3 * N * sizeof(double), h->stream);
     cudaMemsetAsync(h->f_int32, 0, 3 * N * sizeof(float), h->stream);
     cudaMemsetAsync(h->detJ, 0, (size_t)n_elem * h->nqp * sizeof(double), h->stream);
+    cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream);
     cudaStreamSynchronize(h->stream);
     *out = h;
     return TLFEA_OK;
@@ -754,7 +807,7 @@ int tlfea_element_destroy(tlfea_element h) {
     dfree(h->X0x); dfree(h->X0y); dfree(h->X0z);
     dfree(h->ux); dfree(h->uy); dfree(h->uz);
     dfree(h->d_conn); dfree(h->f_int); dfree(h->f_ext); dfree(h->f_int32);
-    dfree(h->detJ); dfree(h->Pst);
+    dfree(h->detJ); dfree(h->Pst); dfree(h->d_err);
     free_tiling(h->tl);
     dfree(h->inc_off); dfree(h->inc_e); dfree(h->inc_a);
     dfree(h->pat_off); dfree(h->pat_col); dfree(h->m_val);
@@ -1126,6 +1179,15 @@ int tlfea_element_compute_internal_force(tlfea_element h, const double* d_v) {
     int st = element_force(h, d_v, h->precision == TLFEA_PRECISION_FP32);
     if (st) return st;
     SYNC_COMPUTE(h);
+    return TLFEA_OK;
+}
+
+int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit) {
+    CHECK_HANDLE(h);
+    if (force_kernel < 0 || force_kernel > 1 || grid_limit < 0) return TLFEA_INVALID_ARG;
+    h->force_kernel = force_kernel;
+    h->pipe_grid_limit = grid_limit;
+    for (int& g : h->pipe_grid) g = 0;
     return TLFEA_OK;
 }
 

@@ -451,8 +451,14 @@ struct tlfea_element_s {
     int *j_off = nullptr, *j_col = nullptr;
     double* j_val = nullptr;
 
-    // generic scratch for the force evaluation
-    int* d_zero_dummy = nullptr;
+    // error word set by kernels whose bounded waits ran out (checked at sync points)
+    int* d_err = nullptr;
+    // grid of the persistent force pipeline per (FP32?, damping?), 0 = not yet sized
+    int pipe_grid[4] = {0, 0, 0, 0};
+    // launch configuration (tlfea_element_set_launch_config): force kernel
+    // 0 = TMA pipeline, 1 = one tile per block; cap on the pipeline grid (0 = none)
+    int force_kernel = 0;
+    int pipe_grid_limit = 0;
 };
 
 namespace tlfea {

@@ -1,0 +1,366 @@
+// force_pipe.cuh -- TMA-fed fused internal-force kernel (sm_100a).
+//
+// Persistent CTAs, each a producer warp plus TILE_ELEMS consumer threads (one
+// element each).  The producer streams, per (tile, QP), the gradient slice
+// [NPE*3][TE] and the dV slice [TE] -- plus, with QP 0, the tile's local
+// connectivity [NPE][TE] -- from HBM into a shared-memory ring with 1-D bulk
+// copies (cp.async.bulk ... mbarrier::complete_tx, no multicast), so several
+// slices are always in flight while the consumers compute.  The consumers
+// prefetch the next tile's node positions with per-thread cp.async into a
+// second buffer, evaluate F, the SVK stress and the element forces QP by QP from
+// the ring, and reduce per node in the fixed incidence order (interior nodes
+// written directly, shared nodes as per-tile partials for k_combine).
+//
+// Every wait is bounded: a wait that runs out sets *err and the kernel carries
+// on without the data (no hang); the host turns a set *err into an error status.
+#pragma once
+
+#include "element.cuh"
+
+namespace tlfea {
+
+constexpr int PIPE_THREADS = TILE_ELEMS + 32;  // consumers + one producer warp
+constexpr long long PIPE_WAIT_LIMIT = 1LL << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Bounded wait for the phase with the given parity; false if the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < PIPE_WAIT_LIMIT; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// 1-D bulk copy global -> shared, completion counted on `bar` (16-byte aligned
+// addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(TILE_ELEMS) : "memory"); }
+
+// Ring geometry shared by host and device.  A QP slice is streamed in PARTS
+// parts (FP64: two halves, nodes 0..NPE/2-1 and the rest) so that the ring,
+// the double-buffered positions and the element forces of two CTAs fit one SM.
+template <typename R, int NPE>
+struct PipeGeom {
+    static constexpr int PARTS = sizeof(R) == 8 ? 2 : 1;
+    static constexpr int PART_NODES = NPE / PARTS;
+    static constexpr uint32_t GRAD_BYTES = PART_NODES * 3 * TILE_ELEMS * sizeof(R);  // one part
+    static constexpr uint32_t DV_BYTES = TILE_ELEMS * sizeof(R);
+    static constexpr uint32_t LCONN_BYTES = NPE * TILE_ELEMS * sizeof(uint16_t);
+    static constexpr uint32_t STAGE_BYTES = GRAD_BYTES + DV_BYTES + LCONN_BYTES;
+    static constexpr int STAGES = sizeof(R) == 4 ? 4 : 3;
+    static_assert(NPE % PARTS == 0, "parts split the nodes evenly");
+    static_assert(GRAD_BYTES % 16 == 0 && DV_BYTES % 16 == 0 && LCONN_BYTES % 16 == 0, "bulk copy alignment");
+};
+
+template <typename R, int NPE>
+inline size_t pipe_smem_bytes(int max_local, bool damp) {
+    using G = PipeGeom<R, NPE>;
+    size_t b = (size_t)G::STAGES * G::STAGE_BYTES;        // ring
+    b += 2 * 3 * (size_t)max_local * sizeof(R);           // positions, double-buffered
+    if (damp) b += 2 * 3 * (size_t)max_local * sizeof(double);  // velocities, double-buffered
+    b += (size_t)3 * NPE * TILE_ELEMS * sizeof(R);        // element forces
+    b = (b + 15) & ~size_t(15);
+    b += 2 * G::STAGES * sizeof(unsigned long long);      // full / empty barriers
+    return b;
+}
+
+// Issue the cp.async copies of tile `tile`'s node positions (and velocities).
+template <typename R, bool DAMP>
+__device__ __forceinline__ void prefetch_nodes(const TileArgs<R>& A, int tile, R* xs, R* ys, R* zs, double* vs) {
+    const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
+    for (int ln = threadIdx.x; ln < nl; ln += TILE_ELEMS) {
+        const int gid = A.ln_gid[lb + ln];
+        cp_async<sizeof(R)>(xs + ln, A.px + gid);
+        cp_async<sizeof(R)>(ys + ln, A.py + gid);
+        cp_async<sizeof(R)>(zs + ln, A.pz + gid);
+        if (DAMP) {
+            cp_async<8>(vs + 3 * ln + 0, A.v + 3 * gid + 0);
+            cp_async<8>(vs + 3 * ln + 1, A.v + 3 * gid + 1);
+            cp_async<8>(vs + 3 * ln + 2, A.v + 3 * gid + 2);
+        }
+    }
+}
+
+template <typename R, int NPE, int NQP, bool DAMP>
+__global__ void __launch_bounds__(PIPE_THREADS, 2) k_force_pipe(TileArgs<R> A, int n_tiles, int* err) {
+    using G = PipeGeom<R, NPE>;
+    constexpr int TE = TILE_ELEMS;
+    constexpr int S = G::STAGES;
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char* ring = smem;
+    R* pos = reinterpret_cast<R*>(smem + (size_t)S * G::STAGE_BYTES);
+    const int ML = A.max_local;
+    double* vel = reinterpret_cast<double*>(pos + 6 * ML);
+    R* fe = reinterpret_cast<R*>(DAMP ? reinterpret_cast<unsigned char*>(vel + 6 * ML)
+                                      : reinterpret_cast<unsigned char*>(vel));
+    size_t bar_off = (size_t)S * G::STAGE_BYTES + 2 * 3 * (size_t)ML * sizeof(R) +
+                     (DAMP ? 2 * 3 * (size_t)ML * sizeof(double) : 0) + (size_t)3 * NPE * TE * sizeof(R);
+    bar_off = (bar_off + 15) & ~size_t(15);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + bar_off);
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + S);
+
+    const int t = threadIdx.x;
+    if (t == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, TE);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (t >= TE) {
+        // ------------------------------------------------------------ producer
+        if (t == TE) {
+            int it = 0;
+            for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+                for (int q = 0; q < NQP; ++q) {
+                    for (int p = 0; p < G::PARTS; ++p, ++it) {
+                        const int s = it % S;
+                        const uint32_t full = full0 + 8 * s, empty = empty0 + 8 * s;
+                        if (it >= S && !mbar_wait(empty, ((it / S) & 1) ^ 1)) atomicExch(err, 1);
+                        const bool last = (p == G::PARTS - 1), first = (q == 0 && p == 0);
+                        const uint32_t bytes = G::GRAD_BYTES + (last ? G::DV_BYTES : 0) + (first ? G::LCONN_BYTES : 0);
+                        mbar_expect_tx(full, bytes);
+                        const uint32_t dst = smem_u32(ring + (size_t)s * G::STAGE_BYTES);
+                        bulk_g2s(dst,
+                                 A.grad + (((size_t)tile * NQP + q) * (NPE * 3) + (size_t)p * G::PART_NODES * 3) * TE,
+                                 G::GRAD_BYTES, full);
+                        if (last)
+                            bulk_g2s(dst + G::GRAD_BYTES, A.dv + ((size_t)tile * NQP + q) * TE, G::DV_BYTES, full);
+                        if (first)
+                            bulk_g2s(dst + G::GRAD_BYTES + G::DV_BYTES, A.lconn + (size_t)tile * NPE * TE,
+                                     G::LCONN_BYTES, full);
+                    }
+                }
+            }
+        }
+        return;
+    }
+
+    // ---------------------------------------------------------------- consumers
+    int it = 0, buf = 0;
+    if (blockIdx.x < n_tiles) prefetch_nodes<R, DAMP>(A, blockIdx.x, pos, pos + ML, pos + 2 * ML, vel);
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, buf ^= 1) {
+        cp_async_wait_all();
+        consumer_sync();  // positions of this tile visible; previous tile's reduction done
+        const int next = tile + gridDim.x;
+        if (next < n_tiles) {
+            R* nx = pos + (buf ^ 1) * 3 * ML;
+            prefetch_nodes<R, DAMP>(A, next, nx, nx + ML, nx + 2 * ML, vel + (DAMP ? (buf ^ 1) * 3 * ML : 0));
+        }
+        const R* xs = pos + buf * 3 * ML;
+        const R* ys = xs + ML;
+        const R* zs = ys + ML;
+        const double* vs = vel + (DAMP ? buf * 3 * ML : 0);
+
+        int lc[NPE];
+        R f[NPE][3];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
+#pragma unroll 1
+        for (int q = 0; q < NQP; ++q) {
+            R g[NPE][3];
+            R dv = R(0);
+#pragma unroll
+            for (int p = 0; p < G::PARTS; ++p, ++it) {
+                const int s = it % S;
+                if (!mbar_wait(full0 + 8 * s, (it / S) & 1)) atomicExch(err, 2);
+                const unsigned char* st = ring + (size_t)s * G::STAGE_BYTES;
+                const R* gs = reinterpret_cast<const R*>(st);
+                if (q == 0 && p == 0) {
+                    const uint16_t* lcs = reinterpret_cast<const uint16_t*>(st + G::GRAD_BYTES + G::DV_BYTES);
+#pragma unroll
+                    for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
+                }
+#pragma unroll
+                for (int a = 0; a < G::PART_NODES; ++a)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) g[p * G::PART_NODES + a][j] = gs[(a * 3 + j) * TE + t];
+                if (p == G::PARTS - 1) dv = reinterpret_cast<const R*>(st + G::GRAD_BYTES)[t];
+                // The producer refills this stage with a bulk copy (async proxy) once
+                // every consumer has arrived; order this thread's generic-proxy
+                // reads of the stage before that write (without the fence the refill
+                // was observed to overtake the reads).
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive(empty0 + 8 * s);  // slice data is in registers now
+            }
+
+            R P[3][3];
+            if constexpr (sizeof(R) == 8) {
+                double F[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) F[i][j] = 0.0;
+#pragma unroll
+                for (int a = 0; a < NPE; ++a) {
+                    const double xa[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) F[i][j] += xa[i] * g[a][j];
+                }
+                svk_p_reference(F, A.lambda, A.mu, P);
+                if (DAMP) {
+                    double Fd[3][3], Pv[3][3];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) Fd[i][j] = 0.0;
+#pragma unroll
+                    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc[a] + i] * g[a][j];
+                    kelvin_voigt<double>(F, Fd, A.eta, A.lamd, Pv);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
+                }
+            } else {
+                R H[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) H[i][j] = R(0);
+#pragma unroll
+                for (int a = 0; a < NPE; ++a) {
+                    const R ua[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) H[i][j] += ua[i] * g[a][j];
+                }
+                R Em[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        R sm = H[i][j] + H[j][i];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) sm += H[k][i] * H[k][j];
+                        Em[i][j] = R(0.5) * sm;
+                    }
+                const R trE = Em[0][0] + Em[1][1] + Em[2][2];
+                R Sm[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) Sm[i][j] = R(2) * A.mu * Em[i][j] + (i == j ? A.lambda * trE : R(0));
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        R sm = Sm[i][j];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) sm += H[i][k] * Sm[k][j];
+                        P[i][j] = sm;
+                    }
+                if (DAMP) {
+                    R F[3][3], Fd[3][3], Pv[3][3];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) {
+                            F[i][j] = H[i][j] + (i == j ? R(1) : R(0));
+                            Fd[i][j] = R(0);
+                        }
+#pragma unroll
+                    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int j = 0; j < 3; ++j) Fd[i][j] += R(vs[3 * lc[a] + i]) * g[a][j];
+                    kelvin_voigt<R>(F, Fd, A.eta, A.lamd, Pv);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
+                }
+            }
+            // f_a += (P grad_a) dV   (FEAT10DataFunc.cuh:417-449)
+#pragma unroll
+            for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    R fc = R(0);
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) fc += P[i][j] * g[a][j];
+                    f[a][i] += fc * dv;
+                }
+        }
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
+        consumer_sync();
+
+        const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
+        const uint16_t* inc = A.inc + (size_t)tile * TE * NPE;
+        for (int ln = t; ln < nl; ln += TE) {
+            const int beg = ln ? A.ln_inc_end[lb + ln - 1] : 0;
+            const int end = A.ln_inc_end[lb + ln];
+            R s0 = R(0), s1 = R(0), s2 = R(0);
+            for (int k = beg; k < end; ++k) {
+                const int ent = inc[k];
+                const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
+                s0 += fe[base];
+                s1 += fe[base + TE];
+                s2 += fe[base + 2 * TE];
+            }
+            const int ps = A.ln_pslot[lb + ln];
+            if (ps < 0) {
+                const int gid = A.ln_gid[lb + ln];
+                A.f_out[3 * gid + 0] = s0;
+                A.f_out[3 * gid + 1] = s1;
+                A.f_out[3 * gid + 2] = s2;
+            } else {
+                A.partial[3 * ps + 0] = s0;
+                A.partial[3 * ps + 1] = s1;
+                A.partial[3 * ps + 2] = s2;
+            }
+        }
+    }
+    cp_async_wait_all();
+}
+
+}  // namespace tlfea
