@@ -169,6 +169,25 @@ int tlfea_element_set_force_precision(tlfea_element h, int precision);
  * grid_limit caps the pipeline's persistent grid (0 = all resident blocks). */
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit);
 
+/* Allocation-free internal force.  No counterpart in the reference.
+ *
+ * For callers that may not allocate device memory once they are running:
+ * hosts whose GPU memory comes from their own pool and forbid cudaMalloc /
+ * cudaFree after start-up, or time-critical loops where an allocation's
+ * implicit device-wide synchronisation would stall their other streams.
+ *
+ * d_f_out (3N doubles, interleaved, caller-allocated) = the FP64 internal force
+ * at the current positions; d_v as in tlfea_element_compute_internal_force.
+ * The same kernels as that entry point, but their scratch (partial sums of
+ * nodes shared between element tiles) lives in one static device array of
+ * 2^20 doubles (8 MiB) that every GPU loading the library holds until exit.
+ * Meshes needing more (3 per shared-node slot, about 7.3 per TET10 element:
+ * roughly above 140k TET10 elements) are rejected with TLFEA_SIZE_MISMATCH.  Nothing is allocated: no
+ * cudaMalloc, cudaFree or allocating library call.  The first call on a
+ * device looks up the array's device address; make that call before any
+ * stream capture.  All calls share the array and it keeps the last call's
+ * contents; calls that overlap on the GPU race. */
+int tlfea_element_compute_internal_force_noalloc(tlfea_element h, const double* d_v, double* d_f_out);
 
 /* Retrieve*ToCPU (FEAT10Data.cu:564-649, 753-757).  Sizes are in elements of
  * the output array and must match exactly. */

@@ -104,6 +104,7 @@ _SIGS = {
     "tlfea_element_compute_internal_force": [_P, _P],
     "tlfea_element_set_force_precision": [_P, C.c_int],
     "tlfea_element_set_launch_config": [_P, C.c_int, C.c_int],
+    "tlfea_element_compute_internal_force_noalloc": [_P, _P, _P],
     "tlfea_element_get_mass_nnz": [_P, C.POINTER(_LL)],
     "tlfea_element_retrieve_mass_csr": [_P, _I, _I, _D],
     "tlfea_element_retrieve_internal_force": [_P, _D, C.c_int],

@@ -666,6 +666,42 @@ static int sync_f_int64(tlfea_element_s* h) {
     return TLFEA_OK;
 }
 
+// ------------------------------------------- scratch of the allocation-free entry
+//
+// The force kernel needs scratch for the per-tile partial sums of nodes shared
+// between tiles (3 values per shared-node slot).  The regular entry point keeps
+// that buffer in the element; the allocation-free entry point uses this array
+// instead.  It is a file-scope device array, so every GPU that loads the
+// library holds these 8 MiB until the process exits.
+constexpr size_t NOALLOC_SCRATCH_DOUBLES = size_t(1) << 20;  // 8 MiB
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+static std::mutex g_noalloc_mutex;
+
+// Device address of the scratch array on `device` (which must be current).  In
+// host code the array's name is a host-side stand-in, not a device address, so
+// the address is looked up once per device with cudaGetSymbolAddress.
+static int noalloc_scratch(int device, double** out) {
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) {
+        set_error("device index out of range for the static scratch table");
+        return TLFEA_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        double* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error(std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+            return TLFEA_CUDA_ERROR;
+        }
+        g_noalloc_ptr[device] = p;
+    }
+    *out = g_noalloc_ptr[device];
+    return TLFEA_OK;
+}
+
 // A kernel's bounded wait ran out: report it once and clear the word.
 static int check_device_error(tlfea_element_s* h) {
     int e = 0;
@@ -1195,6 +1231,51 @@ int tlfea_element_set_force_precision(tlfea_element h, int precision) {
     CHECK_HANDLE(h);
     if (precision != TLFEA_PRECISION_FP64 && precision != TLFEA_PRECISION_FP32) return TLFEA_INVALID_ARG;
     h->precision = precision;
+    return TLFEA_OK;
+}
+
+// Allocation-free variant of tlfea_element_compute_internal_force (FP64): the
+// same tile and combine kernels, with the shared-node partials in the static
+// scratch array and the result in the caller's buffer.  Calls no cudaMalloc,
+// cudaFree or allocating library routine.  The first call on a device looks
+// up the scratch address (cudaGetSymbolAddress); make that first call before
+// any stream capture.  Every call shares the one array per device and it keeps
+// the last call's contents; each call writes every slot it reads before
+// reading it, so nothing has to start at zero.  Calls that overlap on the GPU
+// (other streams, other elements, other threads) race on the array.
+int tlfea_element_compute_internal_force_noalloc(tlfea_element h, const double* d_v, double* d_f_out) {
+    CHECK_HANDLE(h);
+    REQUIRE_SETUP(h);
+    if (!d_f_out) {
+        set_error("output pointer is null");
+        return TLFEA_INVALID_ARG;
+    }
+    if (h->material != TLFEA_MATERIAL_SVK) {
+        set_error("Mooney-Rivlin is not supported by the fused element kernel");
+        return TLFEA_UNSUPPORTED;
+    }
+    const size_t need = 3 * (size_t)h->tl.n_pslots;
+    if (need > NOALLOC_SCRATCH_DOUBLES) {
+        set_error("mesh needs " + std::to_string(need) + " doubles of shared-node scratch; the static scratch holds " +
+                  std::to_string(NOALLOC_SCRATCH_DOUBLES) + " (use tlfea_element_compute_internal_force)");
+        return TLFEA_SIZE_MISMATCH;
+    }
+    double* scratch = nullptr;
+    int st = noalloc_scratch(h->device, &scratch);
+    if (st) return st;
+    TileArgs<double> A = make_args<double>(h, false);
+    A.v = d_v;
+    A.f_out = d_f_out;
+    A.partial = scratch;
+    const bool damp = d_v && (h->eta_d != 0.0 || h->lambda_d != 0.0);
+    if (h->tl.n_orphans) TLFEA_CUDA(cudaMemsetAsync(d_f_out, 0, sizeof(double) * 3 * (size_t)h->N, h->stream));
+    if (h->npe == 10)
+        st = damp ? launch_tiles<double, 10, 5, TILE_FORCE, true>(h, A) : launch_tiles<double, 10, 5, TILE_FORCE, false>(h, A);
+    else
+        st = damp ? launch_tiles<double, 4, 1, TILE_FORCE, true>(h, A) : launch_tiles<double, 4, 1, TILE_FORCE, false>(h, A);
+    if (st) return st;
+    if ((st = launch_combine<double, false>(h, A.partial, A.f_out))) return st;
+    SYNC_COMPUTE(h);
     return TLFEA_OK;
 }
 
