@@ -123,8 +123,15 @@ def elem_force_bytes(E, N, npe, nqp, s):
 
 
 def spmv_bytes(N, nnzb):
-    # 3x3 blocks: 72 B values + 4 B column per block, row offsets, p read, q write
+    """Bytes one block SpMV must move: every 3x3 node block (72 B values +
+    4 B column), the row offsets, p read and q written once."""
     return nnzb * (9 * 8 + 4) + (N + 1) * 4 + 3 * N * 8 * 2
+
+
+def spmv_bytes_full_csr(N, nnzb):
+    """The same product on the reference's full 3N x 3N FP64 CSR (8 B value +
+    4 B column per entry, 3N+1 offsets, p and q)."""
+    return 9 * nnzb * 12 + (3 * N + 1) * 4 + 3 * N * 8 * 2
 
 
 def time_stream(torch, stream_ptr, fn, reps):
@@ -329,7 +336,8 @@ def main():
     ach = b_spmv / (ms_spmv / 1e3) / 1e9
     roofline = {"kernel": "k_cg_spmv_dot", "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": int(b_spmv),
-                "ms": round(ms_spmv, 4), "traffic": None}
+                "format": "row-planar 3x3 node blocks", "ms": round(ms_spmv, 4), "traffic": None,
+                "full_csr_equivalent_gbs": round(spmv_bytes_full_csr(N, nnzb) / (ms_spmv / 1e3) / 1e9, 1)}
     # fused element force, FP32 and FP64
     ef = {}
     for prec, s in (("fp32", 4), ("fp64", 8)):

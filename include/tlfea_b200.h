@@ -165,8 +165,10 @@ int tlfea_element_compute_internal_force(tlfea_element h, const double* d_v);
 /* Force precision for tlfea_element_compute_internal_force and the solvers. */
 int tlfea_element_set_force_precision(tlfea_element h, int precision);
 /* Launch configuration of the fused force kernel (new; the autotuner's knob):
- * force_kernel 0 = persistent TMA pipeline (default), 1 = one tile per block;
- * grid_limit caps the pipeline's persistent grid (0 = all resident blocks). */
+ * force_kernel 0 = one tile per block with bulk-copy double-buffered QP
+ * slices (default), 1 = one tile per block with direct loads, 2 = persistent
+ * producer/consumer pipeline; grid_limit caps the persistent grid (0 = all
+ * resident blocks). */
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit);
 
 /* Allocation-free internal force.  No counterpart in the reference.

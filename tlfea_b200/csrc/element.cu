@@ -151,7 +151,7 @@ __global__ void k_dndu_pre(int n_slots, int E, const int* __restrict__ tile_elem
 
 template <typename R, int NPE, int NQP, int MODE, bool DAMP>
 __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force(TileArgs<R> A) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     process_tile<R, NPE, NQP, MODE, DAMP>(A, blockIdx.x, smem);
 }
 
@@ -594,6 +594,21 @@ static int launch_combine(tlfea_element_s* h, const R* partial, R* f_out) {
     return TLFEA_OK;
 }
 
+// One tile per block, QP slices double-buffered by bulk copies.
+template <typename R, int NPE, int NQP, bool DAMP>
+static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
+    auto kern = k_tile_force_tma<R, NPE, NQP, DAMP>;
+    const size_t smem = tile_tma_smem_bytes<R, NPE>(h->tl.max_local, DAMP);
+    if (smem > 227 * 1024) {
+        set_error("force kernel shared memory exceeds 227 KB (tile touches too many nodes)");
+        return TLFEA_UNSUPPORTED;
+    }
+    if (smem > 48 * 1024) TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<h->tl.n_tiles, TILE_ELEMS, smem, h->stream>>>(A, h->d_err);
+    TLFEA_CHECK_LAUNCH();
+    return TLFEA_OK;
+}
+
 // Persistent TMA-fed force kernel: grid = resident CTAs (occupancy) capped by the tile count.
 template <typename R, int NPE, int NQP, bool DAMP>
 static int launch_pipe(tlfea_element_s* h, const TileArgs<R>& A) {
@@ -631,8 +646,10 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
     int st;
     if (h->force_kernel == 1)
         st = damp ? launch_tiles<R, NPE, NQP, TILE_FORCE, true>(h, A) : launch_tiles<R, NPE, NQP, TILE_FORCE, false>(h, A);
-    else
+    else if (h->force_kernel == 2)
         st = damp ? launch_pipe<R, NPE, NQP, true>(h, A) : launch_pipe<R, NPE, NQP, false>(h, A);
+    else
+        st = damp ? launch_tile_tma<R, NPE, NQP, true>(h, A) : launch_tile_tma<R, NPE, NQP, false>(h, A);
     if (st) return st;
     return launch_combine<R, false>(h, A.partial, A.f_out);
 }
@@ -1220,7 +1237,7 @@ int tlfea_element_compute_internal_force(tlfea_element h, const double* d_v) {
 
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit) {
     CHECK_HANDLE(h);
-    if (force_kernel < 0 || force_kernel > 1 || grid_limit < 0) return TLFEA_INVALID_ARG;
+    if (force_kernel < 0 || force_kernel > 2 || grid_limit < 0) return TLFEA_INVALID_ARG;
     h->force_kernel = force_kernel;
     h->pipe_grid_limit = grid_limit;
     for (int& g : h->pipe_grid) g = 0;

@@ -363,4 +363,251 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2) k_force_pipe(TileArgs<R> A, i
     cp_async_wait_all();
 }
 
+// ---------------------------------------------------------------------------
+// One tile per CTA (4 CTAs/SM in FP32), with the tile's QP slices double-
+// buffered in shared memory by 1-D bulk copies issued from thread 0: QP q+2 is
+// requested as soon as every thread has read QP q into registers, so a slice is
+// always in flight while the CTA computes.  The node positions are gathered by
+// the threads while the first two slices land.
+
+template <typename R, int NPE>
+struct TileTmaGeom {
+    static constexpr uint32_t GRAD_BYTES = NPE * 3 * TILE_ELEMS * sizeof(R);
+    static constexpr uint32_t DV_BYTES = TILE_ELEMS * sizeof(R);
+    static constexpr uint32_t STAGE_BYTES = GRAD_BYTES + DV_BYTES;
+    static constexpr uint32_t LCONN_BYTES = NPE * TILE_ELEMS * sizeof(uint16_t);
+};
+
+// Byte offsets of the regions of k_tile_force_tma's shared memory, each
+// 16-byte aligned: [stage 0][stage 1][lconn][x y z][velocities][forces][2 mbarriers].
+template <typename R, int NPE>
+struct TileTmaLayout {
+    size_t pos, vel, fe, bar, total;
+    __host__ __device__ TileTmaLayout(int max_local, bool damp) {
+        using G = TileTmaGeom<R, NPE>;
+        auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+        pos = 2 * (size_t)G::STAGE_BYTES + G::LCONN_BYTES;
+        vel = al(pos + 3 * (size_t)max_local * sizeof(R));
+        fe = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
+        bar = al(fe + (size_t)3 * NPE * TILE_ELEMS * sizeof(R));
+        total = bar + 2 * sizeof(unsigned long long);
+    }
+};
+
+template <typename R, int NPE>
+inline size_t tile_tma_smem_bytes(int max_local, bool damp) {
+    return TileTmaLayout<R, NPE>(max_local, damp).total;
+}
+
+template <typename R, int NPE, int NQP, bool DAMP>
+__global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, int* err) {
+    using G = TileTmaGeom<R, NPE>;
+    constexpr int TE = TILE_ELEMS;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int tile = blockIdx.x, t = threadIdx.x;
+    const int ML = A.max_local;
+    const TileTmaLayout<R, NPE> L(ML, DAMP);
+    unsigned char* stage0 = smem;
+    const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + 2 * G::STAGE_BYTES);
+    R* xs = reinterpret_cast<R*>(smem + L.pos);
+    R* ys = xs + ML;
+    R* zs = ys + ML;
+    double* vs = reinterpret_cast<double*>(smem + L.vel);
+    R* fe = reinterpret_cast<R*>(smem + L.fe);
+    const uint32_t bar0 = smem_u32(smem + L.bar);
+
+    auto issue = [&](int q) {  // thread 0 only
+        const uint32_t bar = bar0 + 8 * (q & 1);
+        const uint32_t dst = smem_u32(stage0 + (size_t)(q & 1) * G::STAGE_BYTES);
+        const uint32_t extra = (q == 0) ? G::LCONN_BYTES : 0;
+        mbar_expect_tx(bar, G::STAGE_BYTES + extra);
+        bulk_g2s(dst, A.grad + ((size_t)tile * NQP + q) * (NPE * 3) * TE, G::GRAD_BYTES, bar);
+        bulk_g2s(dst + G::GRAD_BYTES, A.dv + ((size_t)tile * NQP + q) * TE, G::DV_BYTES, bar);
+        if (q == 0) bulk_g2s(smem_u32(lcs), A.lconn + (size_t)tile * NPE * TE, G::LCONN_BYTES, bar);
+    };
+    if (t == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(0);
+        if (NQP > 1) issue(1);
+    }
+    const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
+    for (int ln = t; ln < nl; ln += TE) {
+        const int gid = A.ln_gid[lb + ln];
+        xs[ln] = A.px[gid];
+        ys[ln] = A.py[gid];
+        zs[ln] = A.pz[gid];
+        if (DAMP) {
+            vs[3 * ln + 0] = A.v[3 * gid + 0];
+            vs[3 * ln + 1] = A.v[3 * gid + 1];
+            vs[3 * ln + 2] = A.v[3 * gid + 2];
+        }
+    }
+    __syncthreads();  // positions staged; barriers initialised
+
+    int lc[NPE];
+    R f[NPE][3];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
+#pragma unroll 1
+    for (int q = 0; q < NQP; ++q) {
+        if (!mbar_wait(bar0 + 8 * (q & 1), (q >> 1) & 1)) atomicExch(err, 3);
+        const unsigned char* st = stage0 + (size_t)(q & 1) * G::STAGE_BYTES;
+        const R* gs = reinterpret_cast<const R*>(st);
+        if (q == 0) {
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
+        }
+        R g[NPE][3];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) g[a][j] = gs[(a * 3 + j) * TE + t];
+        const R dv = reinterpret_cast<const R*>(st + G::GRAD_BYTES)[t];
+        if (q + 2 < NQP) {
+            // every thread's generic reads of this stage precede the bulk refill
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (t == 0) issue(q + 2);
+        }
+        R P[3][3];
+        if constexpr (sizeof(R) == 8) {
+            double F[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) F[i][j] = 0.0;
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) {
+                const double xa[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) F[i][j] += xa[i] * g[a][j];
+            }
+            svk_p_reference(F, A.lambda, A.mu, P);
+            if (DAMP) {
+                double Fd[3][3], Pv[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) Fd[i][j] = 0.0;
+#pragma unroll
+                for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc[a] + i] * g[a][j];
+                kelvin_voigt<double>(F, Fd, A.eta, A.lamd, Pv);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
+            }
+        } else {
+            R H[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) H[i][j] = R(0);
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) {
+                const R ua[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) H[i][j] += ua[i] * g[a][j];
+            }
+            R Em[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    R sm = H[i][j] + H[j][i];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) sm += H[k][i] * H[k][j];
+                    Em[i][j] = R(0.5) * sm;
+                }
+            const R trE = Em[0][0] + Em[1][1] + Em[2][2];
+            R Sm[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) Sm[i][j] = R(2) * A.mu * Em[i][j] + (i == j ? A.lambda * trE : R(0));
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    R sm = Sm[i][j];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) sm += H[i][k] * Sm[k][j];
+                    P[i][j] = sm;
+                }
+            if (DAMP) {
+                R F[3][3], Fd[3][3], Pv[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        F[i][j] = H[i][j] + (i == j ? R(1) : R(0));
+                        Fd[i][j] = R(0);
+                    }
+#pragma unroll
+                for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) Fd[i][j] += R(vs[3 * lc[a] + i]) * g[a][j];
+                kelvin_voigt<R>(F, Fd, A.eta, A.lamd, Pv);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
+            }
+        }
+        // f_a += (P grad_a) dV   (FEAT10DataFunc.cuh:417-449)
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                R fc = R(0);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) fc += P[i][j] * g[a][j];
+                f[a][i] += fc * dv;
+            }
+    }
+#pragma unroll
+    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
+    __syncthreads();
+
+    const uint16_t* inc = A.inc + (size_t)tile * TE * NPE;
+    for (int ln = t; ln < nl; ln += TE) {
+        const int beg = ln ? A.ln_inc_end[lb + ln - 1] : 0;
+        const int end = A.ln_inc_end[lb + ln];
+        R s0 = R(0), s1 = R(0), s2 = R(0);
+        for (int k = beg; k < end; ++k) {
+            const int ent = inc[k];
+            const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
+            s0 += fe[base];
+            s1 += fe[base + TE];
+            s2 += fe[base + 2 * TE];
+        }
+        const int ps = A.ln_pslot[lb + ln];
+        if (ps < 0) {
+            const int gid = A.ln_gid[lb + ln];
+            A.f_out[3 * gid + 0] = s0;
+            A.f_out[3 * gid + 1] = s1;
+            A.f_out[3 * gid + 2] = s2;
+        } else {
+            A.partial[3 * ps + 0] = s0;
+            A.partial[3 * ps + 1] = s1;
+            A.partial[3 * ps + 2] = s2;
+        }
+    }
+}
+
 }  // namespace tlfea

@@ -17,7 +17,8 @@ namespace tlfea {
 // compute_hessian_assemble_csr (FEAT10DataFunc.cuh:512-684; SVK.cuh:41-67) at
 // the current positions, scaled by h, plus the Kelvin-Voigt block C_ab
 // (:686-768) when damping is set.  Block (a,b) is added to row i's block for
-// node conn(e,b).  No atomics: each row is owned by one thread.
+// node conn(e,b).  No atomics: each row is owned by one thread.  K is
+// row-planar: component c of row i's k-th block is K[9*off[i] + c*nb + k].
 template <int NPE, int NQP>
 __global__ void __launch_bounds__(128) k_stiffness_rows(int N, int E, const int* __restrict__ conn,
                                                         const double* __restrict__ x, const double* __restrict__ y,
@@ -31,8 +32,9 @@ __global__ void __launch_bounds__(128) k_stiffness_rows(int N, int E, const int*
     constexpr int TE = TILE_ELEMS;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    const int rb = off[i], re = off[i + 1];
-    for (long long k = 9LL * rb; k < 9LL * re; ++k) K[k] = 0.0;
+    const int rb = off[i], re = off[i + 1], nbr = re - rb;
+    double* Kr = K + 9LL * rb;
+    for (long long k = 0; k < 9LL * nbr; ++k) Kr[k] = 0.0;
     const bool visc = (eta_d != 0.0 || lambda_d != 0.0);
     for (int k = inc_off[i]; k < inc_off[i + 1]; ++k) {
         const int e = inc_e[k], a = inc_a[k];
@@ -58,7 +60,7 @@ __global__ void __launch_bounds__(128) k_stiffness_rows(int N, int E, const int*
                 else
                     hi = mid - 1;
             }
-            bpos[b] = pos;
+            bpos[b] = pos - rb;  // block index within the row (pattern holds every pair)
         }
         for (int q = 0; q < NQP; ++q) {
             const double* gp = grad64 + ((size_t)tile * NQP + q) * (NPE * 3) * TE + t;
@@ -98,20 +100,20 @@ __global__ void __launch_bounds__(128) k_stiffness_rows(int N, int E, const int*
                 }
                 const double hij = g[b][0] * g[a][0] + g[b][1] * g[a][1] + g[b][2] * g[a][2];
                 const double fdf = Fhb[0] * Fha[0] + Fhb[1] * Fha[1] + Fhb[2] * Fha[2];
-                double* Kb = K + 9LL * bpos[b];
+                double* Kb = Kr + bpos[b];
                 for (int d = 0; d < 3; ++d)
                     for (int ee = 0; ee < 3; ++ee) {
                         const double delta = (d == ee) ? 1.0 : 0.0;
                         const double kv = (lambda * Fha[d] * Fhb[ee] + lambda * trE * hij * delta + mu * fdf * delta +
                                            mu * Fhb[d] * Fha[ee] + mu * hij * FFT[d][ee] + (-mu * hij * delta)) *
                                           dV;
-                        Kb[3 * d + ee] += h * kv;
+                        Kb[(size_t)(3 * d + ee) * nbr] += h * kv;
                     }
                 if (visc) {
                     const double hd = g[a][0] * g[b][0] + g[a][1] * g[b][1] + g[a][2] * g[b][2];
                     for (int d = 0; d < 3; ++d)
                         for (int ee = 0; ee < 3; ++ee)
-                            Kb[3 * d + ee] += (eta_d * (Fhb[d] * Fha[ee]) + eta_d * FFT[d][ee] * hd +
+                            Kb[(size_t)(3 * d + ee) * nbr] += (eta_d * (Fhb[d] * Fha[ee]) + eta_d * FFT[d][ee] * hd +
                                                lambda_d * (Fha[d] * Fhb[ee])) *
                                               dV;
                 }
@@ -126,16 +128,18 @@ __global__ void k_apply_bcs(int N, const int* __restrict__ off, const int* __res
                             const unsigned char* __restrict__ fixed, double* K, double* f) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    for (int k = off[i]; k < off[i + 1]; ++k) {
-        const int cn = col[k];
+    const int rb = off[i], nbr = off[i + 1] - rb;
+    double* Kr = K + 9LL * rb;
+    for (int k = 0; k < nbr; ++k) {
+        const int cn = col[rb + k];
         for (int d = 0; d < 3; ++d) {
             const int row = 3 * i + d;
             for (int e = 0; e < 3; ++e) {
                 const int c = 3 * cn + e;
                 if (fixed[row])
-                    K[9LL * k + 3 * d + e] = (c == row) ? 1.0 : 0.0;
+                    Kr[(size_t)(3 * d + e) * nbr + k] = (c == row) ? 1.0 : 0.0;
                 else if (fixed[c])
-                    K[9LL * k + 3 * d + e] = 0.0;
+                    Kr[(size_t)(3 * d + e) * nbr + k] = 0.0;
             }
         }
     }
@@ -213,9 +217,13 @@ __global__ void k_cg_init(int n, const double* __restrict__ f, double* u, double
     }
 }
 
-// q = K p on 3x3 node blocks (one warp per node row, lanes stride over the
-// row's 9*nb contiguous values) fused with the p.q reduction; the last block
-// sets alpha = rr / p.q (LinearStaticSolver.cu:519-533).
+// q = K p on 3x3 node blocks fused with the p.q reduction; the last block sets
+// alpha = rr / p.q (LinearStaticSolver.cu:519-533).  K is stored row-planar:
+// node row i owns K[9*rb, 9*(rb+nb)) and component c = 3d+e of its k-th block
+// sits at K[9*rb + c*nb + k].  One warp per node row, one lane per block: the
+// nine component loads of a lane are coalesced across the warp, independent
+// of each other and of the column-index load, and the component index is a
+// compile-time constant.
 __global__ void __launch_bounds__(256) k_cg_spmv_dot(int N, const int* __restrict__ off, const int* __restrict__ col,
                                                      const double* __restrict__ K, const double* __restrict__ p,
                                                      double* q, double* partials, CgCtl* ctl) {
@@ -227,20 +235,17 @@ __global__ void __launch_bounds__(256) k_cg_spmv_dot(int N, const int* __restric
     for (int i = warp; i < N; i += nwarps) {
         const int rb = off[i], nb = off[i + 1] - rb;
         const double* Kr = K + 9LL * rb;
-        const int* cr = col + rb;
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        for (int v = lane; v < 9 * nb; v += 32) {
-            const int kb = v / 9;
-            const int r9 = v - 9 * kb;
-            const int d = r9 / 3;
-            const int e = r9 - 3 * d;
-            const double prod = __ldcs(Kr + v) * p[3 * cr[kb] + e];
-            if (d == 0)
-                a0 += prod;
-            else if (d == 1)
-                a1 += prod;
-            else
-                a2 += prod;
+        for (int k = lane; k < nb; k += 32) {
+            const double* kv = Kr + k;
+            double v[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) v[c] = __ldcs(kv + (size_t)c * nb);
+            const int cj = col[rb + k];
+            const double p0 = p[3 * cj + 0], p1 = p[3 * cj + 1], p2 = p[3 * cj + 2];
+            a0 += v[0] * p0 + v[1] * p1 + v[2] * p2;
+            a1 += v[3] * p0 + v[4] * p1 + v[5] * p2;
+            a2 += v[6] * p0 + v[7] * p1 + v[8] * p2;
         }
         a0 = warp_sum(a0);
         a1 = warp_sum(a1);
@@ -362,8 +367,11 @@ int linear_static_prepare(tlfea_solver_s* s) {
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        // persistent grid: every CG kernel strides over rows/DOFs with all resident blocks
+        int per_sm = 0;
+        TLFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_spmv_dot, 256, 0));
         const int rows_warps = (el->N + 7) / 8;
-        s->cg_blocks = std::max(1, std::min(rows_warps, sms * 8));
+        s->cg_blocks = std::max(1, std::min(rows_warps, std::max(per_sm, 1) * sms));
         if ((st = dalloc(&s->cg_part, (size_t)s->cg_blocks))) return st;
     }
     return TLFEA_OK;
@@ -473,17 +481,20 @@ int linear_static_retrieve_k(tlfea_solver_s* s, long long* nnz, int* offsets, in
     TLFEA_CUDA(cudaMemcpy(Kh.data(), s->K, sizeof(double) * Kh.size(), cudaMemcpyDeviceToHost));
     const std::vector<int>& off = el->h_pat_off;
     const std::vector<int>& col = el->h_pat_col;
+    // Full 3N x 3N CSR: entry (3i+d, 3j+e) is component 3d+e of row i's block for j.
     long long o = 0;
-    for (int i = 0; i < N; ++i)
+    for (int i = 0; i < N; ++i) {
+        const int rb = off[i], nbr = off[i + 1] - rb;
         for (int d = 0; d < 3; ++d) {
             if (offsets) offsets[3 * i + d] = (int)o;
-            for (int k = off[i]; k < off[i + 1]; ++k)
+            for (int k = 0; k < nbr; ++k)
                 for (int e = 0; e < 3; ++e) {
-                    if (columns) columns[o] = 3 * col[k] + e;
-                    if (values) values[o] = Kh[9 * (size_t)k + 3 * d + e];
+                    if (columns) columns[o] = 3 * col[rb + k] + e;
+                    if (values) values[o] = Kh[9 * (size_t)rb + (size_t)(3 * d + e) * nbr + k];
                     ++o;
                 }
         }
+    }
     if (offsets) offsets[3 * N] = (int)o;
     return TLFEA_OK;
 }
