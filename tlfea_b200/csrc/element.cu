@@ -6,6 +6,7 @@
 #include <fstream>
 #include <mutex>
 #include <numeric>
+#include <tuple>
 #include <vector>
 
 #include "element.cuh"
@@ -313,7 +314,9 @@ static int build_tiling(tlfea_element_s* h, const double* x, const double* y, co
     }
     double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
     if (!(ext > 0.0)) ext = 1.0;
-    std::vector<std::pair<unsigned long long, int>> key((size_t)E);
+    // (group, Morton code, element): a batch of meshes sorts instance by instance
+    std::vector<std::tuple<int, unsigned long long, int>> key((size_t)E);
+    const bool grouped = h->elem_group.size() == (size_t)E;
     for (int e = 0; e < E; ++e) {
         double c[3] = {0, 0, 0};
         for (int a = 0; a < 4; ++a) {
@@ -329,7 +332,7 @@ static int build_tiling(tlfea_element_s* h, const double* x, const double* y, co
             const unsigned long long qd = (unsigned long long)(u * 2097151.0);
             m |= spread3(qd) << d;
         }
-        key[e] = {m, e};
+        key[e] = {grouped ? h->elem_group[e] : 0, m, e};
     }
     std::sort(key.begin(), key.end());
 
@@ -337,7 +340,7 @@ static int build_tiling(tlfea_element_s* h, const double* x, const double* y, co
     const int n_tiles = (E + TE - 1) / TE;
     tl.n_tiles = n_tiles;
     std::vector<int> tile_elem((size_t)n_tiles * TE, -1);
-    for (int s = 0; s < E; ++s) tile_elem[s] = key[s].second;
+    for (int s = 0; s < E; ++s) tile_elem[s] = std::get<2>(key[s]);
 
     std::vector<int> total_inc((size_t)N, 0);
     for (size_t k = 0; k < conn.size(); ++k) total_inc[conn[k]]++;
@@ -444,7 +447,7 @@ static int build_tiling(tlfea_element_s* h, const double* x, const double* y, co
     if ((st = upload(&tl.lconn, lconn, h->stream))) return st;
     if ((st = upload(&tl.tile_elem, tile_elem, h->stream))) return st;
     std::vector<int> elem_slot((size_t)E);
-    for (int s = 0; s < E; ++s) elem_slot[key[s].second] = s;
+    for (int s = 0; s < E; ++s) elem_slot[std::get<2>(key[s])] = s;
     if ((st = upload(&tl.elem_slot, elem_slot, h->stream))) return st;
     if ((st = upload(&tl.bnode_gid, bgid, h->stream))) return st;
     if ((st = upload(&tl.bnode_off, boff, h->stream))) return st;
@@ -602,6 +605,12 @@ static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
     if (smem > 227 * 1024) {
         set_error("force kernel shared memory exceeds 227 KB (tile touches too many nodes)");
         return TLFEA_UNSUPPORTED;
+    }
+    static bool configured = false;  // one instantiation per template argument set
+    if (!configured) {
+        TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
+        configured = true;
     }
     if (smem > 48 * 1024) TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<h->tl.n_tiles, TILE_ELEMS, smem, h->stream>>>(A, h->d_err);

@@ -407,6 +407,7 @@ struct tlfea_element_s {
     bool j_setup = false;
 
     std::vector<int> conn;  // column-major, original element order
+    std::vector<int> elem_group;  // optional tiling group per element (batch instance), set before setup
     double qx[5] = {0}, qy[5] = {0}, qz[5] = {0}, qw[5] = {0};
 
     double rho = 0, E_mod = 0, nu = 0, mu = 0, lambda = 0, eta_d = 0, lambda_d = 0;

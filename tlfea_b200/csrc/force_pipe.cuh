@@ -376,20 +376,27 @@ struct TileTmaGeom {
     static constexpr uint32_t DV_BYTES = TILE_ELEMS * sizeof(R);
     static constexpr uint32_t STAGE_BYTES = GRAD_BYTES + DV_BYTES;
     static constexpr uint32_t LCONN_BYTES = NPE * TILE_ELEMS * sizeof(uint16_t);
+    static constexpr uint32_t INC_BYTES = NPE * TILE_ELEMS * sizeof(uint16_t);
+    // element forces of the scatter reuse the two stages once the QP loop is done
+    static_assert(3 * NPE * TILE_ELEMS * sizeof(R) <= 2 * STAGE_BYTES, "force table must fit in the stages");
+    static_assert(LCONN_BYTES % 16 == 0 && INC_BYTES % 16 == 0 && STAGE_BYTES % 16 == 0, "bulk sizes");
 };
 
 // Byte offsets of the regions of k_tile_force_tma's shared memory, each
-// 16-byte aligned: [stage 0][stage 1][lconn][x y z][velocities][forces][2 mbarriers].
+// 16-byte aligned: [stage 0 | stage 1, later the element forces][lconn][incidence]
+// [x y z][node destination][incidence end][velocities][2 mbarriers].
 template <typename R, int NPE>
 struct TileTmaLayout {
-    size_t pos, vel, fe, bar, total;
+    size_t inc, pos, dst, iend, vel, bar, total;
     __host__ __device__ TileTmaLayout(int max_local, bool damp) {
         using G = TileTmaGeom<R, NPE>;
         auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
-        pos = 2 * (size_t)G::STAGE_BYTES + G::LCONN_BYTES;
-        vel = al(pos + 3 * (size_t)max_local * sizeof(R));
-        fe = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
-        bar = al(fe + (size_t)3 * NPE * TILE_ELEMS * sizeof(R));
+        inc = 2 * (size_t)G::STAGE_BYTES + G::LCONN_BYTES;
+        pos = inc + G::INC_BYTES;
+        dst = al(pos + 3 * (size_t)max_local * sizeof(R));
+        iend = al(dst + (size_t)max_local * sizeof(int));
+        vel = al(iend + (size_t)max_local * sizeof(uint16_t));
+        bar = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
         total = bar + 2 * sizeof(unsigned long long);
     }
 };
@@ -409,21 +416,27 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
     const TileTmaLayout<R, NPE> L(ML, DAMP);
     unsigned char* stage0 = smem;
     const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + 2 * G::STAGE_BYTES);
+    const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
     R* xs = reinterpret_cast<R*>(smem + L.pos);
     R* ys = xs + ML;
     R* zs = ys + ML;
+    int* dsts = reinterpret_cast<int*>(smem + L.dst);  // global node id, or -(partial slot + 1)
+    uint16_t* iends = reinterpret_cast<uint16_t*>(smem + L.iend);
     double* vs = reinterpret_cast<double*>(smem + L.vel);
-    R* fe = reinterpret_cast<R*>(smem + L.fe);
+    R* fe = reinterpret_cast<R*>(smem);  // aliases the stages after the QP loop
     const uint32_t bar0 = smem_u32(smem + L.bar);
 
     auto issue = [&](int q) {  // thread 0 only
         const uint32_t bar = bar0 + 8 * (q & 1);
         const uint32_t dst = smem_u32(stage0 + (size_t)(q & 1) * G::STAGE_BYTES);
-        const uint32_t extra = (q == 0) ? G::LCONN_BYTES : 0;
+        const uint32_t extra = (q == 0) ? G::LCONN_BYTES + G::INC_BYTES : 0;
         mbar_expect_tx(bar, G::STAGE_BYTES + extra);
         bulk_g2s(dst, A.grad + ((size_t)tile * NQP + q) * (NPE * 3) * TE, G::GRAD_BYTES, bar);
         bulk_g2s(dst + G::GRAD_BYTES, A.dv + ((size_t)tile * NQP + q) * TE, G::DV_BYTES, bar);
-        if (q == 0) bulk_g2s(smem_u32(lcs), A.lconn + (size_t)tile * NPE * TE, G::LCONN_BYTES, bar);
+        if (q == 0) {
+            bulk_g2s(smem_u32(lcs), A.lconn + (size_t)tile * NPE * TE, G::LCONN_BYTES, bar);
+            bulk_g2s(smem_u32(incs), A.inc + (size_t)tile * NPE * TE, G::INC_BYTES, bar);
+        }
     };
     if (t == 0) {
         mbar_init(bar0, 1);
@@ -436,6 +449,9 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
     for (int ln = t; ln < nl; ln += TE) {
         const int gid = A.ln_gid[lb + ln];
+        const int ps = A.ln_pslot[lb + ln];
+        iends[ln] = A.ln_inc_end[lb + ln];
+        dsts[ln] = (ps < 0) ? gid : -(ps + 1);
         xs[ln] = A.px[gid];
         ys[ln] = A.py[gid];
         zs[ln] = A.pz[gid];
@@ -445,7 +461,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
             vs[3 * ln + 2] = A.v[3 * gid + 2];
         }
     }
-    __syncthreads();  // positions staged; barriers initialised
+    __syncthreads();  // positions and node tables staged; barriers initialised
 
     int lc[NPE];
     R f[NPE][3];
@@ -578,31 +594,31 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
                 f[a][i] += fc * dv;
             }
     }
+    __syncthreads();  // every thread is done with the stages the force table reuses
 #pragma unroll
     for (int a = 0; a < NPE; ++a)
 #pragma unroll
         for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
     __syncthreads();
 
-    const uint16_t* inc = A.inc + (size_t)tile * TE * NPE;
     for (int ln = t; ln < nl; ln += TE) {
-        const int beg = ln ? A.ln_inc_end[lb + ln - 1] : 0;
-        const int end = A.ln_inc_end[lb + ln];
+        const int beg = ln ? iends[ln - 1] : 0;
+        const int end = iends[ln];
         R s0 = R(0), s1 = R(0), s2 = R(0);
         for (int k = beg; k < end; ++k) {
-            const int ent = inc[k];
+            const int ent = incs[k];
             const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
             s0 += fe[base];
             s1 += fe[base + TE];
             s2 += fe[base + 2 * TE];
         }
-        const int ps = A.ln_pslot[lb + ln];
-        if (ps < 0) {
-            const int gid = A.ln_gid[lb + ln];
-            A.f_out[3 * gid + 0] = s0;
-            A.f_out[3 * gid + 1] = s1;
-            A.f_out[3 * gid + 2] = s2;
+        const int dn = dsts[ln];
+        if (dn >= 0) {
+            A.f_out[3 * dn + 0] = s0;
+            A.f_out[3 * dn + 1] = s1;
+            A.f_out[3 * dn + 2] = s2;
         } else {
+            const int ps = -dn - 1;
             A.partial[3 * ps + 0] = s0;
             A.partial[3 * ps + 1] = s1;
             A.partial[3 * ps + 2] = s2;
