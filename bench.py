@@ -210,8 +210,9 @@ def setup_element(T, cfg, x, y, z, conn, fixed, f):
 
 
 def kernels_only(args):
-    """Profiling case: the fused element force (2 x FP32 then 2 x FP64) or the CG
-    SpMV (assembly, a 5-iteration solve, then 3 applies) on the --mesh beam."""
+    """Profiling case on the --mesh beam: the fused element force (2 x FP32 then
+    2 x FP64), the CG SpMV (assembly, a 5-iteration solve, then 3 applies), or
+    the benchmark solve capped at --cg-iters iterations."""
     import torch
     import tlfea_b200 as T
 
@@ -225,6 +226,13 @@ def kernels_only(args):
         for prec in ("fp32", "fp32", "fp64", "fp64"):
             el.SetForcePrecision(prec)
             el.ComputeInternalForce()
+    elif args.kernels_only == "cg":
+        # the benchmark's solve capped at --cg-iters iterations: the per-iteration
+        # launch mix of the full solve in a launch list short enough to capture
+        el.ResetPositions()
+        s = T.LinearStaticSolver(el, cfg["tol"], args.cg_iters)
+        s.Solve()
+        del s
     else:
         s = T.LinearStaticSolver(el, cfg["tol"], 5)
         s.Solve()
@@ -239,6 +247,182 @@ def kernels_only(args):
     el.Destroy()
 
 
+def _plain_solve_time(T, x, y, z, conn, fixed, f, E, nu, tol, el=None):
+    """One cold-start LinearStaticSolver solve through the reference-named API;
+    returns (seconds, iterations, element) -- set-up (gradients) is not timed."""
+    import torch
+
+    if el is None:
+        el = T.GPU_FEAT10_Data(conn.shape[0], len(x))
+        el.Initialize()
+        el.SetNodalFixed(fixed)
+        el.Setup(*T.Quadrature.t10(), x, y, z, conn)
+        el.SetDensity(1000.0)
+        el.SetDamping(0.0, 0.0)
+        el.CalcDnDuPre()
+    el.SetSVK(E, nu)
+    el.SetExternalForce(f)
+    el.ResetPositions()
+    s = T.LinearStaticSolver(el, tol, 1000000)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.Solve()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    it = s.GetLastIterCount()
+    del s
+    return dt, it, el
+
+
+def batched_leg(args, T):
+    """Uneven batch: 512 seeded cantilevers (nx ~ U{8..64}, ny = nz ~ U{2..8},
+    h = 0.01 m, length 10 ny h; E log-uniform 1e6..1e9, nu U[0.2, 0.45]; tip
+    load direction on the sphere, magnitude U[1, 500] N) solved to 1e-6 by one
+    persistent graph-captured launch, against single-instance plain solves."""
+    import torch
+    from tlfea_b200 import mesh as M
+
+    n = args.batch_size
+    insts = [M.random_beam(s) for s in range(n)]
+    b = T.BatchedLinearStaticSolver([(d["x"], d["y"], d["z"], d["conn"]) for d in insts], T.TYPE_T10)
+    b.SetMaterial([d["E"] for d in insts], [d["nu"] for d in insts])
+    b.SetNodalFixed([d["fixed"] for d in insts])
+    f_all = np.concatenate([d["f"] for d in insts])
+    b.SetExternalForce(f_all)
+    b.SetPrecision(args.batch_precision)
+    tune = b.Autotune(4)
+    counts = b.GetCounts()
+    st = b.GetStream()
+
+    def step():
+        b.Solve(1e-6, 200000)
+
+    for _ in range(max(1, args.warmup // 3)):
+        step()
+    it, res, status = b.GetResults()
+    reps = max(1, args.steps // 2)
+    ms = time_stream(torch, st, step, reps)
+    # end to end: loads host -> device, solve, displacements device -> host
+    f_pin = torch.from_numpy(f_all).pin_memory()
+    u_host = torch.empty(3 * b.n_nodes, dtype=torch.float64).pin_memory()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        b.SetExternalForce(f_pin.numpy())
+        step()
+        u_host.numpy()[:] = b.RetrieveDisplacement(split=False)
+    t_e2e = (time.perf_counter() - t0) / reps
+    launch = b.GetLaunch()
+    b.Destroy()
+    # plain path: one instance at a time, cold start (a seeded sample of the batch)
+    k = min(args.plain_sample, n)
+    tot, its = 0.0, []
+    for d in insts[:k]:
+        dt, itp, el = _plain_solve_time(T, d["x"], d["y"], d["z"], d["conn"], d["fixed"], d["f"], d["E"], d["nu"],
+                                        1e-6)
+        el.Destroy()
+        tot += dt
+        its.append(itp)
+    plain = k / tot
+    value = n / (ms / 1e3)
+    return {"workload": f"{n} uneven TET10 cantilevers, linear static CG to 1e-6 (one persistent launch)",
+            "elements": counts["elements"], "nodes": counts["nodes"], "dof": 3 * counts["nodes"],
+            "precision": args.batch_precision, "value": round(value, 2), "unit": "solves/s",
+            "ms_per_batch": round(ms, 3), "iters_mean": float(np.mean(it)), "iters_max": int(np.max(it)),
+            "converged": int(np.sum(status == 0)), "max_rel_residual": float(np.max(res)),
+            "e2e": {"value": round(n / t_e2e, 2), "unit": "solves/s", "h2d_bytes_per_step": int(f_all.nbytes),
+                    "d2h_bytes_per_step": int(8 * 3 * counts["nodes"])},
+            "launch": launch, "autotune": tune,
+            "plain_sequential": {"value": round(plain, 2), "unit": "solves/s", "sample": k,
+                                 "iters_mean": float(np.mean(its)),
+                                 "path": "LinearStaticSolver per instance (assembled K, CG graph), cold start"},
+            "speedup_vs_plain": round(value / plain, 2)}
+
+
+def learned_leg(args, T):
+    """Learned warm start on the fixed 40 x 8 x 8 TET10 cantilever (1.0 x 0.1 x
+    0.1 m): 4096 solver-generated training cases (E log-uniform 1e6..1e8, nu
+    U[0.2, 0.45], load direction on the sphere, magnitude U[1, 200] N), PCA to
+    64 modes, a 6-256-256-256-64 GELU MLP trained on the GPU; 512 held-out
+    cases solved warm and cold (batched) and cold one at a time (plain)."""
+    import torch
+    from tlfea_b200 import warmstart as W
+
+    t_setup = time.perf_counter()
+    fm = W.FixedMeshCases(40, 8, 8, 1.0, 0.1, 0.1, batch=512)
+    t_setup = time.perf_counter() - t_setup
+    train = W.sample_cases(args.train_cases, seed=1)
+    t0 = time.perf_counter()
+    us, its = [], []
+    for b0 in range(0, len(train), 512):
+        u, it, res, stt = fm.solve(train[b0:b0 + 512], tol=1e-6)
+        us.append(u)
+        its.append(it)
+    t_gen = time.perf_counter() - t0
+    u_train = np.concatenate(us)
+    ws = W.LearnedWarmStart(hidden=(256, 256, 256), k=64, max_batch=512, seed=0)
+    t0 = time.perf_counter()
+    hist = ws.fit(train, u_train, epochs=args.epochs, batch=512, lr=1e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    test = W.sample_cases(512, seed=12345)
+    st = fm.solver.GetStream()
+    # the held-out loads and materials are resident before each timed region
+    fm._load(test)
+    held = {}
+
+    def cold():
+        fm.solver.SetInitialGuess(None)
+        fm.solver.Solve(1e-6, 200000)
+
+    def warm():
+        # network inference + PCA reconstruction (complete when predict returns),
+        # then the warm-started batched solve
+        held["guess"] = g = ws.predict(test)
+        fm.solver.SetInitialGuess(int(g.data_ptr()))
+        fm.solver.Solve(1e-6, 200000)
+
+    cold()
+    it_c, res_c, st_c = fm.solver.GetResults()
+    u_c = fm.solver.RetrieveDisplacement(split=False).reshape(512, -1)
+    warm()
+    it_w, res_w, st_w = fm.solver.GetResults()
+    g = held["guess"].cpu().numpy()
+    guess_err = np.linalg.norm(g - u_c, axis=1) / np.linalg.norm(u_c, axis=1)
+    reps = max(1, args.steps // 2)
+    ms_cold = time_stream(torch, st, cold, reps)
+    ms_warm = time_stream(torch, st, warm, reps)
+    # plain: one case at a time through LinearStaticSolver, cold start
+    k = min(args.plain_sample, 512)
+    F = fm.loads(test[:k])
+    tot, itp_all, el = 0.0, [], None
+    for i in range(k):
+        dt, itp, el = _plain_solve_time(T, fm.x, fm.y, fm.z, fm.conn, fm.fixed, F[i], test[i, 0], test[i, 1], 1e-6, el)
+        tot += dt
+        itp_all.append(itp)
+    el.Destroy()
+    plain = k / tot
+    learned = 512 / (ms_warm / 1e3)
+    ws.destroy()
+    fm.destroy()
+    return {"workload": "learned warm start, 40x8x8 TET10 cantilever (15,360 elements, 70,227 DOF), "
+                        "512 held-out cases to 1e-6",
+            "value": round(learned, 2), "unit": "solves/s",
+            "learned_batched": {"value": round(learned, 2), "ms_per_batch": round(ms_warm, 3),
+                                "iters_mean": float(np.mean(it_w)), "iters_max": int(np.max(it_w)),
+                                "converged": int(np.sum(st_w == 0)), "max_rel_residual": float(np.max(res_w))},
+            "cold_batched": {"value": round(512 / (ms_cold / 1e3), 2), "ms_per_batch": round(ms_cold, 3),
+                             "iters_mean": float(np.mean(it_c)), "iters_max": int(np.max(it_c))},
+            "plain_sequential": {"value": round(plain, 2), "sample": k, "iters_mean": float(np.mean(itp_all)),
+                                 "path": "LinearStaticSolver per case (assembled K, CG graph), cold start"},
+            "speedup_learned_vs_plain": round(learned / plain, 2),
+            "speedup_learned_vs_cold_batched": round(ms_cold / ms_warm, 2),
+            "guess_rel_error_median": float(np.median(guess_err)),
+            "training": {"cases": int(len(train)), "gen_s": round(t_gen, 2), "train_s": round(t_train, 2),
+                         "epochs": args.epochs, "final_loss": float(hist[-1]), "pca_energy": ws.pca.energy
+                         if hasattr(ws.pca, "energy") else None, "setup_s": round(t_setup, 2),
+                         "train_iters_mean": float(np.mean(np.concatenate(its)))}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -247,9 +431,17 @@ def main():
     ap.add_argument("--impl", default="tlfea", choices=["tlfea", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--kernel-reps", type=int, default=20)
-    ap.add_argument("--kernels-only", choices=["force", "spmv"], default=None,
+    ap.add_argument("--cg-iters", type=int, default=120, help="iteration cap of --kernels-only cg")
+    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg"], default=None,
                     help="profiling case: set up, then launch only the named kernel a few times")
     ap.add_argument("--mesh", default=None, help="cells NXxNYxNZ (default 200x20x20)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
+    ap.add_argument("--batch-size", type=int, default=512)
+    ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--plain-sample", type=int, default=48, help="single-instance solves timed for the plain path")
+    ap.add_argument("--train-cases", type=int, default=4096)
+    ap.add_argument("--epochs", type=int, default=300)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -360,11 +552,15 @@ def main():
                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (K 1.35 GB)"},
            "e2e": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in e2e.items()},
            "roofline": roofline, "elem_force": ef, "gpu_launches": int(launches), "clocks": clk.summary()}
+    el.Destroy()
+    if not args.no_batch:
+        out["batched"] = batched_leg(args, T)
+    if not args.no_learned:
+        out["learned"] = learned_leg(args, T)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_sample(x, y, z, conn, fixed, f, cfg, iters)
     if rank == 0:
         print(json.dumps(out))
-    el.Destroy()
     if dist:
         dist.destroy_process_group()
 

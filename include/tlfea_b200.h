@@ -243,6 +243,79 @@ int tlfea_solver_set_velocity(tlfea_solver s, const double* v_guess, const doubl
 int tlfea_solver_get_multipliers(tlfea_solver s, double* lam, int n);
 int tlfea_solver_get_stats(tlfea_solver s, tlfea_solve_stats* st);
 
+/* ------------------------------------------------- batched linear static
+ * New, no reference counterpart: many independent meshes solved by one
+ * persistent cooperative launch (captured in a CUDA graph).  Per instance the
+ * iteration is LinearStaticSolver's CG (LinearStaticSolver.cu:469-565) on the
+ * linear stiffness at the reference configuration (the tangent of
+ * compute_hessian_assemble_csr, FEAT10DataFunc.cuh:512-684, at F = I),
+ * applied matrix-free, with fixed DOFs eliminated as apply_bcs_kernel does
+ * (LinearStaticSolver.cu:284-306).  Stop rule ||r|| / ||f_free|| < tol (FP64).
+ *
+ * Instances are concatenated: instance i owns nodes [node_off[i], node_off[i+1])
+ * and elements [elem_off[i], elem_off[i+1]); conn is row-major
+ * [elem_off[n_inst]][npe] with node ids local to the instance; x, y, z hold the
+ * concatenated reference positions; the quadrature is Setup()'s. */
+typedef struct tlfea_batch_s* tlfea_batch;
+int tlfea_batch_create(int type, int n_inst, const int* node_off, const int* elem_off, const double* qx,
+                       const double* qy, const double* qz, const double* qw, int n_qp, const double* x,
+                       const double* y, const double* z, const int* conn, tlfea_batch* out);
+int tlfea_batch_destroy(tlfea_batch b);
+int tlfea_batch_get_counts(tlfea_batch b, int* n_inst, int* n_elem, int* n_nodes, int* n_tiles);
+int tlfea_batch_get_stream(tlfea_batch b, void** stream);
+/* Per-instance Young's modulus and Poisson ratio (Lame parameters as SetSVK). */
+int tlfea_batch_set_material(tlfea_batch b, const double* E, const double* nu);
+/* Fixed nodes (concatenated numbering); nodes that no element touches are always fixed. */
+int tlfea_batch_set_fixed(tlfea_batch b, const int* nodes, int n);
+/* External force, 3 * n_nodes interleaved; on_device selects a device pointer. */
+int tlfea_batch_set_external_force(tlfea_batch b, const double* f, long long n, int on_device);
+/* Warm start u0 (3 * n_nodes; NULL = cold start u0 = 0). */
+int tlfea_batch_set_initial_guess(tlfea_batch b, const double* u0, long long n, int on_device);
+/* TLFEA_PRECISION_FP64 (default) or FP32 element work (the CG stays FP64). */
+int tlfea_batch_set_precision(tlfea_batch b, int precision);
+/* Launch shape: resident blocks per SM of the persistent kernel (0 = occupancy
+ * maximum) and nodes per reduction chunk (0 = keep). */
+int tlfea_batch_set_launch(tlfea_batch b, int blocks_per_sm, int chunk_nodes);
+int tlfea_batch_get_launch(tlfea_batch b, int* blocks_per_sm, int* chunk_nodes, int* grid);
+/* Times trial_iters CG iterations per (blocks per SM, chunk size) candidate and
+ * keeps the fastest; overwrites the solution vectors. */
+int tlfea_batch_autotune(tlfea_batch b, int trial_iters, int* best_blocks_per_sm, int* best_chunk, float* best_ms);
+/* Solves every instance; per-instance iterations, ||r||/||f_free|| and status
+ * (0 converged, 1 non-positive p.Kp, 2 max_iter reached). */
+int tlfea_batch_solve(tlfea_batch b, double tol, int max_iter);
+int tlfea_batch_get_results(tlfea_batch b, int* iters, double* rel_residual, int* status);
+int tlfea_batch_retrieve_displacement(tlfea_batch b, double* u, long long n);
+int tlfea_batch_device_ptrs(tlfea_batch b, double** u, double** f_ext, double** u0);
+/* d_y = K_bc d_x over the whole batch (device pointers, 3 * n_nodes). */
+int tlfea_batch_apply(tlfea_batch b, const double* d_x, double* d_y);
+
+/* ------------------------------------------------------ warm-start MLP
+ * New, no reference counterpart: dims[0] -> dims[1] -> ... -> dims[n_layers]
+ * with GELU between layers, BF16 operands and FP32 accumulation on the
+ * tcgen05 tensor cores, FP32 master weights, AdamW, mean-squared-error loss.
+ * Hidden and output widths are multiples of 16; max_batch a multiple of 128.
+ * Flat parameter layout: per layer W [dims[l+1] x dims[l]] row-major, then b.
+ * Tensor arguments named d_* are device pointers (FP32, row-major). */
+typedef struct tlfea_mlp_s* tlfea_mlp;
+int tlfea_mlp_create(int n_layers, const int* dims, int max_batch, unsigned long long seed, tlfea_mlp* out);
+int tlfea_mlp_destroy(tlfea_mlp m);
+int tlfea_mlp_get_stream(tlfea_mlp m, void** stream);
+int tlfea_mlp_param_count(tlfea_mlp m, long long* n);
+int tlfea_mlp_set_params(tlfea_mlp m, const float* params, long long n);
+int tlfea_mlp_get_params(tlfea_mlp m, float* params, long long n);
+int tlfea_mlp_get_grads(tlfea_mlp m, float* grads, long long n);
+int tlfea_mlp_forward(tlfea_mlp m, const float* d_x, int batch, float* d_y);
+int tlfea_mlp_loss_grad(tlfea_mlp m, const float* d_x, const float* d_target, int batch, float* loss);
+int tlfea_mlp_adamw_step(tlfea_mlp m, float lr, float beta1, float beta2, float eps, float weight_decay);
+int tlfea_mlp_train_step(tlfea_mlp m, const float* d_x, const float* d_target, int batch, float lr, float beta1,
+                         float beta2, float eps, float weight_decay, float* loss);
+int tlfea_mlp_sync(tlfea_mlp m);
+/* The MLP's tensor-core product on its own: d_d[M x N] (FP32, leading dim ldd)
+ * = d_a[M x K] (BF16, lda) * d_b[N x K]^T (BF16, ldb) + d_bias[N] (or NULL).
+ * N and K multiples of 16, lda and ldb multiples of 8. */
+int tlfea_mlp_gemm_bf16(int M, int N, int K, const void* d_a, int lda, const void* d_b, int ldb, const float* d_bias,
+                        float* d_d, int ldd, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

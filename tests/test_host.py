@@ -122,3 +122,26 @@ def test_cantilever_loads_sum():
     fixed, f, tip = M.cantilever_loads(x, y, z, (0.0, 0.0, -100.0))
     assert len(fixed) == 25 and len(tip) == 25
     assert f.reshape(-1, 3)[:, 2].sum() == pytest.approx(-100.0)
+
+
+def test_random_beam_instances_follow_the_batch_distribution():
+    """The seeded uneven-batch generator: sizes, material and load ranges,
+    clamped x = 0 face and a tip load of the drawn magnitude."""
+    from tlfea_b200 import mesh as M
+
+    seen_nx, seen_ny = set(), set()
+    for s in range(64):
+        d = M.random_beam(s)
+        assert 8 <= d["nx"] <= 64 and 2 <= d["ny"] <= 8
+        seen_nx.add(d["nx"])
+        seen_ny.add(d["ny"])
+        assert 1e6 <= d["E"] <= 1e9 and 0.2 <= d["nu"] <= 0.45
+        assert abs(np.linalg.norm(d["direction"]) - 1.0) < 1e-12
+        ftot = d["f"].reshape(-1, 3).sum(0)
+        assert np.allclose(ftot, d["magnitude"] * d["direction"], rtol=1e-12, atol=1e-12)
+        nn, ne = M.box_counts(d["nx"], d["ny"], d["ny"])
+        assert len(d["x"]) == nn and d["conn"].shape == (ne, 10)
+        assert np.all(d["x"][d["fixed"]] == 0.0)
+        assert abs(d["x"].max() - 10 * d["ny"] * 0.01) < 1e-12
+        assert M.random_beam(s)["E"] == d["E"]  # seeded
+    assert len(seen_nx) > 10 and len(seen_ny) > 3

@@ -22,6 +22,9 @@ from .api import (
     LinearStaticSolver,
     LinearStaticSolverT10,
     LinearStaticSolverT4,
+    BatchedLinearStaticSolver,
+    WarmStartMLP,
+    gemm_bf16,
     TYPE_3243,
     TYPE_3443,
     TYPE_T10,
@@ -34,6 +37,6 @@ __all__ = [
     "Quadrature", "mesh", "TLFEAError", "launch_count", "last_error", "FEASolver", "ElementBase",
     "GPU_FEAT10_Data", "GPU_FEAT4_Data", "SolverBase", "SyncedNesterovParams", "SyncedNesterovSolver",
     "SyncedAdamWParams", "SyncedAdamWNocoopParams", "SyncedAdamWSolver", "SyncedAdamWNocoopSolver",
-    "LinearStaticSolver", "LinearStaticSolverT10", "LinearStaticSolverT4", "TYPE_3243", "TYPE_3443", "TYPE_T10",
+    "LinearStaticSolver", "LinearStaticSolverT10", "LinearStaticSolverT4", "BatchedLinearStaticSolver", "WarmStartMLP", "gemm_bf16", "TYPE_3243", "TYPE_3443", "TYPE_T10",
     "TYPE_T4", "MATERIAL_MODEL_SVK", "MATERIAL_MODEL_MOONEY_RIVLIN",
 ]

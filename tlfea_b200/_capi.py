@@ -68,6 +68,7 @@ class SolveStats(C.Structure):
 
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
 _I = C.POINTER(C.c_int)
 _LL = C.c_longlong
 
@@ -132,6 +133,36 @@ _SIGS = {
     "tlfea_solver_set_velocity": [_P, _D, _D, C.c_int],
     "tlfea_solver_get_multipliers": [_P, _D, C.c_int],
     "tlfea_solver_get_stats": [_P, C.POINTER(SolveStats)],
+    "tlfea_batch_create": [C.c_int, C.c_int, _I, _I, _D, _D, _D, _D, C.c_int, _D, _D, _D, _I, C.POINTER(_P)],
+    "tlfea_batch_destroy": [_P],
+    "tlfea_batch_get_counts": [_P, _I, _I, _I, _I],
+    "tlfea_batch_get_stream": [_P, C.POINTER(_P)],
+    "tlfea_batch_set_material": [_P, _D, _D],
+    "tlfea_batch_set_fixed": [_P, _I, C.c_int],
+    "tlfea_batch_set_external_force": [_P, _P, _LL, C.c_int],
+    "tlfea_batch_set_initial_guess": [_P, _P, _LL, C.c_int],
+    "tlfea_batch_set_precision": [_P, C.c_int],
+    "tlfea_batch_set_launch": [_P, C.c_int, C.c_int],
+    "tlfea_batch_get_launch": [_P, _I, _I, _I],
+    "tlfea_batch_autotune": [_P, C.c_int, _I, _I, C.POINTER(C.c_float)],
+    "tlfea_batch_solve": [_P, C.c_double, C.c_int],
+    "tlfea_batch_get_results": [_P, _I, _D, _I],
+    "tlfea_batch_retrieve_displacement": [_P, _D, _LL],
+    "tlfea_batch_device_ptrs": [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)],
+    "tlfea_batch_apply": [_P, _P, _P],
+    "tlfea_mlp_create": [C.c_int, _I, C.c_int, C.c_ulonglong, C.POINTER(_P)],
+    "tlfea_mlp_destroy": [_P],
+    "tlfea_mlp_get_stream": [_P, C.POINTER(_P)],
+    "tlfea_mlp_param_count": [_P, C.POINTER(_LL)],
+    "tlfea_mlp_set_params": [_P, _F, _LL],
+    "tlfea_mlp_get_params": [_P, _F, _LL],
+    "tlfea_mlp_get_grads": [_P, _F, _LL],
+    "tlfea_mlp_forward": [_P, _P, C.c_int, _P],
+    "tlfea_mlp_loss_grad": [_P, _P, _P, C.c_int, _F],
+    "tlfea_mlp_adamw_step": [_P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float],
+    "tlfea_mlp_train_step": [_P, _P, _P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _F],
+    "tlfea_mlp_sync": [_P],
+    "tlfea_mlp_gemm_bf16": [C.c_int, C.c_int, C.c_int, _P, C.c_int, _P, C.c_int, _P, _P, C.c_int, _P],
 }
 _RESTYPES = {"tlfea_last_error": C.c_char_p, "tlfea_launch_count": C.c_longlong, "tlfea_version": C.c_char_p}
 
@@ -177,6 +208,11 @@ def launch_count() -> int:
 def dptr(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(_D)
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_F)
 
 
 def iptr(a: np.ndarray):

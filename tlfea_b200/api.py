@@ -453,6 +453,142 @@ LinearStaticSolverT10 = LinearStaticSolver
 LinearStaticSolverT4 = LinearStaticSolver
 
 
+class BatchedLinearStaticSolver:
+    """New, no reference counterpart: many independent meshes solved by one
+    persistent, graph-captured launch.
+
+    Per instance the iteration is LinearStaticSolver's CG
+    (LinearStaticSolver.cu:469-565) on the linear stiffness at the reference
+    configuration, applied matrix-free; fixed DOFs are eliminated as
+    apply_bcs_kernel does.  Stop rule: ||r|| / ||f_free|| < tol in FP64.
+
+    meshes: list of (x, y, z, conn) with conn an (E_i, NPE) array of
+    instance-local node ids.  Device pointers passed in must hold finished
+    data: the library orders its own work on its own stream (GetStream) and
+    does not wait for other streams.
+    """
+
+    def __init__(self, meshes, element_type: int = TYPE_T10):
+        if element_type not in (TYPE_T10, TYPE_T4):
+            raise TLFEAError(capi.INVALID_ARG, "BatchedLinearStaticSolver", "element type must be TYPE_T10 or TYPE_T4")
+        npe = 10 if element_type == TYPE_T10 else 4
+        q = Quadrature.t10() if element_type == TYPE_T10 else Quadrature.t4()
+        self.n_inst = len(meshes)
+        nn = [len(m[0]) for m in meshes]
+        ne = [np.asarray(m[3]).shape[0] for m in meshes]
+        self.node_off = np.zeros(self.n_inst + 1, np.int32)
+        self.elem_off = np.zeros(self.n_inst + 1, np.int32)
+        self.node_off[1:] = np.cumsum(nn)
+        self.elem_off[1:] = np.cumsum(ne)
+        x = _f64(np.concatenate([m[0] for m in meshes]))
+        y = _f64(np.concatenate([m[1] for m in meshes]))
+        z = _f64(np.concatenate([m[2] for m in meshes]))
+        conn = _i32(np.concatenate([np.asarray(m[3], dtype=np.int32).reshape(-1, npe) for m in meshes]))
+        qx, qy, qz, qw = (_f64(a) for a in q)
+        h = C.c_void_p()
+        capi.call("tlfea_batch_create", int(element_type), self.n_inst, capi.iptr(self.node_off),
+                  capi.iptr(self.elem_off), capi.dptr(qx), capi.dptr(qy), capi.dptr(qz), capi.dptr(qw), len(qw),
+                  capi.dptr(x), capi.dptr(y), capi.dptr(z), capi.iptr(conn), C.byref(h))
+        self._h = h
+        self.n_nodes = int(self.node_off[-1])
+
+    def GetCounts(self) -> dict:
+        a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        capi.call("tlfea_batch_get_counts", self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d))
+        return {"instances": a.value, "elements": b.value, "nodes": c.value, "tiles": d.value}
+
+    def GetStream(self) -> int:
+        s = C.c_void_p()
+        capi.call("tlfea_batch_get_stream", self._h, C.byref(s))
+        return s.value or 0
+
+    def SetMaterial(self, E, nu):
+        capi.call("tlfea_batch_set_material", self._h, capi.dptr(_f64(E, self.n_inst, "E")),
+                  capi.dptr(_f64(nu, self.n_inst, "nu")))
+
+    def SetNodalFixed(self, fixed_per_instance):
+        """Fixed nodes, one array of instance-local ids per instance."""
+        g = [np.asarray(f, dtype=np.int64) + int(self.node_off[i]) for i, f in enumerate(fixed_per_instance)]
+        allf = _i32(np.concatenate(g) if g else np.zeros(0))
+        capi.call("tlfea_batch_set_fixed", self._h, capi.iptr(allf) if allf.size else None, int(allf.size))
+
+    def SetExternalForce(self, f):
+        """f: concatenated 3 * n_nodes array, a list of per-instance arrays, or a device pointer (int)."""
+        if isinstance(f, int):
+            capi.call("tlfea_batch_set_external_force", self._h, C.c_void_p(f), 3 * self.n_nodes, 1)
+            return
+        if isinstance(f, (list, tuple)):
+            f = np.concatenate([np.asarray(v, dtype=np.float64).ravel() for v in f])
+        a = _f64(f, 3 * self.n_nodes, "f_ext")
+        capi.call("tlfea_batch_set_external_force", self._h, a.ctypes.data_as(C.c_void_p), a.size, 0)
+
+    def SetInitialGuess(self, u0=None):
+        """Warm start (concatenated 3 * n_nodes, or a device pointer); None = cold start."""
+        if u0 is None:
+            capi.call("tlfea_batch_set_initial_guess", self._h, None, 0, 0)
+        elif isinstance(u0, int):
+            capi.call("tlfea_batch_set_initial_guess", self._h, C.c_void_p(u0), 3 * self.n_nodes, 1)
+        else:
+            a = _f64(u0, 3 * self.n_nodes, "u0")
+            capi.call("tlfea_batch_set_initial_guess", self._h, a.ctypes.data_as(C.c_void_p), a.size, 0)
+
+    def SetPrecision(self, precision: str):
+        p = {"fp64": capi.PRECISION_FP64, "fp32": capi.PRECISION_FP32}[precision.lower()]
+        capi.call("tlfea_batch_set_precision", self._h, p)
+
+    def SetLaunch(self, blocks_per_sm: int = 0, chunk_nodes: int = 0):
+        capi.call("tlfea_batch_set_launch", self._h, int(blocks_per_sm), int(chunk_nodes))
+
+    def GetLaunch(self) -> dict:
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        capi.call("tlfea_batch_get_launch", self._h, C.byref(a), C.byref(b), C.byref(c))
+        return {"blocks_per_sm": a.value, "chunk_nodes": b.value, "grid": c.value}
+
+    def Autotune(self, trial_iters: int = 8) -> dict:
+        a, b, ms = C.c_int(), C.c_int(), C.c_float()
+        capi.call("tlfea_batch_autotune", self._h, int(trial_iters), C.byref(a), C.byref(b), C.byref(ms))
+        return {"blocks_per_sm": a.value, "chunk_nodes": b.value, "trial_ms": ms.value}
+
+    def Solve(self, tol: float = 1e-6, max_iter: int = 100000):
+        capi.call("tlfea_batch_solve", self._h, float(tol), int(max_iter))
+
+    def GetResults(self):
+        """(iterations, ||r||/||f_free||, status) per instance; status 0 converged,
+        1 non-positive p.Kp, 2 max_iter reached."""
+        it = np.zeros(self.n_inst, np.int32)
+        rel = np.zeros(self.n_inst)
+        st = np.zeros(self.n_inst, np.int32)
+        capi.call("tlfea_batch_get_results", self._h, capi.iptr(it), capi.dptr(rel), capi.iptr(st))
+        return it, rel, st
+
+    def RetrieveDisplacement(self, split: bool = True):
+        u = np.zeros(3 * self.n_nodes)
+        capi.call("tlfea_batch_retrieve_displacement", self._h, capi.dptr(u), u.size)
+        if not split:
+            return u
+        return [u[3 * self.node_off[i]:3 * self.node_off[i + 1]] for i in range(self.n_inst)]
+
+    def DevicePtrs(self) -> dict:
+        u, f, u0 = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        capi.call("tlfea_batch_device_ptrs", self._h, C.byref(u), C.byref(f), C.byref(u0))
+        return {"u": u.value, "f_ext": f.value, "u0": u0.value}
+
+    def Apply(self, d_x: int, d_y: int):
+        """y = K_bc x over the whole batch (device pointers, 3 * n_nodes doubles)."""
+        capi.call("tlfea_batch_apply", self._h, C.c_void_p(d_x), C.c_void_p(d_y))
+
+    def Destroy(self):
+        if getattr(self, "_h", None) is not None:
+            capi.call("tlfea_batch_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.Destroy()
+        except Exception:
+            pass
+
+
 # -------------------------------------------------------------------- manager
 
 class FEASolver:
@@ -491,3 +627,83 @@ class FEASolver:
 
     def GetNumSolvers(self) -> int:
         return len(self._solvers)
+
+
+class WarmStartMLP:
+    """New, no reference counterpart: the warm-start network, trained and
+    evaluated by this library's tcgen05 kernels (BF16 operands, FP32
+    accumulation, FP32 master weights, AdamW, mean-squared-error loss).
+
+    dims: layer widths, e.g. (6, 256, 256, 256, 64); GELU between layers.
+    Tensors passed as ints are device pointers (FP32, row-major); the kernels
+    run on the network's own stream (GetStream), so producers of those tensors
+    either run on that stream or finish first.
+    """
+
+    def __init__(self, dims, max_batch: int = 512, seed: int = 0):
+        self.dims = [int(d) for d in dims]
+        d = np.asarray(self.dims, np.int32)
+        h = C.c_void_p()
+        capi.call("tlfea_mlp_create", len(self.dims) - 1, capi.iptr(d), int(max_batch), int(seed), C.byref(h))
+        self._h = h
+        self.max_batch = int(max_batch)
+        n = C.c_longlong()
+        capi.call("tlfea_mlp_param_count", self._h, C.byref(n))
+        self.n_params = n.value
+
+    def GetStream(self) -> int:
+        s = C.c_void_p()
+        capi.call("tlfea_mlp_get_stream", self._h, C.byref(s))
+        return s.value or 0
+
+    def SetParams(self, flat):
+        a = np.ascontiguousarray(np.asarray(flat, dtype=np.float32).ravel())
+        capi.call("tlfea_mlp_set_params", self._h, capi.fptr(a), a.size)
+
+    def GetParams(self) -> np.ndarray:
+        a = np.zeros(self.n_params, np.float32)
+        capi.call("tlfea_mlp_get_params", self._h, capi.fptr(a), a.size)
+        return a
+
+    def GetGrads(self) -> np.ndarray:
+        a = np.zeros(self.n_params, np.float32)
+        capi.call("tlfea_mlp_get_grads", self._h, capi.fptr(a), a.size)
+        return a
+
+    def Forward(self, d_x: int, batch: int, d_y: int):
+        capi.call("tlfea_mlp_forward", self._h, C.c_void_p(d_x), int(batch), C.c_void_p(d_y))
+
+    def LossGrad(self, d_x: int, d_t: int, batch: int) -> float:
+        loss = C.c_float()
+        capi.call("tlfea_mlp_loss_grad", self._h, C.c_void_p(d_x), C.c_void_p(d_t), int(batch), C.byref(loss))
+        return loss.value
+
+    def AdamWStep(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0):
+        capi.call("tlfea_mlp_adamw_step", self._h, lr, beta1, beta2, eps, weight_decay)
+
+    def TrainStep(self, d_x: int, d_t: int, batch: int, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8,
+                  weight_decay=0.0, want_loss=False):
+        loss = C.c_float()
+        capi.call("tlfea_mlp_train_step", self._h, C.c_void_p(d_x), C.c_void_p(d_t), int(batch), lr, beta1, beta2,
+                  eps, weight_decay, C.byref(loss) if want_loss else None)
+        return loss.value if want_loss else None
+
+    def Sync(self):
+        capi.call("tlfea_mlp_sync", self._h)
+
+    def Destroy(self):
+        if getattr(self, "_h", None) is not None:
+            capi.call("tlfea_mlp_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.Destroy()
+        except Exception:
+            pass
+
+
+def gemm_bf16(M, N, K, d_a, lda, d_b, ldb, d_bias, d_d, ldd, stream=0):
+    """The MLP's tcgen05 product on its own: D = A B^T (+ bias), BF16 in, FP32 out."""
+    capi.call("tlfea_mlp_gemm_bf16", int(M), int(N), int(K), C.c_void_p(d_a), int(lda), C.c_void_p(d_b), int(ldb),
+              C.c_void_p(d_bias) if d_bias else None, C.c_void_p(d_d), int(ldd), C.c_void_p(stream))

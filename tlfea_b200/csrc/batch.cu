@@ -1,0 +1,1051 @@
+// batch.cu -- batched linear-static solve: hundreds of independent meshes of
+// uneven size and material solved by one persistent cooperative launch.
+//
+// The instances are concatenated into one mesh (instance-contiguous node
+// numbering; tiles built instance by instance, so a tile holds one instance
+// except where an instance ends mid-tile).  Material is carried per element
+// slot, so a tile that straddles two instances is still exact.
+//
+// Per instance the iteration is the LinearStaticSolver CG (LinearStaticSolver.cu:
+// 469-565): u = u0, r = f - K u0, p = r; alpha = rr / p.Kp (stop on p.Kp <= 0);
+// u += alpha p; r -= alpha Kp; beta = rr_new / rr; p = r + beta p.  K is the
+// linear (small-strain) stiffness at the reference configuration -- the
+// tangent of compute_hessian_assemble_csr (FEAT10DataFunc.cuh:512-684) at F = I,
+// applied matrix-free from the per-QP shape-function gradients, with Dirichlet
+// DOFs eliminated as apply_bcs_kernel does (LinearStaticSolver.cu:284-306).
+// Stop rule: ||r|| / ||f_free|| < tol in FP64, which equals the reference's
+// sqrt(rr / rr0) for a cold start and does not reward a warm start for a
+// smaller initial residual.
+//
+// One launch runs every iteration of every instance: a grid-stride loop over
+// element tiles (K p), then over node chunks (segmented FP64 dots, vector
+// updates); four grid barriers per iteration; per-instance scalars are folded
+// redundantly and deterministically by every block that needs them.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "element.cuh"
+
+namespace cg = cooperative_groups;
+
+struct tlfea_batch_s {
+    int type = TLFEA_TYPE_T10;
+    int n_inst = 0;
+    int N = 0, E = 0;  // combined mesh
+    tlfea_element_s* el = nullptr;
+    std::vector<int> node_off, elem_off;
+    std::vector<double> inst_E, inst_nu;
+    int precision = TLFEA_PRECISION_FP64;
+    // device
+    double *lam = nullptr, *mu = nullptr;  // per element slot (n_tiles * TILE_ELEMS)
+    float *lam32 = nullptr, *mu32 = nullptr;
+    unsigned char* fixed = nullptr;        // per node
+    int* chunk_inst = nullptr;             // per chunk
+    int* chunk_beg = nullptr;              // n_chunks + 1 node offsets
+    int* inst_chunk = nullptr;             // n_inst + 1 chunk offsets
+    int* tile_inst = nullptr;              // 2 per tile: first and last instance of its elements
+    int n_chunks = 0;
+    int chunk_nodes = 256;
+    double *u = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *f = nullptr, *u0 = nullptr;
+    double *cpa = nullptr, *cpb = nullptr;  // per-chunk partials
+    double *rr = nullptr, *fnorm = nullptr, *rel = nullptr;  // rr: 2 * n_inst (iteration parity)
+    int *iters = nullptr, *status = nullptr, *done = nullptr, *n_done = nullptr;
+    bool warm = false;
+    bool material_set = false;
+    // launch
+    int blocks_per_sm = 0;  // 0 = occupancy maximum
+    cudaGraphExec_t graph = nullptr;
+    double graph_tol = -1.0;
+    int graph_max_iter = -1;
+    bool graph_warm = false;
+    int graph_grid = -1;
+};
+
+namespace tlfea {
+
+template <typename R>
+struct BatchArgs {
+    // tiling
+    const int* node_off;
+    const int* ln_gid;
+    const int* ln_pslot;
+    const uint16_t* ln_inc_end;
+    const uint16_t* inc;
+    const uint16_t* lconn;
+    const R* grad;
+    const R* dv;
+    const R* lam;
+    const R* mu;
+    R* partial;
+    const int* node_bidx;
+    const int* bnode_off;
+    const int* bnode_slots;
+    int n_tiles, max_local;
+    // nodes and instances
+    int N, n_inst, n_chunks;
+    const unsigned char* fixed;
+    const int* chunk_inst;
+    const int* chunk_beg;
+    const int* inst_chunk;
+    const int* tile_inst;
+    double *u, *r, *p, *q;
+    const double* f;
+    const double* u0;
+    double *cpa, *cpb, *rr, *fnorm, *rel;
+    int *iters, *status, *done, *n_done;
+};
+
+// q = K p on one tile: H = sum_a p_a (x) gradN_a, P = lambda tr(H) I + mu (H + H^T)
+// (the SVK tangent at F = I), f_a += P gradN_a dV; element forces reduced per
+// node in the tile's fixed incidence order.  Interior nodes are written to q,
+// nodes shared with other tiles to their partial slot.
+template <typename R, int NPE, int NQP>
+__device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int tile, const double* p, double* q,
+                                            unsigned char* smem) {
+    constexpr int TE = TILE_ELEMS;
+    const int t = threadIdx.x;
+    R* ps = reinterpret_cast<R*>(smem);  // 3 * max_local, interleaved
+    R* fe = ps + 3 * A.max_local;        // 3 * NPE * TE
+    const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
+    for (int ln = t; ln < nl; ln += TE) {
+        const int gid = A.ln_gid[lb + ln];
+        ps[3 * ln + 0] = R(p[3 * gid + 0]);
+        ps[3 * ln + 1] = R(p[3 * gid + 1]);
+        ps[3 * ln + 2] = R(p[3 * gid + 2]);
+    }
+    int lc[NPE];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) lc[a] = A.lconn[((size_t)tile * NPE + a) * TE + t];
+    const R lam = A.lam[(size_t)tile * TE + t], mu = A.mu[(size_t)tile * TE + t];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = R(0);
+    __syncthreads();
+#pragma unroll 1
+    for (int qp = 0; qp < NQP; ++qp) {
+        const R* gp = A.grad + ((size_t)tile * NQP + qp) * (NPE * 3) * TE + t;
+        R g[NPE][3];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) g[a][j] = __ldcs(gp + (a * 3 + j) * TE);
+        const R dv = __ldcs(A.dv + ((size_t)tile * NQP + qp) * TE + t);
+        R H[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) H[i][j] = R(0);
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) {
+            const R pa[3] = {ps[3 * lc[a] + 0], ps[3 * lc[a] + 1], ps[3 * lc[a] + 2]};
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) H[i][j] += pa[i] * g[a][j];
+        }
+        const R tr = lam * (H[0][0] + H[1][1] + H[2][2]);
+        R P[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) P[i][j] = (mu * (H[i][j] + H[j][i]) + (i == j ? tr : R(0))) * dv;
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const R fc = P[i][0] * g[a][0] + P[i][1] * g[a][1] + P[i][2] * g[a][2];
+                fe[(a * 3 + i) * TE + t] += fc;
+            }
+    }
+    __syncthreads();
+    const uint16_t* inc = A.inc + (size_t)tile * TE * NPE;
+    for (int ln = t; ln < nl; ln += TE) {
+        const int beg = ln ? A.ln_inc_end[lb + ln - 1] : 0;
+        const int end = A.ln_inc_end[lb + ln];
+        R s0 = R(0), s1 = R(0), s2 = R(0);
+        for (int k = beg; k < end; ++k) {
+            const int ent = inc[k];
+            const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
+            s0 += fe[base];
+            s1 += fe[base + TE];
+            s2 += fe[base + 2 * TE];
+        }
+        const int ps_slot = A.ln_pslot[lb + ln];
+        if (ps_slot < 0) {
+            const int gid = A.ln_gid[lb + ln];
+            q[3 * gid + 0] = double(s0);
+            q[3 * gid + 1] = double(s1);
+            q[3 * gid + 2] = double(s2);
+        } else {
+            A.partial[3 * ps_slot + 0] = s0;
+            A.partial[3 * ps_slot + 1] = s1;
+            A.partial[3 * ps_slot + 2] = s2;
+        }
+    }
+    __syncthreads();  // smem reused by the next tile
+}
+
+// Complete K p at node i: boundary nodes sum their tile partials in tile
+// order; fixed nodes get 0 (eliminated rows and columns).
+template <typename R>
+__device__ __forceinline__ void node_kp(const BatchArgs<R>& A, int i, double* q, double out[3]) {
+    if (A.fixed[i]) {
+        out[0] = out[1] = out[2] = 0.0;
+    } else {
+        const int b = A.node_bidx[i];
+        if (b < 0) {
+            out[0] = q[3 * i + 0];
+            out[1] = q[3 * i + 1];
+            out[2] = q[3 * i + 2];
+        } else {
+            R s0 = R(0), s1 = R(0), s2 = R(0);
+            for (int k = A.bnode_off[b]; k < A.bnode_off[b + 1]; ++k) {
+                const int sl = A.bnode_slots[k];
+                s0 += __ldcg(A.partial + 3 * sl + 0);
+                s1 += __ldcg(A.partial + 3 * sl + 1);
+                s2 += __ldcg(A.partial + 3 * sl + 2);
+            }
+            out[0] = double(s0);
+            out[1] = double(s1);
+            out[2] = double(s2);
+        }
+    }
+    q[3 * i + 0] = out[0];
+    q[3 * i + 1] = out[1];
+    q[3 * i + 2] = out[2];
+}
+
+// Sum of the chunk partials of instance b, folded by warp 0 in a fixed order
+// (every block computing it gets the same bits).  Valid in thread 0 .. 31.
+__device__ __forceinline__ double inst_sum(const double* part, const int* inst_chunk, int b) {
+    double s = 0.0;
+    for (int c = inst_chunk[b] + (threadIdx.x & 31); c < inst_chunk[b + 1]; c += 32) s += __ldcg(part + c);
+    return warp_sum(s);
+}
+
+// K p over every tile; with skip_done, tiles whose instances have all
+// converged are skipped (their q is never read again).  The done flags do not
+// change during this phase, so the skip is uniform across the block.
+template <typename R, int NPE, int NQP>
+__device__ __forceinline__ void apply_all_tiles(const BatchArgs<R>& A, const double* p, double* q,
+                                                unsigned char* smem, bool skip_done) {
+    for (int tile = blockIdx.x; tile < A.n_tiles; tile += gridDim.x) {
+        if (skip_done) {
+            bool all_done = true;
+            for (int i = A.tile_inst[2 * tile]; i <= A.tile_inst[2 * tile + 1] && all_done; ++i)
+                all_done = __ldcg(A.done + i) != 0;
+            if (all_done) continue;
+        }
+        linear_tile<R, NPE, NQP>(A, tile, p, q, smem);
+    }
+}
+
+// The whole batched solve.  mode: 0 = solve, 1 = y = K_bc x only (x in p, y in q).
+template <typename R, int NPE, int NQP>
+__global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double tol, int max_iter, int warm) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double red[32];
+    __shared__ double sh_scal[4];
+    __shared__ int sh_done;
+    const int t = threadIdx.x;
+    // done flag of instance b read once and broadcast, so the block branches uniformly
+    auto block_done = [&](int b) -> bool {
+        __syncthreads();
+        if (t == 0) sh_done = __ldcg(A.done + b);
+        __syncthreads();
+        return sh_done != 0;
+    };
+
+    // ---- prologue: u = u0, r = f_free, ||f_free|| per chunk
+    for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
+        double sf = 0.0;
+        for (int i = A.chunk_beg[c] + t; i < A.chunk_beg[c + 1]; i += blockDim.x) {
+            const bool fx = A.fixed[i];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double fi = fx ? 0.0 : A.f[3 * i + d];
+                const double ui = (warm && !fx) ? A.u0[3 * i + d] : 0.0;
+                A.r[3 * i + d] = fi;
+                A.u[3 * i + d] = ui;
+                A.p[3 * i + d] = ui;
+                sf += fi * fi;
+            }
+        }
+        const double s = block_sum(sf, red);
+        if (t == 0) A.cpa[c] = s;
+    }
+    grid.sync();
+    if (warm) {
+        apply_all_tiles<R, NPE, NQP>(A, A.p, A.q, smem, false);
+        grid.sync();
+    }
+    for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
+        double sr = 0.0;
+        for (int i = A.chunk_beg[c] + t; i < A.chunk_beg[c + 1]; i += blockDim.x) {
+            double kp[3] = {0.0, 0.0, 0.0};
+            if (warm) node_kp<R>(A, i, A.q, kp);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double ri = A.r[3 * i + d] - kp[d];
+                A.r[3 * i + d] = ri;
+                A.p[3 * i + d] = ri;
+                sr += ri * ri;
+            }
+        }
+        const double s = block_sum(sr, red);
+        if (t == 0) A.cpb[c] = s;
+    }
+    grid.sync();
+    for (int b = blockIdx.x; b < A.n_inst; b += gridDim.x) {
+        if (t < 32) {
+            const double ff = inst_sum(A.cpa, A.inst_chunk, b);
+            const double rr0 = inst_sum(A.cpb, A.inst_chunk, b);
+            if (t == 0) {
+                const double fn = sqrt(ff);
+                const double rel = (fn > 0.0) ? sqrt(rr0) / fn : 0.0;
+                A.fnorm[b] = fn;
+                A.rr[b] = rr0;
+                A.rel[b] = rel;
+                A.iters[b] = 0;
+                A.status[b] = 0;
+                const int dn = (fn == 0.0 || rel < tol) ? 1 : 0;
+                A.done[b] = dn;
+                if (dn) atomicAdd(A.n_done, 1);
+            }
+        }
+    }
+    grid.sync();
+
+    // ---- CG iterations
+    for (int it = 0; it < max_iter; ++it) {
+        if (atomicAdd(A.n_done, 0) >= A.n_inst) break;  // uniform: read after a grid barrier
+        const double* rr_old = A.rr + (size_t)(it & 1) * A.n_inst;
+        double* rr_new_out = A.rr + (size_t)((it + 1) & 1) * A.n_inst;
+        // q = K p
+        apply_all_tiles<R, NPE, NQP>(A, A.p, A.q, smem, true);
+        grid.sync();
+        // complete q, p.q per chunk
+        for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
+            const int b = A.chunk_inst[c];
+            double s = 0.0;
+            if (!block_done(b)) {
+                for (int i = A.chunk_beg[c] + t; i < A.chunk_beg[c + 1]; i += blockDim.x) {
+                    double kp[3];
+                    node_kp<R>(A, i, A.q, kp);
+                    s += A.p[3 * i + 0] * kp[0] + A.p[3 * i + 1] * kp[1] + A.p[3 * i + 2] * kp[2];
+                }
+            }
+            s = block_sum(s, red);
+            if (t == 0) A.cpa[c] = s;
+        }
+        grid.sync();
+        // alpha = rr / pq; u += alpha p; r -= alpha q; r.r per chunk
+        for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
+            const int b = A.chunk_inst[c];
+            double s = 0.0;
+            if (!block_done(b)) {
+                if (t < 32) {
+                    const double pq = inst_sum(A.cpa, A.inst_chunk, b);
+                    if (t == 0) sh_scal[0] = pq;
+                }
+                __syncthreads();
+                const double pq = sh_scal[0];
+                __syncthreads();
+                if (pq > 0.0) {
+                    const double alpha = __ldcg(rr_old + b) / pq;
+                    for (int i = A.chunk_beg[c] + t; i < A.chunk_beg[c + 1]; i += blockDim.x) {
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            A.u[3 * i + d] += alpha * A.p[3 * i + d];
+                            const double ri = A.r[3 * i + d] - alpha * A.q[3 * i + d];
+                            A.r[3 * i + d] = ri;
+                            s += ri * ri;
+                        }
+                    }
+                } else if (t == 0 && c == A.inst_chunk[b]) {
+                    // non-positive p.Kp: the reference aborts this solve
+                    A.status[b] = 1;
+                    A.done[b] = 1;
+                    atomicAdd(A.n_done, 1);
+                }
+            }
+            s = block_sum(s, red);
+            if (t == 0) A.cpb[c] = s;
+        }
+        grid.sync();
+        // convergence test, beta = rr_new / rr, p = r + beta p
+        for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
+            const int b = A.chunk_inst[c];
+            if (block_done(b)) continue;
+            if (t < 32) {
+                const double rrn = inst_sum(A.cpb, A.inst_chunk, b);
+                if (t == 0) sh_scal[1] = rrn;
+            }
+            __syncthreads();
+            const double rrn = sh_scal[1];
+            __syncthreads();
+            const double rel = sqrt(rrn) / __ldcg(A.fnorm + b);
+            const bool conv = rel < tol;
+            if (!conv) {
+                const double beta = rrn / __ldcg(rr_old + b);
+                for (int i = A.chunk_beg[c] + t; i < A.chunk_beg[c + 1]; i += blockDim.x)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) A.p[3 * i + d] = A.r[3 * i + d] + beta * A.p[3 * i + d];
+            }
+            __syncthreads();  // every thread has read done[b] before the owner may set it
+            if (t == 0 && c == A.inst_chunk[b]) {
+                rr_new_out[b] = rrn;
+                A.iters[b] = it + 1;
+                A.rel[b] = rel;
+                if (conv) {
+                    A.done[b] = 1;
+                    atomicAdd(A.n_done, 1);
+                } else if (it + 1 >= max_iter) {
+                    A.status[b] = 2;
+                }
+            }
+        }
+        grid.sync();
+    }
+    for (int b = blockIdx.x * blockDim.x + t; b < A.n_inst; b += gridDim.x * blockDim.x)
+        if (!A.done[b] && A.status[b] == 0) A.status[b] = 2;
+}
+
+// y = K_bc x for the whole batch: fixed rows are identity rows and fixed
+// columns are dropped (the BC-applied K of LinearStaticSolver::Apply).
+template <typename R, int NPE, int NQP>
+__global__ void __launch_bounds__(TILE_ELEMS) k_batch_apply(BatchArgs<R> A, const double* x, double* y) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int t = threadIdx.x;
+    for (int i = blockIdx.x * blockDim.x + t; i < A.N; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) A.p[3 * i + d] = A.fixed[i] ? 0.0 : x[3 * i + d];
+    grid.sync();
+    apply_all_tiles<R, NPE, NQP>(A, A.p, A.q, smem, false);
+    grid.sync();
+    for (int i = blockIdx.x * blockDim.x + t; i < A.N; i += gridDim.x * blockDim.x) {
+        double kp[3];
+        node_kp<R>(A, i, A.q, kp);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) y[3 * i + d] = A.fixed[i] ? x[3 * i + d] : kp[d];
+    }
+}
+
+template <typename R>
+static BatchArgs<R> batch_args(tlfea_batch_s* b) {
+    tlfea_element_s* el = b->el;
+    const Tiling& tl = el->tl;
+    BatchArgs<R> A;
+    A.node_off = tl.node_off;
+    A.ln_gid = tl.ln_gid;
+    A.ln_pslot = tl.ln_pslot;
+    A.ln_inc_end = tl.ln_inc_end;
+    A.inc = tl.inc;
+    A.lconn = tl.lconn;
+    if constexpr (sizeof(R) == 8) {
+        A.grad = tl.grad64;
+        A.dv = tl.dv64;
+        A.lam = b->lam;
+        A.mu = b->mu;
+        A.partial = tl.partial64;
+    } else {
+        A.grad = tl.grad32;
+        A.dv = tl.dv32;
+        A.lam = b->lam32;
+        A.mu = b->mu32;
+        A.partial = tl.partial32;
+    }
+    A.node_bidx = tl.node_bidx;
+    A.bnode_off = tl.bnode_off;
+    A.bnode_slots = tl.bnode_slots;
+    A.n_tiles = tl.n_tiles;
+    A.max_local = tl.max_local;
+    A.N = b->N;
+    A.n_inst = b->n_inst;
+    A.n_chunks = b->n_chunks;
+    A.fixed = b->fixed;
+    A.chunk_inst = b->chunk_inst;
+    A.chunk_beg = b->chunk_beg;
+    A.inst_chunk = b->inst_chunk;
+    A.tile_inst = b->tile_inst;
+    A.u = b->u;
+    A.r = b->r;
+    A.p = b->p;
+    A.q = b->q;
+    A.f = b->f;
+    A.u0 = b->u0;
+    A.cpa = b->cpa;
+    A.cpb = b->cpb;
+    A.rr = b->rr;
+    A.fnorm = b->fnorm;
+    A.rel = b->rel;
+    A.iters = b->iters;
+    A.status = b->status;
+    A.done = b->done;
+    A.n_done = b->n_done;
+    return A;
+}
+
+template <typename R>
+static size_t batch_smem(const tlfea_batch_s* b) {
+    return sizeof(R) * (3 * (size_t)b->el->tl.max_local + 3 * (size_t)b->el->npe * TILE_ELEMS);
+}
+
+template <typename R, int NPE, int NQP>
+static int batch_grid(tlfea_batch_s* b, int blocks_per_sm, int* grid_out, bool apply = false) {
+    const void* kern = apply ? (const void*)k_batch_apply<R, NPE, NQP> : (const void*)k_batch_cg<R, NPE, NQP>;
+    const size_t smem = batch_smem<R>(b);
+    if (smem > 200 * 1024) {
+        set_error("batch: a tile touches too many nodes for shared memory");
+        return TLFEA_UNSUPPORTED;
+    }
+    TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, sms = 0;
+    TLFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TILE_ELEMS, smem));
+    TLFEA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->el->device));
+    if (per_sm < 1) {
+        set_error("batch kernel does not fit on an SM");
+        return TLFEA_UNSUPPORTED;
+    }
+    if (blocks_per_sm > 0) per_sm = std::min(per_sm, blocks_per_sm);
+    *grid_out = per_sm * sms;
+    return TLFEA_OK;
+}
+
+template <typename R, int NPE, int NQP>
+static int launch_batch_cg(tlfea_batch_s* b, int grid, double tol, int max_iter, bool warm, cudaStream_t st) {
+    BatchArgs<R> A = batch_args<R>(b);
+    int w = warm ? 1 : 0;
+    void* args[] = {&A, &tol, &max_iter, &w};
+    TLFEA_CUDA(cudaLaunchCooperativeKernel((const void*)k_batch_cg<R, NPE, NQP>, dim3(grid), dim3(TILE_ELEMS), args,
+                                           batch_smem<R>(b), st));
+    TLFEA_LAUNCHED(1);
+    return TLFEA_OK;
+}
+
+static int batch_dispatch_grid(tlfea_batch_s* b, int blocks_per_sm, int* grid, bool apply = false) {
+    const bool f32 = b->precision == TLFEA_PRECISION_FP32;
+    if (b->el->npe == 10)
+        return f32 ? batch_grid<float, 10, 5>(b, blocks_per_sm, grid, apply)
+                   : batch_grid<double, 10, 5>(b, blocks_per_sm, grid, apply);
+    return f32 ? batch_grid<float, 4, 1>(b, blocks_per_sm, grid, apply)
+               : batch_grid<double, 4, 1>(b, blocks_per_sm, grid, apply);
+}
+
+static int batch_launch(tlfea_batch_s* b, int grid, double tol, int max_iter, bool warm, cudaStream_t st) {
+    const bool f32 = b->precision == TLFEA_PRECISION_FP32;
+    if (b->el->npe == 10)
+        return f32 ? launch_batch_cg<float, 10, 5>(b, grid, tol, max_iter, warm, st)
+                   : launch_batch_cg<double, 10, 5>(b, grid, tol, max_iter, warm, st);
+    return f32 ? launch_batch_cg<float, 4, 1>(b, grid, tol, max_iter, warm, st)
+               : launch_batch_cg<double, 4, 1>(b, grid, tol, max_iter, warm, st);
+}
+
+// Node chunks of at most `chunk_nodes` nodes that never straddle instances.
+static int build_chunks(tlfea_batch_s* b, int chunk_nodes) {
+    std::vector<int> cinst, cbeg, ichunk((size_t)b->n_inst + 1, 0);
+    for (int i = 0; i < b->n_inst; ++i) {
+        ichunk[i] = (int)cinst.size();
+        for (int n = b->node_off[i]; n < b->node_off[i + 1]; n += chunk_nodes) {
+            cinst.push_back(i);
+            cbeg.push_back(n);
+        }
+    }
+    ichunk[b->n_inst] = (int)cinst.size();
+    cbeg.push_back(b->N);
+    cudaStream_t st = b->el->stream;
+    TLFEA_CUDA(cudaStreamSynchronize(st));
+    dfree(b->chunk_inst);
+    dfree(b->chunk_beg);
+    dfree(b->inst_chunk);
+    dfree(b->cpa);
+    dfree(b->cpb);
+    b->n_chunks = (int)cinst.size();
+    int s;
+    if ((s = dalloc(&b->chunk_inst, cinst.size())) || (s = dalloc(&b->chunk_beg, cbeg.size())) ||
+        (s = dalloc(&b->inst_chunk, ichunk.size())) || (s = dalloc(&b->cpa, cinst.size())) ||
+        (s = dalloc(&b->cpb, cinst.size())))
+        return s;
+    TLFEA_CUDA(cudaMemcpy(b->chunk_inst, cinst.data(), cinst.size() * sizeof(int), cudaMemcpyHostToDevice));
+    TLFEA_CUDA(cudaMemcpy(b->chunk_beg, cbeg.data(), cbeg.size() * sizeof(int), cudaMemcpyHostToDevice));
+    TLFEA_CUDA(cudaMemcpy(b->inst_chunk, ichunk.data(), ichunk.size() * sizeof(int), cudaMemcpyHostToDevice));
+    b->chunk_nodes = chunk_nodes;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return TLFEA_OK;
+}
+
+static int upload_material(tlfea_batch_s* b) {
+    tlfea_element_s* el = b->el;
+    const Tiling& tl = el->tl;
+    const size_t ns = (size_t)tl.n_tiles * TILE_ELEMS;
+    std::vector<int> elem_inst((size_t)b->E);
+    for (int i = 0; i < b->n_inst; ++i)
+        for (int e = b->elem_off[i]; e < b->elem_off[i + 1]; ++e) elem_inst[e] = i;
+    std::vector<double> lam(ns, 0.0), mu(ns, 0.0);
+    std::vector<float> lam32(ns, 0.f), mu32(ns, 0.f);
+    for (size_t s = 0; s < ns; ++s) {
+        const int e = tl.h_tile_elem[s];
+        if (e < 0) continue;
+        const int i = elem_inst[e];
+        const double Ey = b->inst_E[i], nu = b->inst_nu[i];
+        // Lame parameters as SetSVK computes them (FEAT10Data.cuh:399-409)
+        mu[s] = Ey / (2.0 * (1.0 + nu));
+        lam[s] = Ey * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+        lam32[s] = (float)lam[s];
+        mu32[s] = (float)mu[s];
+    }
+    cudaStream_t st = el->stream;
+    TLFEA_CUDA(cudaMemcpyAsync(b->lam, lam.data(), ns * sizeof(double), cudaMemcpyHostToDevice, st));
+    TLFEA_CUDA(cudaMemcpyAsync(b->mu, mu.data(), ns * sizeof(double), cudaMemcpyHostToDevice, st));
+    TLFEA_CUDA(cudaMemcpyAsync(b->lam32, lam32.data(), ns * sizeof(float), cudaMemcpyHostToDevice, st));
+    TLFEA_CUDA(cudaMemcpyAsync(b->mu32, mu32.data(), ns * sizeof(float), cudaMemcpyHostToDevice, st));
+    TLFEA_CUDA(cudaStreamSynchronize(st));
+    return TLFEA_OK;
+}
+
+}  // namespace tlfea
+
+using namespace tlfea;
+
+#define CHECK_BATCH(b)                \
+    do {                              \
+        if (!(b)) {                   \
+            set_error("null batch");  \
+            return TLFEA_INVALID_ARG; \
+        }                             \
+    } while (0)
+
+extern "C" {
+
+int tlfea_batch_create(int type, int n_inst, const int* node_off, const int* elem_off, const double* qx,
+                       const double* qy, const double* qz, const double* qw, int n_qp, const double* x,
+                       const double* y, const double* z, const int* conn, tlfea_batch* out) {
+    if (!out) return TLFEA_INVALID_ARG;
+    *out = nullptr;
+    if ((type != TLFEA_TYPE_T10 && type != TLFEA_TYPE_T4) || n_inst <= 0 || !node_off || !elem_off || !x || !y ||
+        !z || !conn || !qx || !qy || !qz || !qw) {
+        set_error("batch_create: bad arguments");
+        return TLFEA_INVALID_ARG;
+    }
+    const int npe = (type == TLFEA_TYPE_T10) ? T10_NPE : T4_NPE;
+    const int nqp = (type == TLFEA_TYPE_T10) ? T10_NQP : T4_NQP;
+    if (node_off[0] != 0 || elem_off[0] != 0) {
+        set_error("batch_create: offsets must start at 0");
+        return TLFEA_INVALID_ARG;
+    }
+    for (int i = 0; i < n_inst; ++i)
+        if (node_off[i + 1] <= node_off[i] || elem_off[i + 1] <= elem_off[i]) {
+            set_error("batch_create: every instance needs nodes and elements");
+            return TLFEA_INVALID_ARG;
+        }
+    const long long Nl = node_off[n_inst], El = elem_off[n_inst];
+    if (3 * Nl >= (1LL << 31) || El * npe >= (1LL << 31)) {
+        set_error("batch_create: batch too large for 32-bit indices");
+        return TLFEA_INVALID_ARG;
+    }
+    const int N = (int)Nl, E = (int)El;
+    // combined column-major connectivity with global node ids
+    std::vector<int> gconn((size_t)E * npe);
+    std::vector<int> group((size_t)E);
+    for (int i = 0; i < n_inst; ++i) {
+        const int nb = node_off[i], nn = node_off[i + 1] - nb;
+        for (int e = elem_off[i]; e < elem_off[i + 1]; ++e) {
+            group[e] = i;
+            for (int a = 0; a < npe; ++a) {
+                const int l = conn[(size_t)e * npe + a];
+                if (l < 0 || l >= nn) {
+                    set_error("batch_create: connectivity index out of range of its instance");
+                    return TLFEA_INVALID_ARG;
+                }
+                gconn[e + (size_t)a * E] = nb + l;
+            }
+        }
+    }
+    tlfea_element el = nullptr;
+    int st = tlfea_element_create(type, E, N, &el);
+    if (st) return st;
+    tlfea_batch_s* b = new tlfea_batch_s();
+    b->type = type;
+    b->n_inst = n_inst;
+    b->N = N;
+    b->E = E;
+    b->el = el;
+    b->node_off.assign(node_off, node_off + n_inst + 1);
+    b->elem_off.assign(elem_off, elem_off + n_inst + 1);
+    b->inst_E.assign(n_inst, 0.0);
+    b->inst_nu.assign(n_inst, 0.0);
+    el->elem_group = std::move(group);
+    auto fail = [&](int s) {
+        tlfea_batch_destroy(b);
+        return s;
+    };
+    if (n_qp != nqp) {
+        set_error("batch_create: quadrature size does not match the element type");
+        return fail(TLFEA_SIZE_MISMATCH);
+    }
+    if ((st = tlfea_element_setup(el, qx, qy, qz, qw, n_qp, x, y, z, gconn.data()))) return fail(st);
+    if ((st = tlfea_element_calc_dndu_pre(el))) return fail(st);
+    const size_t ns = (size_t)el->tl.n_tiles * TILE_ELEMS;
+    const size_t n3 = 3 * (size_t)N;
+    {
+        std::vector<int> elem_inst((size_t)E), ti(2 * (size_t)el->tl.n_tiles);
+        for (int i = 0; i < n_inst; ++i)
+            for (int e = elem_off[i]; e < elem_off[i + 1]; ++e) elem_inst[e] = i;
+        for (int t = 0; t < el->tl.n_tiles; ++t) {
+            int lo = n_inst, hi = -1;
+            for (int k = 0; k < TILE_ELEMS; ++k) {
+                const int e = el->tl.h_tile_elem[(size_t)t * TILE_ELEMS + k];
+                if (e < 0) continue;
+                lo = std::min(lo, elem_inst[e]);
+                hi = std::max(hi, elem_inst[e]);
+            }
+            ti[2 * t] = lo;
+            ti[2 * t + 1] = hi;
+        }
+        if ((st = dalloc(&b->tile_inst, ti.size()))) return fail(st);
+        if (cudaMemcpy(b->tile_inst, ti.data(), ti.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+            set_error("batch_create: upload failed");
+            return fail(TLFEA_CUDA_ERROR);
+        }
+    }
+    if ((st = dalloc(&b->lam, ns)) || (st = dalloc(&b->mu, ns)) || (st = dalloc(&b->lam32, ns)) ||
+        (st = dalloc(&b->mu32, ns)) || (st = dalloc(&b->fixed, (size_t)N)) || (st = dalloc(&b->u, n3)) ||
+        (st = dalloc(&b->r, n3)) || (st = dalloc(&b->p, n3)) || (st = dalloc(&b->q, n3)) ||
+        (st = dalloc(&b->f, n3)) || (st = dalloc(&b->u0, n3)) || (st = dalloc(&b->rr, 2 * (size_t)n_inst)) ||
+        (st = dalloc(&b->fnorm, (size_t)n_inst)) || (st = dalloc(&b->rel, (size_t)n_inst)) ||
+        (st = dalloc(&b->iters, (size_t)n_inst)) || (st = dalloc(&b->status, (size_t)n_inst)) ||
+        (st = dalloc(&b->done, (size_t)n_inst)) || (st = dalloc(&b->n_done, 1)))
+        return fail(st);
+    cudaStream_t s = el->stream;
+    // nodes touched by no element carry no stiffness: they are held fixed
+    std::vector<unsigned char> fx((size_t)N, 1);
+    for (int k : gconn) fx[k] = 0;
+    if (cudaMemcpyAsync(b->fixed, fx.data(), (size_t)N, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemsetAsync(b->f, 0, n3 * sizeof(double), s) != cudaSuccess ||
+        cudaMemsetAsync(b->u, 0, n3 * sizeof(double), s) != cudaSuccess ||
+        cudaMemsetAsync(b->u0, 0, n3 * sizeof(double), s) != cudaSuccess ||
+        cudaMemsetAsync(b->iters, 0, n_inst * sizeof(int), s) != cudaSuccess ||
+        cudaMemsetAsync(b->status, 0, n_inst * sizeof(int), s) != cudaSuccess ||
+        cudaMemsetAsync(b->rel, 0, n_inst * sizeof(double), s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        set_error("batch_create: device initialisation failed");
+        return fail(TLFEA_CUDA_ERROR);
+    }
+    if ((st = build_chunks(b, 256))) return fail(st);
+    *out = b;
+    return TLFEA_OK;
+}
+
+int tlfea_batch_destroy(tlfea_batch b) {
+    CHECK_BATCH(b);
+    if (b->el) cudaSetDevice(b->el->device);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    dfree(b->lam); dfree(b->mu); dfree(b->lam32); dfree(b->mu32);
+    dfree(b->fixed); dfree(b->chunk_inst); dfree(b->chunk_beg); dfree(b->inst_chunk); dfree(b->tile_inst);
+    dfree(b->u); dfree(b->r); dfree(b->p); dfree(b->q); dfree(b->f); dfree(b->u0);
+    dfree(b->cpa); dfree(b->cpb); dfree(b->rr); dfree(b->fnorm); dfree(b->rel);
+    dfree(b->iters); dfree(b->status); dfree(b->done); dfree(b->n_done);
+    if (b->el) tlfea_element_destroy(b->el);
+    delete b;
+    return TLFEA_OK;
+}
+
+int tlfea_batch_get_counts(tlfea_batch b, int* n_inst, int* n_elem, int* n_nodes, int* n_tiles) {
+    CHECK_BATCH(b);
+    if (n_inst) *n_inst = b->n_inst;
+    if (n_elem) *n_elem = b->E;
+    if (n_nodes) *n_nodes = b->N;
+    if (n_tiles) *n_tiles = b->el->tl.n_tiles;
+    return TLFEA_OK;
+}
+
+int tlfea_batch_get_stream(tlfea_batch b, void** stream) {
+    CHECK_BATCH(b);
+    if (!stream) return TLFEA_INVALID_ARG;
+    *stream = (void*)b->el->stream;
+    return TLFEA_OK;
+}
+
+int tlfea_batch_set_material(tlfea_batch b, const double* E, const double* nu) {
+    CHECK_BATCH(b);
+    if (!E || !nu) return TLFEA_INVALID_ARG;
+    for (int i = 0; i < b->n_inst; ++i) {
+        if (!(E[i] > 0.0) || !(nu[i] > -1.0 && nu[i] < 0.5)) {
+            set_error("batch_set_material: need E > 0 and -1 < nu < 0.5");
+            return TLFEA_INVALID_ARG;
+        }
+        b->inst_E[i] = E[i];
+        b->inst_nu[i] = nu[i];
+    }
+    const int st = upload_material(b);
+    if (st) return st;
+    b->material_set = true;
+    return TLFEA_OK;
+}
+
+int tlfea_batch_set_fixed(tlfea_batch b, const int* nodes, int n) {
+    CHECK_BATCH(b);
+    if (n < 0 || (n > 0 && !nodes)) return TLFEA_INVALID_ARG;
+    std::vector<unsigned char> fx((size_t)b->N, 1);
+    for (int k : b->el->conn) fx[k] = 0;
+    for (int k = 0; k < n; ++k) {
+        if (nodes[k] < 0 || nodes[k] >= b->N) {
+            set_error("batch_set_fixed: node index out of range");
+            return TLFEA_INVALID_ARG;
+        }
+        fx[nodes[k]] = 1;
+    }
+    TLFEA_CUDA(cudaMemcpyAsync(b->fixed, fx.data(), (size_t)b->N, cudaMemcpyHostToDevice, b->el->stream));
+    TLFEA_CUDA(cudaStreamSynchronize(b->el->stream));
+    return TLFEA_OK;
+}
+
+int tlfea_batch_set_external_force(tlfea_batch b, const double* f, long long n, int on_device) {
+    CHECK_BATCH(b);
+    if (!f || n != 3LL * b->N) {
+        set_error("batch_set_external_force: need 3 * n_nodes values");
+        return TLFEA_SIZE_MISMATCH;
+    }
+    TLFEA_CUDA(cudaMemcpyAsync(b->f, f, (size_t)n * sizeof(double),
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->el->stream));
+    TLFEA_CUDA(cudaStreamSynchronize(b->el->stream));
+    return TLFEA_OK;
+}
+
+int tlfea_batch_set_initial_guess(tlfea_batch b, const double* u0, long long n, int on_device) {
+    CHECK_BATCH(b);
+    if (!u0) {
+        b->warm = false;
+        return TLFEA_OK;
+    }
+    if (n != 3LL * b->N) {
+        set_error("batch_set_initial_guess: need 3 * n_nodes values");
+        return TLFEA_SIZE_MISMATCH;
+    }
+    TLFEA_CUDA(cudaMemcpyAsync(b->u0, u0, (size_t)n * sizeof(double),
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->el->stream));
+    TLFEA_CUDA(cudaStreamSynchronize(b->el->stream));
+    b->warm = true;
+    return TLFEA_OK;
+}
+
+int tlfea_batch_set_precision(tlfea_batch b, int precision) {
+    CHECK_BATCH(b);
+    if (precision != TLFEA_PRECISION_FP64 && precision != TLFEA_PRECISION_FP32) return TLFEA_INVALID_ARG;
+    if (precision != b->precision && b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->precision = precision;
+    return TLFEA_OK;
+}
+
+int tlfea_batch_set_launch(tlfea_batch b, int blocks_per_sm, int chunk_nodes) {
+    CHECK_BATCH(b);
+    if (blocks_per_sm < 0 || (chunk_nodes != 0 && (chunk_nodes < 32 || chunk_nodes > 4096))) return TLFEA_INVALID_ARG;
+    if (chunk_nodes != 0 && chunk_nodes != b->chunk_nodes) {
+        const int st = build_chunks(b, chunk_nodes);
+        if (st) return st;
+    }
+    if (blocks_per_sm != b->blocks_per_sm && b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->blocks_per_sm = blocks_per_sm;
+    return TLFEA_OK;
+}
+
+int tlfea_batch_get_launch(tlfea_batch b, int* blocks_per_sm, int* chunk_nodes, int* grid) {
+    CHECK_BATCH(b);
+    if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
+    if (chunk_nodes) *chunk_nodes = b->chunk_nodes;
+    if (grid) {
+        int g = 0;
+        const int st = batch_dispatch_grid(b, b->blocks_per_sm, &g);
+        if (st) return st;
+        *grid = g;
+    }
+    return TLFEA_OK;
+}
+
+int tlfea_batch_solve(tlfea_batch b, double tol, int max_iter) {
+    CHECK_BATCH(b);
+    if (!b->material_set) {
+        set_error("batch_solve: set the material first");
+        return TLFEA_NOT_SETUP;
+    }
+    if (!(tol > 0.0) || max_iter < 0) return TLFEA_INVALID_ARG;
+    cudaStream_t st = b->el->stream;
+    int grid = 0;
+    int s = batch_dispatch_grid(b, b->blocks_per_sm, &grid);
+    if (s) return s;
+    // one persistent launch, captured once per (grid, tol, max_iter, warm)
+    if (!b->graph || b->graph_tol != tol || b->graph_max_iter != max_iter || b->graph_warm != b->warm ||
+        b->graph_grid != grid) {
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        TLFEA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e1 = cudaMemsetAsync(b->n_done, 0, sizeof(int), st);
+        const int rc = (e1 == cudaSuccess) ? batch_launch(b, grid, tol, max_iter, b->warm, st) : TLFEA_CUDA_ERROR;
+        cudaError_t e2 = cudaStreamEndCapture(st, &g);
+        if (rc != TLFEA_OK || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            set_error("batch_solve: capture of the persistent launch failed");
+            return TLFEA_CUDA_ERROR;
+        }
+        cudaError_t e3 = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) {
+            b->graph = nullptr;
+            set_error(std::string("batch_solve: cudaGraphInstantiate: ") + cudaGetErrorString(e3));
+            return TLFEA_CUDA_ERROR;
+        }
+        b->graph_tol = tol;
+        b->graph_max_iter = max_iter;
+        b->graph_warm = b->warm;
+        b->graph_grid = grid;
+    }
+    TLFEA_CUDA(cudaGraphLaunch(b->graph, st));
+    TLFEA_CUDA(cudaStreamSynchronize(st));
+    return TLFEA_OK;
+}
+
+int tlfea_batch_get_results(tlfea_batch b, int* iters, double* rel, int* status) {
+    CHECK_BATCH(b);
+    cudaStream_t st = b->el->stream;
+    const size_t n = (size_t)b->n_inst;
+    if (iters) TLFEA_CUDA(cudaMemcpyAsync(iters, b->iters, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (rel) TLFEA_CUDA(cudaMemcpyAsync(rel, b->rel, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (status) TLFEA_CUDA(cudaMemcpyAsync(status, b->status, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    TLFEA_CUDA(cudaStreamSynchronize(st));
+    return TLFEA_OK;
+}
+
+int tlfea_batch_retrieve_displacement(tlfea_batch b, double* u, long long n) {
+    CHECK_BATCH(b);
+    if (!u || n != 3LL * b->N) {
+        set_error("batch_retrieve_displacement: need 3 * n_nodes values");
+        return TLFEA_SIZE_MISMATCH;
+    }
+    TLFEA_CUDA(cudaMemcpyAsync(u, b->u, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->el->stream));
+    TLFEA_CUDA(cudaStreamSynchronize(b->el->stream));
+    return TLFEA_OK;
+}
+
+int tlfea_batch_device_ptrs(tlfea_batch b, double** u, double** f, double** u0) {
+    CHECK_BATCH(b);
+    if (u) *u = b->u;
+    if (f) *f = b->f;
+    if (u0) *u0 = b->u0;
+    return TLFEA_OK;
+}
+
+int tlfea_batch_apply(tlfea_batch b, const double* d_x, double* d_y) {
+    CHECK_BATCH(b);
+    if (!b->material_set) {
+        set_error("batch_apply: set the material first");
+        return TLFEA_NOT_SETUP;
+    }
+    if (!d_x || !d_y) return TLFEA_INVALID_ARG;
+    int grid = 0;
+    int s = batch_dispatch_grid(b, 0, &grid, true);
+    if (s) return s;
+    cudaStream_t st = b->el->stream;
+    const bool f32 = b->precision == TLFEA_PRECISION_FP32;
+    const bool t10 = b->el->npe == 10;
+    auto go = [&](auto tag, const void* fn, size_t smem) -> int {
+        using R = typename decltype(tag)::type;
+        BatchArgs<R> A = batch_args<R>(b);
+        void* args[] = {&A, (void*)&d_x, (void*)&d_y};
+        TLFEA_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(TILE_ELEMS), args, smem, st));
+        TLFEA_LAUNCHED(1);
+        return TLFEA_OK;
+    };
+    struct TD { using type = double; };
+    struct TF { using type = float; };
+    if (f32)
+        s = t10 ? go(TF{}, (const void*)k_batch_apply<float, 10, 5>, batch_smem<float>(b))
+                : go(TF{}, (const void*)k_batch_apply<float, 4, 1>, batch_smem<float>(b));
+    else
+        s = t10 ? go(TD{}, (const void*)k_batch_apply<double, 10, 5>, batch_smem<double>(b))
+                : go(TD{}, (const void*)k_batch_apply<double, 4, 1>, batch_smem<double>(b));
+    if (s) return s;
+    TLFEA_CUDA(cudaStreamSynchronize(st));
+    return TLFEA_OK;
+}
+
+// Autotuner: times `trial_iters` CG iterations of this batch for every
+// (blocks per SM, node-chunk size) candidate and keeps the fastest.  The
+// trials overwrite the solution vectors; solve afterwards.
+int tlfea_batch_autotune(tlfea_batch b, int trial_iters, int* best_blocks_per_sm, int* best_chunk, float* best_ms) {
+    CHECK_BATCH(b);
+    if (!b->material_set) {
+        set_error("batch_autotune: set the material first");
+        return TLFEA_NOT_SETUP;
+    }
+    if (trial_iters <= 0) trial_iters = 8;
+    cudaStream_t st = b->el->stream;
+    int max_grid = 0;
+    int s = batch_dispatch_grid(b, 0, &max_grid);
+    if (s) return s;
+    int sms = 0;
+    TLFEA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->el->device));
+    const int max_per_sm = std::max(1, max_grid / std::max(sms, 1));
+    const int chunks[] = {128, 256, 512, 1024};
+    cudaEvent_t e0, e1;
+    TLFEA_CUDA(cudaEventCreate(&e0));
+    TLFEA_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bb = max_per_sm, bc = b->chunk_nodes;
+    for (int c : chunks) {
+        if ((s = build_chunks(b, c))) break;
+        for (int per_sm = 1; per_sm <= max_per_sm; ++per_sm) {
+            const int grid = per_sm * sms;
+            float ms = 0.f;
+            for (int rep = 0; rep < 2 && !s; ++rep) {  // first run warms up
+                if (cudaMemsetAsync(b->n_done, 0, sizeof(int), st) != cudaSuccess) s = TLFEA_CUDA_ERROR;
+                cudaEventRecord(e0, st);
+                if (!s) s = batch_launch(b, grid, 1e-300, trial_iters, false, st);
+                cudaEventRecord(e1, st);
+                if (cudaEventSynchronize(e1) != cudaSuccess) s = TLFEA_CUDA_ERROR;
+                cudaEventElapsedTime(&ms, e0, e1);
+            }
+            if (s) break;
+            if (ms < best) {
+                best = ms;
+                bb = per_sm;
+                bc = c;
+            }
+        }
+        if (s) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s) return s;
+    if ((s = build_chunks(b, bc))) return s;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->blocks_per_sm = bb;
+    if (best_blocks_per_sm) *best_blocks_per_sm = bb;
+    if (best_chunk) *best_chunk = bc;
+    if (best_ms) *best_ms = best;
+    return TLFEA_OK;
+}
+
+}  // extern "C"

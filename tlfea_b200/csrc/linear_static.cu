@@ -223,7 +223,21 @@ __global__ void k_cg_init(int n, const double* __restrict__ f, double* u, double
 // sits at K[9*rb + c*nb + k].  One warp per node row, one lane per block: the
 // nine component loads of a lane are coalesced across the warp, independent
 // of each other and of the column-index load, and the component index is a
-// compile-time constant.
+// compile-time constant.  The next row's extent and first 32 column indices
+// are fetched while the current row is in flight, so the gather of p does not
+// wait behind a load of its own row's indices.
+__device__ __forceinline__ void spmv_block(const double* Kr, int nb, int k, int cj, const double* __restrict__ p,
+                                           double& a0, double& a1, double& a2) {
+    const double* kv = Kr + k;
+    double v[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) v[c] = __ldcs(kv + (size_t)c * nb);
+    const double p0 = p[3 * cj + 0], p1 = p[3 * cj + 1], p2 = p[3 * cj + 2];
+    a0 += v[0] * p0 + v[1] * p1 + v[2] * p2;
+    a1 += v[3] * p0 + v[4] * p1 + v[5] * p2;
+    a2 += v[6] * p0 + v[7] * p1 + v[8] * p2;
+}
+
 __global__ void __launch_bounds__(256) k_cg_spmv_dot(int N, const int* __restrict__ off, const int* __restrict__ col,
                                                      const double* __restrict__ K, const double* __restrict__ p,
                                                      double* q, double* partials, CgCtl* ctl) {
@@ -232,21 +246,24 @@ __global__ void __launch_bounds__(256) k_cg_spmv_dot(int N, const int* __restric
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     double pq = 0.0;
+    int rb = 0, nb = 0, cj = 0;
+    if (warp < N) {
+        rb = off[warp];
+        nb = off[warp + 1] - rb;
+        cj = (lane < nb) ? col[rb + lane] : 0;
+    }
     for (int i = warp; i < N; i += nwarps) {
-        const int rb = off[i], nb = off[i + 1] - rb;
+        const int in = i + nwarps;
+        int rbn = 0, nbn = 0;
+        if (in < N) {
+            rbn = off[in];
+            nbn = off[in + 1] - rbn;
+        }
         const double* Kr = K + 9LL * rb;
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        for (int k = lane; k < nb; k += 32) {
-            const double* kv = Kr + k;
-            double v[9];
-#pragma unroll
-            for (int c = 0; c < 9; ++c) v[c] = __ldcs(kv + (size_t)c * nb);
-            const int cj = col[rb + k];
-            const double p0 = p[3 * cj + 0], p1 = p[3 * cj + 1], p2 = p[3 * cj + 2];
-            a0 += v[0] * p0 + v[1] * p1 + v[2] * p2;
-            a1 += v[3] * p0 + v[4] * p1 + v[5] * p2;
-            a2 += v[6] * p0 + v[7] * p1 + v[8] * p2;
-        }
+        if (lane < nb) spmv_block(Kr, nb, lane, cj, p, a0, a1, a2);
+        for (int k = lane + 32; k < nb; k += 32) spmv_block(Kr, nb, k, col[rb + k], p, a0, a1, a2);
+        const int cjn = (lane < nbn) ? col[rbn + lane] : 0;
         a0 = warp_sum(a0);
         a1 = warp_sum(a1);
         a2 = warp_sum(a2);
@@ -256,6 +273,9 @@ __global__ void __launch_bounds__(256) k_cg_spmv_dot(int N, const int* __restric
             q[3 * i + 2] = a2;
             pq += p[3 * i + 0] * a0 + p[3 * i + 1] * a1 + p[3 * i + 2] * a2;
         }
+        rb = rbn;
+        nb = nbn;
+        cj = cjn;
     }
     double tot;
     if (last_block_sum(pq, partials, &ctl->ticket, &tot) && threadIdx.x == 0) {

@@ -146,3 +146,25 @@ def cantilever_loads(x, y, z, total_force=(0.0, 0.0, -100.0), tol_frac=1e-9):
     for d in range(3):
         f[3 * tip + d] = total_force[d] / len(tip)
     return fixed, f, tip
+
+
+def random_beam(seed: int, nx_range=(8, 64), ny_range=(2, 8), h=0.01, E_range=(1e6, 1e9), nu_range=(0.2, 0.45),
+                load_range=(1.0, 500.0), order: int = 10):
+    """One seeded cantilever of the uneven batch: nx ~ U{nx_range}, ny = nz ~
+    U{ny_range}, cross-section ny*h x ny*h, length 10*ny*h (cell length
+    10*ny*h/nx), E log-uniform, nu uniform, tip force with direction uniform on
+    the unit sphere and uniform magnitude, split over the free-end nodes;
+    the x = 0 face is clamped.  Returns a dict."""
+    r = np.random.default_rng(seed)
+    nx = int(r.integers(nx_range[0], nx_range[1] + 1))
+    ny = int(r.integers(ny_range[0], ny_range[1] + 1))
+    E = float(np.exp(r.uniform(np.log(E_range[0]), np.log(E_range[1]))))
+    nu = float(r.uniform(*nu_range))
+    d = r.standard_normal(3)
+    d /= np.linalg.norm(d)
+    mag = float(r.uniform(*load_range))
+    w = ny * h
+    x, y, z, conn = box_mesh(nx, ny, ny, order, 10.0 * w, w, w)
+    fixed, f, tip = cantilever_loads(x, y, z, tuple(mag * d))
+    return {"x": x, "y": y, "z": z, "conn": conn, "fixed": fixed, "f": f, "E": E, "nu": nu, "nx": nx, "ny": ny,
+            "direction": d, "magnitude": mag}
