@@ -81,6 +81,8 @@ typedef struct {
     int status;            /* TLFEA_OK, TLFEA_NONFINITE, TLFEA_BUDGET_EXCEEDED */
     double last_norm_g;    /* ||g|| at the last evaluated inner iteration */
     double kernel_ms;      /* device time of the solve (CUDA events) */
+    double rel_residual;   /* ||(f_int - f_ext)_free|| / ||f_ext|| at the last inner iteration (stop rule on) */
+    int stop_rule_met;     /* 1 if the relative-residual stop rule ended the solve */
 } tlfea_solve_stats;
 
 /* ------------------------------------------------------------- library */
@@ -242,6 +244,12 @@ int tlfea_solver_get_velocity(tlfea_solver s, double* v_guess, double* v_prev, i
 int tlfea_solver_set_velocity(tlfea_solver s, const double* v_guess, const double* v_prev, int n);
 int tlfea_solver_get_multipliers(tlfea_solver s, double* lam, int n);
 int tlfea_solver_get_stats(tlfea_solver s, tlfea_solve_stats* st);
+/* New (no reference counterpart): relative-residual stop rule of the Nesterov /
+ * AdamW solvers.  With rel_tol > 0 every inner iteration also evaluates
+ * ||(f_int - f_ext)_free|| / ||f_ext|| in FP64 (free = not a fixed node) at the
+ * positions the internal force was computed at, and the solve ends -- keeping
+ * those positions -- once it is below rel_tol.  0 turns it off (default). */
+int tlfea_solver_set_stop_rule(tlfea_solver s, double rel_tol);
 
 /* ------------------------------------------------- batched linear static
  * New, no reference counterpart: many independent meshes solved by one

@@ -63,7 +63,8 @@ class AdamWParams(C.Structure):
 
 class SolveStats(C.Structure):
     _fields_ = [("outer_iters", C.c_int), ("inner_iters_total", C.c_int), ("last_inner_iters", C.c_int),
-                ("status", C.c_int), ("last_norm_g", C.c_double), ("kernel_ms", C.c_double)]
+                ("status", C.c_int), ("last_norm_g", C.c_double), ("kernel_ms", C.c_double),
+                ("rel_residual", C.c_double), ("stop_rule_met", C.c_int)]
 
 
 _P = C.c_void_p
@@ -133,6 +134,7 @@ _SIGS = {
     "tlfea_solver_set_velocity": [_P, _D, _D, C.c_int],
     "tlfea_solver_get_multipliers": [_P, _D, C.c_int],
     "tlfea_solver_get_stats": [_P, C.POINTER(SolveStats)],
+    "tlfea_solver_set_stop_rule": [_P, C.c_double],
     "tlfea_batch_create": [C.c_int, C.c_int, _I, _I, _D, _D, _D, _D, C.c_int, _D, _D, _D, _I, C.POINTER(_P)],
     "tlfea_batch_destroy": [_P],
     "tlfea_batch_get_counts": [_P, _I, _I, _I, _I],

@@ -367,6 +367,11 @@ class _FirstOrder(SolverBase):
         capi.call("tlfea_solver_get_stats", self._h, C.byref(st))
         return {f: getattr(st, f) for f, _ in st._fields_}
 
+    def SetRelativeResidualStop(self, rel_tol: float):
+        """New: end Solve() once ||(f_int - f_ext)_free|| / ||f_ext|| < rel_tol
+        (FP64, evaluated every inner iteration); 0 turns the rule off."""
+        capi.call("tlfea_solver_set_stop_rule", self._h, float(rel_tol))
+
     def __del__(self):
         try:
             if getattr(self, "_h", None) is not None:

@@ -282,8 +282,6 @@ static void free_tiling(Tiling& tl) {
     dfree(tl.dv32);
     dfree(tl.partial64);
     dfree(tl.partial32);
-    dfree(tl.pslot_bnode);
-    dfree(tl.bnode_cnt);
     tl = Tiling();
 }
 
@@ -455,12 +453,6 @@ static int build_tiling(tlfea_element_s* h, const double* x, const double* y, co
     if ((st = upload(&tl.bnode_off, boff, h->stream))) return st;
     if ((st = upload(&tl.bnode_slots, bslots, h->stream))) return st;
     if ((st = upload(&tl.node_bidx, node_bidx, h->stream))) return st;
-    std::vector<int> pslot_bnode((size_t)std::max(n_pslots, 1), 0);
-    for (size_t b = 0; b < bgid.size(); ++b)
-        for (int k = boff[b]; k < boff[b + 1]; ++k) pslot_bnode[bslots[k]] = (int)b;
-    if ((st = upload(&tl.pslot_bnode, pslot_bnode, h->stream))) return st;
-    if ((st = dalloc(&tl.bnode_cnt, (size_t)std::max(tl.n_bnodes, 1)))) return st;
-    TLFEA_CUDA(cudaMemsetAsync(tl.bnode_cnt, 0, sizeof(int) * (size_t)std::max(tl.n_bnodes, 1), h->stream));
     const size_t ng = (size_t)n_tiles * h->nqp * npe * 3 * TE;
     const size_t nd = (size_t)n_tiles * h->nqp * TE;
     if ((st = dalloc(&tl.grad64, ng))) return st;
@@ -665,15 +657,8 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
         st = damp ? launch_tiles<R, NPE, NQP, TILE_FORCE, true>(h, A) : launch_tiles<R, NPE, NQP, TILE_FORCE, false>(h, A);
     else if (h->force_kernel == 2)
         st = damp ? launch_pipe<R, NPE, NQP, true>(h, A) : launch_pipe<R, NPE, NQP, false>(h, A);
-    else {
-        // shared nodes are combined inside the kernel (no k_combine launch)
-        A.pslot_b = h->tl.pslot_bnode;
-        A.bnode_off = h->tl.bnode_off;
-        A.bnode_slots = h->tl.bnode_slots;
-        A.bnode_gid = h->tl.bnode_gid;
-        A.bcnt = h->tl.bnode_cnt;
-        return damp ? launch_tile_tma<R, NPE, NQP, true>(h, A) : launch_tile_tma<R, NPE, NQP, false>(h, A);
-    }
+    else
+        st = damp ? launch_tile_tma<R, NPE, NQP, true>(h, A) : launch_tile_tma<R, NPE, NQP, false>(h, A);
     if (st) return st;
     return launch_combine<R, false>(h, A.partial, A.f_out);
 }

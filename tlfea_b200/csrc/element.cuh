@@ -48,8 +48,6 @@ struct Tiling {
     int* bnode_off = nullptr;       // n_bnodes + 1
     int* bnode_slots = nullptr;     // n_pslots
     int* node_bidx = nullptr;       // N, boundary index or -1
-    int* pslot_bnode = nullptr;     // n_pslots, boundary index of each partial slot
-    int* bnode_cnt = nullptr;       // n_bnodes, arrivals of the current force launch (0 between launches)
     double* grad64 = nullptr;
     double* dv64 = nullptr;
     float* grad32 = nullptr;
@@ -80,13 +78,6 @@ struct TileArgs {
     R* partial;       // 3 * n_pslots
     R lambda, mu, eta, lamd;
     int max_local;
-    // optional in-kernel combine of shared nodes (k_tile_force_tma): the last
-    // tile to write a shared node's partial sums them in tile order
-    const int* pslot_b = nullptr;
-    const int* bnode_off = nullptr;
-    const int* bnode_slots = nullptr;
-    const int* bnode_gid = nullptr;
-    int* bcnt = nullptr;
 };
 
 // Tile routine modes.

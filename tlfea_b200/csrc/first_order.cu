@@ -12,12 +12,15 @@
 //     the per-block partials in block order, so every block takes the same
 //     branch without another barrier) instead of one thread's serial loop;
 //   * about 4 grid barriers per inner iteration instead of 13.
-//   * a non-finite ||g|| ends the solve with TLFEA_NONFINITE.
+//   * a non-finite ||g|| ends the solve with TLFEA_NONFINITE;
+//   * optional relative-residual stop rule (new): ||(f_int - f_ext)_free|| /
+//     ||f_ext|| < rel_tol in FP64 at the positions of the last force evaluation.
 #include <cooperative_groups.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "solver.cuh"
 
@@ -48,8 +51,11 @@ struct FOArgs {
     double *vg, *vp, *vk, *vkm1, *g, *lam, *m, *va, *xp, *yp, *zp;
     double* red;
     int red_stride;
-    int* stat;          // [outer, inner_total, last_inner, status]
+    int* stat;          // [outer, inner_total, last_inner, status, ||g|| (2 ints), rel (2 ints), rule met]
     double* stat_norm;  // last ||g||
+    double* stat_rel;   // last ||(f_int - f_ext)_free|| / ||f_ext|| (stop rule on)
+    double rel_tol;     // relative-residual stop rule (0 = off)
+    const unsigned char* node_fixed;
     // parameters (SyncedNesterovParams / SyncedAdamWParams)
     double alpha, rho, inner_tol, outer_tol, dt;
     int max_outer, max_inner;
@@ -168,15 +174,22 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
     const int check = S.check > 0 ? S.check : 1;
     const int eff_outer = (nocoop && S.nc == 0) ? 1 : S.max_outer;
 
+    const bool rule = S.rel_tol > 0.0;
+    double sf = 0.0;
     for (int i = gt; i < N; i += gs) {
         S.xp[i] = S.x[i];
         S.yp[i] = S.y[i];
         S.zp[i] = S.z[i];
+        if (rule)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) sf += S.f_ext[3 * i + d] * S.f_ext[3 * i + d];
     }
+    if (rule) write_partial(S, 5, sf, red_sh);
     grid.sync();
+    const double fext_norm = rule ? sqrt(fold_partials(S, 5, &fold_sh)) : 0.0;
 
-    int outer_flag = 0, status = 0, n_outer = 0, inner_total = 0, last_inner = 0;
-    double last_norm = 0.0;
+    int outer_flag = 0, status = 0, n_outer = 0, inner_total = 0, last_inner = 0, rule_met = 0;
+    double last_norm = 0.0, last_rel = -1.0;
     for (int outer = 0; outer < eff_outer && !outer_flag && !status; ++outer) {
         ++n_outer;
         double t = 1.0, prev_norm_g = 0.0, norm_g = 0.0, norm_g0 = -1.0, lr = S.lr;
@@ -253,27 +266,45 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
             grid.sync();
             // ---- P3: gradient per node and the norm partials
             const bool do_check = nesterov || (inner % check == 0);
-            double sg = 0.0, sv = 0.0;
+            double sg = 0.0, sv = 0.0, sr = 0.0;
             for (int i = gt; i < N; i += gs) {
                 double f[3], gi[3];
                 node_force<R>(S, A, i, f);
                 grad_node(S, i, f, gi);
+                const bool free_node = rule && !S.node_fixed[i];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     S.g[3 * i + d] = gi[d];
                     sg += gi[d] * gi[d];
                     if (!nesterov) sv += S.vg[3 * i + d] * S.vg[3 * i + d];
+                    if (free_node) {
+                        const double rd = f[d] - S.f_ext[3 * i + d];
+                        sr += rd * rd;
+                    }
                 }
             }
             if (do_check) {
                 write_partial(S, 0, sg, red_sh);
                 if (!nesterov) write_partial(S, 1, sv, red_sh);
+                if (rule) write_partial(S, 4, sr, red_sh);
             }
             grid.sync();
+            bool rule_now = false;
+            if (rule && do_check) {
+                const double rr = sqrt(fold_partials(S, 4, &fold_sh));
+                last_rel = fext_norm > 0.0 ? rr / fext_norm : rr;
+                rule_now = last_rel < S.rel_tol;
+            }
             if (nesterov) {
                 // ---- P4: ||g|| test, v_next = y - alpha g, norm partials of v_next and v_k
                 norm_g = sqrt(fold_partials(S, 0, &fold_sh));
                 if (!isfinite(norm_g)) status = TLFEA_NONFINITE;
+                if (rule_now) {
+                    // stop at the positions the residual was measured at (v = y)
+                    inner_flag = 1;
+                    rule_met = 1;
+                    break;
+                }
                 if (inner > 0 && fabs(norm_g - prev_norm_g) < S.inner_tol) inner_flag = 1;
                 double snv = 0.0, snk = 0.0;
                 for (int i = gt; i < n3; i += gs) {
@@ -300,6 +331,10 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
                 const double tol_abs = S.inner_tol * (1.0 + nv);
                 const double tol_rel = (S.rtol > 0.0 && norm_g0 > 0.0) ? (S.rtol * norm_g0) : 0.0;
                 if (norm_g <= tol_abs || (tol_rel > 0.0 && norm_g <= tol_rel)) inner_flag = 1;
+                if (rule_now) {
+                    inner_flag = 1;
+                    rule_met = 1;
+                }
             }
             if (status) break;
         }
@@ -332,7 +367,9 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
         write_partial(S, 3, sc, red_sh);
         grid.sync();
         const double norm_c = sqrt(fold_partials(S, 3, &fold_sh));
-        if (nocoop) {
+        if (rule_met) {
+            outer_flag = 1;
+        } else if (nocoop) {
             if (S.nc > 0 && norm_c < S.outer_tol && inner_flag) outer_flag = 1;
         } else if (fabs(norm_c) < S.outer_tol) {
             outer_flag = 1;
@@ -346,6 +383,8 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
         S.stat[2] = last_inner;
         S.stat[3] = status;
         *S.stat_norm = last_norm;
+        *S.stat_rel = last_rel;
+        S.stat[8] = rule_met;
     }
 }
 
@@ -382,8 +421,9 @@ int first_order_alloc(tlfea_solver_s* s) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, el->device);
     s->max_blocks = std::max(1, sms * 16);
-    st |= dalloc(&s->red, (size_t)4 * s->max_blocks);
-    st |= dalloc(&s->dstat, 8);
+    st |= dalloc(&s->red, (size_t)6 * s->max_blocks);
+    st |= dalloc(&s->dstat, 16);
+    st |= dalloc(&s->node_fixed, N);
     if (st) return TLFEA_CUDA_ERROR;
     return TLFEA_OK;
 }
@@ -392,7 +432,7 @@ void first_order_free(tlfea_solver_s* s) {
     dfree(s->v_guess); dfree(s->v_prev); dfree(s->v_k); dfree(s->v_km1);
     dfree(s->g); dfree(s->m); dfree(s->va); dfree(s->lam);
     dfree(s->xp); dfree(s->yp); dfree(s->zp);
-    dfree(s->red); dfree(s->dstat);
+    dfree(s->red); dfree(s->dstat); dfree(s->node_fixed);
 }
 
 int first_order_solve(tlfea_solver_s* s) {
@@ -452,6 +492,15 @@ int first_order_solve(tlfea_solver_s* s) {
     S.red_stride = s->max_blocks;
     S.stat = s->dstat;
     S.stat_norm = (double*)(s->dstat + 4);
+    S.stat_rel = (double*)(s->dstat + 6);
+    S.rel_tol = s->rel_tol;
+    S.node_fixed = s->node_fixed;
+    if (s->rel_tol > 0.0) {
+        std::vector<unsigned char> nf((size_t)el->N, 0);
+        for (int n : el->h_fixed) nf[n] = 1;
+        TLFEA_CUDA(cudaMemcpyAsync(s->node_fixed, nf.data(), nf.size(), cudaMemcpyHostToDevice, el->stream));
+        TLFEA_CUDA(cudaStreamSynchronize(el->stream));
+    }
     if (s->kind == KIND_NESTEROV) {
         S.alpha = s->np.alpha; S.rho = s->np.rho; S.inner_tol = s->np.inner_tol; S.outer_tol = s->np.outer_tol;
         S.max_outer = s->np.max_outer; S.max_inner = s->np.max_inner; S.dt = s->np.time_step;
@@ -505,13 +554,15 @@ int first_order_solve(tlfea_solver_s* s) {
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    int hs[8];
+    int hs[16];
     TLFEA_CUDA(cudaMemcpy(hs, s->dstat, sizeof(hs), cudaMemcpyDeviceToHost));
     s->stats.outer_iters = hs[0];
     s->stats.inner_iters_total = hs[1];
     s->stats.last_inner_iters = hs[2];
     s->stats.status = hs[3];
     memcpy(&s->stats.last_norm_g, hs + 4, sizeof(double));
+    memcpy(&s->stats.rel_residual, hs + 6, sizeof(double));
+    s->stats.stop_rule_met = hs[8];
     s->stats.kernel_ms = ms;
     el->f_int_from32 = fp32;
     el->u_dirty = !fp32;  // the kernel keeps u in step with x in FP32 mode

@@ -384,9 +384,7 @@ struct TileTmaGeom {
 
 // Byte offsets of the regions of k_tile_force_tma's shared memory, each
 // 16-byte aligned: [stage 0 | stage 1, later the element forces][lconn][incidence]
-// [positions][node destination][incidence end][velocities][2 mbarriers].
-// Positions: FP32 one (x, y, z, 0) float4 per local node (one 16-byte load per
-// node); FP64 an (x, y) double2 per node, then z.
+// [x y z][node destination][incidence end][velocities][2 mbarriers].
 template <typename R, int NPE>
 struct TileTmaLayout {
     size_t inc, pos, dst, iend, vel, bar, total;
@@ -395,7 +393,7 @@ struct TileTmaLayout {
         auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
         inc = 2 * (size_t)G::STAGE_BYTES + G::LCONN_BYTES;
         pos = inc + G::INC_BYTES;
-        dst = al(pos + (sizeof(R) == 4 ? 16 : 24) * (size_t)max_local);
+        dst = al(pos + 3 * (size_t)max_local * sizeof(R));
         iend = al(dst + (size_t)max_local * sizeof(int));
         vel = al(iend + (size_t)max_local * sizeof(uint16_t));
         bar = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
@@ -419,7 +417,9 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
     unsigned char* stage0 = smem;
     const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + 2 * G::STAGE_BYTES);
     const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
-    unsigned char* pos = smem + L.pos;
+    R* xs = reinterpret_cast<R*>(smem + L.pos);
+    R* ys = xs + ML;
+    R* zs = ys + ML;
     int* dsts = reinterpret_cast<int*>(smem + L.dst);  // global node id, or -(partial slot + 1)
     uint16_t* iends = reinterpret_cast<uint16_t*>(smem + L.iend);
     double* vs = reinterpret_cast<double*>(smem + L.vel);
@@ -452,12 +452,9 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
         const int ps = A.ln_pslot[lb + ln];
         iends[ln] = A.ln_inc_end[lb + ln];
         dsts[ln] = (ps < 0) ? gid : -(ps + 1);
-        if constexpr (sizeof(R) == 4) {
-            reinterpret_cast<float4*>(pos)[ln] = make_float4(A.px[gid], A.py[gid], A.pz[gid], 0.f);
-        } else {
-            reinterpret_cast<double2*>(pos)[ln] = make_double2(A.px[gid], A.py[gid]);
-            reinterpret_cast<double*>(pos + 16 * (size_t)ML)[ln] = A.pz[gid];
-        }
+        xs[ln] = A.px[gid];
+        ys[ln] = A.py[gid];
+        zs[ln] = A.pz[gid];
         if (DAMP) {
             vs[3 * ln + 0] = A.v[3 * gid + 0];
             vs[3 * ln + 1] = A.v[3 * gid + 1];
@@ -500,8 +497,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
                 for (int j = 0; j < 3; ++j) F[i][j] = 0.0;
 #pragma unroll
             for (int a = 0; a < NPE; ++a) {
-                const double2 xy = reinterpret_cast<const double2*>(pos)[lc[a]];
-                const double xa[3] = {xy.x, xy.y, reinterpret_cast<const double*>(pos + 16 * (size_t)ML)[lc[a]]};
+                const double xa[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -534,8 +530,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
                 for (int j = 0; j < 3; ++j) H[i][j] = R(0);
 #pragma unroll
             for (int a = 0; a < NPE; ++a) {
-                const float4 u4 = reinterpret_cast<const float4*>(pos)[lc[a]];
-                const R ua[3] = {R(u4.x), R(u4.y), R(u4.z)};
+                const R ua[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -626,28 +621,6 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
             A.partial[3 * ps + 0] = s0;
             A.partial[3 * ps + 1] = s1;
             A.partial[3 * ps + 2] = s2;
-            if (A.bcnt) {
-                // the last of the node's tiles sums its partials in tile order
-                // (the order k_combine uses), then re-arms the counter
-                __threadfence();
-                const int b = A.pslot_b[ps];
-                const int kb = A.bnode_off[b], ke = A.bnode_off[b + 1];
-                if (atomicAdd(A.bcnt + b, 1) == ke - kb - 1) {
-                    __threadfence();
-                    R t0 = R(0), t1 = R(0), t2 = R(0);
-                    for (int k = kb; k < ke; ++k) {
-                        const int sl = A.bnode_slots[k];
-                        t0 += __ldcg(A.partial + 3 * sl + 0);
-                        t1 += __ldcg(A.partial + 3 * sl + 1);
-                        t2 += __ldcg(A.partial + 3 * sl + 2);
-                    }
-                    const int gid = A.bnode_gid[b];
-                    A.f_out[3 * gid + 0] = t0;
-                    A.f_out[3 * gid + 1] = t1;
-                    A.f_out[3 * gid + 2] = t2;
-                    A.bcnt[b] = 0;
-                }
-            }
         }
     }
 }

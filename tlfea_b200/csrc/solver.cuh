@@ -31,7 +31,9 @@ struct tlfea_solver_s {
     double *v_guess = nullptr, *v_prev = nullptr, *v_k = nullptr, *v_km1 = nullptr;
     double *g = nullptr, *lam = nullptr, *m = nullptr, *va = nullptr;
     double *xp = nullptr, *yp = nullptr, *zp = nullptr;
-    double* red = nullptr;   // per-block partial sums (3 arrays of max_blocks)
+    double* red = nullptr;   // per-block partial sums (6 arrays of max_blocks)
+    double rel_tol = 0.0;    // relative-residual stop rule (0 = off)
+    unsigned char* node_fixed = nullptr;  // N, for the stop rule's free-DOF norm
     int max_blocks = 0;
     int* dstat = nullptr;    // device diagnostics (tlfea_solve_stats fields)
     tlfea_nesterov_params np{};

@@ -180,4 +180,14 @@ int tlfea_solver_get_stats(tlfea_solver s, tlfea_solve_stats* st) {
     return TLFEA_OK;
 }
 
+int tlfea_solver_set_stop_rule(tlfea_solver s, double rel_tol) {
+    if (!s || !(rel_tol >= 0.0)) return TLFEA_INVALID_ARG;
+    if (s->kind == tlfea::KIND_LINEAR_STATIC) {
+        tlfea::set_error("the stop rule applies to the Nesterov / AdamW solvers (CG has its own tolerance)");
+        return TLFEA_UNSUPPORTED;
+    }
+    s->rel_tol = rel_tol;
+    return TLFEA_OK;
+}
+
 }  // extern "C"
