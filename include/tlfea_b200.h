@@ -268,6 +268,14 @@ typedef struct tlfea_batch_s* tlfea_batch;
 int tlfea_batch_create(int type, int n_inst, const int* node_off, const int* elem_off, const double* qx,
                        const double* qy, const double* qz, const double* qw, int n_qp, const double* x,
                        const double* y, const double* z, const int* conn, tlfea_batch* out);
+/* Shared-mesh batch: n_inst instances of ONE mesh (n_nodes nodes, n_elem
+ * elements, conn row-major [n_elem][npe]) that differ only in material, fixed
+ * nodes and loads.  The mesh's tiling and gradients are stored once; node
+ * vectors are concatenated instance by instance (instance i owns nodes
+ * [i*n_nodes, (i+1)*n_nodes)).  Every other batch call works unchanged. */
+int tlfea_batch_create_shared(int type, int n_inst, int n_nodes, int n_elem, const double* qx, const double* qy,
+                              const double* qz, const double* qw, int n_qp, const double* x, const double* y,
+                              const double* z, const int* conn, tlfea_batch* out);
 int tlfea_batch_destroy(tlfea_batch b);
 int tlfea_batch_get_counts(tlfea_batch b, int* n_inst, int* n_elem, int* n_nodes, int* n_tiles);
 int tlfea_batch_get_stream(tlfea_batch b, void** stream);

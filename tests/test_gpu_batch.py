@@ -184,3 +184,45 @@ def test_batch_autotune_and_replay_determinism():
     u3 = b.RetrieveDisplacement(split=False)
     assert rel(u3, u1) < 1e-7
     b.Destroy()
+
+
+@pytest.mark.parametrize("order", [10, 4])
+def test_shared_mesh_batch_matches_the_general_batch(order):
+    """One mesh, many materials / loads / fixed sets: the shared-mesh batch (one
+    tiling for all instances) gives the general batch's products and solutions."""
+    import torch
+
+    d0 = M.random_beam(7, order=order, **SMALL)
+    n = 5
+    r = np.random.default_rng(3)
+    E = np.exp(r.uniform(np.log(1e6), np.log(1e9), n))
+    nu = r.uniform(0.2, 0.45, n)
+    loads = [d0["f"] * s for s in r.uniform(0.5, 2.0, n)]
+    fixed = [d0["fixed"]] * (n - 1) + [np.concatenate([d0["fixed"], [len(d0["x"]) - 1]])]
+    mesh = (d0["x"], d0["y"], d0["z"], d0["conn"])
+    T_ = T.TYPE_T10 if order == 10 else T.TYPE_T4
+    bs = T.BatchedLinearStaticSolver([mesh] * n, T_, shared=True)
+    bg = T.BatchedLinearStaticSolver([mesh] * n, T_)
+    for b in (bs, bg):
+        b.SetMaterial(E, nu)
+        b.SetNodalFixed(fixed)
+        b.SetExternalForce(loads)
+    assert bs.GetCounts()["nodes"] == bg.GetCounts()["nodes"]
+    xv = torch.tensor(r.standard_normal(3 * bs.n_nodes), device="cuda")
+    ys, yg = torch.empty_like(xv), torch.empty_like(xv)
+    torch.cuda.synchronize()
+    bs.Apply(xv.data_ptr(), ys.data_ptr())
+    bg.Apply(xv.data_ptr(), yg.data_ptr())
+    assert rel(ys.cpu().numpy(), yg.cpu().numpy()) < 1e-12
+    for b in (bs, bg):
+        b.Solve(1e-9, 20000)
+    us, ug = bs.RetrieveDisplacement(split=False), bg.RetrieveDisplacement(split=False)
+    its, itg = bs.GetResults()[0], bg.GetResults()[0]
+    assert rel(us, ug) < 1e-7 and np.all(np.abs(its - itg) <= np.maximum(5, 0.05 * itg))
+    for k in range(n):  # each instance against the oracle's assembled system
+        d = dict(d0, E=E[k], nu=nu[k], f=loads[k], fixed=fixed[k])
+        off, cols, kv, fb = _oracle_kbc(d)
+        u_dir = spla.spsolve(sp.csr_matrix((kv, cols, off)).tocsc(), fb)
+        assert rel(us[3 * k * len(d0["x"]):3 * (k + 1) * len(d0["x"])], u_dir) < 1e-6
+    bs.Destroy()
+    bg.Destroy()

@@ -136,6 +136,8 @@ _SIGS = {
     "tlfea_solver_get_stats": [_P, C.POINTER(SolveStats)],
     "tlfea_solver_set_stop_rule": [_P, C.c_double],
     "tlfea_batch_create": [C.c_int, C.c_int, _I, _I, _D, _D, _D, _D, C.c_int, _D, _D, _D, _I, C.POINTER(_P)],
+    "tlfea_batch_create_shared": [C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, _D, _D, C.c_int, _D, _D, _D, _I,
+                                  C.POINTER(_P)],
     "tlfea_batch_destroy": [_P],
     "tlfea_batch_get_counts": [_P, _I, _I, _I, _I],
     "tlfea_batch_get_stream": [_P, C.POINTER(_P)],

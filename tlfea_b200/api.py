@@ -473,7 +473,13 @@ class BatchedLinearStaticSolver:
     does not wait for other streams.
     """
 
-    def __init__(self, meshes, element_type: int = TYPE_T10):
+    def __init__(self, meshes, element_type: int = TYPE_T10, shared: bool = False):
+        """shared=True: every entry of `meshes` is the same mesh (one tiling and
+        gradient stream serve all instances; only material, fixed nodes and loads
+        differ).  Pass the mesh once and the count: meshes=[mesh] * n."""
+        if shared:
+            self._init_shared(meshes[0], len(meshes), element_type)
+            return
         if element_type not in (TYPE_T10, TYPE_T4):
             raise TLFEAError(capi.INVALID_ARG, "BatchedLinearStaticSolver", "element type must be TYPE_T10 or TYPE_T4")
         npe = 10 if element_type == TYPE_T10 else 4
@@ -494,6 +500,25 @@ class BatchedLinearStaticSolver:
         capi.call("tlfea_batch_create", int(element_type), self.n_inst, capi.iptr(self.node_off),
                   capi.iptr(self.elem_off), capi.dptr(qx), capi.dptr(qy), capi.dptr(qz), capi.dptr(qw), len(qw),
                   capi.dptr(x), capi.dptr(y), capi.dptr(z), capi.iptr(conn), C.byref(h))
+        self._h = h
+        self.n_nodes = int(self.node_off[-1])
+
+    def _init_shared(self, mesh, n, element_type):
+        if element_type not in (TYPE_T10, TYPE_T4):
+            raise TLFEAError(capi.INVALID_ARG, "BatchedLinearStaticSolver", "element type must be TYPE_T10 or TYPE_T4")
+        npe = 10 if element_type == TYPE_T10 else 4
+        q = Quadrature.t10() if element_type == TYPE_T10 else Quadrature.t4()
+        x, y, z, conn = _f64(mesh[0]), _f64(mesh[1]), _f64(mesh[2]), np.asarray(mesh[3], dtype=np.int32)
+        nn, ne = len(x), conn.shape[0]
+        self.n_inst = int(n)
+        self.node_off = (np.arange(self.n_inst + 1) * nn).astype(np.int32)
+        self.elem_off = (np.arange(self.n_inst + 1) * ne).astype(np.int32)
+        qx, qy, qz, qw = (_f64(a) for a in q)
+        c = _i32(conn.reshape(-1, npe))
+        h = C.c_void_p()
+        capi.call("tlfea_batch_create_shared", int(element_type), self.n_inst, nn, ne, capi.dptr(qx), capi.dptr(qy),
+                  capi.dptr(qz), capi.dptr(qw), len(qw), capi.dptr(x), capi.dptr(y), capi.dptr(z), capi.iptr(c),
+                  C.byref(h))
         self._h = h
         self.n_nodes = int(self.node_off[-1])
 

@@ -21,6 +21,12 @@
 // element tiles (K p), then over node chunks (segmented FP64 dots, vector
 // updates); four grid barriers per iteration; per-instance scalars are folded
 // redundantly and deterministically by every block that needs them.
+//
+// Shared-mesh mode: when every instance is the same mesh (only material and
+// loads differ) the batch keeps ONE tiling and one gradient stream, and the
+// tile loop runs over (instance, tile) pairs.  Consecutive work items then
+// reuse the same tiles, so the gradient stream is read from L2 and HBM carries
+// little more than the per-instance vectors.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -41,8 +47,11 @@ struct tlfea_batch_s {
     std::vector<double> inst_E, inst_nu;
     int precision = TLFEA_PRECISION_FP64;
     // device
-    double *lam = nullptr, *mu = nullptr;  // per element slot (n_tiles * TILE_ELEMS)
+    double *lam = nullptr, *mu = nullptr;  // per element slot (n_tiles * TILE_ELEMS), shared mode: per instance
     float *lam32 = nullptr, *mu32 = nullptr;
+    bool shared = false;                   // every instance is one mesh (el holds it once)
+    double* part64 = nullptr;              // shared mode: per-instance partial slots
+    float* part32 = nullptr;
     unsigned char* fixed = nullptr;        // per node
     int* chunk_inst = nullptr;             // per chunk
     int* chunk_beg = nullptr;              // n_chunks + 1 node offsets
@@ -84,7 +93,10 @@ struct BatchArgs {
     const int* node_bidx;
     const int* bnode_off;
     const int* bnode_slots;
-    int n_tiles, max_local;
+    int n_tiles, max_local;  // n_tiles: work items (shared mode: instances x mesh tiles)
+    // shared mode: every instance is one mesh of tiles_per_inst tiles, nodes_per_inst
+    // nodes and pslots_per_inst partial slots; 0 otherwise
+    int tiles_per_inst, nodes_per_inst, pslots_per_inst;
     // nodes and instances
     int N, n_inst, n_chunks;
     const unsigned char* fixed;
@@ -104,15 +116,23 @@ struct BatchArgs {
 // node in the tile's fixed incidence order.  Interior nodes are written to q,
 // nodes shared with other tiles to their partial slot.
 template <typename R, int NPE, int NQP>
-__device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int tile, const double* p, double* q,
+__device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int item, const double* p, double* q,
                                             unsigned char* smem) {
     constexpr int TE = TILE_ELEMS;
     const int t = threadIdx.x;
+    // work item -> mesh tile, and the instance's node and partial-slot offsets
+    int tile = item, noff = 0, poff = 0, inst = 0;
+    if (A.tiles_per_inst) {
+        inst = item / A.tiles_per_inst;
+        tile = item - inst * A.tiles_per_inst;
+        noff = inst * A.nodes_per_inst;
+        poff = inst * A.pslots_per_inst;
+    }
     R* ps = reinterpret_cast<R*>(smem);  // 3 * max_local, interleaved
     R* fe = ps + 3 * A.max_local;        // 3 * NPE * TE
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
     for (int ln = t; ln < nl; ln += TE) {
-        const int gid = A.ln_gid[lb + ln];
+        const int gid = noff + A.ln_gid[lb + ln];
         ps[3 * ln + 0] = R(p[3 * gid + 0]);
         ps[3 * ln + 1] = R(p[3 * gid + 1]);
         ps[3 * ln + 2] = R(p[3 * gid + 2]);
@@ -120,7 +140,8 @@ __device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int tile, con
     int lc[NPE];
 #pragma unroll
     for (int a = 0; a < NPE; ++a) lc[a] = A.lconn[((size_t)tile * NPE + a) * TE + t];
-    const R lam = A.lam[(size_t)tile * TE + t], mu = A.mu[(size_t)tile * TE + t];
+    const R lam = A.tiles_per_inst ? A.lam[inst] : A.lam[(size_t)tile * TE + t];
+    const R mu = A.tiles_per_inst ? A.mu[inst] : A.mu[(size_t)tile * TE + t];
 #pragma unroll
     for (int a = 0; a < NPE; ++a)
 #pragma unroll
@@ -177,14 +198,15 @@ __device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int tile, con
         }
         const int ps_slot = A.ln_pslot[lb + ln];
         if (ps_slot < 0) {
-            const int gid = A.ln_gid[lb + ln];
+            const int gid = noff + A.ln_gid[lb + ln];
             q[3 * gid + 0] = double(s0);
             q[3 * gid + 1] = double(s1);
             q[3 * gid + 2] = double(s2);
         } else {
-            A.partial[3 * ps_slot + 0] = s0;
-            A.partial[3 * ps_slot + 1] = s1;
-            A.partial[3 * ps_slot + 2] = s2;
+            R* pt = A.partial + 3 * (size_t)(poff + ps_slot);
+            pt[0] = s0;
+            pt[1] = s1;
+            pt[2] = s2;
         }
     }
     __syncthreads();  // smem reused by the next tile
@@ -197,7 +219,13 @@ __device__ __forceinline__ void node_kp(const BatchArgs<R>& A, int i, double* q,
     if (A.fixed[i]) {
         out[0] = out[1] = out[2] = 0.0;
     } else {
-        const int b = A.node_bidx[i];
+        int local = i, poff = 0;
+        if (A.tiles_per_inst) {
+            const int inst = i / A.nodes_per_inst;
+            local = i - inst * A.nodes_per_inst;
+            poff = inst * A.pslots_per_inst;
+        }
+        const int b = A.node_bidx[local];
         if (b < 0) {
             out[0] = q[3 * i + 0];
             out[1] = q[3 * i + 1];
@@ -205,7 +233,7 @@ __device__ __forceinline__ void node_kp(const BatchArgs<R>& A, int i, double* q,
         } else {
             R s0 = R(0), s1 = R(0), s2 = R(0);
             for (int k = A.bnode_off[b]; k < A.bnode_off[b + 1]; ++k) {
-                const int sl = A.bnode_slots[k];
+                const int sl = poff + A.bnode_slots[k];
                 s0 += __ldcg(A.partial + 3 * sl + 0);
                 s1 += __ldcg(A.partial + 3 * sl + 1);
                 s2 += __ldcg(A.partial + 3 * sl + 2);
@@ -237,8 +265,12 @@ __device__ __forceinline__ void apply_all_tiles(const BatchArgs<R>& A, const dou
     for (int tile = blockIdx.x; tile < A.n_tiles; tile += gridDim.x) {
         if (skip_done) {
             bool all_done = true;
-            for (int i = A.tile_inst[2 * tile]; i <= A.tile_inst[2 * tile + 1] && all_done; ++i)
-                all_done = __ldcg(A.done + i) != 0;
+            if (A.tiles_per_inst) {
+                all_done = __ldcg(A.done + tile / A.tiles_per_inst) != 0;
+            } else {
+                for (int i = A.tile_inst[2 * tile]; i <= A.tile_inst[2 * tile + 1] && all_done; ++i)
+                    all_done = __ldcg(A.done + i) != 0;
+            }
             if (all_done) continue;
         }
         linear_tile<R, NPE, NQP>(A, tile, p, q, smem);
@@ -454,18 +486,21 @@ static BatchArgs<R> batch_args(tlfea_batch_s* b) {
         A.dv = tl.dv64;
         A.lam = b->lam;
         A.mu = b->mu;
-        A.partial = tl.partial64;
+        A.partial = b->shared ? b->part64 : tl.partial64;
     } else {
         A.grad = tl.grad32;
         A.dv = tl.dv32;
         A.lam = b->lam32;
         A.mu = b->mu32;
-        A.partial = tl.partial32;
+        A.partial = b->shared ? b->part32 : tl.partial32;
     }
     A.node_bidx = tl.node_bidx;
     A.bnode_off = tl.bnode_off;
     A.bnode_slots = tl.bnode_slots;
-    A.n_tiles = tl.n_tiles;
+    A.n_tiles = b->shared ? tl.n_tiles * b->n_inst : tl.n_tiles;
+    A.tiles_per_inst = b->shared ? tl.n_tiles : 0;
+    A.nodes_per_inst = b->shared ? el->N : 0;
+    A.pslots_per_inst = b->shared ? tl.n_pslots : 0;
     A.max_local = tl.max_local;
     A.N = b->N;
     A.n_inst = b->n_inst;
@@ -584,9 +619,32 @@ static int build_chunks(tlfea_batch_s* b, int chunk_nodes) {
     return TLFEA_OK;
 }
 
+// Lame parameters as SetSVK computes them (FEAT10Data.cuh:399-409).
+static void lame(double Ey, double nu, double& lam, double& mu) {
+    mu = Ey / (2.0 * (1.0 + nu));
+    lam = Ey * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+}
+
 static int upload_material(tlfea_batch_s* b) {
     tlfea_element_s* el = b->el;
     const Tiling& tl = el->tl;
+    if (b->shared) {  // per instance
+        const size_t n = (size_t)b->n_inst;
+        std::vector<double> lam(n), mu(n);
+        std::vector<float> lam32(n), mu32(n);
+        for (size_t i = 0; i < n; ++i) {
+            lame(b->inst_E[i], b->inst_nu[i], lam[i], mu[i]);
+            lam32[i] = (float)lam[i];
+            mu32[i] = (float)mu[i];
+        }
+        cudaStream_t st = el->stream;
+        TLFEA_CUDA(cudaMemcpyAsync(b->lam, lam.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+        TLFEA_CUDA(cudaMemcpyAsync(b->mu, mu.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+        TLFEA_CUDA(cudaMemcpyAsync(b->lam32, lam32.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+        TLFEA_CUDA(cudaMemcpyAsync(b->mu32, mu32.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+        TLFEA_CUDA(cudaStreamSynchronize(st));
+        return TLFEA_OK;
+    }
     const size_t ns = (size_t)tl.n_tiles * TILE_ELEMS;
     std::vector<int> elem_inst((size_t)b->E);
     for (int i = 0; i < b->n_inst; ++i)
@@ -597,10 +655,7 @@ static int upload_material(tlfea_batch_s* b) {
         const int e = tl.h_tile_elem[s];
         if (e < 0) continue;
         const int i = elem_inst[e];
-        const double Ey = b->inst_E[i], nu = b->inst_nu[i];
-        // Lame parameters as SetSVK computes them (FEAT10Data.cuh:399-409)
-        mu[s] = Ey / (2.0 * (1.0 + nu));
-        lam[s] = Ey * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+        lame(b->inst_E[i], b->inst_nu[i], lam[s], mu[s]);
         lam32[s] = (float)lam[s];
         mu32[s] = (float)mu[s];
     }
@@ -611,6 +666,47 @@ static int upload_material(tlfea_batch_s* b) {
     TLFEA_CUDA(cudaMemcpyAsync(b->mu32, mu32.data(), ns * sizeof(float), cudaMemcpyHostToDevice, st));
     TLFEA_CUDA(cudaStreamSynchronize(st));
     return TLFEA_OK;
+}
+
+// Nodes touched by no element carry no stiffness: they are always held fixed.
+static std::vector<unsigned char> untouched_nodes(const tlfea_batch_s* b) {
+    const int per = b->shared ? b->el->N : b->N;
+    std::vector<unsigned char> base((size_t)per, 1);
+    for (int k : b->el->conn) base[k] = 0;
+    std::vector<unsigned char> fx((size_t)b->N);
+    for (size_t i = 0; i < fx.size(); ++i) fx[i] = base[i % (size_t)per];
+    return fx;
+}
+
+// Solver state of a batch whose element (tiling, gradients) is set up.
+static int batch_alloc_state(tlfea_batch_s* b) {
+    const int n_inst = b->n_inst;
+    const size_t n3 = 3 * (size_t)b->N;
+    const size_t nmat = b->shared ? (size_t)n_inst : (size_t)b->el->tl.n_tiles * TILE_ELEMS;
+    int st;
+    if ((st = dalloc(&b->lam, nmat)) || (st = dalloc(&b->mu, nmat)) || (st = dalloc(&b->lam32, nmat)) ||
+        (st = dalloc(&b->mu32, nmat)) || (st = dalloc(&b->fixed, (size_t)b->N)) || (st = dalloc(&b->u, n3)) ||
+        (st = dalloc(&b->r, n3)) || (st = dalloc(&b->p, n3)) || (st = dalloc(&b->q, n3)) ||
+        (st = dalloc(&b->f, n3)) || (st = dalloc(&b->u0, n3)) || (st = dalloc(&b->rr, 2 * (size_t)n_inst)) ||
+        (st = dalloc(&b->fnorm, (size_t)n_inst)) || (st = dalloc(&b->rel, (size_t)n_inst)) ||
+        (st = dalloc(&b->iters, (size_t)n_inst)) || (st = dalloc(&b->status, (size_t)n_inst)) ||
+        (st = dalloc(&b->done, (size_t)n_inst)) || (st = dalloc(&b->n_done, 1)))
+        return st;
+    if (b->shared) {
+        const size_t np = 3 * (size_t)n_inst * (size_t)std::max(b->el->tl.n_pslots, 1);
+        if ((st = dalloc(&b->part64, np)) || (st = dalloc(&b->part32, np))) return st;
+    }
+    cudaStream_t s = b->el->stream;
+    const std::vector<unsigned char> fx = untouched_nodes(b);
+    TLFEA_CUDA(cudaMemcpyAsync(b->fixed, fx.data(), (size_t)b->N, cudaMemcpyHostToDevice, s));
+    TLFEA_CUDA(cudaMemsetAsync(b->f, 0, n3 * sizeof(double), s));
+    TLFEA_CUDA(cudaMemsetAsync(b->u, 0, n3 * sizeof(double), s));
+    TLFEA_CUDA(cudaMemsetAsync(b->u0, 0, n3 * sizeof(double), s));
+    TLFEA_CUDA(cudaMemsetAsync(b->iters, 0, n_inst * sizeof(int), s));
+    TLFEA_CUDA(cudaMemsetAsync(b->status, 0, n_inst * sizeof(int), s));
+    TLFEA_CUDA(cudaMemsetAsync(b->rel, 0, n_inst * sizeof(double), s));
+    TLFEA_CUDA(cudaStreamSynchronize(s));
+    return build_chunks(b, 256);
 }
 
 }  // namespace tlfea
@@ -695,8 +791,6 @@ int tlfea_batch_create(int type, int n_inst, const int* node_off, const int* ele
     }
     if ((st = tlfea_element_setup(el, qx, qy, qz, qw, n_qp, x, y, z, gconn.data()))) return fail(st);
     if ((st = tlfea_element_calc_dndu_pre(el))) return fail(st);
-    const size_t ns = (size_t)el->tl.n_tiles * TILE_ELEMS;
-    const size_t n3 = 3 * (size_t)N;
     {
         std::vector<int> elem_inst((size_t)E), ti(2 * (size_t)el->tl.n_tiles);
         for (int i = 0; i < n_inst; ++i)
@@ -718,30 +812,66 @@ int tlfea_batch_create(int type, int n_inst, const int* node_off, const int* ele
             return fail(TLFEA_CUDA_ERROR);
         }
     }
-    if ((st = dalloc(&b->lam, ns)) || (st = dalloc(&b->mu, ns)) || (st = dalloc(&b->lam32, ns)) ||
-        (st = dalloc(&b->mu32, ns)) || (st = dalloc(&b->fixed, (size_t)N)) || (st = dalloc(&b->u, n3)) ||
-        (st = dalloc(&b->r, n3)) || (st = dalloc(&b->p, n3)) || (st = dalloc(&b->q, n3)) ||
-        (st = dalloc(&b->f, n3)) || (st = dalloc(&b->u0, n3)) || (st = dalloc(&b->rr, 2 * (size_t)n_inst)) ||
-        (st = dalloc(&b->fnorm, (size_t)n_inst)) || (st = dalloc(&b->rel, (size_t)n_inst)) ||
-        (st = dalloc(&b->iters, (size_t)n_inst)) || (st = dalloc(&b->status, (size_t)n_inst)) ||
-        (st = dalloc(&b->done, (size_t)n_inst)) || (st = dalloc(&b->n_done, 1)))
-        return fail(st);
-    cudaStream_t s = el->stream;
-    // nodes touched by no element carry no stiffness: they are held fixed
-    std::vector<unsigned char> fx((size_t)N, 1);
-    for (int k : gconn) fx[k] = 0;
-    if (cudaMemcpyAsync(b->fixed, fx.data(), (size_t)N, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemsetAsync(b->f, 0, n3 * sizeof(double), s) != cudaSuccess ||
-        cudaMemsetAsync(b->u, 0, n3 * sizeof(double), s) != cudaSuccess ||
-        cudaMemsetAsync(b->u0, 0, n3 * sizeof(double), s) != cudaSuccess ||
-        cudaMemsetAsync(b->iters, 0, n_inst * sizeof(int), s) != cudaSuccess ||
-        cudaMemsetAsync(b->status, 0, n_inst * sizeof(int), s) != cudaSuccess ||
-        cudaMemsetAsync(b->rel, 0, n_inst * sizeof(double), s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
-        set_error("batch_create: device initialisation failed");
-        return fail(TLFEA_CUDA_ERROR);
+    if ((st = batch_alloc_state(b))) return fail(st);
+    *out = b;
+    return TLFEA_OK;
+}
+
+int tlfea_batch_create_shared(int type, int n_inst, int n_nodes, int n_elem, const double* qx, const double* qy,
+                              const double* qz, const double* qw, int n_qp, const double* x, const double* y,
+                              const double* z, const int* conn, tlfea_batch* out) {
+    if (!out) return TLFEA_INVALID_ARG;
+    *out = nullptr;
+    if ((type != TLFEA_TYPE_T10 && type != TLFEA_TYPE_T4) || n_inst <= 0 || n_nodes <= 0 || n_elem <= 0 || !x ||
+        !y || !z || !conn || !qx || !qy || !qz || !qw) {
+        set_error("batch_create_shared: bad arguments");
+        return TLFEA_INVALID_ARG;
     }
-    if ((st = build_chunks(b, 256))) return fail(st);
+    const int npe = (type == TLFEA_TYPE_T10) ? T10_NPE : T4_NPE;
+    const int nqp = (type == TLFEA_TYPE_T10) ? T10_NQP : T4_NQP;
+    if (3LL * n_nodes * n_inst >= (1LL << 31) || (long long)n_elem * n_inst >= (1LL << 31)) {
+        set_error("batch_create_shared: batch too large for 32-bit indices");
+        return TLFEA_INVALID_ARG;
+    }
+    std::vector<int> cm((size_t)n_elem * npe);
+    for (int e = 0; e < n_elem; ++e)
+        for (int a = 0; a < npe; ++a) {
+            const int l = conn[(size_t)e * npe + a];
+            if (l < 0 || l >= n_nodes) {
+                set_error("batch_create_shared: connectivity index out of range");
+                return TLFEA_INVALID_ARG;
+            }
+            cm[e + (size_t)a * n_elem] = l;
+        }
+    tlfea_element el = nullptr;
+    int st = tlfea_element_create(type, n_elem, n_nodes, &el);
+    if (st) return st;
+    tlfea_batch_s* b = new tlfea_batch_s();
+    b->type = type;
+    b->n_inst = n_inst;
+    b->shared = true;
+    b->N = n_nodes * n_inst;
+    b->E = n_elem * n_inst;
+    b->el = el;
+    b->node_off.resize((size_t)n_inst + 1);
+    b->elem_off.resize((size_t)n_inst + 1);
+    for (int i = 0; i <= n_inst; ++i) {
+        b->node_off[i] = i * n_nodes;
+        b->elem_off[i] = i * n_elem;
+    }
+    b->inst_E.assign(n_inst, 0.0);
+    b->inst_nu.assign(n_inst, 0.0);
+    auto fail = [&](int s) {
+        tlfea_batch_destroy(b);
+        return s;
+    };
+    if (n_qp != nqp) {
+        set_error("batch_create_shared: quadrature size does not match the element type");
+        return fail(TLFEA_SIZE_MISMATCH);
+    }
+    if ((st = tlfea_element_setup(el, qx, qy, qz, qw, n_qp, x, y, z, cm.data()))) return fail(st);
+    if ((st = tlfea_element_calc_dndu_pre(el))) return fail(st);
+    if ((st = batch_alloc_state(b))) return fail(st);
     *out = b;
     return TLFEA_OK;
 }
@@ -754,6 +884,7 @@ int tlfea_batch_destroy(tlfea_batch b) {
     dfree(b->fixed); dfree(b->chunk_inst); dfree(b->chunk_beg); dfree(b->inst_chunk); dfree(b->tile_inst);
     dfree(b->u); dfree(b->r); dfree(b->p); dfree(b->q); dfree(b->f); dfree(b->u0);
     dfree(b->cpa); dfree(b->cpb); dfree(b->rr); dfree(b->fnorm); dfree(b->rel);
+    dfree(b->part64); dfree(b->part32);
     dfree(b->iters); dfree(b->status); dfree(b->done); dfree(b->n_done);
     if (b->el) tlfea_element_destroy(b->el);
     delete b;
@@ -765,7 +896,7 @@ int tlfea_batch_get_counts(tlfea_batch b, int* n_inst, int* n_elem, int* n_nodes
     if (n_inst) *n_inst = b->n_inst;
     if (n_elem) *n_elem = b->E;
     if (n_nodes) *n_nodes = b->N;
-    if (n_tiles) *n_tiles = b->el->tl.n_tiles;
+    if (n_tiles) *n_tiles = b->shared ? b->el->tl.n_tiles * b->n_inst : b->el->tl.n_tiles;
     return TLFEA_OK;
 }
 
@@ -796,8 +927,7 @@ int tlfea_batch_set_material(tlfea_batch b, const double* E, const double* nu) {
 int tlfea_batch_set_fixed(tlfea_batch b, const int* nodes, int n) {
     CHECK_BATCH(b);
     if (n < 0 || (n > 0 && !nodes)) return TLFEA_INVALID_ARG;
-    std::vector<unsigned char> fx((size_t)b->N, 1);
-    for (int k : b->el->conn) fx[k] = 0;
+    std::vector<unsigned char> fx = untouched_nodes(b);
     for (int k = 0; k < n; ++k) {
         if (nodes[k] < 0 || nodes[k] >= b->N) {
             set_error("batch_set_fixed: node index out of range");

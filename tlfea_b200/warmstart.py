@@ -67,7 +67,8 @@ class FixedMeshCases:
         self.fixed, _, self.tip = M.cantilever_loads(self.x, self.y, self.z)
         self.N = len(self.x)
         self.batch = int(batch)
-        self.solver = BatchedLinearStaticSolver([(self.x, self.y, self.z, self.conn)] * self.batch, TYPE_T10)
+        self.solver = BatchedLinearStaticSolver([(self.x, self.y, self.z, self.conn)] * self.batch, TYPE_T10,
+                                                shared=True)
         self.solver.SetNodalFixed([self.fixed] * self.batch)
 
     def loads(self, cases: np.ndarray) -> np.ndarray:
