@@ -98,3 +98,25 @@ def test_beam_fixture_tip_deflection():
     delta_eb = abs(P) * L ** 3 / (3 * E_mod * b * h ** 3 / 12)
     assert 0.3 < delta / delta_eb < 1.3
     el.Destroy()
+
+
+def test_cpp_class_driver_solves_like_the_python_path(tmp_path):
+    """The reference's linear-static example flow through the C++ classes
+    (include/tlfea/tlfea.hpp): same displacement as a direct solve of the
+    oracle's system."""
+    import subprocess
+
+    from . import cpp_driver as D
+
+    x, y, z, conn = box(10, 2, 2, 10)
+    fixed, f, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -100.0))
+    exe = D.build(tmp_path)
+    D.write_input(tmp_path / "in.bin", x, y, z, conn, fixed, f)
+    r = subprocess.run([str(exe), str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    it, res, u = D.read_output(tmp_path / "out.bin", len(x))
+    assert it > 0 and res < 1e-10
+    off, cols, kv, fb = _oracle_system(x, y, z, conn, fixed, f)
+    u_dir = spla.spsolve(sp.csr_matrix((kv, cols, off)).tocsc(), fb)
+    assert rel(u, u_dir) < 1e-7

@@ -145,3 +145,19 @@ def test_random_beam_instances_follow_the_batch_distribution():
         assert abs(d["x"].max() - 10 * d["ny"] * 0.01) < 1e-12
         assert M.random_beam(s)["E"] == d["E"]  # seeded
     assert len(seen_nx) > 10 and len(seen_ny) > 3
+
+
+def test_cpp_class_shim_builds_links_and_reports_no_device(tmp_path):
+    """The C++ classes of include/tlfea/tlfea.hpp compile (-Wall -Wextra), link
+    against the library and, without a GPU, end cleanly with the no-device code."""
+    from . import cpp_driver as D
+
+    exe = D.build(tmp_path)
+    x, y, z, conn = M.box_mesh(4, 1, 1, 10)
+    fixed, f, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -1.0))
+    D.write_input(tmp_path / "in.bin", x, y, z, conn, fixed, f)
+    import subprocess
+
+    r = subprocess.run([str(exe), str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], capture_output=True,
+                       text=True, env={"CUDA_VISIBLE_DEVICES": ""})
+    assert r.returncode == 3, r.stderr
