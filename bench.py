@@ -388,6 +388,14 @@ def learned_leg(args, T):
     it_w, res_w, st_w = fm.solver.GetResults()
     g = held["guess"].cpu().numpy()
     guess_err = np.linalg.norm(g - u_c, axis=1) / np.linalg.norm(u_c, axis=1)
+    # starting residual of the guess, ||f - K u0||_free / ||f|| (a cold start's is 1)
+    kg = torch.empty_like(held["guess"])
+    torch.cuda.synchronize()
+    fm.solver.Apply(int(held["guess"].data_ptr()), int(kg.data_ptr()))
+    F = fm.loads(test)
+    r0 = F - kg.cpu().numpy()
+    r0.reshape(512, -1, 3)[:, fm.fixed, :] = 0.0
+    guess_res = np.linalg.norm(r0, axis=1) / np.linalg.norm(F, axis=1)
     reps = max(1, args.steps // 2)
     ms_cold = time_stream(torch, st, cold, reps)
     ms_warm = time_stream(torch, st, warm, reps)
@@ -417,6 +425,7 @@ def learned_leg(args, T):
             "speedup_learned_vs_plain": round(learned / plain, 2),
             "speedup_learned_vs_cold_batched": round(ms_cold / ms_warm, 2),
             "guess_rel_error_median": float(np.median(guess_err)),
+            "guess_rel_residual_median": float(np.median(guess_res)),
             "training": {"cases": int(len(train)), "gen_s": round(t_gen, 2), "train_s": round(t_train, 2),
                          "epochs": args.epochs, "final_loss": float(hist[-1]), "pca_energy": ws.pca.energy
                          if hasattr(ws.pca, "energy") else None, "setup_s": round(t_setup, 2),

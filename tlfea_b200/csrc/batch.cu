@@ -128,11 +128,21 @@ __device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int item, con
         noff = inst * A.nodes_per_inst;
         poff = inst * A.pslots_per_inst;
     }
+    // shared memory: p at the local nodes, element forces, then the tile's
+    // tables (node destination, incidence ends, incidence list) so the scatter
+    // reads no global memory
     R* ps = reinterpret_cast<R*>(smem);  // 3 * max_local, interleaved
     R* fe = ps + 3 * A.max_local;        // 3 * NPE * TE
+    int* dsts = reinterpret_cast<int*>(fe + 3 * NPE * TE);  // max_local: node id, or -(slot + 1)
+    uint16_t* iends = reinterpret_cast<uint16_t*>(dsts + A.max_local);
+    uint16_t* incs = iends + A.max_local;  // NPE * TE
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
+    for (int k = t; k < NPE * TE; k += TE) incs[k] = A.inc[(size_t)tile * TE * NPE + k];
     for (int ln = t; ln < nl; ln += TE) {
         const int gid = noff + A.ln_gid[lb + ln];
+        const int pslot = A.ln_pslot[lb + ln];
+        dsts[ln] = (pslot < 0) ? gid : -(poff + pslot + 1);
+        iends[ln] = A.ln_inc_end[lb + ln];
         ps[3 * ln + 0] = R(p[3 * gid + 0]);
         ps[3 * ln + 1] = R(p[3 * gid + 1]);
         ps[3 * ln + 2] = R(p[3 * gid + 2]);
@@ -184,26 +194,24 @@ __device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int item, con
             }
     }
     __syncthreads();
-    const uint16_t* inc = A.inc + (size_t)tile * TE * NPE;
     for (int ln = t; ln < nl; ln += TE) {
-        const int beg = ln ? A.ln_inc_end[lb + ln - 1] : 0;
-        const int end = A.ln_inc_end[lb + ln];
+        const int beg = ln ? iends[ln - 1] : 0;
+        const int end = iends[ln];
         R s0 = R(0), s1 = R(0), s2 = R(0);
         for (int k = beg; k < end; ++k) {
-            const int ent = inc[k];
+            const int ent = incs[k];
             const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
             s0 += fe[base];
             s1 += fe[base + TE];
             s2 += fe[base + 2 * TE];
         }
-        const int ps_slot = A.ln_pslot[lb + ln];
-        if (ps_slot < 0) {
-            const int gid = noff + A.ln_gid[lb + ln];
-            q[3 * gid + 0] = double(s0);
-            q[3 * gid + 1] = double(s1);
-            q[3 * gid + 2] = double(s2);
+        const int dn = dsts[ln];
+        if (dn >= 0) {
+            q[3 * dn + 0] = double(s0);
+            q[3 * dn + 1] = double(s1);
+            q[3 * dn + 2] = double(s2);
         } else {
-            R* pt = A.partial + 3 * (size_t)(poff + ps_slot);
+            R* pt = A.partial + 3 * (size_t)(-dn - 1);
             pt[0] = s0;
             pt[1] = s1;
             pt[2] = s2;
@@ -530,7 +538,9 @@ static BatchArgs<R> batch_args(tlfea_batch_s* b) {
 
 template <typename R>
 static size_t batch_smem(const tlfea_batch_s* b) {
-    return sizeof(R) * (3 * (size_t)b->el->tl.max_local + 3 * (size_t)b->el->npe * TILE_ELEMS);
+    const size_t ml = (size_t)b->el->tl.max_local;
+    return sizeof(R) * (3 * ml + 3 * (size_t)b->el->npe * TILE_ELEMS) + ml * (sizeof(int) + sizeof(uint16_t)) +
+           (size_t)b->el->npe * TILE_ELEMS * sizeof(uint16_t);
 }
 
 template <typename R, int NPE, int NQP>
