@@ -42,6 +42,12 @@ METRIC = "solves/s at rel. residual 1e-6 (plain CG linear static, 200x20x20 TET1
 # CG iterations the CUDA path needs for this workload (measured on a B200: 7071
 # to 9.76e-7); the reference arm turns its bounded CPU sample into solves/s with it.
 CG_ITERS_CFG2 = 7071
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch from ncu captures:
+# the SpMV on the 120x16x16 beam moved 1.026 x its algorithmic bytes (the 200x20x20 K is
+# too large for a multi-pass capture; traffic scales with the blocks streamed); the FP32
+# tile force kernel on this workload moved 357.03 MB per launch.
+SPMV_TRAFFIC_RATIO = 1.026
+FORCE_FP32_TRAFFIC_BYTES = 357.03e6
 
 
 def peaks():
@@ -537,7 +543,8 @@ def main():
     ach = b_spmv / (ms_spmv / 1e3) / 1e9
     roofline = {"kernel": "k_cg_spmv_dot", "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": int(b_spmv),
-                "format": "row-planar 3x3 node blocks", "ms": round(ms_spmv, 4), "traffic": None,
+                "format": "row-planar 3x3 node blocks", "ms": round(ms_spmv, 4),
+                "traffic": int(SPMV_TRAFFIC_RATIO * b_spmv),
                 "full_csr_equivalent_gbs": round(spmv_bytes_full_csr(N, nnzb) / (ms_spmv / 1e3) / 1e9, 1)}
     # fused element force, FP32 and FP64
     ef = {}
@@ -549,7 +556,8 @@ def main():
         b = elem_force_bytes(E, N, 10, 5, s)
         a = b / (ms_f / 1e3) / 1e9
         ef[prec] = {"kernel": "k_tile_force+k_combine", "bound": "hbm", "achieved": round(a, 1), "peak": hbm,
-                    "unit": "GB/s", "frac": round(a / hbm, 4), "algorithmic_bytes": int(b), "ms": round(ms_f, 4)}
+                    "unit": "GB/s", "frac": round(a / hbm, 4), "algorithmic_bytes": int(b), "ms": round(ms_f, 4),
+                    "traffic": int(FORCE_FP32_TRAFFIC_BYTES) if prec == "fp32" else None}
     el.SetForcePrecision("fp64")
     el.SetBlocking(True)
 
