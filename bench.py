@@ -223,6 +223,16 @@ def kernels_only(args):
     import tlfea_b200 as T
 
     torch.cuda.set_device(0)
+    if args.kernels_only == "batch":
+        # the batched CG: 64 load / material cases on the 40x8x8 TET10 beam, 10 iterations
+        from tlfea_b200 import warmstart as W
+
+        fm = W.FixedMeshCases(40, 8, 8, batch=64)
+        fm.solve(W.sample_cases(64, seed=5), tol=1e-12, max_iter=10)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernels_only": "batch", "cases": 64, "iterations": 10}))
+        fm.destroy()
+        return
     cfg = dict(CFG)
     x, y, z, conn, fixed, f = build_mesh(cfg)
     el = setup_element(T, cfg, x, y, z, conn, fixed, f)
@@ -447,7 +457,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--kernel-reps", type=int, default=20)
     ap.add_argument("--cg-iters", type=int, default=120, help="iteration cap of --kernels-only cg")
-    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg"], default=None,
+    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg", "batch"], default=None,
                     help="profiling case: set up, then launch only the named kernel a few times")
     ap.add_argument("--mesh", default=None, help="cells NXxNYxNZ (default 200x20x20)")
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")
