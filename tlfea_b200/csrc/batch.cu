@@ -160,12 +160,24 @@ __device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int item, con
 #pragma unroll 1
     for (int qp = 0; qp < NQP; ++qp) {
         const R* gp = A.grad + ((size_t)tile * NQP + qp) * (NPE * 3) * TE + t;
+        const R* dp = A.dv + ((size_t)tile * NQP + qp) * TE + t;
         R g[NPE][3];
+        R dv;
+        if (A.tiles_per_inst) {
+            // shared mesh: every instance re-reads these gradients, keep them in L2
 #pragma unroll
-        for (int a = 0; a < NPE; ++a)
+            for (int a = 0; a < NPE; ++a)
 #pragma unroll
-            for (int j = 0; j < 3; ++j) g[a][j] = __ldcs(gp + (a * 3 + j) * TE);
-        const R dv = __ldcs(A.dv + ((size_t)tile * NQP + qp) * TE + t);
+                for (int j = 0; j < 3; ++j) g[a][j] = __ldg(gp + (a * 3 + j) * TE);
+            dv = __ldg(dp);
+        } else {
+            // one instance per tile: a single pass, stream past L2
+#pragma unroll
+            for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) g[a][j] = __ldcs(gp + (a * 3 + j) * TE);
+            dv = __ldcs(dp);
+        }
         R H[3][3];
 #pragma unroll
         for (int i = 0; i < 3; ++i)

@@ -426,12 +426,21 @@ static int build_tiling(tlfea_element_s* h, const double* x, const double* y, co
     std::iota(border.begin(), border.end(), 0);
     std::sort(border.begin(), border.end(), [&](int a, int b) { return bnode_gid[a] < bnode_gid[b]; });
     std::vector<int> bgid, boff(1, 0), bslots, node_bidx((size_t)N, -1);
+    // Partial slots are renumbered by shared node (in node-id order), each node's
+    // slots in tile order: a node's partials are one contiguous range, so the
+    // combine streams them coalesced; the summation order is unchanged.
+    std::vector<int> renum((size_t)std::max(n_pslots, 1), -1);
     for (int k : border) {
         node_bidx[bnode_gid[k]] = (int)bgid.size();
         bgid.push_back(bnode_gid[k]);
-        for (int ps : node_slots[k]) bslots.push_back(ps);
+        for (int ps : node_slots[k]) {
+            renum[ps] = (int)bslots.size();
+            bslots.push_back((int)bslots.size());
+        }
         boff.push_back((int)bslots.size());
     }
+    for (int& ps : ln_pslot)
+        if (ps >= 0) ps = renum[ps];
     tl.max_local = std::max(max_local, 1);
     tl.n_local_total = (long long)ln_gid.size();
     tl.n_pslots = n_pslots;
