@@ -412,9 +412,22 @@ def learned_leg(args, T):
     r0 = F - kg.cpu().numpy()
     r0.reshape(512, -1, 3)[:, fm.fixed, :] = 0.0
     guess_res = np.linalg.norm(r0, axis=1) / np.linalg.norm(F, axis=1)
+    # the Galerkin solution in the same learned basis (no network), for comparison
+    gws = W.GalerkinWarmStart(ws.pca, fm)
+    fm._load(test)
+
+    def galerkin():
+        held["gal"] = g2 = gws.predict(test)
+        fm.solver.SetInitialGuess(int(g2.data_ptr()))
+        fm.solver.Solve(1e-6, 200000)
+
+    galerkin()
+    it_g, res_g, st_g = fm.solver.GetResults()
+    gal_err = np.linalg.norm(held["gal"].cpu().numpy() - u_c, axis=1) / np.linalg.norm(u_c, axis=1)
     reps = max(1, args.steps // 2)
     ms_cold = time_stream(torch, st, cold, reps)
     ms_warm = time_stream(torch, st, warm, reps)
+    ms_gal = time_stream(torch, st, galerkin, reps)
     # plain: one case at a time through LinearStaticSolver, cold start
     k = min(args.plain_sample, 512)
     F = fm.loads(test[:k])
@@ -438,6 +451,11 @@ def learned_leg(args, T):
                              "iters_mean": float(np.mean(it_c)), "iters_max": int(np.max(it_c))},
             "plain_sequential": {"value": round(plain, 2), "sample": k, "iters_mean": float(np.mean(itp_all)),
                                  "path": "LinearStaticSolver per case (assembled K, CG graph), cold start"},
+            "galerkin_batched": {"value": round(512 / (ms_gal / 1e3), 2), "ms_per_batch": round(ms_gal, 3),
+                                 "iters_mean": float(np.mean(it_g)), "iters_max": int(np.max(it_g)),
+                                 "converged": int(np.sum(st_g == 0)), "guess_rel_error_median": float(np.median(gal_err)),
+                                 "speedup_vs_plain": round(512 / (ms_gal / 1e3) / plain, 2),
+                                 "path": "Galerkin solution in the learned PCA basis (no network) as the warm start"},
             "speedup_learned_vs_plain": round(learned / plain, 2),
             "speedup_learned_vs_cold_batched": round(ms_cold / ms_warm, 2),
             "guess_rel_error_median": float(np.median(guess_err)),

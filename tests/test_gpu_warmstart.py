@@ -54,3 +54,27 @@ def test_learned_warm_start_beats_cold_start():
     assert np.array_equal(it2, it_warm)
     ws.destroy()
     fm.destroy()
+
+
+def test_galerkin_warm_start_in_the_learned_basis():
+    """The Galerkin solution in the learned PCA basis (no network) is close to
+    the converged displacement and leaves CG few iterations; the warm-started
+    solve reaches the cold solve's answer."""
+    fm = W.FixedMeshCases(nx=8, ny=2, nz=2, batch=256)
+    train = W.sample_cases(256, seed=2)
+    u_train, it, res, st = fm.solve(train, tol=1e-8)
+    assert np.all(st == 0)
+    pca = W.PCA(16)
+    pca.fit(W.LearnedWarmStart.normalise(u_train, train))
+    gws = W.GalerkinWarmStart(pca, fm)
+    test = W.sample_cases(256, seed=77)
+    u_cold, it_cold, _, st_cold = fm.solve(test, tol=1e-6)
+    guess = gws.predict(test)
+    err = np.linalg.norm(guess.cpu().numpy() - u_cold, axis=1) / np.linalg.norm(u_cold, axis=1)
+    assert np.median(err) < 1e-3
+    u_warm, it_warm, res_warm, st_warm = fm.solve(test, tol=1e-6, u0=guess)
+    assert np.all(st_cold == 0) and np.all(st_warm == 0) and np.all(res_warm < 1e-6)
+    assert it_warm.mean() < 0.5 * it_cold.mean()
+    for k in range(0, 256, 41):
+        assert rel(u_warm[k], u_cold[k]) < 1e-4
+    fm.destroy()

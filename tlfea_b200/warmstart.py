@@ -239,3 +239,58 @@ class LearnedWarmStart:
 
     def destroy(self):
         self.net.Destroy()
+
+
+def lame(E, nu):
+    """Lame parameters as SetSVK computes them (FEAT10Data.cuh:399-409)."""
+    E, nu = np.asarray(E, np.float64), np.asarray(nu, np.float64)
+    return E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), E / (2.0 * (1.0 + nu))
+
+
+class GalerkinWarmStart:
+    """Warm start from the learned basis alone, no network: the Galerkin
+    (Rayleigh-Ritz) solution in span{PCA mean, PCA modes},
+        (B^T K_i B) c = B^T f_i,   u0 = B c,
+    with K_i = lambda_i K_lambda + mu_i K_mu for the fixed mesh (fixed DOFs
+    eliminated; the basis is zero there).  B^T K_lambda B and B^T K_mu B are
+    formed once from two batched products K B; each case then costs one small
+    dense solve.  FP64 throughout (library linear algebra on the GPU)."""
+
+    def __init__(self, pca: PCA, fm: FixedMeshCases, materials=((1e7, 0.3), (1e7, 0.45))):
+        import torch
+
+        B = torch.cat([pca.mean[None, :], pca.modes.T], 0)  # (k+1, dof)
+        k1, n = B.shape
+        if k1 > fm.batch:
+            raise ValueError("the basis has more vectors than the batch holds")
+        self.B = B.contiguous()
+        X = torch.zeros(fm.batch, n, dtype=torch.float64, device="cuda")
+        X[:k1] = B
+        A = []
+        for E, nu in materials:
+            fm.solver.SetMaterial(np.full(fm.batch, E), np.full(fm.batch, nu))
+            Y = torch.empty_like(X)
+            torch.cuda.synchronize()
+            fm.solver.Apply(int(X.data_ptr()), int(Y.data_ptr()))
+            A.append(B @ Y[:k1].T)  # B^T K B
+        l1, m1 = lame(*materials[0])
+        l2, m2 = lame(*materials[1])
+        det = l1 * m2 - l2 * m1
+        self.A_lam = (m2 * A[0] - m1 * A[1]) / float(det)
+        self.A_mu = (l1 * A[1] - l2 * A[0]) / float(det)
+        self.fm = fm
+
+    def predict(self, cases: np.ndarray):
+        """Warm-start displacements (n, dof) on the GPU (FP64 torch tensor)."""
+        import torch
+
+        lam, mu = lame(cases[:, 0], cases[:, 1])
+        lam = torch.as_tensor(lam, device="cuda")[:, None, None]
+        mu = torch.as_tensor(mu, device="cuda")[:, None, None]
+        A = lam * self.A_lam[None] + mu * self.A_mu[None]
+        F = torch.as_tensor(self.fm.loads(cases), device="cuda")
+        rhs = F @ self.B.T  # (n, k+1)
+        c = torch.linalg.solve(A, rhs[:, :, None])[:, :, 0]
+        u = c @ self.B
+        torch.cuda.synchronize()
+        return u
