@@ -82,6 +82,8 @@ class GPU_TetData : public ElementBase {
     void SetExternalForce(const VectorXR& f) {
         check(tlfea_element_set_external_force(h_, f.data(), (int)f.size()), "SetExternalForce");
     }
+    // new: f_ext += M g (consistent-mass row sums); after CalcMassMatrix
+    void AddGravity(Real gx, Real gy, Real gz) { check(tlfea_element_add_gravity(h_, gx, gy, gz), "AddGravity"); }
     void SetNodalFixed(const std::vector<int>& nodes) {
         if (check(tlfea_element_set_nodal_fixed(h_, nodes.data(), (int)nodes.size()), "SetNodalFixed"))
             n_constraint = 3 * (int)nodes.size();

@@ -131,6 +131,10 @@ int tlfea_element_set_svk(tlfea_element h, double E, double nu);
 int tlfea_element_set_mooney_rivlin(tlfea_element h, double mu10, double mu01, double kappa);
 /* SetExternalForce (:589-597); n must be 3*N. */
 int tlfea_element_set_external_force(tlfea_element h, const double* f_ext, int n);
+/* New (no reference counterpart): adds the gravity body force of a uniform
+ * acceleration (gx, gy, gz) to f_ext, f_i += (sum_j M_ij) g with the consistent
+ * mass of CalcMassMatrix (required first).  SetExternalForce replaces f_ext. */
+int tlfea_element_add_gravity(tlfea_element h, double gx, double gy, double gz);
 /* SetNodalFixed (FEAT10Data.cu:650-672) / UpdateNodalFixed (:674-752). */
 int tlfea_element_set_nodal_fixed(tlfea_element h, const int* fixed_nodes, int n_fixed);
 int tlfea_element_update_nodal_fixed(tlfea_element h, const int* fixed_nodes, int n_fixed);

@@ -147,3 +147,21 @@ def test_errors_are_reported():
     with pytest.raises(T.TLFEAError):
         el.SetExternalForce(np.zeros(5))  # size mismatch
     el.Destroy()
+
+
+def test_gravity_body_force_is_mass_row_sums_times_g():
+    """AddGravity adds (sum_j M_ij) g to f_ext; the total equals rho V g."""
+    x, y, z, conn = box(10, 2, 2, 10)
+    f0 = np.random.default_rng(4).standard_normal(3 * len(x))
+    el = make_element(x, y, z, conn, f_ext=f0)
+    g = (0.0, -2.0, -9.81)
+    el.AddGravity(*g)
+    f = el.RetrieveExternalForceToCPU()
+    _, dj = O.dndu_pre(x, y, z, conn)
+    off, cols, vals = O.mass(conn, dj, len(x), RHO)
+    rows = np.add.reduceat(vals, off[:-1])
+    ref = f0 + np.outer(rows, g).ravel()
+    assert rel(f, ref) < 1e-13
+    total = (f - f0).reshape(-1, 3).sum(0)
+    assert np.allclose(total, RHO * 1.0 * 0.1 * 0.1 * np.array(g), rtol=1e-12, atol=1e-12)
+    el.Destroy()

@@ -92,6 +92,7 @@ _SIGS = {
     "tlfea_element_set_svk": [_P, C.c_double, C.c_double],
     "tlfea_element_set_mooney_rivlin": [_P, C.c_double, C.c_double, C.c_double],
     "tlfea_element_set_external_force": [_P, _D, C.c_int],
+    "tlfea_element_add_gravity": [_P, C.c_double, C.c_double, C.c_double],
     "tlfea_element_set_nodal_fixed": [_P, _I, C.c_int],
     "tlfea_element_update_nodal_fixed": [_P, _I, C.c_int],
     "tlfea_element_update_positions": [_P, _D, _D, _D, C.c_int],

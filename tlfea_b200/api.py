@@ -112,6 +112,10 @@ class _TetData(ElementBase):
         f = _f64(h_f_ext)
         capi.call("tlfea_element_set_external_force", self._handle(), capi.dptr(f), int(f.size))
 
+    def AddGravity(self, gx: float, gy: float, gz: float):
+        """New: f_ext += M g (consistent-mass row sums); after CalcMassMatrix."""
+        capi.call("tlfea_element_add_gravity", self._handle(), float(gx), float(gy), float(gz))
+
     def SetNodalFixed(self, fixed_nodes):
         a = _i32(fixed_nodes)
         capi.call("tlfea_element_set_nodal_fixed", self._handle(), capi.iptr(a), int(a.size))

@@ -1026,6 +1026,18 @@ int tlfea_element_set_mooney_rivlin(tlfea_element h, double mu10, double mu01, d
     return TLFEA_OK;
 }
 
+int tlfea_element_add_gravity(tlfea_element h, double gx, double gy, double gz) {
+    CHECK_HANDLE(h);
+    if (!h->mass_setup) {
+        set_error("add_gravity: CalcMassMatrix must be called first");
+        return TLFEA_NOT_SETUP;
+    }
+    k_add_gravity<<<(h->N + 255) / 256, 256, 0, h->stream>>>(h->N, h->pat_off, h->m_val, gx, gy, gz, h->f_ext);
+    TLFEA_CHECK_LAUNCH();
+    SYNC(h);
+    return TLFEA_OK;
+}
+
 int tlfea_element_set_external_force(tlfea_element h, const double* f, int n) {
     CHECK_HANDLE(h);
     if (!f || n != 3 * h->N) {
@@ -1035,6 +1047,19 @@ int tlfea_element_set_external_force(tlfea_element h, const double* f, int n) {
     TLFEA_CUDA(cudaMemcpyAsync(h->f_ext, f, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     SYNC(h);
     return TLFEA_OK;
+}
+
+// f_ext[3i+d] += g_d * sum_j M_ij: the body force of a uniform acceleration g on
+// the consistent mass (the node pattern's mass rows), one thread per node row.
+__global__ void k_add_gravity(int N, const int* __restrict__ off, const double* __restrict__ m, double gx, double gy,
+                              double gz, double* f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double s = 0.0;
+    for (int k = off[i]; k < off[i + 1]; ++k) s += m[k];
+    f[3 * i + 0] += s * gx;
+    f[3 * i + 1] += s * gy;
+    f[3 * i + 2] += s * gz;
 }
 
 static int upload_fixed(tlfea_element h, const int* nodes, int n) {
