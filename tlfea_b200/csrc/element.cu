@@ -181,6 +181,19 @@ __global__ void k_combine(int nb, const int* __restrict__ bgid, const int* __res
     }
 }
 
+// f_ext[3i+d] += g_d * sum_j M_ij: the body force of a uniform acceleration g on
+// the consistent mass (the node pattern's mass rows), one thread per node row.
+__global__ void k_add_gravity(int N, const int* __restrict__ off, const double* __restrict__ m, double gx, double gy,
+                              double gz, double* f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double s = 0.0;
+    for (int k = off[i]; k < off[i + 1]; ++k) s += m[k];
+    f[3 * i + 0] += s * gx;
+    f[3 * i + 1] += s * gy;
+    f[3 * i + 2] += s * gz;
+}
+
 __global__ void k_disp32(int n, const double* __restrict__ x, const double* __restrict__ y,
                          const double* __restrict__ z, const double* __restrict__ X0x, const double* __restrict__ X0y,
                          const double* __restrict__ X0z, float* ux, float* uy, float* uz) {
@@ -1047,19 +1060,6 @@ int tlfea_element_set_external_force(tlfea_element h, const double* f, int n) {
     TLFEA_CUDA(cudaMemcpyAsync(h->f_ext, f, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     SYNC(h);
     return TLFEA_OK;
-}
-
-// f_ext[3i+d] += g_d * sum_j M_ij: the body force of a uniform acceleration g on
-// the consistent mass (the node pattern's mass rows), one thread per node row.
-__global__ void k_add_gravity(int N, const int* __restrict__ off, const double* __restrict__ m, double gx, double gy,
-                              double gz, double* f) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    double s = 0.0;
-    for (int k = off[i]; k < off[i + 1]; ++k) s += m[k];
-    f[3 * i + 0] += s * gx;
-    f[3 * i + 1] += s * gy;
-    f[3 * i + 2] += s * gz;
 }
 
 static int upload_fixed(tlfea_element h, const int* nodes, int n) {
