@@ -195,6 +195,10 @@ class LinearStaticSolver : public SolverBase {
         check(tlfea_linear_static_create(data->handle(), tol, max_iter, &s_), "LinearStaticSolver");
     }
     void SetParameters(void*) override {}
+    // new, opt-in: 1 = block Jacobi on the 3x3 node diagonal blocks, 0 = none (default)
+    void SetPreconditioner(int kind) {
+        check(tlfea_linear_static_set_preconditioner(s_, kind), "SetPreconditioner");
+    }
     int GetLastIterCount() const {
         int it = 0;
         double r = 0.0;

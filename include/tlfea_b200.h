@@ -235,6 +235,11 @@ int tlfea_solver_setup(tlfea_solver s);
 int tlfea_solver_set_parameters(tlfea_solver s, const void* params);
 /* Solve() (SyncedNesterov.cuh:266-268, SyncedAdamW.cuh, LinearStaticSolver.cu:590-603). */
 int tlfea_solver_solve(tlfea_solver s);
+/* New (no reference counterpart, opt-in): preconditioner of the linear static
+ * CG.  kind 0 = none (default, the reference's unpreconditioned CG); 1 = block
+ * Jacobi on the 3x3 node diagonal blocks of K (BCs applied).  The stop test
+ * stays sqrt(r.r / r0.r0) < tol. */
+int tlfea_linear_static_set_preconditioner(tlfea_solver s, int kind);
 /* GetLastIterCount / GetLastResidual (LinearStaticSolver.cuh:68-72). */
 int tlfea_linear_static_last(tlfea_solver s, int* iters, double* rel_residual);
 /* Retrieve the LinearStaticSolver stiffness (BCs applied) as 3N x 3N CSR

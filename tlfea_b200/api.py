@@ -423,6 +423,11 @@ class LinearStaticSolver(SolverBase):
     def SetParameters(self, params=None):
         """No-op: parameters are set through the constructor."""
 
+    def SetPreconditioner(self, kind: str = "none"):
+        """New, opt-in: "block_jacobi" (3x3 node diagonal blocks) or "none" (the
+        reference's unpreconditioned CG, the default)."""
+        capi.call("tlfea_linear_static_set_preconditioner", self._h, {"none": 0, "block_jacobi": 1}[kind])
+
     def _last(self):
         it, res = C.c_int(), C.c_double()
         capi.call("tlfea_linear_static_last", self._h, C.byref(it), C.byref(res))

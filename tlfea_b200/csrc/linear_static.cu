@@ -1,8 +1,9 @@
 // linear_static.cu -- LinearStaticSolver<T> (LinearStaticSolver.cu:196-603) on
 // sm_100a: deterministic row-wise stiffness assembly into 3x3 node blocks,
-// Dirichlet elimination, and an unpreconditioned FP64 CG whose dot products
-// are fused into the SpMV / axpy kernels and whose scalars never leave the
-// device (CUDA graph of several iterations per host check).
+// Dirichlet elimination, and an FP64 CG (unpreconditioned like the reference,
+// or opt-in block Jacobi) whose dot products are fused into the SpMV / axpy
+// kernels and whose scalars never leave the device (CUDA graph of several
+// iterations per host check).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -328,6 +329,151 @@ __global__ void k_cg_pupdate(int n, const double* __restrict__ r, double* p, con
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = r[i] + beta * p[i];
 }
 
+// ---- block-Jacobi preconditioned CG (opt-in; new, no reference counterpart).
+// D = the 3x3 diagonal node blocks of K (BCs applied: a fixed DOF's row and
+// column are the identity's), inverted once per solve; z = D^-1 r.  The
+// stop test stays sqrt(r.r / r0.r0) < tol; alpha = r.z / p.Kp, beta = r.z_new / r.z.
+
+__global__ void k_block_jacobi(int N, const int* __restrict__ off, const int* __restrict__ col,
+                               const double* __restrict__ K, double* dinv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int rb = off[i], nb = off[i + 1] - rb;
+    int kd = 0;
+    for (int k = 0; k < nb; ++k)
+        if (col[rb + k] == i) kd = k;
+    double a[9];
+    for (int c = 0; c < 9; ++c) a[c] = K[9LL * rb + (size_t)c * nb + kd];
+    // inverse by cofactors (the block is symmetric positive definite)
+    const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+    const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    const double id = (det != 0.0) ? 1.0 / det : 0.0;
+    double* d = dinv + 9LL * i;
+    d[0] = c00 * id;
+    d[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    d[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    d[3] = c01 * id;
+    d[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    d[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    d[6] = c02 * id;
+    d[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    d[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+}
+
+// Two last-block-done sums in one pass (partials hold 2 * gridDim.x values).
+__device__ __forceinline__ bool last_block_sum2(double a, double b, double* partials, unsigned int* ticket, double* oa,
+                                                double* ob) {
+    __shared__ double red[32];
+    __shared__ bool am_last;
+    const double sa = block_sum(a, red);
+    const double sb = block_sum(b, red);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = sa;
+        partials[gridDim.x + blockIdx.x] = sb;
+        __threadfence();
+        am_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+    double ta = 0.0, tb = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+        ta += __ldcg(partials + k);
+        tb += __ldcg(partials + gridDim.x + k);
+    }
+    ta = block_sum(ta, red);
+    tb = block_sum(tb, red);
+    if (threadIdx.x == 0) {
+        *oa = ta;
+        *ob = tb;
+        *ticket = 0;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void apply_dinv(const double* __restrict__ d, const double r[3], double z[3]) {
+    z[0] = d[0] * r[0] + d[1] * r[1] + d[2] * r[2];
+    z[1] = d[3] * r[0] + d[4] * r[1] + d[5] * r[2];
+    z[2] = d[6] * r[0] + d[7] * r[1] + d[8] * r[2];
+}
+
+// u = 0, r = f, z = D^-1 f, p = z; rres = r.r (= r0.r0), rr = r.z
+__global__ void k_pcg_init(int N, const double* __restrict__ f, const double* __restrict__ dinv, double* u, double* r,
+                           double* z, double* p, double* partials, CgCtl* ctl, int max_iter) {
+    double srr = 0.0, srz = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        double ri[3], zi[3];
+        for (int d = 0; d < 3; ++d) ri[d] = f[3 * i + d];
+        apply_dinv(dinv + 9LL * i, ri, zi);
+        for (int d = 0; d < 3; ++d) {
+            u[3 * i + d] = 0.0;
+            r[3 * i + d] = ri[d];
+            z[3 * i + d] = zi[d];
+            p[3 * i + d] = zi[d];
+            srr += ri[d] * ri[d];
+            srz += ri[d] * zi[d];
+        }
+    }
+    double trr, trz;
+    if (last_block_sum2(srr, srz, partials, &ctl->ticket, &trr, &trz) && threadIdx.x == 0) {
+        ctl->rr0 = trr;
+        ctl->rres = trr;
+        ctl->rr = trz;
+        ctl->iters = 0;
+        ctl->status = 0;
+        ctl->rel = 1.0;
+        ctl->done = 0;
+        if (trr == 0.0) {
+            ctl->done = 1;
+            ctl->rel = 0.0;
+        } else if (max_iter <= 0) {
+            ctl->done = 1;
+            ctl->status = 2;
+        }
+    }
+}
+
+// u += alpha p; r -= alpha q; z = D^-1 r; r.r for the stop test, r.z for beta.
+__global__ void k_pcg_axpy_dot(int N, const double* __restrict__ dinv, double* u, double* r, double* z,
+                               const double* __restrict__ p, const double* __restrict__ q, double* partials,
+                               CgCtl* ctl, double tol, int max_iter) {
+    if (ctl->done) return;
+    const double alpha = ctl->alpha;
+    double srr = 0.0, srz = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        double ri[3], zi[3];
+        for (int d = 0; d < 3; ++d) {
+            u[3 * i + d] += alpha * p[3 * i + d];
+            ri[d] = r[3 * i + d] - alpha * q[3 * i + d];
+            r[3 * i + d] = ri[d];
+        }
+        apply_dinv(dinv + 9LL * i, ri, zi);
+        for (int d = 0; d < 3; ++d) {
+            z[3 * i + d] = zi[d];
+            srr += ri[d] * ri[d];
+            srz += ri[d] * zi[d];
+        }
+    }
+    double trr, trz;
+    if (last_block_sum2(srr, srz, partials, &ctl->ticket, &trr, &trz) && threadIdx.x == 0) {
+        const double rel = (ctl->rr0 > 0.0) ? sqrt(trr / ctl->rr0) : sqrt(trr);
+        ctl->iters += 1;
+        ctl->rres = trr;
+        if (rel < tol) {
+            ctl->rel = rel;
+            ctl->done = 1;
+        } else {
+            ctl->beta = trz / ctl->rr;
+            ctl->rr = trz;
+            if (ctl->iters >= max_iter) {
+                ctl->rel = rel;
+                ctl->status = 2;
+                ctl->done = 1;
+            }
+        }
+    }
+}
+
 static int cg_grid(const tlfea_solver_s* s) { return s->cg_blocks; }
 
 static int launch_cg_iteration(tlfea_solver_s* s, cudaStream_t st) {
@@ -336,6 +482,14 @@ static int launch_cg_iteration(tlfea_solver_s* s, cudaStream_t st) {
     const int G = cg_grid(s);
     k_cg_spmv_dot<<<G, 256, 0, st>>>(el->N, el->pat_off, el->pat_col, s->K, s->p, s->q, s->cg_part, s->ctl);
     if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+    if (s->precond) {
+        k_pcg_axpy_dot<<<G, 256, 0, st>>>(el->N, s->dinv, s->u, s->r, s->z, s->p, s->q, s->cg_part, s->ctl, s->tol,
+                                          s->max_iter);
+        if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+        k_cg_pupdate<<<G, 256, 0, st>>>(n, s->z, s->p, s->ctl);  // p = z + beta p
+        if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+        return TLFEA_OK;
+    }
     k_cg_axpy_dot<<<G, 256, 0, st>>>(n, s->u, s->r, s->p, s->q, s->cg_part, s->ctl, s->tol, s->max_iter);
     if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
     k_cg_pupdate<<<G, 256, 0, st>>>(n, s->r, s->p, s->ctl);
@@ -368,6 +522,7 @@ static int build_cg_graph(tlfea_solver_s* s, int iters) {
         return TLFEA_CUDA_ERROR;
     }
     s->cg_graph_iters = iters;
+    s->cg_graph_precond = s->precond;
     return TLFEA_OK;
 }
 
@@ -392,7 +547,7 @@ int linear_static_prepare(tlfea_solver_s* s) {
         TLFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_spmv_dot, 256, 0));
         const int rows_warps = (el->N + 7) / 8;
         s->cg_blocks = std::max(1, std::min(rows_warps, std::max(per_sm, 1) * sms));
-        if ((st = dalloc(&s->cg_part, (size_t)s->cg_blocks))) return st;
+        if ((st = dalloc(&s->cg_part, 2 * (size_t)s->cg_blocks))) return st;
     }
     return TLFEA_OK;
 }
@@ -434,7 +589,14 @@ int linear_static_solve(tlfea_solver_s* s) {
     s->k_built = true;
     // SolveLinearSystemCG
     const int G = cg_grid(s);
-    k_cg_init<<<G, 256, 0, stream>>>(n3, s->f, s->u, s->r, s->p, s->cg_part, s->ctl, s->max_iter);
+    if (s->precond) {
+        if (!s->dinv && ((st = dalloc(&s->dinv, 9 * (size_t)N)) || (st = dalloc(&s->z, (size_t)n3)))) return st;
+        k_block_jacobi<<<(N + 255) / 256, 256, 0, stream>>>(N, el->pat_off, el->pat_col, s->K, s->dinv);
+        TLFEA_CHECK_LAUNCH();
+        k_pcg_init<<<G, 256, 0, stream>>>(N, s->f, s->dinv, s->u, s->r, s->z, s->p, s->cg_part, s->ctl, s->max_iter);
+    } else {
+        k_cg_init<<<G, 256, 0, stream>>>(n3, s->f, s->u, s->r, s->p, s->cg_part, s->ctl, s->max_iter);
+    }
     TLFEA_CHECK_LAUNCH();
     int chunk = 8;
     long long launched = 0;
@@ -443,7 +605,7 @@ int linear_static_solve(tlfea_solver_s* s) {
         TLFEA_CUDA(cudaMemcpyAsync(&h, s->ctl, sizeof(CgCtl), cudaMemcpyDeviceToHost, stream));
         TLFEA_CUDA(cudaStreamSynchronize(stream));
         if (h.done || launched >= s->max_iter) break;
-        if (!s->cg_graph || s->cg_graph_iters != chunk) {
+        if (!s->cg_graph || s->cg_graph_iters != chunk || s->cg_graph_precond != s->precond) {
             if ((st = build_cg_graph(s, chunk))) return st;
         }
         TLFEA_CUDA(cudaGraphLaunch(s->cg_graph, stream));
@@ -532,6 +694,8 @@ void linear_static_free(tlfea_solver_s* s) {
     dfree(s->ctl);
     dfree(s->ctl_apply);
     dfree(s->cg_part);
+    dfree(s->dinv);
+    dfree(s->z);
 }
 
 }  // namespace tlfea

@@ -15,8 +15,9 @@ struct CgCtl {
     int done;             // 1 once converged, broken down or out of iterations
     int iters;            // completed iterations
     int status;           // 0 ok, 1 p.Kp <= 0, 2 max_iter reached
-    double rr0, rr, alpha, beta, rel;
+    double rr0, rr, alpha, beta, rel;  // preconditioned: rr holds r.z, rres the true r.r
     double pq;
+    double rres;
 };
 
 }  // namespace tlfea
@@ -51,7 +52,11 @@ struct tlfea_solver_s {
     unsigned char* is_fixed = nullptr;  // 3N
     tlfea::CgCtl* ctl = nullptr;
     tlfea::CgCtl* ctl_apply = nullptr;  // scratch control block of linear_static_apply
-    double* cg_part = nullptr;  // per-block partials
+    double* cg_part = nullptr;  // per-block partials (2 arrays of cg_blocks)
+    int precond = 0;            // 0 none (the reference's CG), 1 block Jacobi (3x3 node diagonal blocks)
+    double* dinv = nullptr;     // block Jacobi: inverse diagonal blocks, 9 per node
+    double* z = nullptr;        // block Jacobi: z = D^-1 r
+    int cg_graph_precond = -1;  // preconditioner the captured graph was built for
     int cg_blocks = 0;
     cudaGraphExec_t cg_graph = nullptr;
     int cg_graph_iters = 0;

@@ -136,6 +136,12 @@ int tlfea_linear_static_retrieve_k(tlfea_solver s, long long* nnz, int* offsets,
     return linear_static_retrieve_k(s, nnz, offsets, columns, values);
 }
 
+int tlfea_linear_static_set_preconditioner(tlfea_solver s, int kind) {
+    if (!s || s->kind != KIND_LINEAR_STATIC || (kind != 0 && kind != 1)) return TLFEA_INVALID_ARG;
+    s->precond = kind;
+    return TLFEA_OK;
+}
+
 int tlfea_linear_static_apply(tlfea_solver s, const double* d_x, double* d_y) {
     if (!s || s->kind != KIND_LINEAR_STATIC || !d_x || !d_y) return TLFEA_INVALID_ARG;
     cudaSetDevice(s->device);
