@@ -156,18 +156,20 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force(TileArgs<R> A) {
     process_tile<R, NPE, NQP, MODE, DAMP>(A, blockIdx.x, smem);
 }
 
-// Sum of each shared node's per-tile partials, in tile order.
+// Sum of each shared node's per-tile partials, in tile order.  Partial slots
+// are numbered by shared node (build_tiling), so node b's partials are the
+// contiguous range [boff[b], boff[b+1]) and consecutive threads read
+// consecutive memory.
 template <typename R, bool ACCUM>
 __global__ void k_combine(int nb, const int* __restrict__ bgid, const int* __restrict__ boff,
-                          const int* __restrict__ bslots, const R* __restrict__ partial, R* f_out) {
+                          const R* __restrict__ partial, R* f_out) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
     R s0 = R(0), s1 = R(0), s2 = R(0);
     for (int k = boff[b]; k < boff[b + 1]; ++k) {
-        const int p = bslots[k];
-        s0 += partial[3 * p + 0];
-        s1 += partial[3 * p + 1];
-        s2 += partial[3 * p + 2];
+        s0 += partial[3 * k + 0];
+        s1 += partial[3 * k + 1];
+        s2 += partial[3 * k + 2];
     }
     const int g = bgid[b];
     if (ACCUM) {
@@ -613,8 +615,8 @@ template <typename R, bool ACCUM>
 static int launch_combine(tlfea_element_s* h, const R* partial, R* f_out) {
     const int nb = h->tl.n_bnodes;
     if (nb == 0) return TLFEA_OK;
-    k_combine<R, ACCUM><<<(nb + 255) / 256, 256, 0, h->stream>>>(nb, h->tl.bnode_gid, h->tl.bnode_off,
-                                                                 h->tl.bnode_slots, partial, f_out);
+    k_combine<R, ACCUM><<<(nb + 255) / 256, 256, 0, h->stream>>>(nb, h->tl.bnode_gid, h->tl.bnode_off, partial,
+                                                                 f_out);
     TLFEA_CHECK_LAUNCH();
     return TLFEA_OK;
 }

@@ -407,7 +407,7 @@ inline size_t tile_tma_smem_bytes(int max_local, bool damp) {
 }
 
 template <typename R, int NPE, int NQP, bool DAMP>
-__global__ void __launch_bounds__(TILE_ELEMS, (sizeof(R) == 4 && !DAMP) ? 5 : 1) k_tile_force_tma(TileArgs<R> A, int* err) {
+__global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, int* err) {
     using G = TileTmaGeom<R, NPE>;
     constexpr int TE = TILE_ELEMS;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -464,7 +464,6 @@ __global__ void __launch_bounds__(TILE_ELEMS, (sizeof(R) == 4 && !DAMP) ? 5 : 1)
     __syncthreads();  // positions and node tables staged; barriers initialised
 
     int lc[NPE];
-    R un[NPE][3];
     R f[NPE][3];
 #pragma unroll
     for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
@@ -476,15 +475,6 @@ __global__ void __launch_bounds__(TILE_ELEMS, (sizeof(R) == 4 && !DAMP) ? 5 : 1)
         if (q == 0) {
 #pragma unroll
             for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
-            if constexpr (sizeof(R) == 4) {
-                // FP32: the element's node displacements stay in registers for every QP
-#pragma unroll
-                for (int a = 0; a < NPE; ++a) {
-                    un[a][0] = xs[lc[a]];
-                    un[a][1] = ys[lc[a]];
-                    un[a][2] = zs[lc[a]];
-                }
-            }
         }
         R g[NPE][3];
 #pragma unroll
@@ -540,7 +530,7 @@ __global__ void __launch_bounds__(TILE_ELEMS, (sizeof(R) == 4 && !DAMP) ? 5 : 1)
                 for (int j = 0; j < 3; ++j) H[i][j] = R(0);
 #pragma unroll
             for (int a = 0; a < NPE; ++a) {
-                const R ua[3] = {un[a][0], un[a][1], un[a][2]};
+                const R ua[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
