@@ -296,7 +296,11 @@ int tlfea_batch_set_fixed(tlfea_batch b, const int* nodes, int n);
 int tlfea_batch_set_external_force(tlfea_batch b, const double* f, long long n, int on_device);
 /* Warm start u0 (3 * n_nodes; NULL = cold start u0 = 0). */
 int tlfea_batch_set_initial_guess(tlfea_batch b, const double* u0, long long n, int on_device);
-/* TLFEA_PRECISION_FP64 (default) or FP32 element work (the CG stays FP64). */
+/* TLFEA_PRECISION_FP64 (default) or FP32 element work.  With FP32 the CG's
+ * vectors, dots and stop test stay FP64, and after the CG the true residual
+ * ||f - K u||_free / ||f_free|| is evaluated with the FP64 operator; instances
+ * still above tol restart the FP32 CG from their solution (up to 4 passes).
+ * The residual reported is that FP64 one, the iterations the sum of passes. */
 int tlfea_batch_set_precision(tlfea_batch b, int precision);
 /* Launch shape: resident blocks per SM of the persistent kernel (0 = occupancy
  * maximum) and nodes per reduction chunk (0 = keep). */

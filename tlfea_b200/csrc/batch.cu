@@ -67,12 +67,23 @@ struct tlfea_batch_s {
     bool material_set = false;
     // launch
     int blocks_per_sm = 0;  // 0 = occupancy maximum
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;  // the captured cold-start solve
+    cudaGraphExec_t graph_w = nullptr;  // the captured warm-start solve
     double graph_tol = -1.0;
     int graph_max_iter = -1;
-    bool graph_warm = false;
     int graph_grid = -1;
+    int graph_precision = -1;
+    // FP32 element work: iterations summed over the refinement passes
+    std::vector<int> iters_total;
+    bool refined = false;
 };
+
+// Captured launches of a batch are rebuilt whenever the launch shape changes.
+static void drop_graphs(tlfea_batch_s* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->graph_w) cudaGraphExecDestroy(b->graph_w);
+    b->graph = b->graph_w = nullptr;
+}
 
 namespace tlfea {
 
@@ -634,10 +645,7 @@ static int build_chunks(tlfea_batch_s* b, int chunk_nodes) {
     TLFEA_CUDA(cudaMemcpy(b->chunk_beg, cbeg.data(), cbeg.size() * sizeof(int), cudaMemcpyHostToDevice));
     TLFEA_CUDA(cudaMemcpy(b->inst_chunk, ichunk.data(), ichunk.size() * sizeof(int), cudaMemcpyHostToDevice));
     b->chunk_nodes = chunk_nodes;
-    if (b->graph) {
-        cudaGraphExecDestroy(b->graph);
-        b->graph = nullptr;
-    }
+    drop_graphs(b);
     return TLFEA_OK;
 }
 
@@ -901,7 +909,7 @@ int tlfea_batch_create_shared(int type, int n_inst, int n_nodes, int n_elem, con
 int tlfea_batch_destroy(tlfea_batch b) {
     CHECK_BATCH(b);
     if (b->el) cudaSetDevice(b->el->device);
-    if (b->graph) cudaGraphExecDestroy(b->graph);
+    drop_graphs(b);
     dfree(b->lam); dfree(b->mu); dfree(b->lam32); dfree(b->mu32);
     dfree(b->fixed); dfree(b->chunk_inst); dfree(b->chunk_beg); dfree(b->inst_chunk); dfree(b->tile_inst);
     dfree(b->u); dfree(b->r); dfree(b->p); dfree(b->q); dfree(b->f); dfree(b->u0);
@@ -994,10 +1002,7 @@ int tlfea_batch_set_initial_guess(tlfea_batch b, const double* u0, long long n, 
 int tlfea_batch_set_precision(tlfea_batch b, int precision) {
     CHECK_BATCH(b);
     if (precision != TLFEA_PRECISION_FP64 && precision != TLFEA_PRECISION_FP32) return TLFEA_INVALID_ARG;
-    if (precision != b->precision && b->graph) {
-        cudaGraphExecDestroy(b->graph);
-        b->graph = nullptr;
-    }
+    if (precision != b->precision) drop_graphs(b);
     b->precision = precision;
     return TLFEA_OK;
 }
@@ -1009,10 +1014,7 @@ int tlfea_batch_set_launch(tlfea_batch b, int blocks_per_sm, int chunk_nodes) {
         const int st = build_chunks(b, chunk_nodes);
         if (st) return st;
     }
-    if (blocks_per_sm != b->blocks_per_sm && b->graph) {
-        cudaGraphExecDestroy(b->graph);
-        b->graph = nullptr;
-    }
+    if (blocks_per_sm != b->blocks_per_sm) drop_graphs(b);
     b->blocks_per_sm = blocks_per_sm;
     return TLFEA_OK;
 }
@@ -1030,6 +1032,43 @@ int tlfea_batch_get_launch(tlfea_batch b, int* blocks_per_sm, int* chunk_nodes, 
     return TLFEA_OK;
 }
 
+// One persistent launch of the whole CG (element work in b->precision),
+// captured once per (grid, tol, max_iter, precision, warm) and replayed.
+static int run_captured(tlfea_batch_s* b, int grid, double tol, int max_iter, bool warm) {
+    cudaStream_t st = b->el->stream;
+    if (b->graph_tol != tol || b->graph_max_iter != max_iter || b->graph_grid != grid ||
+        b->graph_precision != b->precision) {
+        drop_graphs(b);
+        b->graph_tol = tol;
+        b->graph_max_iter = max_iter;
+        b->graph_grid = grid;
+        b->graph_precision = b->precision;
+    }
+    cudaGraphExec_t& ge = warm ? b->graph_w : b->graph;
+    if (!ge) {
+        cudaGraph_t g = nullptr;
+        TLFEA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e1 = cudaMemsetAsync(b->n_done, 0, sizeof(int), st);
+        const int rc = (e1 == cudaSuccess) ? batch_launch(b, grid, tol, max_iter, warm, st) : TLFEA_CUDA_ERROR;
+        cudaError_t e2 = cudaStreamEndCapture(st, &g);
+        if (rc != TLFEA_OK || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            set_error("batch_solve: capture of the persistent launch failed");
+            return TLFEA_CUDA_ERROR;
+        }
+        cudaError_t e3 = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) {
+            ge = nullptr;
+            set_error(std::string("batch_solve: cudaGraphInstantiate: ") + cudaGetErrorString(e3));
+            return TLFEA_CUDA_ERROR;
+        }
+    }
+    TLFEA_CUDA(cudaGraphLaunch(ge, st));
+    return TLFEA_OK;
+}
+
 int tlfea_batch_solve(tlfea_batch b, double tol, int max_iter) {
     CHECK_BATCH(b);
     if (!b->material_set) {
@@ -1041,38 +1080,39 @@ int tlfea_batch_solve(tlfea_batch b, double tol, int max_iter) {
     int grid = 0;
     int s = batch_dispatch_grid(b, b->blocks_per_sm, &grid);
     if (s) return s;
-    // one persistent launch, captured once per (grid, tol, max_iter, warm)
-    if (!b->graph || b->graph_tol != tol || b->graph_max_iter != max_iter || b->graph_warm != b->warm ||
-        b->graph_grid != grid) {
-        if (b->graph) {
-            cudaGraphExecDestroy(b->graph);
-            b->graph = nullptr;
-        }
-        cudaGraph_t g = nullptr;
-        TLFEA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e1 = cudaMemsetAsync(b->n_done, 0, sizeof(int), st);
-        const int rc = (e1 == cudaSuccess) ? batch_launch(b, grid, tol, max_iter, b->warm, st) : TLFEA_CUDA_ERROR;
-        cudaError_t e2 = cudaStreamEndCapture(st, &g);
-        if (rc != TLFEA_OK || e2 != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            cudaGetLastError();
-            set_error("batch_solve: capture of the persistent launch failed");
-            return TLFEA_CUDA_ERROR;
-        }
-        cudaError_t e3 = cudaGraphInstantiate(&b->graph, g, 0);
-        cudaGraphDestroy(g);
-        if (e3 != cudaSuccess) {
-            b->graph = nullptr;
-            set_error(std::string("batch_solve: cudaGraphInstantiate: ") + cudaGetErrorString(e3));
-            return TLFEA_CUDA_ERROR;
-        }
-        b->graph_tol = tol;
-        b->graph_max_iter = max_iter;
-        b->graph_warm = b->warm;
-        b->graph_grid = grid;
+    b->refined = false;
+    if ((s = run_captured(b, grid, tol, max_iter, b->warm))) return s;
+    if (b->precision != TLFEA_PRECISION_FP32) {
+        TLFEA_CUDA(cudaStreamSynchronize(st));
+        return TLFEA_OK;
     }
-    TLFEA_CUDA(cudaGraphLaunch(b->graph, st));
-    TLFEA_CUDA(cudaStreamSynchronize(st));
+    // FP32 element work, FP64 verdict: the true residual ||f - K u||_free / ||f_free||
+    // is evaluated with the FP64 operator (the warm-start prologue of the FP64
+    // kernel, no iterations); instances still above tol restart the FP32 CG from
+    // their current solution.  The reported residual is the FP64 one.
+    const size_t n = (size_t)b->n_inst, n3 = 3 * (size_t)b->N;
+    std::vector<int> it((size_t)n);
+    b->iters_total.assign(n, 0);
+    int grid64 = 0;
+    s = (b->el->npe == 10) ? batch_grid<double, 10, 5>(b, 0, &grid64) : batch_grid<double, 4, 1>(b, 0, &grid64);
+    if (s) return s;
+    constexpr int MAX_REFINE = 4;
+    for (int pass = 0;; ++pass) {
+        TLFEA_CUDA(cudaMemcpyAsync(it.data(), b->iters, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+        TLFEA_CUDA(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < n; ++i) b->iters_total[i] += it[i];
+        TLFEA_CUDA(cudaMemcpyAsync(b->u0, b->u, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        TLFEA_CUDA(cudaMemsetAsync(b->n_done, 0, sizeof(int), st));
+        s = (b->el->npe == 10) ? launch_batch_cg<double, 10, 5>(b, grid64, tol, 0, true, st)
+                               : launch_batch_cg<double, 4, 1>(b, grid64, tol, 0, true, st);
+        if (s) return s;
+        int nd = 0;
+        TLFEA_CUDA(cudaMemcpyAsync(&nd, b->n_done, sizeof(int), cudaMemcpyDeviceToHost, st));
+        TLFEA_CUDA(cudaStreamSynchronize(st));
+        if (nd >= b->n_inst || pass == MAX_REFINE) break;
+        if ((s = run_captured(b, grid, tol, max_iter, true))) return s;
+    }
+    b->refined = true;
     return TLFEA_OK;
 }
 
@@ -1080,7 +1120,12 @@ int tlfea_batch_get_results(tlfea_batch b, int* iters, double* rel, int* status)
     CHECK_BATCH(b);
     cudaStream_t st = b->el->stream;
     const size_t n = (size_t)b->n_inst;
-    if (iters) TLFEA_CUDA(cudaMemcpyAsync(iters, b->iters, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (iters) {
+        if (b->refined)
+            std::memcpy(iters, b->iters_total.data(), n * sizeof(int));
+        else
+            TLFEA_CUDA(cudaMemcpyAsync(iters, b->iters, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    }
     if (rel) TLFEA_CUDA(cudaMemcpyAsync(rel, b->rel, n * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (status) TLFEA_CUDA(cudaMemcpyAsync(status, b->status, n * sizeof(int), cudaMemcpyDeviceToHost, st));
     TLFEA_CUDA(cudaStreamSynchronize(st));
@@ -1189,10 +1234,7 @@ int tlfea_batch_autotune(tlfea_batch b, int trial_iters, int* best_blocks_per_sm
     cudaEventDestroy(e1);
     if (s) return s;
     if ((s = build_chunks(b, bc))) return s;
-    if (b->graph) {
-        cudaGraphExecDestroy(b->graph);
-        b->graph = nullptr;
-    }
+    drop_graphs(b);
     b->blocks_per_sm = bb;
     if (best_blocks_per_sm) *best_blocks_per_sm = bb;
     if (best_chunk) *best_chunk = bc;
