@@ -10,6 +10,7 @@
 // Link with -ltlfea_b200 (tlfea_b200/libtlfea_b200.so).
 #pragma once
 
+#include <algorithm>
 #include <cstdio>
 #include <map>
 #include <stdexcept>
@@ -157,6 +158,16 @@ class SolverBase {
     }
     // new: ||(f_int - f_ext)_free|| / ||f_ext|| < rel_tol ends a solve (0 = off)
     void SetRelativeResidualStop(double rel_tol) { check(tlfea_solver_set_stop_rule(s_, rel_tol), "SetStopRule"); }
+    // new: n_steps Solve() calls in one graph launch, load f_base + amp sin(omega t_k + phase) f_var
+    // (f_var empty = constant load); returns each step's total inner iterations
+    std::vector<int> RunSteps(int n_steps, const VectorXR& f_var = {}, double amp = 1.0, double omega = 0.0,
+                              double phase = 0.0, double t0 = 0.0) {
+        std::vector<int> its((size_t)std::max(n_steps, 1), 0);
+        check(tlfea_solver_run_steps(s_, n_steps, t0, f_var.empty() ? nullptr : f_var.data(), amp, omega, phase,
+                                     its.data()),
+              "RunSteps");
+        return its;
+    }
 
   protected:
     tlfea_solver s_ = nullptr;

@@ -260,6 +260,23 @@ int tlfea_solver_get_stats(tlfea_solver s, tlfea_solve_stats* st);
  * those positions -- once it is below rel_tol.  0 turns it off (default). */
 int tlfea_solver_set_stop_rule(tlfea_solver s, double rel_tol);
 
+/* New, no reference counterpart: n_steps implicit steps of a first-order solver
+ * in one call -- the loop a reference driver writes around SetExternalForce +
+ * Solve (examples/beam_simulation.cc:275-283, examples/test_feat10_nesterov.cc:
+ * 197-199) -- launched as one CUDA graph with
+ * the load computed on the device.  Step k (0-based) ends at
+ * t_k = t0 + (k + 1) * time_step and runs with
+ *     f_ext = f_base + (amp * sin(omega * t_k + phase)) * f_var
+ * (f_base = the external force set before the call, f_var a host array of
+ * 3 * n_nodes doubles; products and sums rounded separately, no fused
+ * multiply-add).  f_var NULL keeps f_ext constant.  inner_iters (NULL or n_steps
+ * ints) receives each step's total inner iterations; the solve statistics are
+ * those of the last step, with status the last non-zero step status.  After
+ * the call f_ext holds the last step's load.  The linear static solver is
+ * refused (TLFEA_INVALID_ARG). */
+int tlfea_solver_run_steps(tlfea_solver s, int n_steps, double t0, const double* f_var, double amp,
+                           double omega, double phase, int* inner_iters);
+
 /* ------------------------------------------------- batched linear static
  * New, no reference counterpart: many independent meshes solved by one
  * persistent cooperative launch (captured in a CUDA graph).  Per instance the

@@ -376,6 +376,20 @@ class _FirstOrder(SolverBase):
         (FP64, evaluated every inner iteration); 0 turns the rule off."""
         capi.call("tlfea_solver_set_stop_rule", self._h, float(rel_tol))
 
+    def RunSteps(self, n_steps: int, f_var=None, amp: float = 1.0, omega: float = 0.0, phase: float = 0.0,
+                 t0: float = 0.0):
+        """New: n_steps calls of Solve() in one launch (one CUDA graph), the loop
+        of examples/beam_simulation.cc:275-283.  With f_var, step k runs with
+        f_ext = f_base + (amp * sin(omega * t_k + phase)) * f_var, where f_base is
+        the external force set before the call and t_k = t0 + (k + 1) * time_step.
+        Returns each step's total inner iterations."""
+        n = int(n_steps)
+        its = np.zeros(max(n, 1), dtype=np.int32)
+        fv = _f64(f_var, 3 * self.n_coef) if f_var is not None else None
+        capi.call("tlfea_solver_run_steps", self._h, n, float(t0), capi.dptr(fv) if fv is not None else None,
+                  float(amp), float(omega), float(phase), capi.iptr(its))
+        return its
+
     def __del__(self):
         try:
             if getattr(self, "_h", None) is not None:

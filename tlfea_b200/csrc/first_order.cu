@@ -435,7 +435,16 @@ void first_order_free(tlfea_solver_s* s) {
     dfree(s->red); dfree(s->dstat); dfree(s->node_fixed);
 }
 
-int first_order_solve(tlfea_solver_s* s) {
+// f_ext = f_base + a * f_var, rounded multiply then rounded add (no fused
+// multiply-add), so a host loop computing the same load in FP64 matches bitwise.
+__global__ void k_step_load(int n3, const double* __restrict__ f_base, const double* __restrict__ f_var,
+                            double a, double* __restrict__ f_ext) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n3) f_ext[i] = __dadd_rn(f_base[i], __dmul_rn(a, f_var[i]));
+}
+
+// One Solve(), or n implicit steps with a time-varying load (new).
+int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* inner_iters) {
     tlfea_element_s* el = s->el;
     if (!el->is_setup) {
         set_error("element must be set up first");
@@ -512,65 +521,135 @@ int first_order_solve(tlfea_solver_s* s) {
         S.rtol = s->ap.inner_rtol;
     }
     const bool damp = (el->eta_d != 0.0 || el->lambda_d != 0.0);
+    TileArgs<float> A32;
+    TileArgs<double> A64;
+    memset(&A32, 0, sizeof(A32));
+    memset(&A64, 0, sizeof(A64));
+    A32.node_off = A64.node_off = el->tl.node_off;
+    A32.ln_gid = A64.ln_gid = el->tl.ln_gid;
+    A32.ln_pslot = A64.ln_pslot = el->tl.ln_pslot;
+    A32.ln_inc_end = A64.ln_inc_end = el->tl.ln_inc_end;
+    A32.inc = A64.inc = el->tl.inc;
+    A32.lconn = A64.lconn = el->tl.lconn;
+    A32.tile_elem = A64.tile_elem = el->tl.tile_elem;
+    A32.v = A64.v = s->v_guess;
+    A32.max_local = A64.max_local = el->tl.max_local;
+    A32.grad = el->tl.grad32; A32.dv = el->tl.dv32; A32.px = el->ux; A32.py = el->uy; A32.pz = el->uz;
+    A32.f_out = el->f_int32; A32.partial = el->tl.partial32;
+    A32.lambda = (float)el->lambda; A32.mu = (float)el->mu; A32.eta = (float)el->eta_d; A32.lamd = (float)el->lambda_d;
+    A64.grad = el->tl.grad64; A64.dv = el->tl.dv64; A64.px = el->x; A64.py = el->y; A64.pz = el->z;
+    A64.f_out = el->f_int; A64.partial = el->tl.partial64;
+    A64.lambda = el->lambda; A64.mu = el->mu; A64.eta = el->eta_d; A64.lamd = el->lambda_d;
+    auto launch_one = [&](FOArgs& SS) -> int {
+        if (fp32) {
+            if (el->npe == 10)
+                return damp ? launch_first_order<float, 10, 5, true>(s, SS, A32)
+                            : launch_first_order<float, 10, 5, false>(s, SS, A32);
+            return damp ? launch_first_order<float, 4, 1, true>(s, SS, A32)
+                        : launch_first_order<float, 4, 1, false>(s, SS, A32);
+        }
+        if (el->npe == 10)
+            return damp ? launch_first_order<double, 10, 5, true>(s, SS, A64)
+                        : launch_first_order<double, 10, 5, false>(s, SS, A64);
+        return damp ? launch_first_order<double, 4, 1, true>(s, SS, A64)
+                    : launch_first_order<double, 4, 1, false>(s, SS, A64);
+    };
+    cudaStream_t stream = el->stream;
+    const int n_steps = std::max(1, steps);
+    int* stat_steps = s->dstat;
+    if (n_steps > 1 && (st = dalloc(&stat_steps, 16 * (size_t)n_steps))) return st;
+    auto release = [&]() {
+        if (stat_steps != s->dstat) dfree(stat_steps);
+    };
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    cudaEventRecord(e0, el->stream);
-    if (fp32) {
-        TileArgs<float> A;
-        memset(&A, 0, sizeof(A));
-        A.node_off = el->tl.node_off; A.ln_gid = el->tl.ln_gid; A.ln_pslot = el->tl.ln_pslot;
-        A.ln_inc_end = el->tl.ln_inc_end; A.inc = el->tl.inc; A.lconn = el->tl.lconn; A.tile_elem = el->tl.tile_elem;
-        A.grad = el->tl.grad32; A.dv = el->tl.dv32; A.px = el->ux; A.py = el->uy; A.pz = el->uz;
-        A.v = s->v_guess; A.f_out = el->f_int32; A.partial = el->tl.partial32;
-        A.lambda = (float)el->lambda; A.mu = (float)el->mu; A.eta = (float)el->eta_d; A.lamd = (float)el->lambda_d;
-        A.max_local = el->tl.max_local;
-        if (el->npe == 10)
-            st = damp ? launch_first_order<float, 10, 5, true>(s, S, A) : launch_first_order<float, 10, 5, false>(s, S, A);
-        else
-            st = damp ? launch_first_order<float, 4, 1, true>(s, S, A) : launch_first_order<float, 4, 1, false>(s, S, A);
+    cudaEventRecord(e0, stream);
+    // every step: the time-varying load, then one implicit step (Solve); more
+    // than one step runs as a single captured graph
+    auto enqueue = [&]() -> int {
+        for (int k = 0; k < n_steps; ++k) {
+            if (load) {
+                const double tk = load->t0 + (k + 1) * S.dt;
+                const double a = load->amp * sin(load->omega * tk + load->phase);
+                const int n3 = 3 * el->N;
+                k_step_load<<<(n3 + 255) / 256, 256, 0, stream>>>(n3, load->f_base, load->f_var, a, el->f_ext);
+                if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+            }
+            FOArgs SS = S;
+            SS.stat = stat_steps + 16 * k;
+            SS.stat_norm = (double*)(SS.stat + 4);
+            SS.stat_rel = (double*)(SS.stat + 6);
+            const int r = launch_one(SS);
+            if (r) return r;
+        }
+        return TLFEA_OK;
+    };
+    if (n_steps == 1) {
+        st = enqueue();
     } else {
-        TileArgs<double> A;
-        memset(&A, 0, sizeof(A));
-        A.node_off = el->tl.node_off; A.ln_gid = el->tl.ln_gid; A.ln_pslot = el->tl.ln_pslot;
-        A.ln_inc_end = el->tl.ln_inc_end; A.inc = el->tl.inc; A.lconn = el->tl.lconn; A.tile_elem = el->tl.tile_elem;
-        A.grad = el->tl.grad64; A.dv = el->tl.dv64; A.px = el->x; A.py = el->y; A.pz = el->z;
-        A.v = s->v_guess; A.f_out = el->f_int; A.partial = el->tl.partial64;
-        A.lambda = el->lambda; A.mu = el->mu; A.eta = el->eta_d; A.lamd = el->lambda_d;
-        A.max_local = el->tl.max_local;
-        if (el->npe == 10)
-            st = damp ? launch_first_order<double, 10, 5, true>(s, S, A) : launch_first_order<double, 10, 5, false>(s, S, A);
-        else
-            st = damp ? launch_first_order<double, 4, 1, true>(s, S, A) : launch_first_order<double, 4, 1, false>(s, S, A);
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+            release();
+            set_error("run_steps: stream capture failed");
+            return TLFEA_CUDA_ERROR;
+        }
+        st = enqueue();
+        const cudaError_t ec = cudaStreamEndCapture(stream, &g);
+        if (!st && ec == cudaSuccess && cudaGraphInstantiate(&ge, g, 0) == cudaSuccess) {
+            if (cudaGraphLaunch(ge, stream) != cudaSuccess) st = TLFEA_CUDA_ERROR;
+        } else if (!st) {
+            st = TLFEA_CUDA_ERROR;
+            set_error("run_steps: graph capture failed");
+        }
+        if (ge) cudaGraphExecDestroy(ge);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
     }
-    cudaEventRecord(e1, el->stream);
+    cudaEventRecord(e1, stream);
     if (st) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
+        release();
         return st;
     }
-    TLFEA_CUDA(cudaStreamSynchronize(el->stream));
+    TLFEA_CUDA(cudaStreamSynchronize(stream));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    int hs[16];
-    TLFEA_CUDA(cudaMemcpy(hs, s->dstat, sizeof(hs), cudaMemcpyDeviceToHost));
-    s->stats.outer_iters = hs[0];
-    s->stats.inner_iters_total = hs[1];
-    s->stats.last_inner_iters = hs[2];
-    s->stats.status = hs[3];
-    memcpy(&s->stats.last_norm_g, hs + 4, sizeof(double));
-    memcpy(&s->stats.rel_residual, hs + 6, sizeof(double));
-    s->stats.stop_rule_met = hs[8];
+    std::vector<int> hs(16 * (size_t)n_steps);
+    if (cudaMemcpy(hs.data(), stat_steps, hs.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        release();
+        set_error("run_steps: statistics read-back failed");
+        return TLFEA_CUDA_ERROR;
+    }
+    release();
+    int status = TLFEA_OK;
+    for (int k = 0; k < n_steps; ++k) {
+        const int* h = hs.data() + 16 * k;
+        if (inner_iters) inner_iters[k] = h[1];
+        if (h[3]) status = h[3];
+    }
+    const int* hl = hs.data() + 16 * (n_steps - 1);
+    s->stats.outer_iters = hl[0];
+    s->stats.inner_iters_total = hl[1];
+    s->stats.last_inner_iters = hl[2];
+    s->stats.status = status;
+    memcpy(&s->stats.last_norm_g, hl + 4, sizeof(double));
+    memcpy(&s->stats.rel_residual, hl + 6, sizeof(double));
+    s->stats.stop_rule_met = hl[8];
     s->stats.kernel_ms = ms;
     el->f_int_from32 = fp32;
     el->u_dirty = !fp32;  // the kernel keeps u in step with x in FP32 mode
-    if (s->stats.status == TLFEA_NONFINITE) {
+    if (status == TLFEA_NONFINITE) {
         set_error("non-finite gradient norm");
         return TLFEA_NONFINITE;
     }
     return TLFEA_OK;
 }
+
+int first_order_solve(tlfea_solver_s* s) { return first_order_steps(s, 1, nullptr, nullptr); }
 
 }  // namespace tlfea

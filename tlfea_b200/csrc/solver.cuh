@@ -20,6 +20,14 @@ struct CgCtl {
     double rres;
 };
 
+// Load of step k of a multi-step run: f_ext = f_base + amp * sin(omega * t_k + phase) * f_var,
+// t_k = t0 + (k + 1) * dt (the time at the end of step k).
+struct StepLoad {
+    const double* f_base;
+    const double* f_var;
+    double t0, amp, omega, phase;
+};
+
 }  // namespace tlfea
 
 struct tlfea_solver_s {

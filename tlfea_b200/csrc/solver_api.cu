@@ -8,6 +8,7 @@ namespace tlfea {
 int first_order_alloc(tlfea_solver_s* s);
 void first_order_free(tlfea_solver_s* s);
 int first_order_solve(tlfea_solver_s* s);
+int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* inner_iters);
 int linear_static_solve(tlfea_solver_s* s);
 int linear_static_retrieve_k(tlfea_solver_s* s, long long* nnz, int* offsets, int* columns, double* values);
 int linear_static_apply(tlfea_solver_s* s, const double* d_x, double* d_y);
@@ -121,6 +122,43 @@ int tlfea_solver_solve(tlfea_solver s) {
     cudaSetDevice(s->device);
     if (s->kind == KIND_LINEAR_STATIC) return linear_static_solve(s);
     return first_order_solve(s);
+}
+
+int tlfea_solver_run_steps(tlfea_solver s, int n_steps, double t0, const double* f_var, double amp,
+                           double omega, double phase, int* inner_iters) {
+    if (!s || n_steps < 1) return TLFEA_INVALID_ARG;
+    if (s->kind == KIND_LINEAR_STATIC) {
+        set_error("run_steps: the linear static solver has no time steps");
+        return TLFEA_INVALID_ARG;
+    }
+    cudaSetDevice(s->device);
+    if (!s->el->is_setup) {
+        set_error("element must be set up first");
+        return TLFEA_NOT_SETUP;
+    }
+    if (!f_var) return first_order_steps(s, n_steps, nullptr, inner_iters);
+    tlfea_element_s* el = s->el;
+    const size_t n3 = 3 * (size_t)el->N;
+    double *base = nullptr, *var = nullptr;
+    if (dalloc(&base, n3) || dalloc(&var, n3)) {
+        dfree(base);
+        dfree(var);
+        return TLFEA_CUDA_ERROR;
+    }
+    int st = TLFEA_OK;
+    if (cudaMemcpyAsync(base, el->f_ext, n3 * sizeof(double), cudaMemcpyDeviceToDevice, el->stream) != cudaSuccess ||
+        cudaMemcpyAsync(var, f_var, n3 * sizeof(double), cudaMemcpyHostToDevice, el->stream) != cudaSuccess) {
+        set_error("run_steps: load upload failed");
+        st = TLFEA_CUDA_ERROR;
+    }
+    if (!st) {
+        StepLoad L{base, var, t0, amp, omega, phase};
+        st = first_order_steps(s, n_steps, &L, inner_iters);
+    }
+    cudaStreamSynchronize(el->stream);
+    dfree(base);
+    dfree(var);
+    return st;
 }
 
 int tlfea_linear_static_last(tlfea_solver s, int* iters, double* rel_residual) {
