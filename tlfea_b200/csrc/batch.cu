@@ -149,14 +149,20 @@ __device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int item, con
     uint16_t* incs = iends + A.max_local;  // NPE * TE
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
     for (int k = t; k < NPE * TE; k += TE) incs[k] = A.inc[(size_t)tile * TE * NPE + k];
+    // p relative to the tile's first node, differenced in FP64: the gradients
+    // sum to zero over an element's nodes, so K p is unchanged, but the FP32
+    // copy no longer carries the (large, cancelling) common part of p and H =
+    // sum_a p_a (x) grad N_a keeps FP32 accuracy relative to the local variation
+    const int g0 = noff + A.ln_gid[lb];
+    const double r0 = p[3 * g0 + 0], r1 = p[3 * g0 + 1], r2 = p[3 * g0 + 2];
     for (int ln = t; ln < nl; ln += TE) {
         const int gid = noff + A.ln_gid[lb + ln];
         const int pslot = A.ln_pslot[lb + ln];
         dsts[ln] = (pslot < 0) ? gid : -(poff + pslot + 1);
         iends[ln] = A.ln_inc_end[lb + ln];
-        ps[3 * ln + 0] = R(p[3 * gid + 0]);
-        ps[3 * ln + 1] = R(p[3 * gid + 1]);
-        ps[3 * ln + 2] = R(p[3 * gid + 2]);
+        ps[3 * ln + 0] = R(p[3 * gid + 0] - r0);
+        ps[3 * ln + 1] = R(p[3 * gid + 1] - r1);
+        ps[3 * ln + 2] = R(p[3 * gid + 2] - r2);
     }
     int lc[NPE];
 #pragma unroll
