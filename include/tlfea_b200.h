@@ -313,11 +313,14 @@ int tlfea_batch_set_fixed(tlfea_batch b, const int* nodes, int n);
 int tlfea_batch_set_external_force(tlfea_batch b, const double* f, long long n, int on_device);
 /* Warm start u0 (3 * n_nodes; NULL = cold start u0 = 0). */
 int tlfea_batch_set_initial_guess(tlfea_batch b, const double* u0, long long n, int on_device);
-/* TLFEA_PRECISION_FP64 (default) or FP32 element work.  With FP32 the CG's
- * vectors, dots and stop test stay FP64, and after the CG the true residual
- * ||f - K u||_free / ||f_free|| is evaluated with the FP64 operator; instances
- * still above tol restart the FP32 CG from their solution (up to 4 passes).
- * The residual reported is that FP64 one, the iterations the sum of passes. */
+/* TLFEA_PRECISION_FP64 (default) or FP32 element work.  With FP32 the solve is
+ * iterative refinement: the true residual r = f - K u (free DOFs) is evaluated
+ * with the FP64 operator, the correction K d = r is solved by the CG with FP32
+ * element work (vectors, dots and its stop test FP64) to the relative tolerance
+ * max(tol, min(0.1, max(1e-4, sqrt(tol) / 2))), u += d, and again until every
+ * instance's FP64 residual ||r|| / ||f_free|| is below tol (at most 8 passes).
+ * The residual and status reported are the FP64 ones, the iterations the sum
+ * over passes.  FP32 solves are not graph-captured. */
 int tlfea_batch_set_precision(tlfea_batch b, int precision);
 /* Launch shape: resident blocks per SM of the persistent kernel (0 = occupancy
  * maximum) and nodes per reduction chunk (0 = keep). */

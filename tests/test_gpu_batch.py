@@ -151,9 +151,10 @@ def test_batch_edge_cases():
 
 
 def test_batch_fp32_elements_with_fp64_refinement():
-    """FP32 element work, FP64 verdict: the reported residual is the true
-    ||f - K u|| / ||f|| with the FP64 operator, refinement passes restart the
-    FP32 CG until it is below tol, and the answer matches the FP64 solve."""
+    """FP32 element work, FP64 verdict: iterative refinement (FP64 residual,
+    FP32-element CG on the correction) until the true ||f - K u|| / ||f|| with
+    the FP64 operator is below tol; the answer matches the FP64 solve and the
+    reported residual is the FP64 one."""
     import torch
 
     insts = _instances(4)

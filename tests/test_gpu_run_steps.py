@@ -111,7 +111,9 @@ def test_run_steps_tracks_the_oracle_trajectory():
     xg = el.RetrievePositionToCPU()
     du = np.stack([xg[0] - x, xg[1] - y, xg[2] - z])
     du_ref = np.stack([m.x - x, m.y - y, m.z - z])
-    assert rel(du, du_ref) < 1e-10
+    # positions agree to ~1e-16 (the fixed-count Nesterov tests); the tip
+    # displacement here is ~1e-7, so the relative tolerance on it is 1e-8
+    assert rel(du, du_ref) < 1e-8
     el.Destroy()
 
 

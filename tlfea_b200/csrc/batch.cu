@@ -76,6 +76,7 @@ struct tlfea_batch_s {
     // FP32 element work: iterations summed over the refinement passes
     std::vector<int> iters_total;
     bool refined = false;
+    double *rhs = nullptr, *uacc = nullptr;  // correction right-hand side, accumulated solution
 };
 
 // Captured launches of a batch are rebuilt whenever the launch shape changes.
@@ -594,8 +595,11 @@ static int batch_grid(tlfea_batch_s* b, int blocks_per_sm, int* grid_out, bool a
 }
 
 template <typename R, int NPE, int NQP>
-static int launch_batch_cg(tlfea_batch_s* b, int grid, double tol, int max_iter, bool warm, cudaStream_t st) {
+static int launch_batch_cg(tlfea_batch_s* b, int grid, double tol, int max_iter, bool warm, cudaStream_t st,
+                           const double* f_over = nullptr, const double* u0_over = nullptr) {
     BatchArgs<R> A = batch_args<R>(b);
+    if (f_over) A.f = f_over;
+    if (u0_over) A.u0 = u0_over;
     int w = warm ? 1 : 0;
     void* args[] = {&A, &tol, &max_iter, &w};
     TLFEA_CUDA(cudaLaunchCooperativeKernel((const void*)k_batch_cg<R, NPE, NQP>, dim3(grid), dim3(TILE_ELEMS), args,
@@ -919,6 +923,7 @@ int tlfea_batch_destroy(tlfea_batch b) {
     dfree(b->lam); dfree(b->mu); dfree(b->lam32); dfree(b->mu32);
     dfree(b->fixed); dfree(b->chunk_inst); dfree(b->chunk_beg); dfree(b->inst_chunk); dfree(b->tile_inst);
     dfree(b->u); dfree(b->r); dfree(b->p); dfree(b->q); dfree(b->f); dfree(b->u0);
+    dfree(b->rhs); dfree(b->uacc);
     dfree(b->cpa); dfree(b->cpb); dfree(b->rr); dfree(b->fnorm); dfree(b->rel);
     dfree(b->part64); dfree(b->part32);
     dfree(b->iters); dfree(b->status); dfree(b->done); dfree(b->n_done);
@@ -1038,6 +1043,21 @@ int tlfea_batch_get_launch(tlfea_batch b, int* blocks_per_sm, int* chunk_nodes, 
     return TLFEA_OK;
 }
 
+// Right-hand side of a correction pass: the FP64 residual of every instance
+// not yet converged, zero for the converged ones (their correction is zero).
+__global__ void k_batch_rhs(int n_chunks, const int* __restrict__ chunk_beg, const int* __restrict__ chunk_inst,
+                            const int* __restrict__ done, const double* __restrict__ r, double* rhs) {
+    for (int c = blockIdx.x; c < n_chunks; c += gridDim.x) {
+        const bool dn = done[chunk_inst[c]] != 0;
+        for (int i = 3 * chunk_beg[c] + threadIdx.x; i < 3 * chunk_beg[c + 1]; i += blockDim.x) rhs[i] = dn ? 0.0 : r[i];
+    }
+}
+
+__global__ void k_batch_accumulate(long long n, const double* __restrict__ d, double* u) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        u[i] += d[i];
+}
+
 // One persistent launch of the whole CG (element work in b->precision),
 // captured once per (grid, tol, max_iter, precision, warm) and replayed.
 static int run_captured(tlfea_batch_s* b, int grid, double tol, int max_iter, bool warm) {
@@ -1087,37 +1107,58 @@ int tlfea_batch_solve(tlfea_batch b, double tol, int max_iter) {
     int s = batch_dispatch_grid(b, b->blocks_per_sm, &grid);
     if (s) return s;
     b->refined = false;
-    if ((s = run_captured(b, grid, tol, max_iter, b->warm))) return s;
     if (b->precision != TLFEA_PRECISION_FP32) {
+        if ((s = run_captured(b, grid, tol, max_iter, b->warm))) return s;
         TLFEA_CUDA(cudaStreamSynchronize(st));
         return TLFEA_OK;
     }
-    // FP32 element work, FP64 verdict: the true residual ||f - K u||_free / ||f_free||
-    // is evaluated with the FP64 operator (the warm-start prologue of the FP64
-    // kernel, no iterations); instances still above tol restart the FP32 CG from
-    // their current solution.  The reported residual is the FP64 one.
+    // FP32 element work, FP64 verdict: iterative refinement on the correction
+    // equation.  Each pass evaluates the true residual r = f - K u with the FP64
+    // operator (the prologue of the FP64 kernel at u, no iterations), solves
+    // K d = r with the FP32-element CG to a relative tolerance tau, and adds d
+    // to u.  The FP32 rounding then acts on the correction, not on u, so every
+    // pass gains a factor of about max(tau, FP32 operator error) on the FP64
+    // residual.  The reported residual and stop test are the FP64 ones.
     const size_t n = (size_t)b->n_inst, n3 = 3 * (size_t)b->N;
-    std::vector<int> it((size_t)n);
+    if (!b->rhs && (dalloc(&b->rhs, n3) || dalloc(&b->uacc, n3))) return TLFEA_CUDA_ERROR;
+    std::vector<int> it(n);
     b->iters_total.assign(n, 0);
     int grid64 = 0;
     s = (b->el->npe == 10) ? batch_grid<double, 10, 5>(b, 0, &grid64) : batch_grid<double, 4, 1>(b, 0, &grid64);
     if (s) return s;
-    constexpr int MAX_REFINE = 4;
-    for (int pass = 0;; ++pass) {
-        TLFEA_CUDA(cudaMemcpyAsync(it.data(), b->iters, n * sizeof(int), cudaMemcpyDeviceToHost, st));
-        TLFEA_CUDA(cudaStreamSynchronize(st));
-        for (size_t i = 0; i < n; ++i) b->iters_total[i] += it[i];
-        TLFEA_CUDA(cudaMemcpyAsync(b->u0, b->u, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    const bool t10 = (b->el->npe == 10);
+    auto eval64 = [&](bool at_u, const double* u_at) -> int {  // FP64 residual at u_at (or at 0)
         TLFEA_CUDA(cudaMemsetAsync(b->n_done, 0, sizeof(int), st));
-        s = (b->el->npe == 10) ? launch_batch_cg<double, 10, 5>(b, grid64, tol, 0, true, st)
-                               : launch_batch_cg<double, 4, 1>(b, grid64, tol, 0, true, st);
-        if (s) return s;
+        return t10 ? launch_batch_cg<double, 10, 5>(b, grid64, tol, 0, at_u, st, nullptr, u_at)
+                   : launch_batch_cg<double, 4, 1>(b, grid64, tol, 0, at_u, st, nullptr, u_at);
+    };
+    const double tau = std::max(tol, std::min(0.1, std::max(1e-4, 0.5 * std::sqrt(tol))));
+    constexpr int MAX_PASSES = 8;
+    if ((s = eval64(b->warm, b->u0))) return s;
+    for (int pass = 0;; ++pass) {
         int nd = 0;
         TLFEA_CUDA(cudaMemcpyAsync(&nd, b->n_done, sizeof(int), cudaMemcpyDeviceToHost, st));
         TLFEA_CUDA(cudaStreamSynchronize(st));
-        if (nd >= b->n_inst || pass == MAX_REFINE) break;
-        if ((s = run_captured(b, grid, tol, max_iter, true))) return s;
+        if (nd >= b->n_inst || pass == MAX_PASSES) break;
+        // u (the FP64 kernel's copy of the evaluation point) is the accumulated solution
+        TLFEA_CUDA(cudaMemcpyAsync(b->uacc, b->u, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        k_batch_rhs<<<std::min(b->n_chunks, 4096), 256, 0, st>>>(b->n_chunks, b->chunk_beg, b->chunk_inst, b->done,
+                                                                 b->r, b->rhs);
+        TLFEA_CUDA(cudaGetLastError());
+        TLFEA_LAUNCHED(1);
+        TLFEA_CUDA(cudaMemsetAsync(b->n_done, 0, sizeof(int), st));
+        s = t10 ? launch_batch_cg<float, 10, 5>(b, grid, tau, max_iter, false, st, b->rhs, nullptr)
+                : launch_batch_cg<float, 4, 1>(b, grid, tau, max_iter, false, st, b->rhs, nullptr);
+        if (s) return s;
+        TLFEA_CUDA(cudaMemcpyAsync(it.data(), b->iters, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+        TLFEA_CUDA(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < n; ++i) b->iters_total[i] += it[i];
+        k_batch_accumulate<<<1184, 256, 0, st>>>((long long)n3, b->u, b->uacc);
+        TLFEA_CUDA(cudaGetLastError());
+        TLFEA_LAUNCHED(1);
+        if ((s = eval64(true, b->uacc))) return s;
     }
+    TLFEA_CUDA(cudaStreamSynchronize(st));
     b->refined = true;
     return TLFEA_OK;
 }
