@@ -98,6 +98,7 @@ struct BatchArgs {
     const uint16_t* inc;
     const uint16_t* lconn;
     const R* grad;
+    const R* ji;  // J^-1 per (tile, QP): the compact geometry stream
     const R* dv;
     const R* lam;
     const R* mu;
@@ -121,6 +122,7 @@ struct BatchArgs {
     const double* u0;
     double *cpa, *cpb, *rr, *fnorm, *rel;
     int *iters, *status, *done, *n_done;
+    QpBary qb;
 };
 
 // q = K p on one tile: H = sum_a p_a (x) gradN_a, P = lambda tr(H) I + mu (H + H^T)
@@ -177,51 +179,38 @@ __device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int item, con
     __syncthreads();
 #pragma unroll 1
     for (int qp = 0; qp < NQP; ++qp) {
-        const R* gp = A.grad + ((size_t)tile * NQP + qp) * (NPE * 3) * TE + t;
+        R xa[NPE][3];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) xa[a][d] = ps[3 * lc[a] + d];
+        const R* jp = A.ji + ((size_t)tile * NQP + qp) * 9 * TE + t;
         const R* dp = A.dv + ((size_t)tile * NQP + qp) * TE + t;
-        R g[NPE][3];
+        R ji[9];
         R dv;
         if (A.tiles_per_inst) {
-            // shared mesh: every instance re-reads these gradients, keep them in L2
+            // shared mesh: every instance re-reads this geometry, keep it in L2
 #pragma unroll
-            for (int a = 0; a < NPE; ++a)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) g[a][j] = __ldg(gp + (a * 3 + j) * TE);
+            for (int m = 0; m < 9; ++m) ji[m] = __ldg(jp + m * TE);
             dv = __ldg(dp);
         } else {
             // one instance per tile: a single pass, stream past L2
 #pragma unroll
-            for (int a = 0; a < NPE; ++a)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) g[a][j] = __ldcs(gp + (a * 3 + j) * TE);
+            for (int m = 0; m < 9; ++m) ji[m] = __ldcs(jp + m * TE);
             dv = __ldcs(dp);
         }
-        R H[3][3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) H[i][j] = R(0);
-#pragma unroll
-        for (int a = 0; a < NPE; ++a) {
-            const R pa[3] = {ps[3 * lc[a] + 0], ps[3 * lc[a] + 1], ps[3 * lc[a] + 2]};
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) H[i][j] += pa[i] * g[a][j];
-        }
+        const R L[4] = {R(A.qb.L[qp][0]), R(A.qb.L[qp][1]), R(A.qb.L[qp][2]), R(A.qb.L[qp][3])};
+        R G[3][3], H[3][3];
+        tet_dx_dxi<R, NPE>(xa, L, G);
+        mul_jinv(G, ji, H);
         const R tr = lam * (H[0][0] + H[1][1] + H[2][2]);
-        R P[3][3];
+        R P[3][3], Q[3][3];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
             for (int j = 0; j < 3; ++j) P[i][j] = (mu * (H[i][j] + H[j][i]) + (i == j ? tr : R(0))) * dv;
-#pragma unroll
-        for (int a = 0; a < NPE; ++a)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const R fc = P[i][0] * g[a][0] + P[i][1] * g[a][1] + P[i][2] * g[a][2];
-                fe[(a * 3 + i) * TE + t] += fc;
-            }
+        mul_jinv_t(P, ji, Q);
+        tet_scatter<R, NPE>(Q, L, [&](int a, int d, R v) { fe[(a * 3 + d) * TE + t] += v; });
     }
     __syncthreads();
     for (int ln = t; ln < nl; ln += TE) {
@@ -521,12 +510,14 @@ static BatchArgs<R> batch_args(tlfea_batch_s* b) {
     A.lconn = tl.lconn;
     if constexpr (sizeof(R) == 8) {
         A.grad = tl.grad64;
+        A.ji = tl.ji64;
         A.dv = tl.dv64;
         A.lam = b->lam;
         A.mu = b->mu;
         A.partial = b->shared ? b->part64 : tl.partial64;
     } else {
         A.grad = tl.grad32;
+        A.ji = tl.ji32;
         A.dv = tl.dv32;
         A.lam = b->lam32;
         A.mu = b->mu32;
@@ -535,6 +526,7 @@ static BatchArgs<R> batch_args(tlfea_batch_s* b) {
     A.node_bidx = tl.node_bidx;
     A.bnode_off = tl.bnode_off;
     A.bnode_slots = tl.bnode_slots;
+    A.qb = qp_bary(el);
     A.n_tiles = b->shared ? tl.n_tiles * b->n_inst : tl.n_tiles;
     A.tiles_per_inst = b->shared ? tl.n_tiles : 0;
     A.nodes_per_inst = b->shared ? el->N : 0;

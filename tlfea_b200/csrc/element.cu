@@ -72,7 +72,8 @@ __device__ __forceinline__ double det3(const double J[3][3]) {
 template <int NPE, int NQP>
 __global__ void k_dndu_pre(int n_slots, int E, const int* __restrict__ tile_elem, const int* __restrict__ conn,
                            const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
-                           QuadParams qp, double* grad64, float* grad32, double* dv64, float* dv32, double* detJ) {
+                           QuadParams qp, double* grad64, float* grad32, double* dv64, float* dv32, double* detJ,
+                           double* ji64, float* ji32) {
     constexpr int TE = TILE_ELEMS;
     const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gtid >= (long long)n_slots * NQP) return;
@@ -81,6 +82,7 @@ __global__ void k_dndu_pre(int n_slots, int E, const int* __restrict__ tile_elem
     const int tile = slot / TE, t = slot % TE;
     const int e = tile_elem[slot];
     double gN[NPE][3];
+    double Jinv[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};  // dxi/dX
     double dj = 0.0;
     if (e >= 0) {
         double dN[NPE][3];
@@ -115,6 +117,13 @@ __global__ void k_dndu_pre(int n_slots, int E, const int* __restrict__ tile_elem
             for (int j = 0; j < 3; ++j) JT[i][j] = J[j][i];
         if (NPE == 10) {
             for (int a = 0; a < NPE; ++a) solve3_pivot(JT, dN[a], gN[a]);
+            // row k of J^-1 solves J^T y = e_k by the same elimination, so a
+            // degenerate element (tiny pivot) gets a zero inverse, as its
+            // gradients are zero
+            for (int k = 0; k < 3; ++k) {
+                const double ek[3] = {k == 0 ? 1.0 : 0.0, k == 1 ? 1.0 : 0.0, k == 2 ? 1.0 : 0.0};
+                solve3_pivot(JT, ek, Jinv[k]);
+            }
         } else {
             const double dT = det3(JT);
             const double inv = (dT != 0.0) ? 1.0 / dT : 0.0;
@@ -134,6 +143,8 @@ __global__ void k_dndu_pre(int n_slots, int E, const int* __restrict__ tile_elem
                     for (int j = 0; j < 3; ++j) s += Ji[i][j] * dN[a][j];
                     gN[a][i] = s;
                 }
+            for (int k = 0; k < 3; ++k)
+                for (int j = 0; j < 3; ++j) Jinv[k][j] = Ji[j][k];  // Ji = (J^T)^-1
         }
         detJ[(size_t)e * NQP + q] = dj;
     } else {
@@ -148,6 +159,12 @@ __global__ void k_dndu_pre(int n_slots, int E, const int* __restrict__ tile_elem
     const double dv = (e >= 0) ? dj * qp.qw[q] : 0.0;
     dv64[((size_t)tile * NQP + q) * TE + t] = dv;
     dv32[((size_t)tile * NQP + q) * TE + t] = (float)dv;
+    const size_t jb = ((size_t)tile * NQP + q) * 9 * TE + t;
+    for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j) {
+            ji64[jb + (size_t)(3 * k + j) * TE] = Jinv[k][j];
+            ji32[jb + (size_t)(3 * k + j) * TE] = (float)Jinv[k][j];
+        }
 }
 
 template <typename R, int NPE, int NQP, int MODE, bool DAMP>
@@ -295,6 +312,8 @@ static void free_tiling(Tiling& tl) {
     dfree(tl.dv64);
     dfree(tl.grad32);
     dfree(tl.dv32);
+    dfree(tl.ji64);
+    dfree(tl.ji32);
     dfree(tl.partial64);
     dfree(tl.partial32);
     tl = Tiling();
@@ -483,6 +502,11 @@ static int build_tiling(tlfea_element_s* h, const double* x, const double* y, co
     if ((st = dalloc(&tl.grad32, ng))) return st;
     if ((st = dalloc(&tl.dv64, nd))) return st;
     if ((st = dalloc(&tl.dv32, nd))) return st;
+    const size_t nj = (size_t)n_tiles * h->nqp * 9 * TE;
+    if ((st = dalloc(&tl.ji64, nj))) return st;
+    if ((st = dalloc(&tl.ji32, nj))) return st;
+    TLFEA_CUDA(cudaMemsetAsync(tl.ji64, 0, nj * sizeof(double), h->stream));
+    TLFEA_CUDA(cudaMemsetAsync(tl.ji32, 0, nj * sizeof(float), h->stream));
     if ((st = dalloc(&tl.partial64, (size_t)3 * std::max(n_pslots, 1)))) return st;
     if ((st = dalloc(&tl.partial32, (size_t)3 * std::max(n_pslots, 1)))) return st;
     TLFEA_CUDA(cudaMemsetAsync(tl.grad64, 0, ng * sizeof(double), h->stream));
@@ -1141,10 +1165,12 @@ int tlfea_element_calc_dndu_pre(tlfea_element h) {
     Tiling& tl = h->tl;
     if (h->npe == 10)
         k_dndu_pre<10, 5><<<blocks, 128, 0, h->stream>>>(n_slots, h->E, tl.tile_elem, h->d_conn, h->x, h->y, h->z, qp,
-                                                        tl.grad64, tl.grad32, tl.dv64, tl.dv32, h->detJ);
+                                                        tl.grad64, tl.grad32, tl.dv64, tl.dv32, h->detJ,
+                                                        tl.ji64, tl.ji32);
     else
         k_dndu_pre<4, 1><<<blocks, 128, 0, h->stream>>>(n_slots, h->E, tl.tile_elem, h->d_conn, h->x, h->y, h->z, qp,
-                                                       tl.grad64, tl.grad32, tl.dv64, tl.dv32, h->detJ);
+                                                       tl.grad64, tl.grad32, tl.dv64, tl.dv32, h->detJ,
+                                                        tl.ji64, tl.ji32);
     TLFEA_CHECK_LAUNCH();
     const size_t nb = (size_t)h->N * sizeof(double);
     TLFEA_CUDA(cudaMemcpyAsync(h->X0x, h->x, nb, cudaMemcpyDeviceToDevice, h->stream));

@@ -52,6 +52,10 @@ struct Tiling {
     double* dv64 = nullptr;
     float* grad32 = nullptr;
     float* dv32 = nullptr;
+    // J^-1 = dxi/dX per (tile, QP), [tile][q][3 * k + j][TILE_ELEMS]: the
+    // compact geometry stream (9 values instead of 3 * NPE gradients)
+    double* ji64 = nullptr;
+    float* ji32 = nullptr;
     double* partial64 = nullptr;
     float* partial32 = nullptr;
     std::vector<int> h_tile_elem;  // host copy of tile_elem
@@ -82,6 +86,97 @@ struct TileArgs {
 
 // Tile routine modes.
 enum { TILE_FORCE = 0, TILE_STORE_P = 1, TILE_FORCE_FROM_P = 2 };
+
+// Barycentric coordinates L = (1 - xi - eta - zeta, xi, eta, zeta) of the
+// quadrature points, the only per-QP data the compact geometry stream needs.
+struct QpBary {
+    double L[5][4];
+};
+
+// ----------------------------------------------------------------------------
+// Compact geometry: with J^-1 = dxi/dX stored per QP, gradN_a = J^-T dN_a/dxi and
+//   F (or H) = sum_a x_a (x) gradN_a = G J^-1,      G = dx/dxi = sum_a x_a (x) dN_a/dxi,
+//   f_a += dV P gradN_a = Q dN_a/dxi,               Q = dV P J^-T,
+// and for the tetrahedra of the reference node order (corners 0..3, edge nodes
+// 4..9 on (0,1) (1,2) (0,2) (0,3) (1,3) (2,3)) both sums follow the barycentric
+// structure of the shape functions (corner N_i = L_i (2 L_i - 1), edge
+// N_ij = 4 L_i L_j, dL_0/dxi_k = -1, dL_(k+1)/dxi_k = 1):
+//   y_i = dx/dL_i = (4 L_i - 1) x_i + 4 sum_(j != i) L_j x_ij,  G[:, k] = y_(k+1) - y_0,
+//   r_0 = -(Q[:,0] + Q[:,1] + Q[:,2]), r_(k+1) = Q[:, k],
+//   f_i += (4 L_i - 1) r_i,  f_ij += 4 (L_i r_j + L_j r_i).
+// The same F and forces as the per-node gradients, from 9 stored values per QP
+// instead of 3 * NPE.
+// ----------------------------------------------------------------------------
+
+// G[d][k] = dx_d/dxi_k from the nodal values xa[a][d].
+template <typename R, int NPE>
+__device__ __forceinline__ void tet_dx_dxi(const R (&xa)[NPE][3], const R L[4], R G[3][3]) {
+    if constexpr (NPE == 10) {
+        const R c0 = R(4) * L[0] - R(1), c1 = R(4) * L[1] - R(1), c2 = R(4) * L[2] - R(1), c3 = R(4) * L[3] - R(1);
+        const R l0 = R(4) * L[0], l1 = R(4) * L[1], l2 = R(4) * L[2], l3 = R(4) * L[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const R y0 = c0 * xa[0][d] + l1 * xa[4][d] + l2 * xa[6][d] + l3 * xa[7][d];
+            const R y1 = c1 * xa[1][d] + l0 * xa[4][d] + l2 * xa[5][d] + l3 * xa[8][d];
+            const R y2 = c2 * xa[2][d] + l1 * xa[5][d] + l0 * xa[6][d] + l3 * xa[9][d];
+            const R y3 = c3 * xa[3][d] + l0 * xa[7][d] + l1 * xa[8][d] + l2 * xa[9][d];
+            G[d][0] = y1 - y0;
+            G[d][1] = y2 - y0;
+            G[d][2] = y3 - y0;
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            G[d][0] = xa[1][d] - xa[0][d];
+            G[d][1] = xa[2][d] - xa[0][d];
+            G[d][2] = xa[3][d] - xa[0][d];
+        }
+    }
+}
+
+// acc(a, d, Q[d][:] . dN_a/dxi) for every node a and component d.
+template <typename R, int NPE, typename Acc>
+__device__ __forceinline__ void tet_scatter(const R Q[3][3], const R L[4], Acc acc) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const R r0 = -(Q[d][0] + Q[d][1] + Q[d][2]), r1 = Q[d][0], r2 = Q[d][1], r3 = Q[d][2];
+        if constexpr (NPE == 10) {
+            const R l0 = R(4) * L[0], l1 = R(4) * L[1], l2 = R(4) * L[2], l3 = R(4) * L[3];
+            acc(0, d, (l0 - R(1)) * r0);
+            acc(1, d, (l1 - R(1)) * r1);
+            acc(2, d, (l2 - R(1)) * r2);
+            acc(3, d, (l3 - R(1)) * r3);
+            acc(4, d, l0 * r1 + l1 * r0);
+            acc(5, d, l1 * r2 + l2 * r1);
+            acc(6, d, l0 * r2 + l2 * r0);
+            acc(7, d, l0 * r3 + l3 * r0);
+            acc(8, d, l1 * r3 + l3 * r1);
+            acc(9, d, l2 * r3 + l3 * r2);
+        } else {
+            acc(0, d, r0);
+            acc(1, d, r1);
+            acc(2, d, r2);
+            acc(3, d, r3);
+        }
+    }
+}
+
+// M J^-1 (ji row-major J^-1) and M J^-T.
+template <typename R>
+__device__ __forceinline__ void mul_jinv(const R M[3][3], const R ji[9], R out[3][3]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) out[i][j] = M[i][0] * ji[j] + M[i][1] * ji[3 + j] + M[i][2] * ji[6 + j];
+}
+template <typename R>
+__device__ __forceinline__ void mul_jinv_t(const R M[3][3], const R ji[9], R out[3][3]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            out[i][k] = M[i][0] * ji[3 * k] + M[i][1] * ji[3 * k + 1] + M[i][2] * ji[3 * k + 2];
+}
 
 template <typename R>
 __device__ __forceinline__ R ld_stream(const R* p) {
@@ -467,4 +562,16 @@ namespace tlfea {
 int element_build_pattern(tlfea_element_s* h);
 int element_refresh_u32(tlfea_element_s* h);
 int element_force(tlfea_element_s* h, const double* d_v, bool fp32);
+
+// Barycentric coordinates of the element's quadrature points.
+inline QpBary qp_bary(const tlfea_element_s* h) {
+    QpBary b;
+    for (int q = 0; q < 5; ++q) {
+        b.L[q][0] = 1.0 - h->qx[q] - h->qy[q] - h->qz[q];
+        b.L[q][1] = h->qx[q];
+        b.L[q][2] = h->qy[q];
+        b.L[q][3] = h->qz[q];
+    }
+    return b;
+}
 }  // namespace tlfea
