@@ -63,6 +63,8 @@ struct tlfea_batch_s {
     double *cpa = nullptr, *cpb = nullptr;  // per-chunk partials
     double *rr = nullptr, *fnorm = nullptr, *rel = nullptr;  // rr: 2 * n_inst (iteration parity)
     int *iters = nullptr, *status = nullptr, *done = nullptr, *n_done = nullptr;
+    double *alpha = nullptr, *beta = nullptr;  // per instance, folded once per phase
+    int *flag = nullptr, *ticket = nullptr;    // per instance: 0 go, 1 converged, 2 broke down; fold tickets
     bool warm = false;
     bool material_set = false;
     // launch
@@ -122,6 +124,8 @@ struct BatchArgs {
     const double* u0;
     double *cpa, *cpb, *rr, *fnorm, *rel;
     int *iters, *status, *done, *n_done;
+    double *alpha, *beta;
+    int *flag, *ticket;
     QpBary qb;
 };
 
@@ -260,7 +264,7 @@ __device__ __forceinline__ void node_kp(const BatchArgs<R>& A, int i, double* q,
         } else {
             R s0 = R(0), s1 = R(0), s2 = R(0);
             for (int k = A.bnode_off[b]; k < A.bnode_off[b + 1]; ++k) {
-                const int sl = poff + A.bnode_slots[k];
+                const int sl = poff + k;  // partial slots are numbered by shared node
                 s0 += __ldcg(A.partial + 3 * sl + 0);
                 s1 += __ldcg(A.partial + 3 * sl + 1);
                 s2 += __ldcg(A.partial + 3 * sl + 2);
@@ -275,12 +279,177 @@ __device__ __forceinline__ void node_kp(const BatchArgs<R>& A, int i, double* q,
     q[3 * i + 2] = out[2];
 }
 
-// Sum of the chunk partials of instance b, folded by warp 0 in a fixed order
-// (every block computing it gets the same bits).  Valid in thread 0 .. 31.
+// Sum of the chunk partials of instance b, folded by one warp in a fixed order
+// (any warp computing it gets the same bits, in every lane).
 __device__ __forceinline__ double inst_sum(const double* part, const int* inst_chunk, int b) {
     double s = 0.0;
     for (int c = inst_chunk[b] + (threadIdx.x & 31); c < inst_chunk[b + 1]; c += 32) s += __ldcg(part + c);
     return warp_sum(s);
+}
+
+// Shared-mesh mode: one mesh tile for a group of SHARED_GROUP instances.  The
+// tile's tables (incidence, node ids, partial slots, local connectivity) are
+// staged once for the group; each active instance's p is gathered with cp.async
+// into one of two buffers while the previous instance is computed and
+// scattered, so the gather latency overlaps the element work.
+constexpr int SHARED_GROUP = 8;
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Byte offsets of the group tile's shared memory (16-byte aligned regions).
+template <typename R, int NPE>
+struct GroupLayout {
+    size_t fe, gid, slot, iend, inc, total;
+    __host__ __device__ GroupLayout(int ml) {
+        auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+        fe = al(2 * 3 * (size_t)ml * sizeof(double));  // two gather buffers first
+        gid = al(fe + 3 * (size_t)NPE * TILE_ELEMS * sizeof(R));
+        slot = al(gid + (size_t)ml * sizeof(int));
+        iend = al(slot + (size_t)ml * sizeof(int));
+        inc = al(iend + (size_t)ml * sizeof(uint16_t));
+        total = inc + (size_t)NPE * TILE_ELEMS * sizeof(uint16_t);
+    }
+};
+
+template <typename R, int NPE, int NQP>
+__device__ __forceinline__ void shared_group_tile(const BatchArgs<R>& A, int tile, int g0, const double* p, double* q,
+                                                  unsigned char* smem, bool skip_done) {
+    constexpr int TE = TILE_ELEMS;
+    const int t = threadIdx.x;
+    const int ml = A.max_local;
+    const GroupLayout<R, NPE> L(ml);
+    double* psb = reinterpret_cast<double*>(smem);
+    R* fe = reinterpret_cast<R*>(smem + L.fe);
+    int* gid_s = reinterpret_cast<int*>(smem + L.gid);
+    int* slot_s = reinterpret_cast<int*>(smem + L.slot);
+    uint16_t* iends = reinterpret_cast<uint16_t*>(smem + L.iend);
+    uint16_t* incs = reinterpret_cast<uint16_t*>(smem + L.inc);
+    const int g1 = min(g0 + SHARED_GROUP, A.n_inst);
+    // next instance of the group to compute (done[] is stable in this phase)
+    auto next_active = [&](int from) -> int {
+        for (int i = from; i < g1; ++i)
+            if (!skip_done || !__ldcg(A.done + i)) return i;
+        return -1;
+    };
+    int cur = next_active(g0);
+    if (cur < 0) return;  // uniform: every thread read the same flags
+    const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
+    for (int k = t; k < NPE * TE; k += TE) incs[k] = A.inc[(size_t)tile * TE * NPE + k];
+    for (int ln = t; ln < nl; ln += TE) {
+        const int gid = A.ln_gid[lb + ln];
+        gid_s[ln] = gid;
+        slot_s[ln] = A.ln_pslot[lb + ln];
+        iends[ln] = A.ln_inc_end[lb + ln];
+        // this thread's own gathers of the first instance start right away
+        const double* src = p + 3 * ((size_t)cur * A.nodes_per_inst + gid);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) cp_async8(psb + 3 * ln + d, src + d);
+    }
+    cp_async_commit();
+    int lc[NPE];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) lc[a] = A.lconn[((size_t)tile * NPE + a) * TE + t];
+    __syncthreads();  // node tables staged (the next gathers read gid_s)
+    int buf = 0;
+    while (cur >= 0) {
+        const int nxt = next_active(cur + 1);
+        if (nxt >= 0) {
+            double* dst = psb + (buf ^ 1) * 3 * ml;
+            for (int ln = t; ln < nl; ln += TE) {
+                const double* src = p + 3 * ((size_t)nxt * A.nodes_per_inst + gid_s[ln]);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) cp_async8(dst + 3 * ln + d, src + d);
+            }
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();  // instance cur's p visible in buffer buf
+        const double* ps = psb + buf * 3 * ml;
+        const R lam = A.lam[cur], mu = A.mu[cur];
+        // FP32: p relative to the tile's first node, differenced in FP64 (the
+        // gradients sum to zero per element, so K p is unchanged)
+        double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+        if constexpr (sizeof(R) == 4) {
+            r0 = ps[0];
+            r1 = ps[1];
+            r2 = ps[2];
+        }
+#pragma unroll 1
+        for (int qp = 0; qp < NQP; ++qp) {
+            R xa[NPE][3];
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) {
+                if constexpr (sizeof(R) == 4) {
+                    xa[a][0] = R(ps[3 * lc[a] + 0] - r0);
+                    xa[a][1] = R(ps[3 * lc[a] + 1] - r1);
+                    xa[a][2] = R(ps[3 * lc[a] + 2] - r2);
+                } else {
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) xa[a][d] = ps[3 * lc[a] + d];
+                }
+            }
+            const R* jp = A.ji + ((size_t)tile * NQP + qp) * 9 * TE + t;
+            R ji[9];
+#pragma unroll
+            for (int m = 0; m < 9; ++m) ji[m] = __ldg(jp + m * TE);
+            const R dv = __ldg(A.dv + ((size_t)tile * NQP + qp) * TE + t);
+            const R Lq[4] = {R(A.qb.L[qp][0]), R(A.qb.L[qp][1]), R(A.qb.L[qp][2]), R(A.qb.L[qp][3])};
+            R G[3][3], H[3][3];
+            tet_dx_dxi<R, NPE>(xa, Lq, G);
+            mul_jinv(G, ji, H);
+            const R tr = lam * (H[0][0] + H[1][1] + H[2][2]);
+            R P[3][3], Q[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) P[i][j] = (mu * (H[i][j] + H[j][i]) + (i == j ? tr : R(0))) * dv;
+            mul_jinv_t(P, ji, Q);
+            if (qp == 0)
+                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { fe[(a * 3 + d) * TE + t] = v; });
+            else
+                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { fe[(a * 3 + d) * TE + t] += v; });
+        }
+        __syncthreads();  // element forces complete
+        const size_t noff = (size_t)cur * A.nodes_per_inst, poff = (size_t)cur * A.pslots_per_inst;
+        for (int ln = t; ln < nl; ln += TE) {
+            const int beg = ln ? iends[ln - 1] : 0;
+            const int end = iends[ln];
+            R s0 = R(0), s1 = R(0), s2 = R(0);
+            for (int k = beg; k < end; ++k) {
+                const int ent = incs[k];
+                const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
+                s0 += fe[base];
+                s1 += fe[base + TE];
+                s2 += fe[base + 2 * TE];
+            }
+            const int sl = slot_s[ln];
+            if (sl < 0) {
+                double* qd = q + 3 * (noff + gid_s[ln]);
+                qd[0] = double(s0);
+                qd[1] = double(s1);
+                qd[2] = double(s2);
+            } else {
+                R* pt = A.partial + 3 * (poff + sl);
+                pt[0] = s0;
+                pt[1] = s1;
+                pt[2] = s2;
+            }
+        }
+        __syncthreads();  // forces and buffer buf free for reuse
+        cur = nxt;
+        buf ^= 1;
+    }
 }
 
 // K p over every tile; with skip_done, tiles whose instances have all
@@ -289,6 +458,13 @@ __device__ __forceinline__ double inst_sum(const double* part, const int* inst_c
 template <typename R, int NPE, int NQP>
 __device__ __forceinline__ void apply_all_tiles(const BatchArgs<R>& A, const double* p, double* q,
                                                 unsigned char* smem, bool skip_done) {
+    if (A.tiles_per_inst) {
+        const int T = A.tiles_per_inst;
+        const int n_items = T * ((A.n_inst + SHARED_GROUP - 1) / SHARED_GROUP);
+        for (int item = blockIdx.x; item < n_items; item += gridDim.x)
+            shared_group_tile<R, NPE, NQP>(A, item % T, (item / T) * SHARED_GROUP, p, q, smem, skip_done);
+        return;
+    }
     for (int tile = blockIdx.x; tile < A.n_tiles; tile += gridDim.x) {
         if (skip_done) {
             bool all_done = true;
@@ -310,16 +486,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
     cg::grid_group grid = cg::this_grid();
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double red[32];
-    __shared__ double sh_scal[4];
-    __shared__ int sh_done;
     const int t = threadIdx.x;
-    // done flag of instance b read once and broadcast, so the block branches uniformly
-    auto block_done = [&](int b) -> bool {
-        __syncthreads();
-        if (t == 0) sh_done = __ldcg(A.done + b);
-        __syncthreads();
-        return sh_done != 0;
-    };
 
     // ---- prologue: u = u0, r = f_free, ||f_free|| per chunk
     for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
@@ -373,6 +540,8 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
                 A.rel[b] = rel;
                 A.iters[b] = 0;
                 A.status[b] = 0;
+                A.flag[b] = 0;
+                A.ticket[b] = 0;
                 const int dn = (fn == 0.0 || rel < tol) ? 1 : 0;
                 A.done[b] = dn;
                 if (dn) atomicAdd(A.n_done, 1);
@@ -381,7 +550,31 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
     }
     grid.sync();
 
-    // ---- CG iterations
+    // ---- CG iterations.  The per-instance scalars are folded once per phase, by
+    // the chunk-block of the instance that posts its partial last (a ticket per
+    // instance; the fold runs in chunk order, so its bits do not depend on which
+    // block it is): alpha in the p.q phase, then rr_new, the convergence test and
+    // beta in the r.r phase.  The next phase reads them after the grid barrier.
+    // done[] changes only in the last phase of an iteration, so every other
+    // phase branches on it uniformly.
+    // Node phases run one warp per chunk (no block barriers): a chunk's partial
+    // is the warp's lane-strided sum folded by shuffles, so its bits are fixed.
+    const int lane = t & 31;
+    const int gw = blockIdx.x * (TILE_ELEMS / 32) + (t >> 5), n_warps = gridDim.x * (TILE_ELEMS / 32);
+    auto post_last = [&](double* part, int c, int b, double s) -> bool {  // s: the warp's sum (all lanes)
+        int last = 0;
+        if (lane == 0) {
+            part[c] = s;
+            __threadfence();
+            const int nch = A.inst_chunk[b + 1] - A.inst_chunk[b];
+            const int tk = atomicAdd(A.ticket + b, 1);
+            last = (tk == nch - 1);
+            if (last) A.ticket[b] = 0;  // every ticket of this phase is taken
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last) __threadfence();
+        return last != 0;
+    };
     for (int it = 0; it < max_iter; ++it) {
         if (atomicAdd(A.n_done, 0) >= A.n_inst) break;  // uniform: read after a grid barrier
         const double* rr_old = A.rr + (size_t)(it & 1) * A.n_inst;
@@ -389,85 +582,146 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
         // q = K p
         apply_all_tiles<R, NPE, NQP>(A, A.p, A.q, smem, true);
         grid.sync();
-        // complete q, p.q per chunk
-        for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
+        // complete q, p.q per chunk; alpha = rr / p.q
+        for (int c = gw; c < A.n_chunks; c += n_warps) {
             const int b = A.chunk_inst[c];
+            const int i_end = A.chunk_beg[c + 1];
+            if (__ldcg(A.done + b)) continue;
             double s = 0.0;
-            if (!block_done(b)) {
-                for (int i = A.chunk_beg[c] + t; i < A.chunk_beg[c + 1]; i += blockDim.x) {
-                    double kp[3];
-                    node_kp<R>(A, i, A.q, kp);
-                    s += A.p[3 * i + 0] * kp[0] + A.p[3 * i + 1] * kp[1] + A.p[3 * i + 2] * kp[2];
-                }
-            }
-            s = block_sum(s, red);
-            if (t == 0) A.cpa[c] = s;
-        }
-        grid.sync();
-        // alpha = rr / pq; u += alpha p; r -= alpha q; r.r per chunk
-        for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
-            const int b = A.chunk_inst[c];
-            double s = 0.0;
-            if (!block_done(b)) {
-                if (t < 32) {
-                    const double pq = inst_sum(A.cpa, A.inst_chunk, b);
-                    if (t == 0) sh_scal[0] = pq;
-                }
-                __syncthreads();
-                const double pq = sh_scal[0];
-                __syncthreads();
-                if (pq > 0.0) {
-                    const double alpha = __ldcg(rr_old + b) / pq;
-                    for (int i = A.chunk_beg[c] + t; i < A.chunk_beg[c + 1]; i += blockDim.x) {
+            // two nodes per lane per step: every load of both is issued before
+            // the first use (the chunk's nodes all belong to instance b)
+            const int noff = A.tiles_per_inst ? b * A.nodes_per_inst : 0;
+            const int poff = A.tiles_per_inst ? b * A.pslots_per_inst : 0;
+            for (int i0 = A.chunk_beg[c] + lane; i0 < i_end; i0 += 64) {
+                double pv[2][3], qv[2][3];
+                int fx[2], bi[2];
 #pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            A.u[3 * i + d] += alpha * A.p[3 * i + d];
-                            const double ri = A.r[3 * i + d] - alpha * A.q[3 * i + d];
-                            A.r[3 * i + d] = ri;
-                            s += ri * ri;
-                        }
+                for (int k = 0; k < 2; ++k) {
+                    const int i = i0 + 32 * k;
+                    const bool ok = i < i_end;
+                    fx[k] = ok ? A.fixed[i] : 1;
+                    bi[k] = ok ? A.node_bidx[i - noff] : -1;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        pv[k][d] = ok ? __ldcg(A.p + 3 * i + d) : 0.0;
+                        qv[k][d] = ok ? __ldcg(A.q + 3 * i + d) : 0.0;
                     }
-                } else if (t == 0 && c == A.inst_chunk[b]) {
-                    // non-positive p.Kp: the reference aborts this solve
-                    A.status[b] = 1;
-                    A.done[b] = 1;
-                    atomicAdd(A.n_done, 1);
+                }
+                int kb[2], ke[2];
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    kb[k] = (bi[k] >= 0) ? A.bnode_off[bi[k]] : 0;
+                    ke[k] = (bi[k] >= 0) ? A.bnode_off[bi[k] + 1] : 0;
+                }
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const int i = i0 + 32 * k;
+                    if (bi[k] >= 0) {
+                        R s0 = R(0), s1 = R(0), s2 = R(0);
+                        for (int m = kb[k]; m < ke[k]; ++m) {
+                            const R* pt = A.partial + 3 * (size_t)(poff + m);
+                            s0 += __ldcg(pt + 0);
+                            s1 += __ldcg(pt + 1);
+                            s2 += __ldcg(pt + 2);
+                        }
+                        qv[k][0] = double(s0);
+                        qv[k][1] = double(s1);
+                        qv[k][2] = double(s2);
+                    }
+                    if (fx[k]) qv[k][0] = qv[k][1] = qv[k][2] = 0.0;
+                    if (i < i_end) {
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) A.q[3 * i + d] = qv[k][d];
+                    }
+                    s += pv[k][0] * qv[k][0] + pv[k][1] * qv[k][1] + pv[k][2] * qv[k][2];
                 }
             }
-            s = block_sum(s, red);
-            if (t == 0) A.cpb[c] = s;
+            s = warp_sum(s);
+            if (post_last(A.cpa, c, b, s)) {
+                const double pq = inst_sum(A.cpa, A.inst_chunk, b);
+                if (lane == 0) {
+                    // non-positive p.Kp: the reference aborts this solve (flag 2)
+                    A.alpha[b] = (pq > 0.0) ? __ldcg(rr_old + b) / pq : 0.0;
+                    A.flag[b] = (pq > 0.0) ? 0 : 2;
+                }
+            }
         }
         grid.sync();
-        // convergence test, beta = rr_new / rr, p = r + beta p
-        for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
+        // u += alpha p; r -= alpha q; r.r per chunk; then rr_new, the test, beta
+        for (int c = gw; c < A.n_chunks; c += n_warps) {
             const int b = A.chunk_inst[c];
-            if (block_done(b)) continue;
-            if (t < 32) {
-                const double rrn = inst_sum(A.cpb, A.inst_chunk, b);
-                if (t == 0) sh_scal[1] = rrn;
-            }
-            __syncthreads();
-            const double rrn = sh_scal[1];
-            __syncthreads();
-            const double rel = sqrt(rrn) / __ldcg(A.fnorm + b);
-            const bool conv = rel < tol;
-            if (!conv) {
-                const double beta = rrn / __ldcg(rr_old + b);
-                for (int i = A.chunk_beg[c] + t; i < A.chunk_beg[c + 1]; i += blockDim.x)
+            const int dn = __ldcg(A.done + b), fl = __ldcg(A.flag + b);  // loads issued together
+            const double alpha = __ldcg(A.alpha + b);
+            if (dn || fl == 2) continue;
+            double s = 0.0;
+            // flat over the chunk's 3n values, four per lane per step with every
+            // load issued before the first store
+            const int j1 = 3 * A.chunk_beg[c + 1];
+            for (int j0 = 3 * A.chunk_beg[c] + lane; j0 < j1; j0 += 128) {
+                double uv[4], pv[4], rv[4], qv[4];
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) A.p[3 * i + d] = A.r[3 * i + d] + beta * A.p[3 * i + d];
-            }
-            __syncthreads();  // every thread has read done[b] before the owner may set it
-            if (t == 0 && c == A.inst_chunk[b]) {
-                rr_new_out[b] = rrn;
-                A.iters[b] = it + 1;
-                A.rel[b] = rel;
-                if (conv) {
-                    A.done[b] = 1;
-                    atomicAdd(A.n_done, 1);
-                } else if (it + 1 >= max_iter) {
-                    A.status[b] = 2;
+                for (int k = 0; k < 4; ++k) {
+                    const int j = j0 + 32 * k;
+                    const bool ok = j < j1;
+                    uv[k] = ok ? __ldcg(A.u + j) : 0.0;
+                    pv[k] = ok ? __ldcg(A.p + j) : 0.0;
+                    rv[k] = ok ? __ldcg(A.r + j) : 0.0;
+                    qv[k] = ok ? __ldcg(A.q + j) : 0.0;
                 }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int j = j0 + 32 * k;
+                    const double rj = rv[k] - alpha * qv[k];
+                    if (j < j1) {
+                        A.u[j] = uv[k] + alpha * pv[k];
+                        A.r[j] = rj;
+                    }
+                    s += rj * rj;
+                }
+            }
+            s = warp_sum(s);
+            if (post_last(A.cpb, c, b, s)) {
+                const double rrn = inst_sum(A.cpb, A.inst_chunk, b);
+                if (lane == 0) {
+                    const double rel = sqrt(rrn) / __ldcg(A.fnorm + b);
+                    const bool conv = rel < tol;
+                    rr_new_out[b] = rrn;
+                    A.beta[b] = rrn / __ldcg(rr_old + b);
+                    A.iters[b] = it + 1;
+                    A.rel[b] = rel;
+                    A.flag[b] = conv ? 1 : 0;
+                    if (!conv && it + 1 >= max_iter) A.status[b] = 2;
+                }
+            }
+        }
+        grid.sync();
+        // p = r + beta p; instances that converged or broke down retire (their
+        // first chunk sets done; every warp skips them either way)
+        for (int c = gw; c < A.n_chunks; c += n_warps) {
+            const int b = A.chunk_inst[c];
+            const int dn = __ldcg(A.done + b), fl = __ldcg(A.flag + b);  // loads issued together
+            const double beta = __ldcg(A.beta + b);
+            if (dn) continue;
+            if (fl == 0) {
+                const int j1 = 3 * A.chunk_beg[c + 1];
+                for (int j0 = 3 * A.chunk_beg[c] + lane; j0 < j1; j0 += 128) {
+                    double pv[4], rv[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int j = j0 + 32 * k;
+                        pv[k] = (j < j1) ? __ldcg(A.p + j) : 0.0;
+                        rv[k] = (j < j1) ? __ldcg(A.r + j) : 0.0;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int j = j0 + 32 * k;
+                        if (j < j1) A.p[j] = rv[k] + beta * pv[k];
+                    }
+                }
+            } else if (lane == 0 && c == A.inst_chunk[b]) {
+                if (fl == 2) A.status[b] = 1;
+                A.done[b] = 1;
+                atomicAdd(A.n_done, 1);
             }
         }
         grid.sync();
@@ -555,12 +809,18 @@ static BatchArgs<R> batch_args(tlfea_batch_s* b) {
     A.status = b->status;
     A.done = b->done;
     A.n_done = b->n_done;
+    A.alpha = b->alpha;
+    A.beta = b->beta;
+    A.flag = b->flag;
+    A.ticket = b->ticket;
     return A;
 }
 
 template <typename R>
 static size_t batch_smem(const tlfea_batch_s* b) {
     const size_t ml = (size_t)b->el->tl.max_local;
+    if (b->shared)
+        return (b->el->npe == 10) ? GroupLayout<R, 10>((int)ml).total : GroupLayout<R, 4>((int)ml).total;
     return sizeof(R) * (3 * ml + 3 * (size_t)b->el->npe * TILE_ELEMS) + ml * (sizeof(int) + sizeof(uint16_t)) +
            (size_t)b->el->npe * TILE_ELEMS * sizeof(uint16_t);
 }
@@ -722,7 +982,9 @@ static int batch_alloc_state(tlfea_batch_s* b) {
         (st = dalloc(&b->f, n3)) || (st = dalloc(&b->u0, n3)) || (st = dalloc(&b->rr, 2 * (size_t)n_inst)) ||
         (st = dalloc(&b->fnorm, (size_t)n_inst)) || (st = dalloc(&b->rel, (size_t)n_inst)) ||
         (st = dalloc(&b->iters, (size_t)n_inst)) || (st = dalloc(&b->status, (size_t)n_inst)) ||
-        (st = dalloc(&b->done, (size_t)n_inst)) || (st = dalloc(&b->n_done, 1)))
+        (st = dalloc(&b->done, (size_t)n_inst)) || (st = dalloc(&b->n_done, 1)) ||
+        (st = dalloc(&b->alpha, (size_t)n_inst)) || (st = dalloc(&b->beta, (size_t)n_inst)) ||
+        (st = dalloc(&b->flag, (size_t)n_inst)) || (st = dalloc(&b->ticket, (size_t)n_inst)))
         return st;
     if (b->shared) {
         const size_t np = 3 * (size_t)n_inst * (size_t)std::max(b->el->tl.n_pslots, 1);
@@ -917,6 +1179,7 @@ int tlfea_batch_destroy(tlfea_batch b) {
     dfree(b->u); dfree(b->r); dfree(b->p); dfree(b->q); dfree(b->f); dfree(b->u0);
     dfree(b->rhs); dfree(b->uacc);
     dfree(b->cpa); dfree(b->cpb); dfree(b->rr); dfree(b->fnorm); dfree(b->rel);
+    dfree(b->alpha); dfree(b->beta); dfree(b->flag); dfree(b->ticket);
     dfree(b->part64); dfree(b->part32);
     dfree(b->iters); dfree(b->status); dfree(b->done); dfree(b->n_done);
     if (b->el) tlfea_element_destroy(b->el);
