@@ -492,7 +492,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
     ap.add_argument("--batch-size", type=int, default=512)
-    ap.add_argument("--batch-precision", default="fp32", choices=["fp64", "fp32"],
+    ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "fp32"],
                     help="element work of the batched solves (the CG and its stop test stay FP64)")
     ap.add_argument("--plain-sample", type=int, default=48, help="single-instance solves timed for the plain path")
     ap.add_argument("--train-cases", type=int, default=4096)
