@@ -128,6 +128,12 @@ def elem_force_bytes(E, N, npe, nqp, s):
     return E * (4 * npe + nqp * npe * 3 * s + nqp * s) + N * 6 * s
 
 
+def elem_force_bytes_compact(E, N, npe, nqp, s):
+    """The compact geometry stream: J^-1 (9 values) and dV per QP instead of the
+    3 * NPE gradients."""
+    return E * (4 * npe + nqp * 10 * s) + N * 6 * s
+
+
 def spmv_bytes(N, nnzb):
     """Bytes one block SpMV must move: every 3x3 node block (72 B values +
     4 B column), the row offsets, p read and q written once."""
@@ -239,9 +245,12 @@ def kernels_only(args):
     r = np.random.default_rng(1)
     el.UpdatePositions(*(v + 1e-4 * r.standard_normal(v.shape) for v in (x, y, z)))
     if args.kernels_only == "force":
-        for prec in ("fp32", "fp32", "fp64", "fp64"):
-            el.SetForcePrecision(prec)
-            el.ComputeInternalForce()
+        # gradient-stream kernel, then the compact-geometry kernel
+        for kern in ("tma", "compact"):
+            el.SetLaunchConfig(kern)
+            for prec in ("fp32", "fp32", "fp64", "fp64"):
+                el.SetForcePrecision(prec)
+                el.ComputeInternalForce()
     elif args.kernels_only == "cg":
         # the benchmark's solve capped at --cg-iters iterations: the per-iteration
         # launch mix of the full solve in a launch list short enough to capture
@@ -609,6 +618,21 @@ def main():
         ef[prec] = {"kernel": "k_tile_force+k_combine", "bound": "hbm", "achieved": round(a, 1), "peak": hbm,
                     "unit": "GB/s", "frac": round(a / hbm, 4), "algorithmic_bytes": int(b), "ms": round(ms_f, 4),
                     "traffic": int(FORCE_FP32_TRAFFIC_BYTES) if prec == "fp32" else None}
+    # the same forces from the compact geometry stream (J^-1 and dV per QP)
+    el.SetLaunchConfig("compact")
+    for prec, s in (("fp32", 4), ("fp64", 8)):
+        el.SetForcePrecision(prec)
+        for _ in range(3):
+            el.ComputeInternalForce()
+        ms_f = time_stream(torch, stream, el.ComputeInternalForce, args.kernel_reps)
+        b = elem_force_bytes_compact(E, N, 10, 5, s)
+        a = b / (ms_f / 1e3) / 1e9
+        ef["compact_" + prec] = {"kernel": "k_tile_force_geo+k_combine", "achieved": round(a, 1), "peak": hbm,
+                                 "unit": "GB/s", "frac": round(a / hbm, 4), "algorithmic_bytes": int(b),
+                                 "ms": round(ms_f, 4),
+                                 "gradient_stream_equivalent_gbs": round(
+                                     elem_force_bytes(E, N, 10, 5, s) / (ms_f / 1e3) / 1e9, 1)}
+    el.SetLaunchConfig("tma")
     el.SetForcePrecision("fp64")
     el.SetBlocking(True)
 

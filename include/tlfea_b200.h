@@ -172,9 +172,10 @@ int tlfea_element_compute_internal_force(tlfea_element h, const double* d_v);
 int tlfea_element_set_force_precision(tlfea_element h, int precision);
 /* Launch configuration of the fused force kernel (new; the autotuner's knob):
  * force_kernel 0 = one tile per block with bulk-copy double-buffered QP
- * slices (default), 1 = one tile per block with direct loads, 2 = persistent
- * producer/consumer pipeline; grid_limit caps the persistent grid (0 = all
- * resident blocks). */
+ * slices of the gradient stream (default), 1 = one tile per block with direct
+ * loads, 2 = persistent producer/consumer pipeline, 3 = as 0 on the compact
+ * geometry stream (J^-1 and dV per QP, gradients formed in registers);
+ * grid_limit caps the persistent grid (0 = all resident blocks). */
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit);
 
 /* Allocation-free internal force.  No counterpart in the reference.

@@ -41,8 +41,9 @@ def test_rule_fires_at_the_first_evaluation_when_loose():
     s.Solve()
     st = s.GetStats()
     assert st["stop_rule_met"] == 1 and st["inner_iters_total"] == 1 and st["outer_iters"] == 1
-    # first evaluation at the reference positions: f_int = 0, residual = ||f_free|| / ||f|| = 1
-    assert st["rel_residual"] == pytest.approx(1.0, rel=1e-14)
+    # first evaluation at the reference positions: f_int = 0 up to the rounding of
+    # F = (dX/dxi) J^-1 = I (E ~ 1e7 times 1e-16), so ||f_free|| / ||f|| = 1 to ~1e-11
+    assert st["rel_residual"] == pytest.approx(1.0, rel=1e-10)
     xs = el.RetrievePositionToCPU()
     assert all(np.array_equal(a, b) for a, b in zip(xs, (x, y, z)))
     el.Destroy()

@@ -173,6 +173,15 @@ class _TetData(ElementBase):
         p = {"fp64": capi.PRECISION_FP64, "fp32": capi.PRECISION_FP32}[precision]
         capi.call("tlfea_element_set_force_precision", self._handle(), p)
 
+    FORCE_KERNELS = {"tma": 0, "direct": 1, "pipeline": 2, "compact": 3}
+
+    def SetLaunchConfig(self, force_kernel="tma", grid_limit: int = 0):
+        """New: the fused force kernel -- "tma" (gradient stream, bulk-copy double
+        buffered), "direct", "pipeline" (persistent producer/consumer) or
+        "compact" (J^-1 stream, gradients formed in registers)."""
+        k = self.FORCE_KERNELS[force_kernel] if isinstance(force_kernel, str) else int(force_kernel)
+        capi.call("tlfea_element_set_launch_config", self._handle(), k, int(grid_limit))
+
     # -- retrieval ---------------------------------------------------------------
     def RetrieveMassCSRToCPU(self):
         nnz = C.c_longlong()

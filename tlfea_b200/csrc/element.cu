@@ -601,6 +601,7 @@ static TileArgs<R> make_args(tlfea_element_s* h, bool fp32) {
     A.max_local = tl.max_local;
     if constexpr (sizeof(R) == 8) {
         A.grad = (const R*)tl.grad64;
+        A.ji = (const R*)tl.ji64;
         A.dv = (const R*)tl.dv64;
         A.px = (const R*)h->x;
         A.py = (const R*)h->y;
@@ -609,6 +610,7 @@ static TileArgs<R> make_args(tlfea_element_s* h, bool fp32) {
         A.partial = (R*)tl.partial64;
     } else {
         A.grad = (const R*)tl.grad32;
+        A.ji = (const R*)tl.ji32;
         A.dv = (const R*)tl.dv32;
         A.px = (const R*)h->ux;
         A.py = (const R*)h->uy;
@@ -616,6 +618,7 @@ static TileArgs<R> make_args(tlfea_element_s* h, bool fp32) {
         A.f_out = (R*)h->f_int32;
         A.partial = (R*)tl.partial32;
     }
+    A.qb = qp_bary(h);
     (void)fp32;
     return A;
 }
@@ -650,6 +653,27 @@ template <typename R, int NPE, int NQP, bool DAMP>
 static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
     auto kern = k_tile_force_tma<R, NPE, NQP, DAMP>;
     const size_t smem = tile_tma_smem_bytes<R, NPE>(h->tl.max_local, DAMP);
+    if (smem > 227 * 1024) {
+        set_error("force kernel shared memory exceeds 227 KB (tile touches too many nodes)");
+        return TLFEA_UNSUPPORTED;
+    }
+    static bool configured = false;  // one instantiation per template argument set
+    if (!configured) {
+        TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
+        configured = true;
+    }
+    if (smem > 48 * 1024) TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<h->tl.n_tiles, TILE_ELEMS, smem, h->stream>>>(A, h->d_err);
+    TLFEA_CHECK_LAUNCH();
+    return TLFEA_OK;
+}
+
+// One tile per block on the compact geometry stream (J^-1 and dV per QP).
+template <typename R, int NPE, int NQP, bool DAMP>
+static int launch_tile_geo(tlfea_element_s* h, const TileArgs<R>& A) {
+    auto kern = k_tile_force_geo<R, NPE, NQP, DAMP>;
+    const size_t smem = tile_geo_smem_bytes<R, NPE>(h->tl.max_local, DAMP);
     if (smem > 227 * 1024) {
         set_error("force kernel shared memory exceeds 227 KB (tile touches too many nodes)");
         return TLFEA_UNSUPPORTED;
@@ -705,6 +729,8 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
         st = damp ? launch_tiles<R, NPE, NQP, TILE_FORCE, true>(h, A) : launch_tiles<R, NPE, NQP, TILE_FORCE, false>(h, A);
     else if (h->force_kernel == 2)
         st = damp ? launch_pipe<R, NPE, NQP, true>(h, A) : launch_pipe<R, NPE, NQP, false>(h, A);
+    else if (h->force_kernel == 3)
+        st = damp ? launch_tile_geo<R, NPE, NQP, true>(h, A) : launch_tile_geo<R, NPE, NQP, false>(h, A);
     else
         st = damp ? launch_tile_tma<R, NPE, NQP, true>(h, A) : launch_tile_tma<R, NPE, NQP, false>(h, A);
     if (st) return st;
@@ -1308,7 +1334,7 @@ int tlfea_element_compute_internal_force(tlfea_element h, const double* d_v) {
 
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit) {
     CHECK_HANDLE(h);
-    if (force_kernel < 0 || force_kernel > 2 || grid_limit < 0) return TLFEA_INVALID_ARG;
+    if (force_kernel < 0 || force_kernel > 3 || grid_limit < 0) return TLFEA_INVALID_ARG;
     h->force_kernel = force_kernel;
     h->pipe_grid_limit = grid_limit;
     for (int& g : h->pipe_grid) g = 0;

@@ -62,6 +62,12 @@ struct Tiling {
 };
 
 // Per-call arguments of the tile routine.
+// Barycentric coordinates L = (1 - xi - eta - zeta, xi, eta, zeta) of the
+// quadrature points, the only per-QP data the compact geometry stream needs.
+struct QpBary {
+    double L[5][4];
+};
+
 template <typename R>
 struct TileArgs {
     const int* node_off;
@@ -72,6 +78,7 @@ struct TileArgs {
     const uint16_t* lconn;
     const int* tile_elem;
     const R* grad;
+    const R* ji;  // J^-1 per (tile, QP), the compact geometry stream
     const R* dv;
     const R* px;  // FP64: positions x; FP32: displacement u = x - X0
     const R* py;
@@ -82,16 +89,12 @@ struct TileArgs {
     R* partial;       // 3 * n_pslots
     R lambda, mu, eta, lamd;
     int max_local;
+    QpBary qb;
 };
 
 // Tile routine modes.
 enum { TILE_FORCE = 0, TILE_STORE_P = 1, TILE_FORCE_FROM_P = 2 };
 
-// Barycentric coordinates L = (1 - xi - eta - zeta, xi, eta, zeta) of the
-// quadrature points, the only per-QP data the compact geometry stream needs.
-struct QpBary {
-    double L[5][4];
-};
 
 // ----------------------------------------------------------------------------
 // Compact geometry: with J^-1 = dxi/dX stored per QP, gradN_a = J^-T dN_a/dxi and
@@ -266,6 +269,80 @@ __device__ __forceinline__ void kelvin_voigt(const R F[3][3], const R Fd[3][3], 
 //             the FP32 displacement, and P = (I + H) S, S = lambda tr(E) I + 2 mu E,
 //             E = (H + H^T + H^T H)/2 -- algebraically the same SVK stress,
 //             without the cancellation of tr(F^T F) - 3 near F = I.
+// First Piola stress of one QP from the compact-geometry gradient: FP64 takes
+// F itself (the reference's SVK form), FP32 the displacement gradient H (F =
+// I + H, the cancellation-free form); with DAMP the Kelvin-Voigt term of the
+// velocity gradient Fd is added.
+template <typename R, bool DAMP>
+__device__ __forceinline__ void tile_stress(const R H[3][3], const R Fd[3][3], const TileArgs<R>& A, R P[3][3]) {
+    if constexpr (sizeof(R) == 8) {
+        svk_p_reference(H, A.lambda, A.mu, P);
+    } else {
+        R Em[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                R sm = H[i][j] + H[j][i];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) sm += H[k][i] * H[k][j];
+                Em[i][j] = R(0.5) * sm;
+            }
+        const R trE = Em[0][0] + Em[1][1] + Em[2][2];
+        R Sm[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) Sm[i][j] = R(2) * A.mu * Em[i][j] + (i == j ? A.lambda * trE : R(0));
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                R sm = Sm[i][j];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) sm += H[i][k] * Sm[k][j];
+                P[i][j] = sm;
+            }
+    }
+    if constexpr (DAMP) {
+        R F[3][3], Pv[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) F[i][j] = (sizeof(R) == 8) ? H[i][j] : H[i][j] + (i == j ? R(1) : R(0));
+        kelvin_voigt<R>(F, Fd, A.eta, A.lamd, Pv);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
+    }
+}
+
+// One QP of the compact-geometry force: F (or H) = (dx/dxi) J^-1 from the
+// nodal values xa, the stress, and f_a (+)= (dV P J^-T) dN_a/dxi.
+template <typename R, int NPE, bool DAMP, bool FIRST>
+__device__ __forceinline__ void compact_qp(const TileArgs<R>& A, const R (&xa)[NPE][3], const R (&va)[NPE][3],
+                                           const R ji[9], R dv, const R Lq[4], R (&f)[NPE][3]) {
+    R Gx[3][3], H[3][3], Fd[3][3], P[3][3], Q[3][3];
+    tet_dx_dxi<R, NPE>(xa, Lq, Gx);
+    mul_jinv(Gx, ji, H);
+    if constexpr (DAMP) {
+        R Gv[3][3];
+        tet_dx_dxi<R, NPE>(va, Lq, Gv);
+        mul_jinv(Gv, ji, Fd);
+    }
+    tile_stress<R, DAMP>(H, Fd, A, P);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) P[i][j] *= dv;
+    mul_jinv_t(P, ji, Q);
+    if constexpr (FIRST)
+        tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] = v; });
+    else
+        tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] += v; });
+}
+
 template <typename R, int NPE, int NQP, int MODE, bool DAMP>
 __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, unsigned char* smem_raw) {
     constexpr int TE = TILE_ELEMS;
@@ -302,7 +379,29 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
     for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
 
 #pragma unroll 1
-    for (int q = 0; q < NQP; ++q) {
+    for (int q = 0; q < NQP && MODE == TILE_FORCE; ++q) {
+        // the force alone: compact geometry stream (J^-1 and dV per QP)
+        const R* jp = A.ji + ((size_t)tile * NQP + q) * 9 * TE + t;
+        R ji[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) ji[m] = ld_stream(jp + m * TE);
+        const R dv = ld_stream(A.dv + ((size_t)tile * NQP + q) * TE + t);
+        const R Lq[4] = {R(A.qb.L[q][0]), R(A.qb.L[q][1]), R(A.qb.L[q][2]), R(A.qb.L[q][3])};
+        R xa[NPE][3], va[NPE][3];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) {
+            xa[a][0] = xs[lc[a]];
+            xa[a][1] = ys[lc[a]];
+            xa[a][2] = zs[lc[a]];
+            if (DAMP) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) va[a][d] = vs[3 * lc[a] + d];
+            }
+        }
+        compact_qp<R, NPE, DAMP, false>(A, xa, va, ji, dv, Lq, f);
+    }
+#pragma unroll 1
+    for (int q = 0; q < NQP && MODE != TILE_FORCE; ++q) {
         const R* gp = A.grad + ((size_t)tile * NQP + q) * (NPE * 3) * TE + t;
         R g[NPE][3];
 #pragma unroll

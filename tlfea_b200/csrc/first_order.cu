@@ -534,6 +534,9 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     A32.tile_elem = A64.tile_elem = el->tl.tile_elem;
     A32.v = A64.v = s->v_guess;
     A32.max_local = A64.max_local = el->tl.max_local;
+    A32.qb = A64.qb = qp_bary(el);
+    A32.ji = el->tl.ji32;
+    A64.ji = el->tl.ji64;
     A32.grad = el->tl.grad32; A32.dv = el->tl.dv32; A32.px = el->ux; A32.py = el->uy; A32.pz = el->uz;
     A32.f_out = el->f_int32; A32.partial = el->tl.partial32;
     A32.lambda = (float)el->lambda; A32.mu = (float)el->mu; A32.eta = (float)el->eta_d; A32.lamd = (float)el->lambda_d;

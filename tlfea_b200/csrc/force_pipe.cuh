@@ -625,4 +625,176 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
     }
 }
 
+// ---------------------------------------------------------------------------
+// Compact-geometry variant of k_tile_force_tma: the per-QP slices hold J^-1
+// (9 values) and dV instead of 3 * NPE gradients, and F = (dx/dxi) J^-1 and the
+// nodal forces Q dN/dxi (Q = dV P J^-T) follow the barycentric structure of the
+// tetrahedral shape functions (tet_dx_dxi / tet_scatter).  Same forces to
+// rounding, 10 / (3 NPE + 1) of the element stream.
+
+template <typename R, int NPE>
+struct TileGeoGeom {
+    static constexpr uint32_t JI_BYTES = 9 * TILE_ELEMS * sizeof(R);
+    static constexpr uint32_t DV_BYTES = TILE_ELEMS * sizeof(R);
+    static constexpr uint32_t STAGE_BYTES = JI_BYTES + DV_BYTES;
+    static constexpr uint32_t LCONN_BYTES = NPE * TILE_ELEMS * sizeof(uint16_t);
+    static constexpr uint32_t INC_BYTES = NPE * TILE_ELEMS * sizeof(uint16_t);
+    static constexpr uint32_t FE_BYTES = 3 * NPE * TILE_ELEMS * sizeof(R);
+    // the two stages, and after the QP loop the element forces of the scatter
+    static constexpr uint32_t REGION0 =
+        ((2 * STAGE_BYTES > FE_BYTES ? 2 * STAGE_BYTES : FE_BYTES) + 15u) & ~15u;
+    static_assert(LCONN_BYTES % 16 == 0 && INC_BYTES % 16 == 0 && STAGE_BYTES % 16 == 0, "bulk sizes");
+};
+
+template <typename R, int NPE>
+struct TileGeoLayout {
+    size_t lconn, inc, pos, dst, iend, vel, bar, total;
+    __host__ __device__ TileGeoLayout(int max_local, bool damp) {
+        using G = TileGeoGeom<R, NPE>;
+        auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+        lconn = G::REGION0;
+        inc = lconn + G::LCONN_BYTES;
+        pos = inc + G::INC_BYTES;
+        dst = al(pos + 3 * (size_t)max_local * sizeof(R));
+        iend = al(dst + (size_t)max_local * sizeof(int));
+        vel = al(iend + (size_t)max_local * sizeof(uint16_t));
+        bar = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
+        total = bar + 2 * sizeof(unsigned long long);
+    }
+};
+
+template <typename R, int NPE>
+inline size_t tile_geo_smem_bytes(int max_local, bool damp) {
+    return TileGeoLayout<R, NPE>(max_local, damp).total;
+}
+
+template <typename R, int NPE, int NQP, bool DAMP>
+__global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, int* err) {
+    using G = TileGeoGeom<R, NPE>;
+    constexpr int TE = TILE_ELEMS;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int tile = blockIdx.x, t = threadIdx.x;
+    const int ML = A.max_local;
+    const TileGeoLayout<R, NPE> L(ML, DAMP);
+    unsigned char* stage0 = smem;
+    const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + L.lconn);
+    const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
+    R* xs = reinterpret_cast<R*>(smem + L.pos);
+    R* ys = xs + ML;
+    R* zs = ys + ML;
+    int* dsts = reinterpret_cast<int*>(smem + L.dst);  // global node id, or -(partial slot + 1)
+    uint16_t* iends = reinterpret_cast<uint16_t*>(smem + L.iend);
+    double* vs = reinterpret_cast<double*>(smem + L.vel);
+    R* fe = reinterpret_cast<R*>(smem);  // aliases the stages after the QP loop
+    const uint32_t bar0 = smem_u32(smem + L.bar);
+
+    auto issue = [&](int q) {  // thread 0 only
+        const uint32_t bar = bar0 + 8 * (q & 1);
+        const uint32_t dst = smem_u32(stage0 + (size_t)(q & 1) * G::STAGE_BYTES);
+        const uint32_t extra = (q == 0) ? G::LCONN_BYTES + G::INC_BYTES : 0;
+        mbar_expect_tx(bar, G::STAGE_BYTES + extra);
+        bulk_g2s(dst, A.ji + ((size_t)tile * NQP + q) * 9 * TE, G::JI_BYTES, bar);
+        bulk_g2s(dst + G::JI_BYTES, A.dv + ((size_t)tile * NQP + q) * TE, G::DV_BYTES, bar);
+        if (q == 0) {
+            bulk_g2s(smem_u32(lcs), A.lconn + (size_t)tile * NPE * TE, G::LCONN_BYTES, bar);
+            bulk_g2s(smem_u32(incs), A.inc + (size_t)tile * NPE * TE, G::INC_BYTES, bar);
+        }
+    };
+    if (t == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(0);
+        if (NQP > 1) issue(1);
+    }
+    const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
+    for (int ln = t; ln < nl; ln += TE) {
+        const int gid = A.ln_gid[lb + ln];
+        const int ps = A.ln_pslot[lb + ln];
+        iends[ln] = A.ln_inc_end[lb + ln];
+        dsts[ln] = (ps < 0) ? gid : -(ps + 1);
+        xs[ln] = A.px[gid];
+        ys[ln] = A.py[gid];
+        zs[ln] = A.pz[gid];
+        if (DAMP) {
+            vs[3 * ln + 0] = A.v[3 * gid + 0];
+            vs[3 * ln + 1] = A.v[3 * gid + 1];
+            vs[3 * ln + 2] = A.v[3 * gid + 2];
+        }
+    }
+    __syncthreads();  // positions and node tables staged; barriers initialised
+
+    int lc[NPE];
+    R f[NPE][3];
+#pragma unroll 1
+    for (int q = 0; q < NQP; ++q) {
+        if (!mbar_wait(bar0 + 8 * (q & 1), (q >> 1) & 1)) atomicExch(err, 3);
+        const unsigned char* st = stage0 + (size_t)(q & 1) * G::STAGE_BYTES;
+        const R* js = reinterpret_cast<const R*>(st);
+        if (q == 0) {
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
+        }
+        R ji[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) ji[m] = js[m * TE + t];
+        const R dv = reinterpret_cast<const R*>(st + G::JI_BYTES)[t];
+        if (q + 2 < NQP) {
+            // every thread's generic reads of this stage precede the bulk refill
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (t == 0) issue(q + 2);
+        }
+        const R Lq[4] = {R(A.qb.L[q][0]), R(A.qb.L[q][1]), R(A.qb.L[q][2]), R(A.qb.L[q][3])};
+        R xa[NPE][3], va[NPE][3];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) {
+            xa[a][0] = xs[lc[a]];
+            xa[a][1] = ys[lc[a]];
+            xa[a][2] = zs[lc[a]];
+            if (DAMP) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) va[a][d] = R(vs[3 * lc[a] + d]);
+            }
+        }
+        // F (FP64) or H (FP32), the stress, f_a (+)= (dV P J^-T) dN_a/dxi
+        // (FEAT10DataFunc.cuh:417-449 with gradN = J^-T dN/dxi)
+        if (q == 0)
+            compact_qp<R, NPE, DAMP, true>(A, xa, va, ji, dv, Lq, f);
+        else
+            compact_qp<R, NPE, DAMP, false>(A, xa, va, ji, dv, Lq, f);
+    }
+    __syncthreads();  // every thread is done with the stages the force table reuses
+#pragma unroll
+    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
+    __syncthreads();
+
+    for (int ln = t; ln < nl; ln += TE) {
+        const int beg = ln ? iends[ln - 1] : 0;
+        const int end = iends[ln];
+        R s0 = R(0), s1 = R(0), s2 = R(0);
+        for (int k = beg; k < end; ++k) {
+            const int ent = incs[k];
+            const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
+            s0 += fe[base];
+            s1 += fe[base + TE];
+            s2 += fe[base + 2 * TE];
+        }
+        const int dn = dsts[ln];
+        if (dn >= 0) {
+            A.f_out[3 * dn + 0] = s0;
+            A.f_out[3 * dn + 1] = s1;
+            A.f_out[3 * dn + 2] = s2;
+        } else {
+            const int ps = -dn - 1;
+            A.partial[3 * ps + 0] = s0;
+            A.partial[3 * ps + 1] = s1;
+            A.partial[3 * ps + 2] = s2;
+        }
+    }
+}
+
 }  // namespace tlfea

@@ -126,8 +126,12 @@ class FixedMeshCases:
 class PCA:
     """k-mode PCA of normalised snapshots via the FP64 Gram matrix (torch / cuSOLVER)."""
 
-    def __init__(self, k: int = 64):
+    def __init__(self, k: int = 64, coef_scale: str = "mode"):
+        """coef_scale "mode": every coefficient standardised to unit variance;
+        "global": one scale for all (the largest mode's), so a squared
+        coefficient error is the squared displacement error."""
         self.k = k
+        self.coef_scale = coef_scale
 
     def fit(self, W: np.ndarray):
         import torch
@@ -145,6 +149,8 @@ class PCA:
         C = Wc @ self.modes
         self.c_mean = C.mean(0)
         self.c_std = C.std(0).clamp_min(1e-300)
+        if self.coef_scale == "global":
+            self.c_std = self.c_std.max().expand_as(self.c_std).clone()
         return ((C - self.c_mean) / self.c_std).cpu().numpy()
 
     def coefficients(self, W) -> np.ndarray:
@@ -164,10 +170,10 @@ class PCA:
 class LearnedWarmStart:
     """PCA + WarmStartMLP on one fixed mesh."""
 
-    def __init__(self, hidden=(256, 256, 256), k=64, max_batch=512, seed=0):
+    def __init__(self, hidden=(256, 256, 256), k=64, max_batch=512, seed=0, coef_scale="mode"):
         import torch
 
-        self.pca = PCA(k)
+        self.pca = PCA(k, coef_scale)
         self.dims = [6, *hidden, k]
         self.net = WarmStartMLP(self.dims, max_batch=max_batch, seed=seed)
         self.max_batch = max_batch
