@@ -385,20 +385,21 @@ __device__ __forceinline__ void shared_group_tile(const BatchArgs<R>& A, int til
             r1 = ps[1];
             r2 = ps[2];
         }
+        R f[NPE][3];
+        R xa[NPE][3];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) {
+            if constexpr (sizeof(R) == 4) {
+                xa[a][0] = R(ps[3 * lc[a] + 0] - r0);
+                xa[a][1] = R(ps[3 * lc[a] + 1] - r1);
+                xa[a][2] = R(ps[3 * lc[a] + 2] - r2);
+            } else {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) xa[a][d] = ps[3 * lc[a] + d];
+            }
+        }
 #pragma unroll 1
         for (int qp = 0; qp < NQP; ++qp) {
-            R xa[NPE][3];
-#pragma unroll
-            for (int a = 0; a < NPE; ++a) {
-                if constexpr (sizeof(R) == 4) {
-                    xa[a][0] = R(ps[3 * lc[a] + 0] - r0);
-                    xa[a][1] = R(ps[3 * lc[a] + 1] - r1);
-                    xa[a][2] = R(ps[3 * lc[a] + 2] - r2);
-                } else {
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) xa[a][d] = ps[3 * lc[a] + d];
-                }
-            }
             const R* jp = A.ji + ((size_t)tile * NQP + qp) * 9 * TE + t;
             R ji[9];
 #pragma unroll
@@ -416,10 +417,14 @@ __device__ __forceinline__ void shared_group_tile(const BatchArgs<R>& A, int til
                 for (int j = 0; j < 3; ++j) P[i][j] = (mu * (H[i][j] + H[j][i]) + (i == j ? tr : R(0))) * dv;
             mul_jinv_t(P, ji, Q);
             if (qp == 0)
-                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { fe[(a * 3 + d) * TE + t] = v; });
+                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] = v; });
             else
-                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { fe[(a * 3 + d) * TE + t] += v; });
+                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] += v; });
         }
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
         __syncthreads();  // element forces complete
         const size_t noff = (size_t)cur * A.nodes_per_inst, poff = (size_t)cur * A.pslots_per_inst;
         for (int ln = t; ln < nl; ln += TE) {
@@ -456,15 +461,8 @@ __device__ __forceinline__ void shared_group_tile(const BatchArgs<R>& A, int til
 // converged are skipped (their q is never read again).  The done flags do not
 // change during this phase, so the skip is uniform across the block.
 template <typename R, int NPE, int NQP>
-__device__ __forceinline__ void apply_all_tiles(const BatchArgs<R>& A, const double* p, double* q,
-                                                unsigned char* smem, bool skip_done) {
-    if (A.tiles_per_inst) {
-        const int T = A.tiles_per_inst;
-        const int n_items = T * ((A.n_inst + SHARED_GROUP - 1) / SHARED_GROUP);
-        for (int item = blockIdx.x; item < n_items; item += gridDim.x)
-            shared_group_tile<R, NPE, NQP>(A, item % T, (item / T) * SHARED_GROUP, p, q, smem, skip_done);
-        return;
-    }
+__device__ __forceinline__ void general_tiles(const BatchArgs<R>& A, const double* p, double* q, unsigned char* smem,
+                                              bool skip_done) {
     for (int tile = blockIdx.x; tile < A.n_tiles; tile += gridDim.x) {
         if (skip_done) {
             bool all_done = true;
@@ -480,8 +478,23 @@ __device__ __forceinline__ void apply_all_tiles(const BatchArgs<R>& A, const dou
     }
 }
 
+// SH: the shared-mesh instantiation (instance groups per tile); the general one
+// keeps its lower register count, and so its occupancy, for uneven batches.
+template <typename R, int NPE, int NQP, bool SH>
+__device__ __forceinline__ void apply_all_tiles(const BatchArgs<R>& A, const double* p, double* q,
+                                                unsigned char* smem, bool skip_done) {
+    if constexpr (SH) {
+        const int T = A.tiles_per_inst;
+        const int n_items = T * ((A.n_inst + SHARED_GROUP - 1) / SHARED_GROUP);
+        for (int item = blockIdx.x; item < n_items; item += gridDim.x)
+            shared_group_tile<R, NPE, NQP>(A, item % T, (item / T) * SHARED_GROUP, p, q, smem, skip_done);
+    } else {
+        general_tiles<R, NPE, NQP>(A, p, q, smem, skip_done);
+    }
+}
+
 // The whole batched solve.  mode: 0 = solve, 1 = y = K_bc x only (x in p, y in q).
-template <typename R, int NPE, int NQP>
+template <typename R, int NPE, int NQP, bool SH>
 __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double tol, int max_iter, int warm) {
     cg::grid_group grid = cg::this_grid();
     extern __shared__ __align__(16) unsigned char smem[];
@@ -508,7 +521,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
     }
     grid.sync();
     if (warm) {
-        apply_all_tiles<R, NPE, NQP>(A, A.p, A.q, smem, false);
+        apply_all_tiles<R, NPE, NQP, SH>(A, A.p, A.q, smem, false);
         grid.sync();
     }
     for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
@@ -580,7 +593,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
         const double* rr_old = A.rr + (size_t)(it & 1) * A.n_inst;
         double* rr_new_out = A.rr + (size_t)((it + 1) & 1) * A.n_inst;
         // q = K p
-        apply_all_tiles<R, NPE, NQP>(A, A.p, A.q, smem, true);
+        apply_all_tiles<R, NPE, NQP, SH>(A, A.p, A.q, smem, true);
         grid.sync();
         // complete q, p.q per chunk; alpha = rr / p.q
         for (int c = gw; c < A.n_chunks; c += n_warps) {
@@ -657,10 +670,10 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
             // flat over the chunk's 3n values, four per lane per step with every
             // load issued before the first store
             const int j1 = 3 * A.chunk_beg[c + 1];
-            for (int j0 = 3 * A.chunk_beg[c] + lane; j0 < j1; j0 += 128) {
-                double uv[4], pv[4], rv[4], qv[4];
+            for (int j0 = 3 * A.chunk_beg[c] + lane; j0 < j1; j0 += 256) {
+                double uv[8], pv[8], rv[8], qv[8];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < 8; ++k) {
                     const int j = j0 + 32 * k;
                     const bool ok = j < j1;
                     uv[k] = ok ? __ldcg(A.u + j) : 0.0;
@@ -669,7 +682,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
                     qv[k] = ok ? __ldcg(A.q + j) : 0.0;
                 }
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < 8; ++k) {
                     const int j = j0 + 32 * k;
                     const double rj = rv[k] - alpha * qv[k];
                     if (j < j1) {
@@ -704,16 +717,16 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
             if (dn) continue;
             if (fl == 0) {
                 const int j1 = 3 * A.chunk_beg[c + 1];
-                for (int j0 = 3 * A.chunk_beg[c] + lane; j0 < j1; j0 += 128) {
-                    double pv[4], rv[4];
+                for (int j0 = 3 * A.chunk_beg[c] + lane; j0 < j1; j0 += 256) {
+                    double pv[8], rv[8];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
+                    for (int k = 0; k < 8; ++k) {
                         const int j = j0 + 32 * k;
                         pv[k] = (j < j1) ? __ldcg(A.p + j) : 0.0;
                         rv[k] = (j < j1) ? __ldcg(A.r + j) : 0.0;
                     }
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
+                    for (int k = 0; k < 8; ++k) {
                         const int j = j0 + 32 * k;
                         if (j < j1) A.p[j] = rv[k] + beta * pv[k];
                     }
@@ -732,7 +745,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
 
 // y = K_bc x for the whole batch: fixed rows are identity rows and fixed
 // columns are dropped (the BC-applied K of LinearStaticSolver::Apply).
-template <typename R, int NPE, int NQP>
+template <typename R, int NPE, int NQP, bool SH>
 __global__ void __launch_bounds__(TILE_ELEMS) k_batch_apply(BatchArgs<R> A, const double* x, double* y) {
     cg::grid_group grid = cg::this_grid();
     extern __shared__ __align__(16) unsigned char smem[];
@@ -741,7 +754,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_apply(BatchArgs<R> A, cons
 #pragma unroll
         for (int d = 0; d < 3; ++d) A.p[3 * i + d] = A.fixed[i] ? 0.0 : x[3 * i + d];
     grid.sync();
-    apply_all_tiles<R, NPE, NQP>(A, A.p, A.q, smem, false);
+    apply_all_tiles<R, NPE, NQP, SH>(A, A.p, A.q, smem, false);
     grid.sync();
     for (int i = blockIdx.x * blockDim.x + t; i < A.N; i += gridDim.x * blockDim.x) {
         double kp[3];
@@ -825,9 +838,17 @@ static size_t batch_smem(const tlfea_batch_s* b) {
            (size_t)b->el->npe * TILE_ELEMS * sizeof(uint16_t);
 }
 
+// The kernel instantiation of this batch (shared-mesh or general).
+template <typename R, int NPE, int NQP>
+static const void* batch_kernel(const tlfea_batch_s* b, bool apply) {
+    if (b->shared)
+        return apply ? (const void*)k_batch_apply<R, NPE, NQP, true> : (const void*)k_batch_cg<R, NPE, NQP, true>;
+    return apply ? (const void*)k_batch_apply<R, NPE, NQP, false> : (const void*)k_batch_cg<R, NPE, NQP, false>;
+}
+
 template <typename R, int NPE, int NQP>
 static int batch_grid(tlfea_batch_s* b, int blocks_per_sm, int* grid_out, bool apply = false) {
-    const void* kern = apply ? (const void*)k_batch_apply<R, NPE, NQP> : (const void*)k_batch_cg<R, NPE, NQP>;
+    const void* kern = batch_kernel<R, NPE, NQP>(b, apply);
     const size_t smem = batch_smem<R>(b);
     if (smem > 200 * 1024) {
         set_error("batch: a tile touches too many nodes for shared memory");
@@ -854,7 +875,7 @@ static int launch_batch_cg(tlfea_batch_s* b, int grid, double tol, int max_iter,
     if (u0_over) A.u0 = u0_over;
     int w = warm ? 1 : 0;
     void* args[] = {&A, &tol, &max_iter, &w};
-    TLFEA_CUDA(cudaLaunchCooperativeKernel((const void*)k_batch_cg<R, NPE, NQP>, dim3(grid), dim3(TILE_ELEMS), args,
+    TLFEA_CUDA(cudaLaunchCooperativeKernel(batch_kernel<R, NPE, NQP>(b, false), dim3(grid), dim3(TILE_ELEMS), args,
                                            batch_smem<R>(b), st));
     TLFEA_LAUNCHED(1);
     return TLFEA_OK;
@@ -1477,11 +1498,11 @@ int tlfea_batch_apply(tlfea_batch b, const double* d_x, double* d_y) {
     struct TD { using type = double; };
     struct TF { using type = float; };
     if (f32)
-        s = t10 ? go(TF{}, (const void*)k_batch_apply<float, 10, 5>, batch_smem<float>(b))
-                : go(TF{}, (const void*)k_batch_apply<float, 4, 1>, batch_smem<float>(b));
+        s = t10 ? go(TF{}, batch_kernel<float, 10, 5>(b, true), batch_smem<float>(b))
+                : go(TF{}, batch_kernel<float, 4, 1>(b, true), batch_smem<float>(b));
     else
-        s = t10 ? go(TD{}, (const void*)k_batch_apply<double, 10, 5>, batch_smem<double>(b))
-                : go(TD{}, (const void*)k_batch_apply<double, 4, 1>, batch_smem<double>(b));
+        s = t10 ? go(TD{}, batch_kernel<double, 10, 5>(b, true), batch_smem<double>(b))
+                : go(TD{}, batch_kernel<double, 4, 1>(b, true), batch_smem<double>(b));
     if (s) return s;
     TLFEA_CUDA(cudaStreamSynchronize(st));
     return TLFEA_OK;
