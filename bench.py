@@ -505,7 +505,7 @@ def main():
                     help="element work of the batched solves (the CG and its stop test stay FP64)")
     ap.add_argument("--plain-sample", type=int, default=48, help="single-instance solves timed for the plain path")
     ap.add_argument("--train-cases", type=int, default=4096)
-    ap.add_argument("--epochs", type=int, default=300)
+    ap.add_argument("--epochs", type=int, default=1500)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
