@@ -126,8 +126,12 @@ int tlfea_element_set_density(tlfea_element h, double rho0);
 int tlfea_element_set_damping(tlfea_element h, double eta_damp, double lambda_damp);
 int tlfea_element_set_svk_default(tlfea_element h);
 int tlfea_element_set_svk(tlfea_element h, double E, double nu);
-/* Stores the Mooney-Rivlin parameters and selects the model; force, stiffness
- * and solver calls then return TLFEA_UNSUPPORTED (SVK is the supported law). */
+/* Stores the Mooney-Rivlin parameters and selects the model (SetMooneyRivlin,
+ * FEAT10Data.cuh:576-587).  The internal force (every entry point; on the
+ * compact-geometry kernel), CalcP / CalcInternalForce and the first-order
+ * solvers then use the Mooney-Rivlin stress of MooneyRivlin.cuh:46-104 (in FP64,
+ * also in FP32 force mode); the stiffness (LinearStaticSolver) returns
+ * TLFEA_UNSUPPORTED. */
 int tlfea_element_set_mooney_rivlin(tlfea_element h, double mu10, double mu01, double kappa);
 /* SetExternalForce (:589-597); n must be 3*N. */
 int tlfea_element_set_external_force(tlfea_element h, const double* f_ext, int n);

@@ -66,6 +66,22 @@ def get_threads() -> int:
     return int(lib().orc_get_threads())
 
 
+class mooney_rivlin:
+    """Context: the oracle's stress routines use the Mooney-Rivlin law
+    (MooneyRivlin.cuh:46-104) instead of SVK while it is active."""
+
+    def __init__(self, mu10: float, mu01: float, kappa: float):
+        self.prm = (float(mu10), float(mu01), float(kappa))
+
+    def __enter__(self):
+        lib().orc_set_material(1, C.c_double(self.prm[0]), C.c_double(self.prm[1]), C.c_double(self.prm[2]))
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_material(0, C.c_double(0.0), C.c_double(0.0), C.c_double(0.0))
+        return False
+
+
 def colmajor(conn):
     """(E, NPE) -> reference layout conn[e + a*E]."""
     return i32(np.asarray(conn).T.ravel())

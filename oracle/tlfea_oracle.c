@@ -257,8 +257,63 @@ void orc_dndu_pre_t4(int E, const double* x, const double* y, const double* z, c
 
 /* ======================================================== stress and force */
 
-/* compute_p for one (e,q): F, SVK P (SVK.cuh:17-39 via the trFtF/FFtF path),
- * optional Kelvin-Voigt term (FEAT10DataFunc.cuh:130-231). */
+/* Material of the stress routines: 0 = SVK (lambda, mu passed per call), 1 =
+ * Mooney-Rivlin with these parameters (FEAT10Data.cuh material_model switch). */
+static int g_material = 0;
+static double g_mu10 = 0.0, g_mu01 = 0.0, g_kappa = 0.0;
+
+void orc_set_material(int model, double mu10, double mu01, double kappa) {
+    g_material = model;
+    g_mu10 = mu10;
+    g_mu01 = mu01;
+    g_kappa = kappa;
+}
+
+/* Mooney-Rivlin first Piola stress (mr_compute_P, MooneyRivlin.cuh:46-104):
+ * C = F^T F, I1 = tr C, I2 = (I1^2 - tr C^2) / 2, J = det F, F^-T by cofactors
+ * with |J| clamped to 1e-12 for the inverse, and
+ * P = 2 mu10 J^-2/3 (F - I1/3 F^-T) + 2 mu01 J^-4/3 (I1 F - F C - 2 I2/3 F^-T)
+ *   + kappa (J - 1) J F^-T. */
+static void mr_p(const double F[3][3], double mu10, double mu01, double kappa, double P[3][3]) {
+    double C[3][3] = {{0}}, C2[3][3] = {{0}}, FC[3][3] = {{0}}, FiT[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k) C[i][j] += F[k][i] * F[k][j];
+    const double I1 = C[0][0] + C[1][1] + C[2][2];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k) C2[i][j] += C[i][k] * C[k][j];
+    const double I2 = 0.5 * (I1 * I1 - (C2[0][0] + C2[1][1] + C2[2][2]));
+    const double J = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
+                     F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+                     F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+    double dj = J;
+    if (fabs(dj) < 1e-12) dj = (dj >= 0.0) ? 1e-12 : -1e-12;
+    const double id = 1.0 / dj;
+    FiT[0][0] = (F[1][1] * F[2][2] - F[1][2] * F[2][1]) * id;
+    FiT[0][1] = (F[1][2] * F[2][0] - F[1][0] * F[2][2]) * id;
+    FiT[0][2] = (F[1][0] * F[2][1] - F[1][1] * F[2][0]) * id;
+    FiT[1][0] = (F[0][2] * F[2][1] - F[0][1] * F[2][2]) * id;
+    FiT[1][1] = (F[0][0] * F[2][2] - F[0][2] * F[2][0]) * id;
+    FiT[1][2] = (F[0][1] * F[2][0] - F[0][0] * F[2][1]) * id;
+    FiT[2][0] = (F[0][1] * F[1][2] - F[0][2] * F[1][1]) * id;
+    FiT[2][1] = (F[0][2] * F[1][0] - F[0][0] * F[1][2]) * id;
+    FiT[2][2] = (F[0][0] * F[1][1] - F[0][1] * F[1][0]) * id;
+    const double j13 = cbrt(J);
+    const double jm23 = 1.0 / (j13 * j13), jm43 = jm23 * jm23;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k) FC[i][j] += F[i][k] * C[k][j];
+    const double t1 = 2.0 * mu10 * jm23, t2 = 2.0 * mu01 * jm43, t3 = kappa * (J - 1.0) * J;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            P[i][j] = t1 * (F[i][j] - (I1 / 3.0) * FiT[i][j]) +
+                      t2 * (I1 * F[i][j] - FC[i][j] - (2.0 * I2 / 3.0) * FiT[i][j]) + t3 * FiT[i][j];
+}
+
+/* compute_p for one (e,q): F, SVK P (SVK.cuh:17-39 via the trFtF/FFtF path) or
+ * the Mooney-Rivlin P (FEAT10DataFunc.cuh:273-278), plus the optional
+ * Kelvin-Voigt term (FEAT10DataFunc.cuh:130-231). */
 static void qp_stress(int npe, const double X[][3], const double* gq, double lambda, double mu, double eta,
                       double lamd, const double V[][3], double F[3][3], double P[3][3], double Fd[3][3],
                       double Pv[3][3]) {
@@ -303,6 +358,13 @@ static void qp_stress(int npe, const double X[][3], const double* gq, double lam
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j)
             for (int k = 0; k < 3; ++k) FFtF[i][j] += FFt[i][k] * F[k][j];
+    if (g_material == 1) {
+        double Pm[3][3];
+        mr_p(F, g_mu10, g_mu01, g_kappa, Pm);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) P[i][j] = Pm[i][j] + Pv[i][j];
+        return;
+    }
     double lf = lambda * (0.5 * tr - 1.5);
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) P[i][j] = lf * F[i][j] + mu * (FFtF[i][j] - F[i][j]) + Pv[i][j];

@@ -184,6 +184,8 @@ double orc_static_residual(const orc_problem* pb);
 
 /* Threads used by the OpenMP loops (0 = library default). */
 void orc_set_threads(int n);
+/* Material of the stress routines: 0 = SVK (default), 1 = Mooney-Rivlin(mu10, mu01, kappa). */
+void orc_set_material(int model, double mu10, double mu01, double kappa);
 int orc_get_threads(void);
 
 #ifdef __cplusplus

@@ -93,6 +93,49 @@ def test_homogeneous_deformation_patch(order):
     assert np.abs(f[interior]).max() < 1e-9 * np.abs(f).max()
 
 
+def _mr_energy(F, mu10, mu01, kappa):
+    """Mooney-Rivlin strain energy mu10 (I1bar - 3) + mu01 (I2bar - 3) + kappa/2 (J - 1)^2,
+    whose derivative dW/dF is the first Piola stress of MooneyRivlin.cuh:46-104."""
+    C = F.T @ F
+    I1 = np.trace(C)
+    I2 = 0.5 * (I1 ** 2 - np.trace(C @ C))
+    J = np.linalg.det(F)
+    return mu10 * (J ** (-2 / 3) * I1 - 3) + mu01 * (J ** (-4 / 3) * I2 - 3) + 0.5 * kappa * (J - 1) ** 2
+
+
+@pytest.mark.parametrize("order", [10, 4])
+def test_mooney_rivlin_stress_is_the_energy_derivative(order):
+    """Known answer for the Mooney-Rivlin oracle: under a homogeneous deformation
+    x = A X the stress at every QP is dW/dF at A (central differences), a rigid
+    rotation gives zero force, and interior nodes are in equilibrium."""
+    mu10, mu01, kappa = 2.0e5, 5.0e4, 1.0e7
+    x, y, z, conn = O.box_mesh(4, 2, 2, order, 0.4, 0.2, 0.2)
+    g, dj = O.dndu_pre(x, y, z, conn)
+    A = np.array([[1.04, 0.02, -0.01], [0.01, 0.97, 0.03], [0.02, -0.01, 1.01]])
+    with O.mooney_rivlin(mu10, mu01, kappa):
+        F, P = O.calc_p(*(A @ np.stack([x, y, z])), conn, g, 0.0, 0.0)
+        th = 0.5
+        R = np.array([[np.cos(th), -np.sin(th), 0.0], [np.sin(th), np.cos(th), 0.0], [0.0, 0.0, 1.0]])
+        f_rigid = O.force(*(R @ np.stack([x, y, z]) + 0.3), conn, g, dj, 0.0, 0.0)
+        f_hom = O.force(*(A @ np.stack([x, y, z])), conn, g, dj, 0.0, 0.0).reshape(-1, 3)
+    P = P.reshape(-1, 3, 3).transpose(0, 2, 1)
+    h = 1e-6
+    dW = np.zeros((3, 3))
+    for i in range(3):
+        for j in range(3):
+            Ap, Am = A.copy(), A.copy()
+            Ap[i, j] += h
+            Am[i, j] -= h
+            dW[i, j] = (_mr_energy(Ap, mu10, mu01, kappa) - _mr_energy(Am, mu10, mu01, kappa)) / (2 * h)
+    assert rel(P, np.broadcast_to(dW, P.shape)) < 1e-7
+    assert np.abs(f_rigid).max() < 1e-9 * np.abs(f_hom).max()
+    tol = 1e-12
+    interior = ~(np.isclose(x, x.min(), atol=tol) | np.isclose(x, x.max(), atol=tol) | np.isclose(y, y.min(), atol=tol)
+                 | np.isclose(y, y.max(), atol=tol) | np.isclose(z, z.min(), atol=tol) | np.isclose(z, z.max(), atol=tol))
+    if interior.any():
+        assert np.abs(f_hom[interior]).max() < 1e-9 * np.abs(f_hom).max()
+
+
 @pytest.mark.parametrize("order", [10, 4])
 def test_internal_force_from_p_matches_fused(order):
     x, y, z, conn = O.box_mesh(5, 2, 2, order, 0.5, 0.2, 0.2)

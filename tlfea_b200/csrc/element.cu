@@ -167,10 +167,10 @@ __global__ void k_dndu_pre(int n_slots, int E, const int* __restrict__ tile_elem
         }
 }
 
-template <typename R, int NPE, int NQP, int MODE, bool DAMP>
+template <typename R, int NPE, int NQP, int MODE, bool DAMP, bool MR>
 __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force(TileArgs<R> A) {
     extern __shared__ __align__(128) unsigned char smem[];
-    process_tile<R, NPE, NQP, MODE, DAMP>(A, blockIdx.x, smem);
+    process_tile<R, NPE, NQP, MODE, DAMP, MR>(A, blockIdx.x, smem);
 }
 
 // Sum of each shared node's per-tile partials, in tile order.  Partial slots
@@ -619,11 +619,14 @@ static TileArgs<R> make_args(tlfea_element_s* h, bool fp32) {
         A.partial = (R*)tl.partial32;
     }
     A.qb = qp_bary(h);
+    A.mu10 = h->mu10;
+    A.mu01 = h->mu01;
+    A.kappa = h->kappa;
     (void)fp32;
     return A;
 }
 
-template <typename R, int NPE, int NQP, int MODE, bool DAMP>
+template <typename R, int NPE, int NQP, int MODE, bool DAMP, bool MR = false>
 static int launch_tiles(tlfea_element_s* h, const TileArgs<R>& A) {
     const size_t smem = tile_smem_bytes<R>(NPE, h->tl.max_local, DAMP);
     if (smem > 200 * 1024) {
@@ -631,9 +634,9 @@ static int launch_tiles(tlfea_element_s* h, const TileArgs<R>& A) {
         return TLFEA_UNSUPPORTED;
     }
     if (smem > 48 * 1024)
-        TLFEA_CUDA(cudaFuncSetAttribute(k_tile_force<R, NPE, NQP, MODE, DAMP>,
+        TLFEA_CUDA(cudaFuncSetAttribute(k_tile_force<R, NPE, NQP, MODE, DAMP, MR>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tile_force<R, NPE, NQP, MODE, DAMP><<<h->tl.n_tiles, TILE_ELEMS, smem, h->stream>>>(A);
+    k_tile_force<R, NPE, NQP, MODE, DAMP, MR><<<h->tl.n_tiles, TILE_ELEMS, smem, h->stream>>>(A);
     TLFEA_CHECK_LAUNCH();
     return TLFEA_OK;
 }
@@ -670,9 +673,9 @@ static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
 }
 
 // One tile per block on the compact geometry stream (J^-1 and dV per QP).
-template <typename R, int NPE, int NQP, bool DAMP>
+template <typename R, int NPE, int NQP, bool DAMP, bool MR = false>
 static int launch_tile_geo(tlfea_element_s* h, const TileArgs<R>& A) {
-    auto kern = k_tile_force_geo<R, NPE, NQP, DAMP>;
+    auto kern = k_tile_force_geo<R, NPE, NQP, DAMP, MR>;
     const size_t smem = tile_geo_smem_bytes<R, NPE>(h->tl.max_local, DAMP);
     if (smem > 227 * 1024) {
         set_error("force kernel shared memory exceeds 227 KB (tile touches too many nodes)");
@@ -725,7 +728,9 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
     if (h->tl.n_orphans)
         TLFEA_CUDA(cudaMemsetAsync(A.f_out, 0, sizeof(R) * 3 * (size_t)h->N, h->stream));
     int st;
-    if (h->force_kernel == 1)
+    if (h->material == TLFEA_MATERIAL_MOONEY_RIVLIN)  // Mooney-Rivlin runs on the compact-geometry kernel
+        st = damp ? launch_tile_geo<R, NPE, NQP, true, true>(h, A) : launch_tile_geo<R, NPE, NQP, false, true>(h, A);
+    else if (h->force_kernel == 1)
         st = damp ? launch_tiles<R, NPE, NQP, TILE_FORCE, true>(h, A) : launch_tiles<R, NPE, NQP, TILE_FORCE, false>(h, A);
     else if (h->force_kernel == 2)
         st = damp ? launch_pipe<R, NPE, NQP, true>(h, A) : launch_pipe<R, NPE, NQP, false>(h, A);
@@ -740,10 +745,6 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
 // f_int (FP64) or f_int32 (FP32) = internal force at the current positions.
 // Asynchronous on h->stream (the solvers call it inside their loops).
 int element_force(tlfea_element_s* h, const double* d_v, bool fp32) {
-    if (h->material != TLFEA_MATERIAL_SVK) {
-        set_error("Mooney-Rivlin is not supported by the fused element kernel");
-        return TLFEA_UNSUPPORTED;
-    }
     int st;
     if (fp32) {
         if ((st = element_refresh_u32(h))) return st;
@@ -1236,16 +1237,16 @@ int tlfea_element_calc_mass_matrix(tlfea_element h) {
 int tlfea_element_calc_p(tlfea_element h) {
     CHECK_HANDLE(h);
     REQUIRE_SETUP(h);
-    if (h->material != TLFEA_MATERIAL_SVK) {
-        set_error("Mooney-Rivlin is not supported");
-        return TLFEA_UNSUPPORTED;
-    }
     int st = ensure_pst(h);
     if (st) return st;
     TileArgs<double> A = make_args<double>(h, false);
     A.Pst = h->Pst;
-    st = (h->npe == 10) ? launch_tiles<double, 10, 5, TILE_STORE_P, false>(h, A)
-                        : launch_tiles<double, 4, 1, TILE_STORE_P, false>(h, A);
+    if (h->material == TLFEA_MATERIAL_MOONEY_RIVLIN)
+        st = (h->npe == 10) ? launch_tiles<double, 10, 5, TILE_STORE_P, false, true>(h, A)
+                            : launch_tiles<double, 4, 1, TILE_STORE_P, false, true>(h, A);
+    else
+        st = (h->npe == 10) ? launch_tiles<double, 10, 5, TILE_STORE_P, false>(h, A)
+                            : launch_tiles<double, 4, 1, TILE_STORE_P, false>(h, A);
     if (st) return st;
     SYNC_COMPUTE(h);
     return TLFEA_OK;
@@ -1364,10 +1365,6 @@ int tlfea_element_compute_internal_force_noalloc(tlfea_element h, const double* 
         set_error("output pointer is null");
         return TLFEA_INVALID_ARG;
     }
-    if (h->material != TLFEA_MATERIAL_SVK) {
-        set_error("Mooney-Rivlin is not supported by the fused element kernel");
-        return TLFEA_UNSUPPORTED;
-    }
     const size_t need = 3 * (size_t)h->tl.n_pslots;
     if (need > NOALLOC_SCRATCH_DOUBLES) {
         set_error("mesh needs " + std::to_string(need) + " doubles of shared-node scratch; the static scratch holds " +
@@ -1383,10 +1380,22 @@ int tlfea_element_compute_internal_force_noalloc(tlfea_element h, const double* 
     A.partial = scratch;
     const bool damp = d_v && (h->eta_d != 0.0 || h->lambda_d != 0.0);
     if (h->tl.n_orphans) TLFEA_CUDA(cudaMemsetAsync(d_f_out, 0, sizeof(double) * 3 * (size_t)h->N, h->stream));
-    if (h->npe == 10)
-        st = damp ? launch_tiles<double, 10, 5, TILE_FORCE, true>(h, A) : launch_tiles<double, 10, 5, TILE_FORCE, false>(h, A);
-    else
-        st = damp ? launch_tiles<double, 4, 1, TILE_FORCE, true>(h, A) : launch_tiles<double, 4, 1, TILE_FORCE, false>(h, A);
+    const bool mr = (h->material == TLFEA_MATERIAL_MOONEY_RIVLIN);
+    if (h->npe == 10) {
+        if (mr)
+            st = damp ? launch_tiles<double, 10, 5, TILE_FORCE, true, true>(h, A)
+                      : launch_tiles<double, 10, 5, TILE_FORCE, false, true>(h, A);
+        else
+            st = damp ? launch_tiles<double, 10, 5, TILE_FORCE, true>(h, A)
+                      : launch_tiles<double, 10, 5, TILE_FORCE, false>(h, A);
+    } else {
+        if (mr)
+            st = damp ? launch_tiles<double, 4, 1, TILE_FORCE, true, true>(h, A)
+                      : launch_tiles<double, 4, 1, TILE_FORCE, false, true>(h, A);
+        else
+            st = damp ? launch_tiles<double, 4, 1, TILE_FORCE, true>(h, A)
+                      : launch_tiles<double, 4, 1, TILE_FORCE, false>(h, A);
+    }
     if (st) return st;
     if ((st = launch_combine<double, false>(h, A.partial, A.f_out))) return st;
     SYNC_COMPUTE(h);

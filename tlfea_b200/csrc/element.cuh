@@ -88,6 +88,7 @@ struct TileArgs {
     R* f_out;         // interleaved 3N
     R* partial;       // 3 * n_pslots
     R lambda, mu, eta, lamd;
+    double mu10, mu01, kappa;  // Mooney-Rivlin (MR instantiations)
     int max_local;
     QpBary qb;
 };
@@ -269,13 +270,74 @@ __device__ __forceinline__ void kelvin_voigt(const R F[3][3], const R Fd[3][3], 
 //             the FP32 displacement, and P = (I + H) S, S = lambda tr(E) I + 2 mu E,
 //             E = (H + H^T + H^T H)/2 -- algebraically the same SVK stress,
 //             without the cancellation of tr(F^T F) - 3 near F = I.
+// Mooney-Rivlin first Piola stress (mr_compute_P, MooneyRivlin.cuh:46-104), FP64:
+// C = F^T F, I1 = tr C, I2 = (I1^2 - tr C^2) / 2, J = det F, F^-T by cofactors
+// with |J| clamped to 1e-12 for the inverse, and
+// P = 2 mu10 J^-2/3 (F - I1/3 F^-T) + 2 mu01 J^-4/3 (I1 F - F C - 2 I2/3 F^-T)
+//   + kappa (J - 1) J F^-T.
+__device__ __forceinline__ void mooney_rivlin_p(const double F[3][3], double mu10, double mu01, double kappa,
+                                                double P[3][3]) {
+    double C[3][3], FC[3][3], FiT[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) C[i][j] = F[0][i] * F[0][j] + F[1][i] * F[1][j] + F[2][i] * F[2][j];
+    const double I1 = C[0][0] + C[1][1] + C[2][2];
+    double trC2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) trC2 += C[i][k] * C[k][i];
+    const double I2 = 0.5 * (I1 * I1 - trC2);
+    const double J = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
+                     F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+                     F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+    const double dj = (fabs(J) < 1e-12) ? ((J >= 0.0) ? 1e-12 : -1e-12) : J;
+    const double id = 1.0 / dj;
+    FiT[0][0] = (F[1][1] * F[2][2] - F[1][2] * F[2][1]) * id;
+    FiT[0][1] = (F[1][2] * F[2][0] - F[1][0] * F[2][2]) * id;
+    FiT[0][2] = (F[1][0] * F[2][1] - F[1][1] * F[2][0]) * id;
+    FiT[1][0] = (F[0][2] * F[2][1] - F[0][1] * F[2][2]) * id;
+    FiT[1][1] = (F[0][0] * F[2][2] - F[0][2] * F[2][0]) * id;
+    FiT[1][2] = (F[0][1] * F[2][0] - F[0][0] * F[2][1]) * id;
+    FiT[2][0] = (F[0][1] * F[1][2] - F[0][2] * F[1][1]) * id;
+    FiT[2][1] = (F[0][2] * F[1][0] - F[0][0] * F[1][2]) * id;
+    FiT[2][2] = (F[0][0] * F[1][1] - F[0][1] * F[1][0]) * id;
+    const double j13 = cbrt(J);
+    const double jm23 = 1.0 / (j13 * j13), jm43 = jm23 * jm23;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) FC[i][j] = F[i][0] * C[0][j] + F[i][1] * C[1][j] + F[i][2] * C[2][j];
+    const double t1 = 2.0 * mu10 * jm23, t2 = 2.0 * mu01 * jm43, t3 = kappa * (J - 1.0) * J;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            P[i][j] = t1 * (F[i][j] - (I1 / 3.0) * FiT[i][j]) +
+                      t2 * (I1 * F[i][j] - FC[i][j] - (2.0 * I2 / 3.0) * FiT[i][j]) + t3 * FiT[i][j];
+}
+
 // First Piola stress of one QP from the compact-geometry gradient: FP64 takes
 // F itself (the reference's SVK form), FP32 the displacement gradient H (F =
 // I + H, the cancellation-free form); with DAMP the Kelvin-Voigt term of the
 // velocity gradient Fd is added.
-template <typename R, bool DAMP>
+template <typename R, bool DAMP, bool MR = false>
 __device__ __forceinline__ void tile_stress(const R H[3][3], const R Fd[3][3], const TileArgs<R>& A, R P[3][3]) {
-    if constexpr (sizeof(R) == 8) {
+    if constexpr (MR) {
+        // Mooney-Rivlin in FP64 whatever R is (FP32 mode: F = I + H formed in FP64)
+        double F64[3][3], P64[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                F64[i][j] = (sizeof(R) == 8) ? double(H[i][j]) : double(H[i][j]) + (i == j ? 1.0 : 0.0);
+        mooney_rivlin_p(F64, A.mu10, A.mu01, A.kappa, P64);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) P[i][j] = R(P64[i][j]);
+    } else if constexpr (sizeof(R) == 8) {
         svk_p_reference(H, A.lambda, A.mu, P);
     } else {
         R Em[3][3];
@@ -320,7 +382,7 @@ __device__ __forceinline__ void tile_stress(const R H[3][3], const R Fd[3][3], c
 
 // One QP of the compact-geometry force: F (or H) = (dx/dxi) J^-1 from the
 // nodal values xa, the stress, and f_a (+)= (dV P J^-T) dN_a/dxi.
-template <typename R, int NPE, bool DAMP, bool FIRST>
+template <typename R, int NPE, bool DAMP, bool FIRST, bool MR = false>
 __device__ __forceinline__ void compact_qp(const TileArgs<R>& A, const R (&xa)[NPE][3], const R (&va)[NPE][3],
                                            const R ji[9], R dv, const R Lq[4], R (&f)[NPE][3]) {
     R Gx[3][3], H[3][3], Fd[3][3], P[3][3], Q[3][3];
@@ -331,7 +393,7 @@ __device__ __forceinline__ void compact_qp(const TileArgs<R>& A, const R (&xa)[N
         tet_dx_dxi<R, NPE>(va, Lq, Gv);
         mul_jinv(Gv, ji, Fd);
     }
-    tile_stress<R, DAMP>(H, Fd, A, P);
+    tile_stress<R, DAMP, MR>(H, Fd, A, P);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -343,7 +405,7 @@ __device__ __forceinline__ void compact_qp(const TileArgs<R>& A, const R (&xa)[N
         tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] += v; });
 }
 
-template <typename R, int NPE, int NQP, int MODE, bool DAMP>
+template <typename R, int NPE, int NQP, int MODE, bool DAMP, bool MR = false>
 __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, unsigned char* smem_raw) {
     constexpr int TE = TILE_ELEMS;
     const int t = threadIdx.x;
@@ -398,7 +460,7 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
                 for (int d = 0; d < 3; ++d) va[a][d] = vs[3 * lc[a] + d];
             }
         }
-        compact_qp<R, NPE, DAMP, false>(A, xa, va, ji, dv, Lq, f);
+        compact_qp<R, NPE, DAMP, false, MR>(A, xa, va, ji, dv, Lq, f);
     }
 #pragma unroll 1
     for (int q = 0; q < NQP && MODE != TILE_FORCE; ++q) {
@@ -417,99 +479,31 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
 #pragma unroll
                 for (int j = 0; j < 3; ++j)
                     P[i][j] = (eo >= 0) ? R(A.Pst[((size_t)eo * NQP + q) * 9 + i + 3 * j]) : R(0);
-        } else if constexpr (sizeof(R) == 8) {
-            double F[3][3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) F[i][j] = 0.0;
-#pragma unroll
-            for (int a = 0; a < NPE; ++a) {
-                const double xa[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) F[i][j] += xa[i] * g[a][j];
-            }
-            svk_p_reference(F, A.lambda, A.mu, P);
-            if (DAMP) {
-                double Fd[3][3], Pv[3][3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) Fd[i][j] = 0.0;
-#pragma unroll
-                for (int a = 0; a < NPE; ++a)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc[a] + i] * g[a][j];
-                kelvin_voigt<double>(F, Fd, A.eta, A.lamd, Pv);
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
-            }
         } else {
-            R H[3][3];
+            // F (FP64) or H (FP32) from the gradients, the velocity gradient for
+            // the Kelvin-Voigt term, then the material law
+            R H[3][3], Fd[3][3];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int j = 0; j < 3; ++j) H[i][j] = R(0);
+                for (int j = 0; j < 3; ++j) H[i][j] = Fd[i][j] = R(0);
 #pragma unroll
             for (int a = 0; a < NPE; ++a) {
-                const R ua[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+                const R xa[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) H[i][j] += ua[i] * g[a][j];
+                    for (int j = 0; j < 3; ++j) H[i][j] += xa[i] * g[a][j];
             }
-            R Em[3][3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    R s = H[i][j] + H[j][i];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) s += H[k][i] * H[k][j];
-                    Em[i][j] = R(0.5) * s;
-                }
-            const R trE = Em[0][0] + Em[1][1] + Em[2][2];
-            R S[3][3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) S[i][j] = R(2) * A.mu * Em[i][j] + (i == j ? A.lambda * trE : R(0));
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    R s = S[i][j];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) s += H[i][k] * S[k][j];
-                    P[i][j] = s;
-                }
             if (DAMP) {
-                R F[3][3], Fd[3][3], Pv[3][3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        F[i][j] = H[i][j] + (i == j ? R(1) : R(0));
-                        Fd[i][j] = R(0);
-                    }
 #pragma unroll
                 for (int a = 0; a < NPE; ++a)
 #pragma unroll
                     for (int i = 0; i < 3; ++i)
 #pragma unroll
                         for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc[a] + i] * g[a][j];
-                kelvin_voigt<R>(F, Fd, A.eta, A.lamd, Pv);
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
             }
+            tile_stress<R, DAMP, MR>(H, Fd, A, P);
         }
 
         if constexpr (MODE == TILE_STORE_P) {

@@ -149,9 +149,10 @@ __device__ __forceinline__ void grad_node(const FOArgs& S, int i, const double f
     }
 }
 
-template <typename R, int NPE, int NQP, bool DAMP>
+template <typename R, int NPE, int NQP, bool DAMP, bool MR>
 __device__ __forceinline__ void force_phase(const FOArgs& S, const TileArgs<R>& A, unsigned char* smem) {
-    for (int tile = blockIdx.x; tile < S.n_tiles; tile += gridDim.x) process_tile<R, NPE, NQP, TILE_FORCE, DAMP>(A, tile, smem);
+    for (int tile = blockIdx.x; tile < S.n_tiles; tile += gridDim.x)
+        process_tile<R, NPE, NQP, TILE_FORCE, DAMP, MR>(A, tile, smem);
     const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
     for (int k = gt; k < S.n_fixed; k += gs) {
         const int n = S.fixed[k];
@@ -161,7 +162,7 @@ __device__ __forceinline__ void force_phase(const FOArgs& S, const TileArgs<R>& 
     }
 }
 
-template <typename R, int NPE, int NQP, bool DAMP>
+template <typename R, int NPE, int NQP, bool DAMP, bool MR>
 __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R> A) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double red_sh[32];
@@ -262,7 +263,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
             }
             grid.sync();
             // ---- P2: internal force (fused tiles) and constraint values
-            force_phase<R, NPE, NQP, DAMP>(S, A, smem);
+            force_phase<R, NPE, NQP, DAMP, MR>(S, A, smem);
             grid.sync();
             // ---- P3: gradient per node and the norm partials
             const bool do_check = nesterov || (inner % check == 0);
@@ -388,10 +389,10 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
     }
 }
 
-template <typename R, int NPE, int NQP, bool DAMP>
+template <typename R, int NPE, int NQP, bool DAMP, bool MR>
 static int launch_first_order(tlfea_solver_s* s, FOArgs& S, TileArgs<R>& A) {
     tlfea_element_s* el = s->el;
-    auto kern = k_first_order<R, NPE, NQP, DAMP>;
+    auto kern = k_first_order<R, NPE, NQP, DAMP, MR>;
     const size_t smem = tile_smem_bytes<R>(NPE, el->tl.max_local, DAMP);
     if (smem > 48 * 1024) TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0, sms = 0;
@@ -457,10 +458,6 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     if (!el->mass_setup) {
         set_error("CalcMassMatrix must be called before Solve");
         return TLFEA_NOT_SETUP;
-    }
-    if (el->material != TLFEA_MATERIAL_SVK) {
-        set_error("Mooney-Rivlin is not supported");
-        return TLFEA_UNSUPPORTED;
     }
     if (s->n_constraints != el->n_constraint) {
         set_error("solver constraint count differs from the element's");
@@ -535,6 +532,9 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     A32.v = A64.v = s->v_guess;
     A32.max_local = A64.max_local = el->tl.max_local;
     A32.qb = A64.qb = qp_bary(el);
+    A32.mu10 = A64.mu10 = el->mu10;
+    A32.mu01 = A64.mu01 = el->mu01;
+    A32.kappa = A64.kappa = el->kappa;
     A32.ji = el->tl.ji32;
     A64.ji = el->tl.ji64;
     A32.grad = el->tl.grad32; A32.dv = el->tl.dv32; A32.px = el->ux; A32.py = el->uy; A32.pz = el->uz;
@@ -543,19 +543,34 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     A64.grad = el->tl.grad64; A64.dv = el->tl.dv64; A64.px = el->x; A64.py = el->y; A64.pz = el->z;
     A64.f_out = el->f_int; A64.partial = el->tl.partial64;
     A64.lambda = el->lambda; A64.mu = el->mu; A64.eta = el->eta_d; A64.lamd = el->lambda_d;
+    const bool mr = (el->material == TLFEA_MATERIAL_MOONEY_RIVLIN);
     auto launch_one = [&](FOArgs& SS) -> int {
         if (fp32) {
-            if (el->npe == 10)
-                return damp ? launch_first_order<float, 10, 5, true>(s, SS, A32)
-                            : launch_first_order<float, 10, 5, false>(s, SS, A32);
-            return damp ? launch_first_order<float, 4, 1, true>(s, SS, A32)
-                        : launch_first_order<float, 4, 1, false>(s, SS, A32);
+            if (el->npe == 10) {
+                if (mr)
+                    return damp ? launch_first_order<float, 10, 5, true, true>(s, SS, A32)
+                                : launch_first_order<float, 10, 5, false, true>(s, SS, A32);
+                return damp ? launch_first_order<float, 10, 5, true, false>(s, SS, A32)
+                            : launch_first_order<float, 10, 5, false, false>(s, SS, A32);
+            }
+            if (mr)
+                return damp ? launch_first_order<float, 4, 1, true, true>(s, SS, A32)
+                            : launch_first_order<float, 4, 1, false, true>(s, SS, A32);
+            return damp ? launch_first_order<float, 4, 1, true, false>(s, SS, A32)
+                        : launch_first_order<float, 4, 1, false, false>(s, SS, A32);
         }
-        if (el->npe == 10)
-            return damp ? launch_first_order<double, 10, 5, true>(s, SS, A64)
-                        : launch_first_order<double, 10, 5, false>(s, SS, A64);
-        return damp ? launch_first_order<double, 4, 1, true>(s, SS, A64)
-                    : launch_first_order<double, 4, 1, false>(s, SS, A64);
+        if (el->npe == 10) {
+            if (mr)
+                return damp ? launch_first_order<double, 10, 5, true, true>(s, SS, A64)
+                            : launch_first_order<double, 10, 5, false, true>(s, SS, A64);
+            return damp ? launch_first_order<double, 10, 5, true, false>(s, SS, A64)
+                        : launch_first_order<double, 10, 5, false, false>(s, SS, A64);
+        }
+        if (mr)
+            return damp ? launch_first_order<double, 4, 1, true, true>(s, SS, A64)
+                        : launch_first_order<double, 4, 1, false, true>(s, SS, A64);
+        return damp ? launch_first_order<double, 4, 1, true, false>(s, SS, A64)
+                    : launch_first_order<double, 4, 1, false, false>(s, SS, A64);
     };
     cudaStream_t stream = el->stream;
     const int n_steps = std::max(1, steps);

@@ -668,7 +668,7 @@ inline size_t tile_geo_smem_bytes(int max_local, bool damp) {
     return TileGeoLayout<R, NPE>(max_local, damp).total;
 }
 
-template <typename R, int NPE, int NQP, bool DAMP>
+template <typename R, int NPE, int NQP, bool DAMP, bool MR = false>
 __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, int* err) {
     using G = TileGeoGeom<R, NPE>;
     constexpr int TE = TILE_ELEMS;
@@ -761,9 +761,9 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, in
         // F (FP64) or H (FP32), the stress, f_a (+)= (dV P J^-T) dN_a/dxi
         // (FEAT10DataFunc.cuh:417-449 with gradN = J^-T dN/dxi)
         if (q == 0)
-            compact_qp<R, NPE, DAMP, true>(A, xa, va, ji, dv, Lq, f);
+            compact_qp<R, NPE, DAMP, true, MR>(A, xa, va, ji, dv, Lq, f);
         else
-            compact_qp<R, NPE, DAMP, false>(A, xa, va, ji, dv, Lq, f);
+            compact_qp<R, NPE, DAMP, false, MR>(A, xa, va, ji, dv, Lq, f);
     }
     __syncthreads();  // every thread is done with the stages the force table reuses
 #pragma unroll
