@@ -130,8 +130,8 @@ int tlfea_element_set_svk(tlfea_element h, double E, double nu);
  * FEAT10Data.cuh:576-587).  The internal force (every entry point; on the
  * compact-geometry kernel), CalcP / CalcInternalForce and the first-order
  * solvers then use the Mooney-Rivlin stress of MooneyRivlin.cuh:46-104 (in FP64,
- * also in FP32 force mode); the stiffness (LinearStaticSolver) returns
- * TLFEA_UNSUPPORTED. */
+ * also in FP32 force mode), and LinearStaticSolver its consistent tangent
+ * (MooneyRivlin.cuh:106-221). */
 int tlfea_element_set_mooney_rivlin(tlfea_element h, double mu10, double mu01, double kappa);
 /* SetExternalForce (:589-597); n must be 3*N. */
 int tlfea_element_set_external_force(tlfea_element h, const double* f_ext, int n);

@@ -311,6 +311,73 @@ static void mr_p(const double F[3][3], double mu10, double mu01, double kappa, d
                       t2 * (I1 * F[i][j] - FC[i][j] - (2.0 * I2 / 3.0) * FiT[i][j]) + t3 * FiT[i][j];
 }
 
+/* Mooney-Rivlin consistent tangent A_ijkl = dP_ij / dF_kl (mr_compute_tangent_tensor,
+ * MooneyRivlin.cuh:106-221: the exact derivative of mr_p, term by term) contracted
+ * with the gradient of node a: B[i][k][l] = sum_j A_ijkl ga[j], so that the
+ * (a, b) stiffness block is K[i][k] = sum_l B[i][k][l] gb[l] dV. */
+static void mr_tangent_a(const double F[3][3], double mu10, double mu01, double kappa, const double ga[3],
+                         double B[3][3][3]) {
+    double C[3][3] = {{0}}, C2[3][3] = {{0}}, FC[3][3] = {{0}}, FFT[3][3] = {{0}}, FiT[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k) {
+                C[i][j] += F[k][i] * F[k][j];
+                FFT[i][j] += F[i][k] * F[j][k];
+            }
+    const double I1 = C[0][0] + C[1][1] + C[2][2];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k) C2[i][j] += C[i][k] * C[k][j];
+    const double I2 = 0.5 * (I1 * I1 - (C2[0][0] + C2[1][1] + C2[2][2]));
+    const double J = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
+                     F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+                     F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+    double dj = J;
+    if (fabs(dj) < 1e-12) dj = (dj >= 0.0) ? 1e-12 : -1e-12;
+    const double id = 1.0 / dj;
+    FiT[0][0] = (F[1][1] * F[2][2] - F[1][2] * F[2][1]) * id;
+    FiT[0][1] = (F[1][2] * F[2][0] - F[1][0] * F[2][2]) * id;
+    FiT[0][2] = (F[1][0] * F[2][1] - F[1][1] * F[2][0]) * id;
+    FiT[1][0] = (F[0][2] * F[2][1] - F[0][1] * F[2][2]) * id;
+    FiT[1][1] = (F[0][0] * F[2][2] - F[0][2] * F[2][0]) * id;
+    FiT[1][2] = (F[0][1] * F[2][0] - F[0][0] * F[2][1]) * id;
+    FiT[2][0] = (F[0][1] * F[1][2] - F[0][2] * F[1][1]) * id;
+    FiT[2][1] = (F[0][2] * F[1][0] - F[0][0] * F[1][2]) * id;
+    FiT[2][2] = (F[0][0] * F[1][1] - F[0][1] * F[1][0]) * id;
+    const double j13 = cbrt(J);
+    const double jm23 = 1.0 / (j13 * j13), jm43 = jm23 * jm23;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k) FC[i][j] += F[i][k] * C[k][j];
+    const double t1 = 2.0 * mu10 * jm23, t2 = 2.0 * mu01 * jm43, t3 = kappa * (J - 1.0) * J;
+    double T1[3][3], T2[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            T1[i][j] = F[i][j] - (I1 / 3.0) * FiT[i][j];
+            T2[i][j] = I1 * F[i][j] - FC[i][j] - (2.0 * I2 / 3.0) * FiT[i][j];
+        }
+    const double dt3c = kappa * (2.0 * J - 1.0) * J;
+    for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l) {
+                double s = 0.0;
+                for (int j = 0; j < 3; ++j) {
+                    const double dik = (i == k) ? 1.0 : 0.0, djl = (j == l) ? 1.0 : 0.0;
+                    const double dFiT = -FiT[i][l] * FiT[k][j];
+                    const double dT1 = dik * djl - (2.0 / 3.0) * F[k][l] * FiT[i][j] + (I1 / 3.0) * FiT[i][l] * FiT[k][j];
+                    const double dT2 = 2.0 * F[k][l] * F[i][j] + I1 * dik * djl -
+                                       (dik * C[l][j] + F[i][l] * F[k][j] + djl * FFT[i][k]) -
+                                       (4.0 / 3.0) * (I1 * F[k][l] - FC[k][l]) * FiT[i][j] +
+                                       (2.0 * I2 / 3.0) * FiT[i][l] * FiT[k][j];
+                    const double A = (-2.0 / 3.0) * t1 * FiT[k][l] * T1[i][j] + t1 * dT1 +
+                                     (-4.0 / 3.0) * t2 * FiT[k][l] * T2[i][j] + t2 * dT2 +
+                                     dt3c * FiT[k][l] * FiT[i][j] + t3 * dFiT;
+                    s += A * ga[j];
+                }
+                B[i][k][l] = s;
+            }
+}
+
 /* compute_p for one (e,q): F, SVK P (SVK.cuh:17-39 via the trFtF/FFtF path) or
  * the Mooney-Rivlin P (FEAT10DataFunc.cuh:273-278), plus the optional
  * Kelvin-Voigt term (FEAT10DataFunc.cuh:130-231). */
@@ -680,6 +747,8 @@ void orc_stiffness_assemble(int npe, int nqp, int E, int N, const double* x, con
                         for (int c = 0; c < 3; ++c) Fh[b][r] += F[r][c] * g[b][c];
                     }
                 const double dV = detJ[e * nqp + q] * qw[q];
+                double Bmr[3][3][3];
+                if (g_material == 1) mr_tangent_a(F, g_mu10, g_mu01, g_kappa, g[a], Bmr);
                 for (int b = 0; b < npe; ++b) {
                     const int nb = conn[e + b * E];
                     /* svk_compute_tangent_block(Fh_a, Fh_b, ...) (SVK.cuh:41-67) */
@@ -692,13 +761,20 @@ void orc_stiffness_assemble(int npe, int nqp, int E, int N, const double* x, con
                             const int p = find_col(cols, offsets[row], offsets[row + 1], 3 * nb + ee);
                             if (p < 0) continue;
                             const double delta = (d == ee) ? 1.0 : 0.0;
-                            const double A = lambda * Fh[a][d] * Fh[b][ee];
-                            const double B = lambda * trE * hij * delta;
-                            const double C1 = mu * fdf * delta;
-                            const double D = mu * Fh[b][d] * Fh[a][ee];
-                            const double Et = mu * hij * FFT[d][ee];
-                            const double Ft = -mu * hij * delta;
-                            vals[p] += h * ((A + B + C1 + D + Et + Ft) * dV);
+                            if (g_material == 1) {
+                                /* the Mooney-Rivlin block, FEAT10DataFunc.cuh:607-640 */
+                                const double kb = Bmr[d][ee][0] * g[b][0] + Bmr[d][ee][1] * g[b][1] +
+                                                  Bmr[d][ee][2] * g[b][2];
+                                vals[p] += h * (kb * dV);
+                            } else {
+                                const double A = lambda * Fh[a][d] * Fh[b][ee];
+                                const double B = lambda * trE * hij * delta;
+                                const double C1 = mu * fdf * delta;
+                                const double D = mu * Fh[b][d] * Fh[a][ee];
+                                const double Et = mu * hij * FFT[d][ee];
+                                const double Ft = -mu * hij * delta;
+                                vals[p] += h * ((A + B + C1 + D + Et + Ft) * dV);
+                            }
                             /* Kelvin-Voigt block, FEAT10DataFunc.cuh:686-768 (not scaled by h) */
                             if (visc)
                                 vals[p] += (eta_d * (Fh[b][d] * Fh[a][ee]) + eta_d * FFT[d][ee] * hd +

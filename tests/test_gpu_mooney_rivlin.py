@@ -1,7 +1,8 @@
 """Mooney-Rivlin (SetMooneyRivlin, MooneyRivlin.cuh:46-104) on the GPU against
 the oracle: the fused internal force (FP64 rel 1e-10, FP32 rel 1e-5) with and
 without Kelvin-Voigt damping, CalcP / CalcInternalForce, the allocation-free
-entry point, a fixed-count Nesterov trajectory, and the stiffness refusal."""
+entry point, a fixed-count Nesterov trajectory, and the Mooney-Rivlin tangent
+of LinearStaticSolver."""
 import ctypes as C
 
 import numpy as np
@@ -107,12 +108,41 @@ def test_mooney_rivlin_nesterov_fixed_iterations():
     el.Destroy()
 
 
-def test_mooney_rivlin_stiffness_is_refused():
-    x, y, z, conn = box(4, 2, 2, 10)
-    fixed, f, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -10.0))
+@pytest.mark.parametrize("order", [10, 4])
+def test_mooney_rivlin_stiffness_and_linear_static_solve(order):
+    """LinearStaticSolver on a Mooney-Rivlin element: the tangent assembled at
+    deformed positions against the oracle's, and the solve against a direct one."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    x, y, z, conn = box(8, 2, 2, order)
+    fixed, f, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -100.0))
     el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
     el.SetMooneyRivlin(*MR)
-    ls = T.LinearStaticSolver(el, 1e-8, 100)
-    with pytest.raises(_capi.TLFEAError):
-        ls.Solve()
+    xs = perturb(x, y, z, 1e-3, 21)
+    el.UpdatePositions(*xs)
+    s = T.LinearStaticSolver(el, 1e-11, 50000)
+    s.Solve()
+    g, dj = O.dndu_pre(x, y, z, conn)
+    with O.mooney_rivlin(*MR):
+        off, cols, vals = O.stiffness(*xs, conn, g, dj, 0.0, 0.0)
+    kv, fb = O.apply_bcs(off, cols, vals, f, fixed)
+    o2, c2, v2 = s.RetrieveStiffnessCSRToCPU()
+    assert np.array_equal(o2, off) and np.array_equal(c2, cols)
+    assert rel(v2, kv) < 1e-12
+    el.Destroy()
+    # at the reference configuration (stress free, K positive definite) the CG
+    # solve matches a direct solve of the oracle's system
+    el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
+    el.SetMooneyRivlin(*MR)
+    s = T.LinearStaticSolver(el, 1e-11, 50000)
+    s.Solve()
+    assert s.GetLastResidual() < 1e-11
+    with O.mooney_rivlin(*MR):
+        off, cols, vals = O.stiffness(x, y, z, conn, g, dj, 0.0, 0.0)
+    kv, fb = O.apply_bcs(off, cols, vals, f, fixed)
+    x2, y2, z2 = el.RetrievePositionToCPU()
+    u = np.stack([x2 - x, y2 - y, z2 - z], 1).ravel()
+    u_dir = spla.spsolve(sp.csr_matrix((kv, cols, off)).tocsc(), fb)
+    assert rel(u, u_dir) < 1e-7
     el.Destroy()

@@ -178,6 +178,24 @@ def test_stiffness_is_consistent_tangent(order):
     assert abs(K - K.T).max() < 1e-8 * abs(K).max()
 
 
+@pytest.mark.parametrize("order", [10, 4])
+def test_mooney_rivlin_stiffness_is_consistent_tangent(order):
+    """The oracle's Mooney-Rivlin stiffness is d f_int / d x of its Mooney-Rivlin force."""
+    x, y, z, conn = O.box_mesh(4, 2, 2, order, 0.4, 0.2, 0.2)
+    g, dj = O.dndu_pre(x, y, z, conn)
+    r = np.random.default_rng(5)
+    xs = [v + 3e-3 * r.standard_normal(v.shape) for v in (x, y, z)]
+    du = 1e-7 * r.standard_normal(3 * len(x))
+    X = np.stack(xs, 1).ravel()
+    with O.mooney_rivlin(2.0e6, 5.0e5, 5.0e7):
+        off, cols, vals = O.stiffness(*xs, conn, g, dj, 0.0, 0.0)
+        fp = O.force(*(X + du).reshape(-1, 3).T, conn, g, dj, 0.0, 0.0)
+        fm = O.force(*(X - du).reshape(-1, 3).T, conn, g, dj, 0.0, 0.0)
+    K = sp.csr_matrix((vals, cols, off))
+    assert rel((fp - fm) / 2, K @ du) < 1e-6
+    assert abs(K - K.T).max() < 1e-8 * abs(K).max()
+
+
 def test_cg_matches_direct_solve():
     x, y, z, conn = O.box_mesh(10, 2, 2, 10)
     g, dj = O.dndu_pre(x, y, z, conn)

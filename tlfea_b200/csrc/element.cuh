@@ -318,6 +318,69 @@ __device__ __forceinline__ void mooney_rivlin_p(const double F[3][3], double mu1
                       t2 * (I1 * F[i][j] - FC[i][j] - (2.0 * I2 / 3.0) * FiT[i][j]) + t3 * FiT[i][j];
 }
 
+// Mooney-Rivlin consistent tangent A_ijkl = dP_ij / dF_kl (mr_compute_tangent_tensor,
+// MooneyRivlin.cuh:106-221: the exact derivative of mooney_rivlin_p, term by
+// term), contracted with node a's gradient: B[i][k][l] = sum_j A_ijkl ga[j], so
+// the (a, b) stiffness block is K[i][k] = sum_l B[i][k][l] gb[l] dV.
+__device__ __forceinline__ void mooney_rivlin_tangent_a(const double F[3][3], double mu10, double mu01, double kappa,
+                                                        const double ga[3], double B[3][3][3]) {
+    double C[3][3], FC[3][3], FFT[3][3], FiT[3][3], T1[3][3], T2[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            C[i][j] = F[0][i] * F[0][j] + F[1][i] * F[1][j] + F[2][i] * F[2][j];
+            FFT[i][j] = F[i][0] * F[j][0] + F[i][1] * F[j][1] + F[i][2] * F[j][2];
+        }
+    const double I1 = C[0][0] + C[1][1] + C[2][2];
+    double trC2 = 0.0;
+    for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k) trC2 += C[i][k] * C[k][i];
+    const double I2 = 0.5 * (I1 * I1 - trC2);
+    const double J = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
+                     F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+                     F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+    const double dj = (fabs(J) < 1e-12) ? ((J >= 0.0) ? 1e-12 : -1e-12) : J;
+    const double id = 1.0 / dj;
+    FiT[0][0] = (F[1][1] * F[2][2] - F[1][2] * F[2][1]) * id;
+    FiT[0][1] = (F[1][2] * F[2][0] - F[1][0] * F[2][2]) * id;
+    FiT[0][2] = (F[1][0] * F[2][1] - F[1][1] * F[2][0]) * id;
+    FiT[1][0] = (F[0][2] * F[2][1] - F[0][1] * F[2][2]) * id;
+    FiT[1][1] = (F[0][0] * F[2][2] - F[0][2] * F[2][0]) * id;
+    FiT[1][2] = (F[0][1] * F[2][0] - F[0][0] * F[2][1]) * id;
+    FiT[2][0] = (F[0][1] * F[1][2] - F[0][2] * F[1][1]) * id;
+    FiT[2][1] = (F[0][2] * F[1][0] - F[0][0] * F[1][2]) * id;
+    FiT[2][2] = (F[0][0] * F[1][1] - F[0][1] * F[1][0]) * id;
+    const double j13 = cbrt(J);
+    const double jm23 = 1.0 / (j13 * j13), jm43 = jm23 * jm23;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) FC[i][j] = F[i][0] * C[0][j] + F[i][1] * C[1][j] + F[i][2] * C[2][j];
+    const double t1 = 2.0 * mu10 * jm23, t2 = 2.0 * mu01 * jm43, t3 = kappa * (J - 1.0) * J;
+    const double dt3c = kappa * (2.0 * J - 1.0) * J;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            T1[i][j] = F[i][j] - (I1 / 3.0) * FiT[i][j];
+            T2[i][j] = I1 * F[i][j] - FC[i][j] - (2.0 * I2 / 3.0) * FiT[i][j];
+        }
+    for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l) {
+                double s = 0.0;
+                for (int j = 0; j < 3; ++j) {
+                    const double dik = (i == k) ? 1.0 : 0.0, djl = (j == l) ? 1.0 : 0.0;
+                    const double dFiT = -FiT[i][l] * FiT[k][j];
+                    const double dT1 = dik * djl - (2.0 / 3.0) * F[k][l] * FiT[i][j] + (I1 / 3.0) * FiT[i][l] * FiT[k][j];
+                    const double dT2 = 2.0 * F[k][l] * F[i][j] + I1 * dik * djl -
+                                       (dik * C[l][j] + F[i][l] * F[k][j] + djl * FFT[i][k]) -
+                                       (4.0 / 3.0) * (I1 * F[k][l] - FC[k][l]) * FiT[i][j] +
+                                       (2.0 * I2 / 3.0) * FiT[i][l] * FiT[k][j];
+                    const double A = (-2.0 / 3.0) * t1 * FiT[k][l] * T1[i][j] + t1 * dT1 +
+                                     (-4.0 / 3.0) * t2 * FiT[k][l] * T2[i][j] + t2 * dT2 + dt3c * FiT[k][l] * FiT[i][j] +
+                                     t3 * dFiT;
+                    s += A * ga[j];
+                }
+                B[i][k][l] = s;
+            }
+}
+
 // First Piola stress of one QP from the compact-geometry gradient: FP64 takes
 // F itself (the reference's SVK form), FP32 the displacement gradient H (F =
 // I + H, the cancellation-free form); with DAMP the Kelvin-Voigt term of the

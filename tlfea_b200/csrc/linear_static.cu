@@ -17,10 +17,11 @@ namespace tlfea {
 // in element order and every QP: the SVK tangent blocks K_ab of
 // compute_hessian_assemble_csr (FEAT10DataFunc.cuh:512-684; SVK.cuh:41-67) at
 // the current positions, scaled by h, plus the Kelvin-Voigt block C_ab
-// (:686-768) when damping is set.  Block (a,b) is added to row i's block for
-// node conn(e,b).  No atomics: each row is owned by one thread.  K is
-// row-planar: component c of row i's k-th block is K[9*off[i] + c*nb + k].
-template <int NPE, int NQP>
+// (:686-768) when damping is set; with MR the Mooney-Rivlin blocks
+// sum_JL A[d][J][e][L] gN_aJ gN_bL dV (:607-640).  Block (a,b) is added to row
+// i's block for node conn(e,b).  No atomics: each row is owned by one thread.
+// K is row-planar: component c of row i's k-th block is K[9*off[i] + c*nb + k].
+template <int NPE, int NQP, bool MR>
 __global__ void __launch_bounds__(128) k_stiffness_rows(int N, int E, const int* __restrict__ conn,
                                                         const double* __restrict__ x, const double* __restrict__ y,
                                                         const double* __restrict__ z, const int* __restrict__ elem_slot,
@@ -29,7 +30,8 @@ __global__ void __launch_bounds__(128) k_stiffness_rows(int N, int E, const int*
                                                         const int* __restrict__ inc_off, const int* __restrict__ inc_e,
                                                         const int* __restrict__ inc_a, const int* __restrict__ off,
                                                         const int* __restrict__ col, double* K, double lambda,
-                                                        double mu, double eta_d, double lambda_d, double h) {
+                                                        double mu, double eta_d, double lambda_d, double h,
+                                                        double mu10, double mu01, double kappa) {
     constexpr int TE = TILE_ELEMS;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
@@ -91,6 +93,8 @@ __global__ void __launch_bounds__(128) k_stiffness_rows(int N, int E, const int*
                 for (int c = 0; c < 3; ++c) s += F[r][c] * g[a][c];
                 Fha[r] = s;
             }
+            double Bmr[3][3][3];
+            if constexpr (MR) mooney_rivlin_tangent_a(F, mu10, mu01, kappa, g[a], Bmr);
             for (int b = 0; b < NPE; ++b) {
                 if (bpos[b] < 0) continue;
                 double Fhb[3];
@@ -104,6 +108,11 @@ __global__ void __launch_bounds__(128) k_stiffness_rows(int N, int E, const int*
                 double* Kb = Kr + bpos[b];
                 for (int d = 0; d < 3; ++d)
                     for (int ee = 0; ee < 3; ++ee) {
+                        if constexpr (MR) {
+                            const double kb = Bmr[d][ee][0] * g[b][0] + Bmr[d][ee][1] * g[b][1] + Bmr[d][ee][2] * g[b][2];
+                            Kb[(size_t)(3 * d + ee) * nbr] += h * (kb * dV);
+                            continue;
+                        }
                         const double delta = (d == ee) ? 1.0 : 0.0;
                         const double kv = (lambda * Fha[d] * Fhb[ee] + lambda * trE * hij * delta + mu * fdf * delta +
                                            mu * Fhb[d] * Fha[ee] + mu * hij * FFT[d][ee] + (-mu * hij * delta)) *
@@ -558,23 +567,18 @@ int linear_static_solve(tlfea_solver_s* s) {
         set_error("element must be set up first");
         return TLFEA_NOT_SETUP;
     }
-    if (el->material != TLFEA_MATERIAL_SVK) {
-        set_error("Mooney-Rivlin is not supported");
-        return TLFEA_UNSUPPORTED;
-    }
     int st = linear_static_prepare(s);
     if (st) return st;
     cudaStream_t stream = el->stream;
     const int N = el->N, n3 = 3 * N;
     // AssembleLinearStiffness (h = 1)
-    if (el->npe == 10)
-        k_stiffness_rows<10, 5><<<(N + 127) / 128, 128, 0, stream>>>(
-            N, el->E, el->d_conn, el->x, el->y, el->z, el->tl.elem_slot, el->tl.grad64, el->tl.dv64, el->inc_off,
-            el->inc_e, el->inc_a, el->pat_off, el->pat_col, s->K, el->lambda, el->mu, el->eta_d, el->lambda_d, 1.0);
-    else
-        k_stiffness_rows<4, 1><<<(N + 127) / 128, 128, 0, stream>>>(
-            N, el->E, el->d_conn, el->x, el->y, el->z, el->tl.elem_slot, el->tl.grad64, el->tl.dv64, el->inc_off,
-            el->inc_e, el->inc_a, el->pat_off, el->pat_col, s->K, el->lambda, el->mu, el->eta_d, el->lambda_d, 1.0);
+    const bool mr = (el->material == TLFEA_MATERIAL_MOONEY_RIVLIN);
+    auto kern = (el->npe == 10) ? (mr ? k_stiffness_rows<10, 5, true> : k_stiffness_rows<10, 5, false>)
+                                : (mr ? k_stiffness_rows<4, 1, true> : k_stiffness_rows<4, 1, false>);
+    kern<<<(N + 127) / 128, 128, 0, stream>>>(N, el->E, el->d_conn, el->x, el->y, el->z, el->tl.elem_slot,
+                                               el->tl.grad64, el->tl.dv64, el->inc_off, el->inc_e, el->inc_a,
+                                               el->pat_off, el->pat_col, s->K, el->lambda, el->mu, el->eta_d,
+                                               el->lambda_d, 1.0, el->mu10, el->mu01, el->kappa);
     TLFEA_CHECK_LAUNCH();
     TLFEA_CUDA(cudaMemcpyAsync(s->f, el->f_ext, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
     // ApplyDirichletBCs
