@@ -372,6 +372,73 @@ def batched_leg(args, T):
             "speedup_vs_plain": round(value / plain, 2)}
 
 
+def dynamics_leg(args, T):
+    """Configuration 5, one sequence: 100x10x10 TET10 cantilever (60,000 elements),
+    SVK E = 1e7, nu = 0.3, rho = 1000, clamped at x = 0; gravity 9.81 m/s^2 in -z
+    (consistent-mass row sums) plus a 50 sin(2 pi 5 t) N tip load in -z; SyncedNesterov
+    with dt = 1e-3 (test_feat10_nesterov.cc:189 parameters).  `--dyn-steps` implicit
+    steps run as one CUDA graph with the load computed on the device (RunSteps),
+    against the reference's host loop of SetExternalForce + Solve (same answer)."""
+    import torch
+    from tlfea_b200 import mesh as M
+
+    x, y, z, conn = M.box_mesh(100, 10, 10, 10, 1.0, 0.1, 0.1)
+    fixed, f_tip, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -50.0))
+    params = T.SyncedNesterovParams(1.0e-8, 1e14, 1.0e-6, 1.0e-6, 5, 300, 1.0e-3)
+    omega = 2 * np.pi * 5.0
+    n = args.dyn_steps
+
+    def make():
+        el = T.GPU_FEAT10_Data(conn.shape[0], len(x))
+        el.Initialize()
+        el.SetNodalFixed(fixed)
+        el.SetExternalForce(np.zeros(3 * len(x)))
+        el.Setup(*T.Quadrature.t10(), x, y, z, conn)
+        el.SetDensity(1000.0)
+        el.SetDamping(0.0, 0.0)
+        el.SetSVK(1e7, 0.3)
+        el.CalcDnDuPre()
+        el.CalcMassMatrix()
+        el.CalcConstraintData()
+        el.ConvertToCSR_ConstraintJacT()
+        el.AddGravity(0.0, 0.0, -9.81)
+        s = T.SyncedNesterovSolver(el, el.get_n_constraint())
+        s.Setup()
+        s.SetParameters(params)
+        return el, s
+
+    el, s = make()
+    s.RunSteps(1)  # warm-up: first launch, graph build
+    el.Destroy()
+    el, s = make()
+    f_grav = el.RetrieveExternalForceToCPU()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    its = s.RunSteps(n, f_tip, amp=1.0, omega=omega, phase=0.0, t0=0.0)
+    t_graph = time.perf_counter() - t0
+    x_graph = np.stack(el.RetrievePositionToCPU())
+    el.Destroy()
+    el, s = make()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    its_h = []
+    for k in range(n):
+        el.SetExternalForce(f_grav + np.sin(omega * ((k + 1) * 1.0e-3)) * f_tip)
+        s.Solve()
+        its_h.append(s.GetStats()["inner_iters_total"])
+    t_host = time.perf_counter() - t0
+    x_host = np.stack(el.RetrievePositionToCPU())
+    tip_z = float((x_graph[2] - z).min())
+    el.Destroy()
+    return {"workload": f"configuration 5 (one sequence): 100x10x10 TET10, gravity + 50 sin(2 pi 5 t) N tip load, "
+                        f"SyncedNesterov dt 1e-3, {n} steps", "elements": int(conn.shape[0]), "nodes": int(len(x)),
+            "value": round(n / t_graph, 3), "unit": "steps/s", "inner_iters_per_step": float(np.mean(its)),
+            "host_loop": {"value": round(n / t_host, 3), "unit": "steps/s",
+                          "inner_iters_per_step": float(np.mean(its_h))},
+            "graph_vs_host_loop_max_abs_position_diff": float(np.abs(x_graph - x_host).max()),
+            "tip_deflection_min_z": tip_z}
+
+
 def learned_leg(args, T):
     """Learned warm start on the fixed 40 x 8 x 8 TET10 cantilever (1.0 x 0.1 x
     0.1 m): 4096 solver-generated training cases (E log-uniform 1e6..1e8, nu
@@ -500,6 +567,8 @@ def main():
     ap.add_argument("--mesh", default=None, help="cells NXxNYxNZ (default 200x20x20)")
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
+    ap.add_argument("--no-dynamics", action="store_true", help="skip the time-stepping leg")
+    ap.add_argument("--dyn-steps", type=int, default=20, help="implicit steps of the time-stepping leg")
     ap.add_argument("--batch-size", type=int, default=512)
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "fp32"],
                     help="element work of the batched solves (the CG and its stop test stay FP64)")
@@ -649,6 +718,8 @@ def main():
         out["batched"] = batched_leg(args, T)
     if not args.no_learned:
         out["learned"] = learned_leg(args, T)
+    if not args.no_dynamics:
+        out["dynamics"] = dynamics_leg(args, T)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_sample(x, y, z, conn, fixed, f, cfg, iters)
     if rank == 0:
