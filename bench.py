@@ -375,16 +375,17 @@ def batched_leg(args, T):
 def dynamics_leg(args, T):
     """Configuration 5, one sequence: 100x10x10 TET10 cantilever (60,000 elements),
     SVK E = 1e7, nu = 0.3, rho = 1000, clamped at x = 0; gravity 9.81 m/s^2 in -z
-    (consistent-mass row sums) plus a 50 sin(2 pi 5 t) N tip load in -z; SyncedNesterov
-    with dt = 1e-3 (test_feat10_nesterov.cc:189 parameters).  `--dyn-steps` implicit
-    steps run as one CUDA graph with the load computed on the device (RunSteps),
-    against the reference's host loop of SetExternalForce + Solve (same answer)."""
+    (consistent-mass row sums) plus a 50 sin(2 pi 5 t) N tip load in -z; SyncedAdamW
+    with dt = 1e-3 and the damping and parameters of the reference's dynamics example
+    (beam_simulation.cc:203, 226).  `--dyn-steps` implicit steps run as one CUDA graph
+    with the load computed on the device (RunSteps), against the reference's host
+    loop of SetExternalForce + Solve (beam_simulation.cc:275-283; same answer)."""
     import torch
     from tlfea_b200 import mesh as M
 
     x, y, z, conn = M.box_mesh(100, 10, 10, 10, 1.0, 0.1, 0.1)
     fixed, f_tip, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -50.0))
-    params = T.SyncedNesterovParams(1.0e-8, 1e14, 1.0e-6, 1.0e-6, 5, 300, 1.0e-3)
+    params = T.SyncedAdamWParams(2e-4, 0.9, 0.999, 1e-8, 1e-4, 0.995, 1e-1, 1e-6, 1e14, 5, 300, 1e-3, 10, 0.0)
     omega = 2 * np.pi * 5.0
     n = args.dyn_steps
 
@@ -395,14 +396,14 @@ def dynamics_leg(args, T):
         el.SetExternalForce(np.zeros(3 * len(x)))
         el.Setup(*T.Quadrature.t10(), x, y, z, conn)
         el.SetDensity(1000.0)
-        el.SetDamping(0.0, 0.0)
+        el.SetDamping(0.0, 0.1)
         el.SetSVK(1e7, 0.3)
         el.CalcDnDuPre()
         el.CalcMassMatrix()
         el.CalcConstraintData()
         el.ConvertToCSR_ConstraintJacT()
         el.AddGravity(0.0, 0.0, -9.81)
-        s = T.SyncedNesterovSolver(el, el.get_n_constraint())
+        s = T.SyncedAdamWSolver(el, el.get_n_constraint())
         s.Setup()
         s.SetParameters(params)
         return el, s
@@ -431,7 +432,7 @@ def dynamics_leg(args, T):
     tip_z = float((x_graph[2] - z).min())
     el.Destroy()
     return {"workload": f"configuration 5 (one sequence): 100x10x10 TET10, gravity + 50 sin(2 pi 5 t) N tip load, "
-                        f"SyncedNesterov dt 1e-3, {n} steps", "elements": int(conn.shape[0]), "nodes": int(len(x)),
+                        f"SyncedAdamW dt 1e-3, {n} steps", "elements": int(conn.shape[0]), "nodes": int(len(x)),
             "value": round(n / t_graph, 3), "unit": "steps/s", "inner_iters_per_step": float(np.mean(its)),
             "host_loop": {"value": round(n / t_host, 3), "unit": "steps/s",
                           "inner_iters_per_step": float(np.mean(its_h))},
@@ -568,7 +569,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
     ap.add_argument("--no-dynamics", action="store_true", help="skip the time-stepping leg")
-    ap.add_argument("--dyn-steps", type=int, default=20, help="implicit steps of the time-stepping leg")
+    ap.add_argument("--dyn-steps", type=int, default=50, help="implicit steps of the time-stepping leg")
     ap.add_argument("--batch-size", type=int, default=512)
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "fp32"],
                     help="element work of the batched solves (the CG and its stop test stay FP64)")

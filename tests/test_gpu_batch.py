@@ -248,3 +248,33 @@ def test_shared_mesh_batch_matches_the_general_batch(order):
         assert rel(us[3 * k * len(d0["x"]):3 * (k + 1) * len(d0["x"])], u_dir) < 1e-6
     bs.Destroy()
     bg.Destroy()
+
+
+def test_shared_mesh_single_instance_and_fp32_refinement():
+    """A shared-mesh batch of one instance, and a shared-mesh batch in FP32
+    element work with FP64 refinement, against the general batch."""
+    d0 = M.random_beam(11, order=10, **SMALL)
+    mesh = (d0["x"], d0["y"], d0["z"], d0["conn"])
+    for n in (1, 9):
+        r = np.random.default_rng(n)
+        E = np.exp(r.uniform(np.log(1e6), np.log(1e9), n))
+        nu = r.uniform(0.2, 0.45, n)
+        loads = [d0["f"] * s for s in r.uniform(0.5, 2.0, n)]
+        bs = T.BatchedLinearStaticSolver([mesh] * n, T.TYPE_T10, shared=True)
+        bg = T.BatchedLinearStaticSolver([mesh] * n, T.TYPE_T10)
+        for b in (bs, bg):
+            b.SetMaterial(E, nu)
+            b.SetNodalFixed([d0["fixed"]] * n)
+            b.SetExternalForce(loads)
+        bg.Solve(1e-10, 20000)
+        ug = bg.RetrieveDisplacement(split=False)
+        bs.Solve(1e-10, 20000)
+        assert np.all(bs.GetResults()[2] == 0)
+        assert rel(bs.RetrieveDisplacement(split=False), ug) < 1e-7
+        bs.SetPrecision("fp32")
+        bs.Solve(1e-8, 20000)
+        it, res, st = bs.GetResults()
+        assert np.all(st == 0) and np.all(res < 1e-8)
+        assert rel(bs.RetrieveDisplacement(split=False), ug) < 1e-6
+        bs.Destroy()
+        bg.Destroy()

@@ -117,6 +117,44 @@ def test_run_steps_tracks_the_oracle_trajectory():
     el.Destroy()
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_run_steps_tet4_with_damping_and_stop_rule(prec):
+    """TET4, Kelvin-Voigt damping, FP32 or FP64 forces and the relative-residual
+    stop rule: the graph of steps equals the host loop bitwise."""
+    x, y, z, conn = box(10, 2, 2, 4)
+    fixed, f, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -100.0))
+    fvar = np.zeros_like(f)
+    fvar.reshape(-1, 3)[np.nonzero(np.abs(x - x.max()) < 1e-9)[0], 1] = 10.0
+
+    def make():
+        el = make_element(x, y, z, conn, fixed=fixed, f_ext=f, eta=50.0, lamd=10.0)
+        if prec != "fp64":
+            el.SetForcePrecision(prec)
+        s = T.SyncedNesterovSolver(el, el.get_n_constraint())
+        s.Setup()
+        s.SetParameters(T.SyncedNesterovParams(*NESTEROV))
+        s.SetRelativeResidualStop(1e-3)
+        return el, s
+
+    n, amp, omega = 4, 2.0, 100.0
+    el_a, s_a = make()
+    its_a, rel_a = [], []
+    for k in range(n):
+        el_a.SetExternalForce(f + _scale(k, 0.0, NESTEROV[6], amp, omega, 0.0) * fvar)
+        s_a.Solve()
+        st = s_a.GetStats()
+        its_a.append(st["inner_iters_total"])
+        rel_a.append(st["rel_residual"])
+    el_b, s_b = make()
+    its_b = s_b.RunSteps(n, fvar, amp=amp, omega=omega)
+    assert list(its_b) == its_a
+    assert s_b.GetStats()["rel_residual"] == rel_a[-1]
+    for a, b in zip(el_a.RetrievePositionToCPU(), el_b.RetrievePositionToCPU()):
+        assert np.array_equal(a, b)
+    el_a.Destroy()
+    el_b.Destroy()
+
+
 def test_run_steps_refuses_bad_input():
     el, s, _, _ = _solver("nesterov")
     with pytest.raises(Exception):
