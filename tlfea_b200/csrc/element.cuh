@@ -89,6 +89,8 @@ struct TileArgs {
     R* partial;       // 3 * n_pslots
     R lambda, mu, eta, lamd;
     double mu10, mu01, kappa;  // Mooney-Rivlin (MR instantiations)
+    const double* vp;          // MASS instantiations: previous-step velocity (interleaved 3N)
+    double mass_scale;         // MASS instantiations: rho / dt
     int max_local;
     QpBary qb;
 };
@@ -445,6 +447,46 @@ __device__ __forceinline__ void tile_stress(const R H[3][3], const R Fd[3][3], c
 
 // One QP of the compact-geometry force: F (or H) = (dx/dxi) J^-1 from the
 // nodal values xa, the stress, and f_a (+)= (dV P J^-T) dN_a/dxi.
+// Shape-function values at barycentric L (reference node order): corners
+// L_i (2 L_i - 1), edges 4 L_i L_j; TET4 N_a = L_a.
+template <typename R, int NPE>
+__device__ __forceinline__ void tet_shape(const R L[4], R N[NPE]) {
+    if constexpr (NPE == 10) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) N[i] = L[i] * (R(2) * L[i] - R(1));
+        N[4] = R(4) * L[0] * L[1];
+        N[5] = R(4) * L[1] * L[2];
+        N[6] = R(4) * L[0] * L[2];
+        N[7] = R(4) * L[0] * L[3];
+        N[8] = R(4) * L[1] * L[3];
+        N[9] = R(4) * L[2] * L[3];
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) N[i] = L[i];
+    }
+}
+
+// The element's share of M (v - v_prev) / dt at one QP, added to the nodal
+// forces: f_a += N_a dV w(q), w(q) = sum_b N_b w_b with w_b = rho (v_b - vp_b) / dt
+// (the consistent mass M_ab = sum_q rho N_a N_b dV_q, FEAT10Data.cu:200-271,
+// applied element by element instead of as an assembled row pass).
+template <typename R, int NPE>
+__device__ __forceinline__ void mass_qp(const R (&wa)[NPE][3], const R Lq[4], R dv, R (&f)[NPE][3]) {
+    R N[NPE];
+    tet_shape<R, NPE>(Lq, N);
+    R w[3] = {R(0), R(0), R(0)};
+#pragma unroll
+    for (int b = 0; b < NPE; ++b)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) w[d] += N[b] * wa[b][d];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+        const R s = N[a] * dv;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) f[a][d] += s * w[d];
+    }
+}
+
 template <typename R, int NPE, bool DAMP, bool FIRST, bool MR = false>
 __device__ __forceinline__ void compact_qp(const TileArgs<R>& A, const R (&xa)[NPE][3], const R (&va)[NPE][3],
                                            const R ji[9], R dv, const R Lq[4], R (&f)[NPE][3]) {
@@ -468,7 +510,9 @@ __device__ __forceinline__ void compact_qp(const TileArgs<R>& A, const R (&xa)[N
         tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] += v; });
 }
 
-template <typename R, int NPE, int NQP, int MODE, bool DAMP, bool MR = false>
+// MASS (force mode only): the element-wise mass term M (v - v_prev) / dt of the
+// first-order solvers' gradient is added to the nodal forces (see mass_qp).
+template <typename R, int NPE, int NQP, int MODE, bool DAMP, bool MR = false, bool MASS = false>
 __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, unsigned char* smem_raw) {
     constexpr int TE = TILE_ELEMS;
     const int t = threadIdx.x;
@@ -476,7 +520,8 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
     R* ys = xs + A.max_local;
     R* zs = ys + A.max_local;
     R* vs = zs + A.max_local;
-    R* fe = DAMP ? vs + 3 * A.max_local : vs;
+    R* ws = DAMP ? vs + 3 * A.max_local : vs;
+    R* fe = MASS ? ws + 3 * A.max_local : ws;
 
     const int lb = A.node_off[tile];
     const int nl = A.node_off[tile + 1] - lb;
@@ -490,6 +535,10 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
                 vs[3 * ln + 0] = R(A.v[3 * gid + 0]);
                 vs[3 * ln + 1] = R(A.v[3 * gid + 1]);
                 vs[3 * ln + 2] = R(A.v[3 * gid + 2]);
+            }
+            if (MASS) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) ws[3 * ln + d] = R((A.v[3 * gid + d] - A.vp[3 * gid + d]) * A.mass_scale);
             }
         }
     }
@@ -524,6 +573,14 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
             }
         }
         compact_qp<R, NPE, DAMP, false, MR>(A, xa, va, ji, dv, Lq, f);
+        if constexpr (MASS) {
+            R wa[NPE][3];
+#pragma unroll
+            for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) wa[a][d] = ws[3 * lc[a] + d];
+            mass_qp<R, NPE>(wa, Lq, dv, f);
+        }
     }
 #pragma unroll 1
     for (int q = 0; q < NQP && MODE != TILE_FORCE; ++q) {
@@ -632,8 +689,8 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
 
 // Shared memory bytes of one tile block.
 template <typename R>
-inline size_t tile_smem_bytes(int npe, int max_local, bool damp) {
-    return sizeof(R) * ((size_t)max_local * (damp ? 6 : 3) + (size_t)3 * npe * TILE_ELEMS);
+inline size_t tile_smem_bytes(int npe, int max_local, bool damp, bool mass = false) {
+    return sizeof(R) * ((size_t)max_local * (3 + (damp ? 3 : 0) + (mass ? 3 : 0)) + (size_t)3 * npe * TILE_ELEMS);
 }
 
 }  // namespace tlfea

@@ -121,11 +121,14 @@ __device__ __forceinline__ void node_force(const FOArgs& S, const TileArgs<R>& A
     }
 }
 
-// solver_grad_L (SyncedNesterov.cu:32-95) for the 3 DOFs of node i.
+// solver_grad_L (SyncedNesterov.cu:32-95) for the 3 DOFs of node i.  With
+// MASS the force f already holds M (v - v_prev) / dt (added element by element in
+// the force phase) and the mass-row pass is skipped.
+template <bool MASS>
 __device__ __forceinline__ void grad_node(const FOArgs& S, int i, const double f[3], double gi[3]) {
     const double inv_dt = 1.0 / S.dt;
     double r[3] = {0.0, 0.0, 0.0};
-    for (int k = S.m_off[i]; k < S.m_off[i + 1]; ++k) {
+    for (int k = MASS ? 0 : S.m_off[i]; k < (MASS ? 0 : S.m_off[i + 1]); ++k) {
         const int j = S.m_col[k];
         const double mij = S.m_val[k];
 #pragma unroll
@@ -149,10 +152,10 @@ __device__ __forceinline__ void grad_node(const FOArgs& S, int i, const double f
     }
 }
 
-template <typename R, int NPE, int NQP, bool DAMP, bool MR>
+template <typename R, int NPE, int NQP, bool DAMP, bool MR, bool MASS>
 __device__ __forceinline__ void force_phase(const FOArgs& S, const TileArgs<R>& A, unsigned char* smem) {
     for (int tile = blockIdx.x; tile < S.n_tiles; tile += gridDim.x)
-        process_tile<R, NPE, NQP, TILE_FORCE, DAMP, MR>(A, tile, smem);
+        process_tile<R, NPE, NQP, TILE_FORCE, DAMP, MR, MASS>(A, tile, smem);
     const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
     for (int k = gt; k < S.n_fixed; k += gs) {
         const int n = S.fixed[k];
@@ -162,7 +165,7 @@ __device__ __forceinline__ void force_phase(const FOArgs& S, const TileArgs<R>& 
     }
 }
 
-template <typename R, int NPE, int NQP, bool DAMP, bool MR>
+template <typename R, int NPE, int NQP, bool DAMP, bool MR, bool MASS>
 __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R> A) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double red_sh[32];
@@ -263,7 +266,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
             }
             grid.sync();
             // ---- P2: internal force (fused tiles) and constraint values
-            force_phase<R, NPE, NQP, DAMP, MR>(S, A, smem);
+            force_phase<R, NPE, NQP, DAMP, MR, MASS>(S, A, smem);
             grid.sync();
             // ---- P3: gradient per node and the norm partials
             const bool do_check = nesterov || (inner % check == 0);
@@ -271,7 +274,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
             for (int i = gt; i < N; i += gs) {
                 double f[3], gi[3];
                 node_force<R>(S, A, i, f);
-                grad_node(S, i, f, gi);
+                grad_node<MASS>(S, i, f, gi);
                 const bool free_node = rule && !S.node_fixed[i];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
@@ -389,11 +392,11 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
     }
 }
 
-template <typename R, int NPE, int NQP, bool DAMP, bool MR>
+template <typename R, int NPE, int NQP, bool DAMP, bool MR, bool MASS>
 static int launch_first_order(tlfea_solver_s* s, FOArgs& S, TileArgs<R>& A) {
     tlfea_element_s* el = s->el;
-    auto kern = k_first_order<R, NPE, NQP, DAMP, MR>;
-    const size_t smem = tile_smem_bytes<R>(NPE, el->tl.max_local, DAMP);
+    auto kern = k_first_order<R, NPE, NQP, DAMP, MR, MASS>;
+    const size_t smem = tile_smem_bytes<R>(NPE, el->tl.max_local, DAMP, MASS);
     if (smem > 48 * 1024) TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0, sms = 0;
     TLFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TILE_ELEMS, smem));
@@ -544,33 +547,22 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     A64.f_out = el->f_int; A64.partial = el->tl.partial64;
     A64.lambda = el->lambda; A64.mu = el->mu; A64.eta = el->eta_d; A64.lamd = el->lambda_d;
     const bool mr = (el->material == TLFEA_MATERIAL_MOONEY_RIVLIN);
+    // the element-wise mass term replaces the assembled row pass unless the stop
+    // rule needs f_int alone (and for Mooney-Rivlin, which keeps the row pass)
+    const bool mass = (s->rel_tol <= 0.0) && !mr;
+    A32.vp = A64.vp = s->v_prev;
+    A32.mass_scale = A64.mass_scale = el->rho / S.dt;
     auto launch_one = [&](FOArgs& SS) -> int {
-        if (fp32) {
-            if (el->npe == 10) {
-                if (mr)
-                    return damp ? launch_first_order<float, 10, 5, true, true>(s, SS, A32)
-                                : launch_first_order<float, 10, 5, false, true>(s, SS, A32);
-                return damp ? launch_first_order<float, 10, 5, true, false>(s, SS, A32)
-                            : launch_first_order<float, 10, 5, false, false>(s, SS, A32);
-            }
-            if (mr)
-                return damp ? launch_first_order<float, 4, 1, true, true>(s, SS, A32)
-                            : launch_first_order<float, 4, 1, false, true>(s, SS, A32);
-            return damp ? launch_first_order<float, 4, 1, true, false>(s, SS, A32)
-                        : launch_first_order<float, 4, 1, false, false>(s, SS, A32);
-        }
-        if (el->npe == 10) {
-            if (mr)
-                return damp ? launch_first_order<double, 10, 5, true, true>(s, SS, A64)
-                            : launch_first_order<double, 10, 5, false, true>(s, SS, A64);
-            return damp ? launch_first_order<double, 10, 5, true, false>(s, SS, A64)
-                        : launch_first_order<double, 10, 5, false, false>(s, SS, A64);
-        }
-        if (mr)
-            return damp ? launch_first_order<double, 4, 1, true, true>(s, SS, A64)
-                        : launch_first_order<double, 4, 1, false, true>(s, SS, A64);
-        return damp ? launch_first_order<double, 4, 1, true, false>(s, SS, A64)
-                    : launch_first_order<double, 4, 1, false, false>(s, SS, A64);
+#define TLFEA_FO_LAUNCH(R_, NPE_, NQP_, AA)                                                                     \
+    (mr ? (damp ? launch_first_order<R_, NPE_, NQP_, true, true, false>(s, SS, AA)                             \
+                : launch_first_order<R_, NPE_, NQP_, false, true, false>(s, SS, AA))                           \
+        : mass ? (damp ? launch_first_order<R_, NPE_, NQP_, true, false, true>(s, SS, AA)                      \
+                       : launch_first_order<R_, NPE_, NQP_, false, false, true>(s, SS, AA))                    \
+               : (damp ? launch_first_order<R_, NPE_, NQP_, true, false, false>(s, SS, AA)                     \
+                       : launch_first_order<R_, NPE_, NQP_, false, false, false>(s, SS, AA)))
+        if (fp32) return (el->npe == 10) ? TLFEA_FO_LAUNCH(float, 10, 5, A32) : TLFEA_FO_LAUNCH(float, 4, 1, A32);
+        return (el->npe == 10) ? TLFEA_FO_LAUNCH(double, 10, 5, A64) : TLFEA_FO_LAUNCH(double, 4, 1, A64);
+#undef TLFEA_FO_LAUNCH
     };
     cudaStream_t stream = el->stream;
     const int n_steps = std::max(1, steps);
