@@ -688,6 +688,18 @@ def main():
         ef[prec] = {"kernel": "k_tile_force+k_combine", "bound": "hbm", "achieved": round(a, 1), "peak": hbm,
                     "unit": "GB/s", "frac": round(a / hbm, 4), "algorithmic_bytes": int(b), "ms": round(ms_f, 4),
                     "traffic": int(FORCE_FP32_TRAFFIC_BYTES) if prec == "fp32" else None}
+    # the same contract with the persistent producer/consumer pipeline kernel
+    el.SetLaunchConfig("pipeline")
+    for prec, s in (("fp32", 4), ("fp64", 8)):
+        el.SetForcePrecision(prec)
+        for _ in range(3):
+            el.ComputeInternalForce()
+        ms_f = time_stream(torch, stream, el.ComputeInternalForce, args.kernel_reps)
+        b = elem_force_bytes(E, N, 10, 5, s)
+        a = b / (ms_f / 1e3) / 1e9
+        ef["pipeline_" + prec] = {"kernel": "k_force_pipe+k_combine", "bound": "hbm", "achieved": round(a, 1),
+                                  "peak": hbm, "unit": "GB/s", "frac": round(a / hbm, 4), "algorithmic_bytes": int(b),
+                                  "ms": round(ms_f, 4)}
     # the same forces from the compact geometry stream (J^-1 and dV per QP)
     el.SetLaunchConfig("compact")
     for prec, s in (("fp32", 4), ("fp64", 8)):
