@@ -11,21 +11,22 @@
 // u += alpha p; r -= alpha Kp; beta = rr_new / rr; p = r + beta p.  K is the
 // linear (small-strain) stiffness at the reference configuration -- the
 // tangent of compute_hessian_assemble_csr (FEAT10DataFunc.cuh:512-684) at F = I,
-// applied matrix-free from the per-QP shape-function gradients, with Dirichlet
-// DOFs eliminated as apply_bcs_kernel does (LinearStaticSolver.cu:284-306).
-// Stop rule: ||r|| / ||f_free|| < tol in FP64, which equals the reference's
-// sqrt(rr / rr0) for a cold start and does not reward a warm start for a
-// smaller initial residual.
+// applied matrix-free from the compact geometry stream (J^-1 and dV per QP),
+// with Dirichlet DOFs eliminated as apply_bcs_kernel does
+// (LinearStaticSolver.cu:284-306).  Stop rule: ||r|| / ||f_free|| < tol in FP64,
+// which equals the reference's sqrt(rr / rr0) for a cold start and does not
+// reward a warm start for a smaller initial residual.
 //
 // One launch runs every iteration of every instance: a grid-stride loop over
-// element tiles (K p), then over node chunks (segmented FP64 dots, vector
-// updates); four grid barriers per iteration; per-instance scalars are folded
-// redundantly and deterministically by every block that needs them.
+// element tiles (K p), then over node chunks, one warp per chunk (segmented FP64
+// dots, vector updates); four grid barriers per iteration; the per-instance
+// scalars of a phase are folded once, in chunk order, by the warp that posts
+// the instance's last chunk partial.
 //
 // Shared-mesh mode: when every instance is the same mesh (only material and
-// loads differ) the batch keeps ONE tiling and one gradient stream, and the
-// tile loop runs over (instance, tile) pairs.  Consecutive work items then
-// reuse the same tiles, so the gradient stream is read from L2 and HBM carries
+// loads differ) the batch keeps ONE tiling and one geometry stream, and the
+// tile loop runs over (tile, group of instances) items: the tile's tables are
+// staged once per group, the geometry stream stays in L2, and HBM carries
 // little more than the per-instance vectors.
 #include <cooperative_groups.h>
 
