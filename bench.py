@@ -229,6 +229,12 @@ def kernels_only(args):
     import tlfea_b200 as T
 
     torch.cuda.set_device(0)
+    if args.kernels_only == "steps":
+        # the persistent first-order solver: 2 AdamW steps of the configuration-5 sequence
+        class _A:
+            dyn_steps = 2
+        print(json.dumps({"kernels_only": "steps", "dynamics": dynamics_leg(_A, T)["value"]}))
+        return
     if args.kernels_only == "batch":
         # the batched CG: 64 load / material cases on the 40x8x8 TET10 beam, 10 iterations
         from tlfea_b200 import warmstart as W
@@ -563,7 +569,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--kernel-reps", type=int, default=20)
     ap.add_argument("--cg-iters", type=int, default=120, help="iteration cap of --kernels-only cg")
-    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg", "batch"], default=None,
+    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg", "batch", "steps"], default=None,
                     help="profiling case: set up, then launch only the named kernel a few times")
     ap.add_argument("--mesh", default=None, help="cells NXxNYxNZ (default 200x20x20)")
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")
