@@ -8,6 +8,9 @@
 //     AdamW refuses such sizes);
 //   * the internal force is the fused tile routine (no F/P round trip through
 //     HBM, no atomics) and the gradient reads it back per node;
+//   * the inertial term M (v - v_prev) / dt is added element by element in the
+//     same tiles (the consistent mass from the shape functions at the QPs) when
+//     the stop rule is off, instead of an assembled mass-row pass per node;
 //   * norms are two-level reductions (block shuffles, then every block folds
 //     the per-block partials in block order, so every block takes the same
 //     branch without another barrier) instead of one thread's serial loop;
