@@ -162,6 +162,36 @@ def test_mass_total_and_symmetry(order):
 
 
 @pytest.mark.parametrize("order", [10, 4])
+def test_elementwise_mass_product_equals_assembled(order):
+    """The first-order solvers apply M (v - v_prev) element by element: per QP,
+    w(q) = sum_b N_b(q) w_b and f_a += rho N_a(q) dV w(q), with the corner
+    L_i (2 L_i - 1) and edge 4 L_i L_j shape functions at the barycentric QPs.
+    That product equals the oracle's assembled consistent mass times w."""
+    x, y, z, conn = O.box_mesh(4, 2, 2, order, 0.4, 0.2, 0.2)
+    N, E = len(x), conn.shape[0]
+    g, dj = O.dndu_pre(x, y, z, conn)
+    rho = 1000.0
+    off, cols, vals = O.mass(conn, dj, N, rho)
+    w = np.random.default_rng(7).standard_normal((N, 3))
+    ref = sp.csr_matrix((vals, cols, off)) @ w
+    qx, qy, qz, qw = O.quadrature(conn.shape[1])
+    nqp = len(qw)
+    L = np.stack([1.0 - qx - qy - qz, qx, qy, qz], 1)  # (nqp, 4)
+    if order == 10:
+        edges = [(0, 1), (1, 2), (0, 2), (0, 3), (1, 3), (2, 3)]
+        Nq = np.concatenate([L * (2.0 * L - 1.0), np.stack([4.0 * L[:, i] * L[:, j] for i, j in edges], 1)], 1)
+    else:
+        Nq = L
+    dV = dj.reshape(E, nqp) * qw[None, :]
+    we = w[conn]                                        # (E, NPE, 3)
+    wq = np.einsum("qb,ebd->eqd", Nq, we)               # w at the QPs
+    fe = rho * np.einsum("qa,eq,eqd->ead", Nq, dV, wq)  # element contributions
+    out = np.zeros((N, 3))
+    np.add.at(out, conn.ravel(), fe.reshape(-1, 3))
+    assert rel(out, ref) < 1e-13
+
+
+@pytest.mark.parametrize("order", [10, 4])
 def test_stiffness_is_consistent_tangent(order):
     x, y, z, conn = O.box_mesh(4, 2, 2, order, 0.4, 0.2, 0.2)
     g, dj = O.dndu_pre(x, y, z, conn)
