@@ -124,6 +124,23 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(dist, seconds, device):
+    """The slowest rank's time; every rank calls this in the same order (replicas
+    only: this is the one collective of the benchmark)."""
+    if not dist:
+        return seconds
+    import torch
+
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank, seconds):
+    """Units of all ranks divided by the slowest rank's time."""
+    return world * units_per_rank / seconds
+
+
 def elem_force_bytes(E, N, npe, nqp, s):
     return E * (4 * npe + nqp * npe * 3 * s + nqp * s) + N * 6 * s
 
@@ -626,12 +643,8 @@ def main():
     with ClockSampler(local) as clk:
         ms = time_stream(torch, stream, step, args.steps)
     launches = T.launch_count() - l0
-    t_total = ms * args.steps / 1e3
-    if dist:
-        tt = torch.tensor([t_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_total = float(tt.item())
-    value = world * args.steps / t_total
+    t_total = max_over_ranks(dist, ms * args.steps / 1e3, "cuda")
+    value = whole_job_rate(world, args.steps, t_total)
 
     # opt-in block-Jacobi preconditioned CG on the same workload (not the headline:
     # the reference's method is the unpreconditioned CG above)
@@ -656,12 +669,8 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
-    t_e2e = time.perf_counter() - t0
-    if dist:
-        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
-    e2e = {"value": world * args.steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": 6 * N * 8,
+    t_e2e = max_over_ranks(dist, time.perf_counter() - t0, "cuda")
+    e2e = {"value": whole_job_rate(world, args.steps, t_e2e), "unit": "solves/s", "h2d_bytes_per_step": 6 * N * 8,
            "d2h_bytes_per_step": 3 * N * 8}
 
     hbm, peak_kind = peaks()
