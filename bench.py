@@ -360,13 +360,17 @@ def batched_leg(args, T):
         u_host.numpy()[:] = b.RetrieveDisplacement(split=False)
     t_e2e = (time.perf_counter() - t0) / reps
     launch = b.GetLaunch()
-    # the same batch with FP64 element work, for comparison
+    u_main = b.RetrieveDisplacement(split=False)
+    # the same batch with the other element precision, for comparison
     other = "fp64" if args.batch_precision == "fp32" else "fp32"
     b.SetPrecision(other)
     step()
     ms_other = time_stream(torch, st, step, 1)
     it_o, res_o, st_o = b.GetResults()
+    u_other = b.RetrieveDisplacement(split=False)
     b.Destroy()
+    u64, u32 = (u_main, u_other) if other == "fp32" else (u_other, u_main)
+    disp_err = float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64))
     # plain path: one instance at a time, cold start (a seeded sample of the batch)
     k = min(args.plain_sample, n)
     tot, its = 0.0, []
@@ -388,7 +392,8 @@ def batched_leg(args, T):
             "launch": launch, "autotune": tune,
             "other_precision": {"precision": other, "value": round(n / (ms_other / 1e3), 2),
                                 "ms_per_batch": round(ms_other, 3), "iters_mean": float(np.mean(it_o)),
-                                "converged": int(np.sum(st_o == 0)), "max_rel_residual": float(np.max(res_o))},
+                                "converged": int(np.sum(st_o == 0)), "max_rel_residual": float(np.max(res_o)),
+                                "fp32_displacement_rel_error_vs_fp64": disp_err},
             "plain_sequential": {"value": round(plain, 2), "unit": "solves/s", "sample": k,
                                  "iters_mean": float(np.mean(its)),
                                  "path": "LinearStaticSolver per instance (assembled K, CG graph), cold start"},
@@ -693,16 +698,21 @@ def main():
                 "full_csr_equivalent_gbs": round(spmv_bytes_full_csr(N, nnzb) / (ms_spmv / 1e3) / 1e9, 1)}
     # fused element force, FP32 and FP64
     ef = {}
+    f_by_prec = {}
     for prec, s in (("fp32", 4), ("fp64", 8)):
         el.SetForcePrecision(prec)
         for _ in range(3):
             el.ComputeInternalForce()
         ms_f = time_stream(torch, stream, el.ComputeInternalForce, args.kernel_reps)
+        f_by_prec[prec] = el.RetrieveInternalForceToCPU()
         b = elem_force_bytes(E, N, 10, 5, s)
         a = b / (ms_f / 1e3) / 1e9
         ef[prec] = {"kernel": "k_tile_force+k_combine", "bound": "hbm", "achieved": round(a, 1), "peak": hbm,
                     "unit": "GB/s", "frac": round(a / hbm, 4), "algorithmic_bytes": int(b), "ms": round(ms_f, 4),
                     "traffic": int(FORCE_FP32_TRAFFIC_BYTES) if prec == "fp32" else None}
+    # FP32 force error against the FP64 force at the same (deformed) positions
+    ef["fp32"]["rel_error_vs_fp64"] = float(np.linalg.norm(f_by_prec["fp32"] - f_by_prec["fp64"]) /
+                                            np.linalg.norm(f_by_prec["fp64"]))
     # the same contract with the persistent producer/consumer pipeline kernel
     el.SetLaunchConfig("pipeline")
     for prec, s in (("fp32", 4), ("fp64", 8)):
