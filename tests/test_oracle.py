@@ -73,6 +73,33 @@ def test_rigid_motion_gives_zero_stress(order):
 
 
 @pytest.mark.parametrize("order", [10, 4])
+def test_kelvin_voigt_damping_known_answers(order):
+    """Known answers for the oracle's Kelvin-Voigt term (FEAT10DataFunc.cuh:130-231):
+    a rigid spin v = w x (x - c) of a deformed body has zero rate of strain, so
+    the damped force equals the undamped one; under a homogeneous deformation
+    x = A X moving with v = B X, the viscous stress at every QP is
+    P_vis = A (2 eta Ed + lambda_d tr(Ed) I), Ed = (B^T A + A^T B) / 2."""
+    eta, lamd = 3.0e3, 7.0e2
+    x, y, z, conn = O.box_mesh(4, 2, 2, order, 0.4, 0.2, 0.2)
+    g, dj = O.dndu_pre(x, y, z, conn)
+    xs = np.stack([x, y, z]) + 2e-3 * np.random.default_rng(3).standard_normal((3, len(x)))
+    w = np.array([0.3, -1.1, 0.7])
+    v = np.cross(w, (xs - xs.mean(1, keepdims=True)).T).ravel()
+    f0 = O.force(*xs, conn, g, dj, LAM, MU)
+    fd = O.force(*xs, conn, g, dj, LAM, MU, eta, lamd, v)
+    assert rel(fd, f0) < 1e-10
+    A = np.array([[1.02, 0.01, 0.0], [0.0, 0.99, 0.02], [0.01, 0.0, 1.01]])
+    B = np.array([[0.3, -0.1, 0.2], [0.05, -0.2, 0.1], [0.0, 0.15, 0.25]])
+    X = np.stack([x, y, z])
+    F, P = O.calc_p(*(A @ X), conn, g, LAM, MU)
+    _, Pd = O.calc_p(*(A @ X), conn, g, LAM, MU, eta, lamd, (B @ X).T.ravel())
+    Ed = 0.5 * (B.T @ A + A.T @ B)
+    Pv = A @ (2 * eta * Ed + lamd * np.trace(Ed) * np.eye(3))
+    dP = (Pd - P).reshape(-1, 3, 3).transpose(0, 2, 1)
+    assert rel(dP, np.broadcast_to(Pv, dP.shape)) < 1e-10
+
+
+@pytest.mark.parametrize("order", [10, 4])
 def test_homogeneous_deformation_patch(order):
     x, y, z, conn = O.box_mesh(6, 3, 3, order, 0.6, 0.3, 0.3)
     g, dj = O.dndu_pre(x, y, z, conn)
