@@ -195,7 +195,11 @@ int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_
  * nodes shared between element tiles) lives in one static device array of
  * 2^20 doubles (8 MiB) that every GPU loading the library holds until exit.
  * Meshes needing more (3 per shared-node slot, about 7.3 per TET10 element:
- * roughly above 140k TET10 elements) are rejected with TLFEA_SIZE_MISMATCH.  Nothing is allocated: no
+ * roughly above 140k TET10 elements) are rejected with TLFEA_SIZE_MISMATCH.
+ * It computes in FP64 only: an element in FP32 force mode is refused with
+ * TLFEA_UNSUPPORTED.  The looked-up address is kept for the process; after a
+ * cudaDeviceReset of that device it is stale, so do not call this entry point
+ * again on a device that has been reset.  Nothing is allocated: no
  * cudaMalloc, cudaFree or allocating library call.  The first call on a
  * device looks up the array's device address; make that call before any
  * stream capture.  All calls share the array and it keeps the last call's
@@ -214,6 +218,14 @@ int tlfea_element_retrieve_dndu_pre(tlfea_element h, double* g, long long n); /*
 int tlfea_element_retrieve_detj(tlfea_element h, double* detJ, long long n);  /* E*QP */
 int tlfea_element_retrieve_connectivity(tlfea_element h, int* conn_colmajor, long long n);
 int tlfea_element_retrieve_constraint(tlfea_element h, double* c, int n);
+/* The constraint Jacobian CSR built by ConvertToCSR_ConstraintJac (which = 0: J,
+ * n_constraint rows) or ConvertToCSR_ConstraintJacT (which = 1: J^T, 3N rows);
+ * n_constraint unit entries each.  The reference keeps these arrays private and
+ * reads them through device accessors (FEAT10Data.cuh:262-286); this is the
+ * host-side view a caller needs to check them.  offsets has rows + 1 entries,
+ * columns and values n_constraint; TLFEA_NOT_SETUP if that CSR was not built. */
+int tlfea_element_retrieve_constraint_jac_csr(tlfea_element h, int which, int* offsets, int* columns,
+                                              double* values);
 /* WriteOutputVTK (FEAT10Data.cu:759-794): legacy ASCII VTK of the current mesh. */
 int tlfea_element_write_vtk(tlfea_element h, const char* filename);
 /* Get{X,Y,Z}12DevicePtr, GetExternalForceDevicePtr (FEAT10Data.cuh:599-621). */

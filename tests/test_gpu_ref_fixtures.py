@@ -1,0 +1,154 @@
+"""The CUDA path against fixtures produced by the reference's own CUDA build.
+
+The fixtures (``tests/golden/ref_*.npz``, written on a B200 by
+``tests/golden/make_ref_fixtures.py`` from the reference's unchanged sources) hold what
+the reference returned for the inputs of ``ref_cases.py``: the reference gradients,
+detJ, mass CSR, P and internal force (CalcP + CalcInternalForce on a fresh Setup), the
+constraint arrays, the stiffness with Dirichlet BCs, CG iterates after 25 iterations and
+at convergence, and SyncedNesterov / SyncedAdamW / SyncedAdamWNocoop trajectories; for
+the configuration-2 meshes, norms, seeded projections and samples of the long vectors.
+
+Bars: FP64 rel 1e-10 for results (1e-12 for element arrays, which differ only by the
+reference's atomicAdd summation order); FP32 force mode rel 1e-5; integer patterns
+bit-exact.  Converged CG solutions (two different rounding sequences stopped at the same
+relative residual) compare at 1e-7, iteration counts within 1%.
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import tlfea_b200 as T
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE / "golden"))
+import ref_cases as RC  # noqa: E402
+
+from .helpers import make_element, rel  # noqa: E402
+from .test_ref_fixtures import first_order_runs, load  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+TOL32 = 1e-5
+
+
+def element(c, fixed=None, f=None, eta=0.0, lamd=0.0, mass=True):
+    return make_element(c["x"], c["y"], c["z"], c["conn"], E_mod=c["E"], nu=c["nu"], rho=c["rho"],
+                        fixed=c["fixed"] if fixed is None else fixed, f_ext=c["f"] if f is None else f, eta=eta,
+                        lamd=lamd, mass=mass)
+
+
+def check_long(name, key, v, fx, tol):
+    if name in RC.LARGE:
+        s = RC.summary(v)
+        assert abs(s["norm"] - fx[f"{key}_norm"][0]) <= tol * s["norm"], key
+        assert rel(s["proj"], fx[f"{key}_proj"]) < 10 * tol, key
+        assert rel(s["sample"], fx[f"{key}_sample"]) < tol, key
+    else:
+        assert rel(v, fx[key]) < tol, (key, rel(v, fx[key]))
+
+
+@pytest.mark.parametrize("name", RC.ALL)
+def test_force_matches_reference(name):
+    fx = load(name)
+    c = RC.case(name)
+    el = element(c, mass=name not in RC.LARGE)
+    xp = RC.perturbed(c)
+    el.UpdatePositions(*xp)
+    # fused internal force (FP64, then FP32 force mode)
+    el.ComputeInternalForce()
+    check_long(name, "f_int", el.RetrieveInternalForceToCPU(), fx, 1e-12)
+    el.SetForcePrecision("fp32")
+    el.ComputeInternalForce()
+    check_long(name, "f_int", el.RetrieveInternalForceToCPU(), fx, TOL32)
+    el.SetForcePrecision("fp64")
+    el.Destroy()
+    # CalcP + CalcInternalForce on a fresh element (CalcInternalForce accumulates)
+    el = element(c, mass=False)
+    el.UpdatePositions(*xp)
+    el.CalcP()
+    el.CalcInternalForce()
+    check_long(name, "f_int", el.RetrieveInternalForceToCPU(), fx, 1e-12)
+    if "P" in fx:
+        P = el.RetrievePFromFToCPU()  # (E, QP, 3, 3) -> reference layout i + 3j
+        assert rel(P.transpose(0, 1, 3, 2).ravel(), fx["P"]) < 1e-13
+    el.Destroy()
+
+
+@pytest.mark.parametrize("name", RC.SMALL)
+def test_element_arrays_and_constraints_match_reference(name):
+    fx = load(name)
+    c = RC.case(name)
+    el = element(c)
+    g = el.RetrieveDnDuPreToCPU()  # (E, QP, NPE, 3) -> reference layout a + NPE*j
+    assert rel(g.transpose(0, 1, 3, 2).ravel(), fx["grad"]) < 1e-13
+    assert rel(el.RetrieveDetJToCPU().ravel(), fx["detj"]) < 1e-14
+    off, cols, vals = el.RetrieveMassCSRToCPU()
+    assert np.array_equal(off, fx["mass_off"]) and np.array_equal(cols, fx["mass_col"])
+    assert rel(vals, fx["mass_val"]) < 1e-13
+    el.UpdatePositions(*RC.perturbed(c))
+    el.CalcConstraintData()
+    assert rel(el.RetrieveConstraintDataToCPU(), fx["constraint"]) < 1e-15
+    el.ConvertToCSR_ConstraintJac()
+    for tr, pre in ((False, "j"), (True, "jt")):
+        o, cl, v = el.RetrieveConstraintJacobianCSRToCPU(transpose=tr)
+        assert np.array_equal(o, fx[f"{pre}_off"]) and np.array_equal(cl, fx[f"{pre}_col"])
+        assert np.array_equal(v, fx[f"{pre}_val"])
+    el.Destroy()
+
+
+@pytest.mark.parametrize("name", RC.ALL)
+def test_linear_static_matches_reference(name):
+    fx = load(name)
+    c = RC.case(name)
+    tol = 1e-6 if name in RC.LARGE else 1e-10
+    X0 = np.stack([c["x"], c["y"], c["z"]])
+    el = element(c, mass=False)
+    for tag, max_iter in (("cg25", 25), ("cg", 200000)):
+        el.ResetPositions()
+        s = T.LinearStaticSolver(el, tol, max_iter)
+        s.Solve()
+        u = (np.stack(el.RetrievePositionToCPU()) - X0).T.ravel()
+        it = s.GetLastIterCount()
+        it_ref = int(fx[f"{tag}_iters"][0])
+        if tag == "cg25":
+            assert it == it_ref == 25
+            check_long(name, "u_cg25", u, fx, 1e-10)
+            if "K_val" in fx:
+                off, cols, vals = s.RetrieveStiffnessCSRToCPU()
+                assert np.array_equal(off, fx["K_off"]) and np.array_equal(cols, fx["K_col"])
+                assert rel(vals, fx["K_val"]) < 1e-12
+        else:
+            assert abs(it - it_ref) <= max(2, 0.01 * it_ref), (it, it_ref)
+            check_long(name, "u_cg", u, fx, 1e-7 if name not in RC.LARGE else 1e-5)
+        del s
+    el.Destroy()
+
+
+@pytest.mark.parametrize("name", RC.SMALL)
+def test_first_order_solvers_match_reference(name):
+    fx = load(name)
+    c = RC.case(name)
+    X0 = np.stack([c["x"], c["y"], c["z"]])
+    for tag, kind, params, steps, load_kind, tol_x, tol_v in first_order_runs(name):
+        fixed, f, lamd = c["fixed"], c["f"], 0.0
+        if load_kind == "generic":
+            fixed, f = RC.generic_load(c)
+        elif load_kind == "damped":
+            lamd = 0.1
+        el = element(c, fixed=fixed, f=f, lamd=lamd)
+        cls = {"nesterov": T.SyncedNesterovSolver, "adamw": T.SyncedAdamWSolver,
+               "nocoop": T.SyncedAdamWNocoopSolver}[kind]
+        s = cls(el, el.get_n_constraint())
+        s.Setup()
+        s.SetParameters(T.SyncedNesterovParams(*params) if kind == "nesterov" else T.SyncedAdamWParams(*params))
+        ref = fx[f"{tag}_pos"]
+        for k in range(steps):
+            s.Solve()
+            pos = np.stack(el.RetrievePositionToCPU())
+            assert rel(pos - X0, ref[k] - X0) < tol_x, (tag, k, rel(pos - X0, ref[k] - X0))
+        if tol_v is not None:
+            vg, _ = s.GetVelocity()
+            assert rel(vg, fx[f"{tag}_v"]) < tol_v, (tag, rel(vg, fx[f"{tag}_v"]))
+        del s
+        el.Destroy()

@@ -40,3 +40,17 @@ def test_noalloc_force_matches_regular_entry_point(order):
         assert np.isfinite(f).all(), f"call {call}"
         assert rel(f, f_ref) < TOL64, f"call {call}"
     el.Destroy()
+
+
+def test_noalloc_refuses_fp32_force_mode():
+    import torch
+
+    from tlfea_b200 import TLFEAError
+
+    x, y, z, conn = box(4, 2, 2, 10)
+    el = make_element(x, y, z, conn, mass=False)
+    el.SetForcePrecision("fp32")
+    out = torch.zeros(3 * len(x), dtype=torch.float64, device="cuda")
+    with pytest.raises(TLFEAError):
+        _capi.call("tlfea_element_compute_internal_force_noalloc", el._handle(), None, C.c_void_p(out.data_ptr()))
+    el.Destroy()

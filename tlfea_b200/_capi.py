@@ -118,6 +118,7 @@ _SIGS = {
     "tlfea_element_retrieve_detj": [_P, _D, _LL],
     "tlfea_element_retrieve_connectivity": [_P, _I, _LL],
     "tlfea_element_retrieve_constraint": [_P, _D, C.c_int],
+    "tlfea_element_retrieve_constraint_jac_csr": [_P, C.c_int, _I, _I, _D],
     "tlfea_element_write_vtk": [_P, C.c_char_p],
     "tlfea_element_device_ptrs": [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)],
     "tlfea_nesterov_create": [_P, C.c_int, C.POINTER(_P)],

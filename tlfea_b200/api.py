@@ -236,6 +236,17 @@ class _TetData(ElementBase):
             capi.call("tlfea_element_retrieve_constraint", self._handle(), capi.dptr(c), c.size)
         return c
 
+    def RetrieveConstraintJacobianCSRToCPU(self, transpose: bool = False):
+        """New: (offsets, columns, values) of J (or J^T) as built by
+        ConvertToCSR_ConstraintJac(T) (FEAT10Data.cu:420-562)."""
+        rows = 3 * self.n_coef if transpose else self.n_constraint
+        off = np.zeros(rows + 1, np.int32)
+        cols = np.zeros(max(self.n_constraint, 1), np.int32)
+        vals = np.zeros(max(self.n_constraint, 1))
+        capi.call("tlfea_element_retrieve_constraint_jac_csr", self._handle(), int(transpose), capi.iptr(off),
+                  capi.iptr(cols), capi.dptr(vals))
+        return off, cols[:self.n_constraint], vals[:self.n_constraint]
+
     def WriteOutputVTK(self, filename: str):
         capi.call("tlfea_element_write_vtk", self._handle(), str(filename).encode())
 

@@ -11,6 +11,7 @@ from __future__ import annotations
 import os
 import shutil
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -45,10 +46,25 @@ def library_sources():
 
 
 def build_library(force: bool = False, verbose: bool = False, extra=None) -> Path:
+    """One nvcc per source (in parallel, objects under tlfea_b200/_build/), then one link."""
     srcs, deps = library_sources()
     if not force and _newer(LIB, deps):
         return LIB
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *(extra or []), "-o", str(LIB), *map(str, srcs)]
+    obj_dir = PKG / "_build"
+    obj_dir.mkdir(exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+    def compile_one(src: Path) -> Path:
+        obj = obj_dir / (src.stem + ".o")
+        cmd = [nvcc(), *ARCH, *compile_flags, *(extra or []), "-c", "-o", str(obj), str(src)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True, cwd=str(ROOT))
+        return obj
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(compile_one, srcs))
+    cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(LIB), *map(str, objs)]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True, cwd=str(ROOT))

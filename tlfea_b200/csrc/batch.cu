@@ -1194,7 +1194,7 @@ int tlfea_batch_create_shared(int type, int n_inst, int n_nodes, int n_elem, con
 
 int tlfea_batch_destroy(tlfea_batch b) {
     CHECK_BATCH(b);
-    if (b->el) cudaSetDevice(b->el->device);
+    if (b->el) TLFEA_CUDA(cudaSetDevice(b->el->device));
     drop_graphs(b);
     dfree(b->lam); dfree(b->mu); dfree(b->lam32); dfree(b->mu32);
     dfree(b->fixed); dfree(b->chunk_inst); dfree(b->chunk_beg); dfree(b->inst_chunk); dfree(b->tile_inst);

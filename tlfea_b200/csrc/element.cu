@@ -150,11 +150,11 @@ __global__ void k_dndu_pre(int n_slots, int E, const int* __restrict__ tile_elem
     } else {
         for (int a = 0; a < NPE; ++a) gN[a][0] = gN[a][1] = gN[a][2] = 0.0;
     }
-    const size_t gb = ((size_t)tile * NQP + q) * (NPE * 3) * TE + t;
+    const size_t gb = ((size_t)tile * NQP + q) * (NPE * 3) * TE;
     for (int a = 0; a < NPE; ++a)
         for (int j = 0; j < 3; ++j) {
-            grad64[gb + (size_t)(a * 3 + j) * TE] = gN[a][j];
-            grad32[gb + (size_t)(a * 3 + j) * TE] = (float)gN[a][j];
+            grad64[gb + grad_slot<double>(a, j, t)] = gN[a][j];
+            grad32[gb + grad_slot<float>(a, j, t)] = (float)gN[a][j];
         }
     const double dv = (e >= 0) ? dj * qp.qw[q] : 0.0;
     dv64[((size_t)tile * NQP + q) * TE + t] = dv;
@@ -211,16 +211,6 @@ __global__ void k_add_gravity(int N, const int* __restrict__ off, const double* 
     f[3 * i + 0] += s * gx;
     f[3 * i + 1] += s * gy;
     f[3 * i + 2] += s * gz;
-}
-
-__global__ void k_disp32(int n, const double* __restrict__ x, const double* __restrict__ y,
-                         const double* __restrict__ z, const double* __restrict__ X0x, const double* __restrict__ X0y,
-                         const double* __restrict__ X0z, float* ux, float* uy, float* uz) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    ux[i] = (float)(x[i] - X0x[i]);
-    uy[i] = (float)(y[i] - X0y[i]);
-    uz[i] = (float)(z[i] - X0z[i]);
 }
 
 __global__ void k_f32_to_f64(long long n, const float* __restrict__ a, double* b) {
@@ -572,15 +562,6 @@ int element_build_pattern(tlfea_element_s* h) {
     return TLFEA_OK;
 }
 
-int element_refresh_u32(tlfea_element_s* h) {
-    if (!h->u_dirty) return TLFEA_OK;
-    const int n = h->N;
-    k_disp32<<<(n + 255) / 256, 256, 0, h->stream>>>(n, h->x, h->y, h->z, h->X0x, h->X0y, h->X0z, h->ux, h->uy, h->uz);
-    TLFEA_CHECK_LAUNCH();
-    h->u_dirty = false;
-    return TLFEA_OK;
-}
-
 template <typename R>
 static TileArgs<R> make_args(tlfea_element_s* h, bool fp32) {
     TileArgs<R> A;
@@ -612,9 +593,13 @@ static TileArgs<R> make_args(tlfea_element_s* h, bool fp32) {
         A.grad = (const R*)tl.grad32;
         A.ji = (const R*)tl.ji32;
         A.dv = (const R*)tl.dv32;
-        A.px = (const R*)h->ux;
-        A.py = (const R*)h->uy;
-        A.pz = (const R*)h->uz;
+        A.px = A.py = A.pz = nullptr;  // staged from x64 - X0 relative to each tile's anchor
+        A.x64 = h->x;
+        A.y64 = h->y;
+        A.z64 = h->z;
+        A.X0x = h->X0x;
+        A.X0y = h->X0y;
+        A.X0z = h->X0z;
         A.f_out = (R*)h->f_int32;
         A.partial = (R*)tl.partial32;
     }
@@ -747,7 +732,6 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
 int element_force(tlfea_element_s* h, const double* d_v, bool fp32) {
     int st;
     if (fp32) {
-        if ((st = element_refresh_u32(h))) return st;
         st = (h->npe == 10) ? force_dispatch<float, 10, 5>(h, d_v, true) : force_dispatch<float, 4, 1>(h, d_v, true);
     } else {
         st = (h->npe == 10) ? force_dispatch<double, 10, 5>(h, d_v, false)
@@ -853,7 +837,11 @@ using namespace tlfea;
             set_error("null handle");                    \
             return TLFEA_INVALID_ARG;                    \
         }                                                \
-        cudaSetDevice((h)->device);                      \
+        const cudaError_t dev_e_ = cudaSetDevice((h)->device); \
+        if (dev_e_ != cudaSuccess) {                     \
+            set_error(std::string("cudaSetDevice: ") + cudaGetErrorString(dev_e_)); \
+            return TLFEA_CUDA_ERROR;                     \
+        }                                                \
     } while (0)
 
 #define SYNC(h) TLFEA_CUDA(cudaStreamSynchronize((h)->stream))
@@ -917,7 +905,6 @@ int tlfea_element_create(int type, int n_elem, int n_nodes, tlfea_element* out) 
     st |= dalloc(&h->x, N) | dalloc(&h->y, N) | dalloc(&h->z, N);
     st |= dalloc(&h->xj, N) | dalloc(&h->yj, N) | dalloc(&h->zj, N);
     st |= dalloc(&h->X0x, N) | dalloc(&h->X0y, N) | dalloc(&h->X0z, N);
-    st |= dalloc(&h->ux, N) | dalloc(&h->uy, N) | dalloc(&h->uz, N);
     st |= dalloc(&h->d_conn, (size_t)n_elem * h->npe);
     st |= dalloc(&h->f_int, 3 * N) | dalloc(&h->f_ext, 3 * N) | dalloc(&h->f_int32, 3 * N);
     st |= dalloc(&h->detJ, (size_t)n_elem * h->nqp);
@@ -938,11 +925,10 @@ int tlfea_element_create(int type, int n_elem, int n_nodes, tlfea_element* out) 
 
 int tlfea_element_destroy(tlfea_element h) {
     if (!h) return TLFEA_INVALID_ARG;
-    cudaSetDevice(h->device);
+    TLFEA_CUDA(cudaSetDevice(h->device));
     dfree(h->x); dfree(h->y); dfree(h->z);
     dfree(h->xj); dfree(h->yj); dfree(h->zj);
     dfree(h->X0x); dfree(h->X0y); dfree(h->X0z);
-    dfree(h->ux); dfree(h->uy); dfree(h->uz);
     dfree(h->d_conn); dfree(h->f_int); dfree(h->f_ext); dfree(h->f_int32);
     dfree(h->detJ); dfree(h->Pst); dfree(h->d_err);
     free_tiling(h->tl);
@@ -985,7 +971,6 @@ int tlfea_element_reset_positions(tlfea_element h) {
     TLFEA_CUDA(cudaMemcpyAsync(h->x, h->X0x, nb, cudaMemcpyDeviceToDevice, h->stream));
     TLFEA_CUDA(cudaMemcpyAsync(h->y, h->X0y, nb, cudaMemcpyDeviceToDevice, h->stream));
     TLFEA_CUDA(cudaMemcpyAsync(h->z, h->X0z, nb, cudaMemcpyDeviceToDevice, h->stream));
-    h->u_dirty = true;
     SYNC_COMPUTE(h);
     return TLFEA_OK;
 }
@@ -1043,7 +1028,6 @@ int tlfea_element_setup(tlfea_element h, const double* qx, const double* qy, con
     if (st) return st;
     if ((st = build_incidence(h))) return st;
     SYNC(h);
-    h->u_dirty = true;
     h->is_setup = true;
     return TLFEA_OK;
 }
@@ -1168,7 +1152,6 @@ static int copy_positions(tlfea_element h, double* dx, double* dy, double* dz, c
 
 int tlfea_element_update_positions(tlfea_element h, const double* x, const double* y, const double* z, int n) {
     CHECK_HANDLE(h);
-    h->u_dirty = true;
     return copy_positions(h, h->x, h->y, h->z, x, y, z, n);
 }
 
@@ -1203,7 +1186,6 @@ int tlfea_element_calc_dndu_pre(tlfea_element h) {
     TLFEA_CUDA(cudaMemcpyAsync(h->X0x, h->x, nb, cudaMemcpyDeviceToDevice, h->stream));
     TLFEA_CUDA(cudaMemcpyAsync(h->X0y, h->y, nb, cudaMemcpyDeviceToDevice, h->stream));
     TLFEA_CUDA(cudaMemcpyAsync(h->X0z, h->z, nb, cudaMemcpyDeviceToDevice, h->stream));
-    h->u_dirty = true;
     h->precomputed = true;
     SYNC(h);
     return TLFEA_OK;
@@ -1365,6 +1347,11 @@ int tlfea_element_compute_internal_force_noalloc(tlfea_element h, const double* 
         set_error("output pointer is null");
         return TLFEA_INVALID_ARG;
     }
+    if (h->precision != TLFEA_PRECISION_FP64) {
+        set_error("the allocation-free internal force runs in FP64 only; this element is in FP32 force mode "
+                  "(use tlfea_element_compute_internal_force)");
+        return TLFEA_UNSUPPORTED;
+    }
     const size_t need = 3 * (size_t)h->tl.n_pslots;
     if (need > NOALLOC_SCRATCH_DOUBLES) {
         set_error("mesh needs " + std::to_string(need) + " doubles of shared-node scratch; the static scratch holds " +
@@ -1502,6 +1489,25 @@ int tlfea_element_retrieve_constraint(tlfea_element h, double* c, int n) {
     if (n == 0) return TLFEA_OK;
     SYNC(h);
     D2H(c, h->c, sizeof(double) * (size_t)n);
+    return TLFEA_OK;
+}
+
+int tlfea_element_retrieve_constraint_jac_csr(tlfea_element h, int which, int* offsets, int* columns,
+                                              double* values) {
+    CHECK_HANDLE(h);
+    if (which != 0 && which != 1) return TLFEA_INVALID_ARG;
+    if (!offsets || !columns || !values) return TLFEA_INVALID_ARG;
+    const bool built = which ? h->jt_setup : h->j_setup;
+    if (!built) {
+        set_error("the constraint Jacobian CSR was not built (ConvertToCSR_ConstraintJac / _ConstraintJacT)");
+        return TLFEA_NOT_SETUP;
+    }
+    const size_t rows = which ? 3 * (size_t)h->N : (size_t)h->n_constraint;
+    const size_t nnz = (size_t)h->n_constraint;
+    SYNC(h);
+    D2H(offsets, which ? h->jt_off : h->j_off, sizeof(int) * (rows + 1));
+    D2H(columns, which ? h->jt_col : h->j_col, sizeof(int) * nnz);
+    D2H(values, which ? h->jt_val : h->j_val, sizeof(double) * nnz);
     return TLFEA_OK;
 }
 

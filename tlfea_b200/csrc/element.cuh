@@ -80,9 +80,17 @@ struct TileArgs {
     const R* grad;
     const R* ji;  // J^-1 per (tile, QP), the compact geometry stream
     const R* dv;
-    const R* px;  // FP64: positions x; FP32: displacement u = x - X0
+    const R* px;  // FP64 mode: positions x (null in FP32 mode)
     const R* py;
     const R* pz;
+    // FP32 mode: FP64 positions and reference positions; each tile stages its nodes'
+    // displacements relative to its first local node (tile_anchor / stage_pos)
+    const double* x64;
+    const double* y64;
+    const double* z64;
+    const double* X0x;
+    const double* X0y;
+    const double* X0z;
     const double* v;  // interleaved velocities for the Kelvin-Voigt term, or null
     double* Pst;      // stored P in the reference layout (CalcP / CalcInternalForce)
     R* f_out;         // interleaved 3N
@@ -94,6 +102,51 @@ struct TileArgs {
     int max_local;
     QpBary qb;
 };
+
+// Offset of gradient (node a, component j) of the element in lane t within one QP
+// slice of the gradient stream.  FP64: component-major [a*3 + j][t].  FP32: node
+// pairs interleaved, [(a/2)*3 + j][t][a%2], so that one 8-byte shared-memory load
+// gives (gradN_a, gradN_(a+1)) for the paired FP32 arithmetic of the force kernel
+// (NPE is even: 10 or 4).
+template <typename R>
+__host__ __device__ __forceinline__ size_t grad_slot(int a, int j, int t) {
+    if constexpr (sizeof(R) == 4)
+        return ((size_t)((a >> 1) * 3 + j) * TILE_ELEMS + t) * 2 + (a & 1);
+    else
+        return (size_t)(a * 3 + j) * TILE_ELEMS + t;
+}
+
+// Node values staged for a tile.  FP64 mode: the positions themselves (F =
+// sum_a x_a (x) gradN_a, the reference's formula).  FP32 mode: the displacement
+// relative to the tile's first local node ("anchor"), differenced in FP64 and
+// rounded once, u_a - u_0 = (x_a - X0_a) - (x_0 - X0_0).  The shape-function
+// gradients sum to zero, so H = sum_a (u_a - u_0) (x) gradN_a exactly; with the
+// anchor both roundings -- of u_a and of the FP32 gradients -- scale with how much
+// u varies across the tile instead of with |u|, which keeps the FP32 force
+// accurate at large displacements.
+template <typename R>
+__device__ __forceinline__ void tile_anchor(const TileArgs<R>& A, int gid0, double u0[3]) {
+    if constexpr (sizeof(R) == 4) {
+        u0[0] = A.x64[gid0] - A.X0x[gid0];
+        u0[1] = A.y64[gid0] - A.X0y[gid0];
+        u0[2] = A.z64[gid0] - A.X0z[gid0];
+    } else {
+        u0[0] = u0[1] = u0[2] = 0.0;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void stage_pos(const TileArgs<R>& A, int gid, const double u0[3], R& x, R& y, R& z) {
+    if constexpr (sizeof(R) == 4) {
+        x = (float)((A.x64[gid] - A.X0x[gid]) - u0[0]);
+        y = (float)((A.y64[gid] - A.X0y[gid]) - u0[1]);
+        z = (float)((A.z64[gid] - A.X0z[gid]) - u0[2]);
+    } else {
+        x = A.px[gid];
+        y = A.py[gid];
+        z = A.pz[gid];
+    }
+}
 
 // Tile routine modes.
 enum { TILE_FORCE = 0, TILE_STORE_P = 1, TILE_FORCE_FROM_P = 2 };
@@ -526,15 +579,21 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
     const int lb = A.node_off[tile];
     const int nl = A.node_off[tile + 1] - lb;
     if (MODE != TILE_FORCE_FROM_P) {
+        double u0[3], v0[3] = {0.0, 0.0, 0.0};
+        tile_anchor(A, A.ln_gid[lb], u0);
+        if (DAMP && sizeof(R) == 4) {  // FP32: velocities relative to the anchor too (Fdot = sum v_a (x) gradN_a)
+            const int g0 = A.ln_gid[lb];
+            v0[0] = A.v[3 * g0 + 0];
+            v0[1] = A.v[3 * g0 + 1];
+            v0[2] = A.v[3 * g0 + 2];
+        }
         for (int ln = t; ln < nl; ln += TE) {
             const int gid = A.ln_gid[lb + ln];
-            xs[ln] = A.px[gid];
-            ys[ln] = A.py[gid];
-            zs[ln] = A.pz[gid];
+            stage_pos(A, gid, u0, xs[ln], ys[ln], zs[ln]);
             if (DAMP) {
-                vs[3 * ln + 0] = R(A.v[3 * gid + 0]);
-                vs[3 * ln + 1] = R(A.v[3 * gid + 1]);
-                vs[3 * ln + 2] = R(A.v[3 * gid + 2]);
+                vs[3 * ln + 0] = R(A.v[3 * gid + 0] - v0[0]);
+                vs[3 * ln + 1] = R(A.v[3 * gid + 1] - v0[1]);
+                vs[3 * ln + 2] = R(A.v[3 * gid + 2] - v0[2]);
             }
             if (MASS) {
 #pragma unroll
@@ -584,12 +643,12 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
     }
 #pragma unroll 1
     for (int q = 0; q < NQP && MODE != TILE_FORCE; ++q) {
-        const R* gp = A.grad + ((size_t)tile * NQP + q) * (NPE * 3) * TE + t;
+        const R* gp = A.grad + ((size_t)tile * NQP + q) * (NPE * 3) * TE;
         R g[NPE][3];
 #pragma unroll
         for (int a = 0; a < NPE; ++a)
 #pragma unroll
-            for (int j = 0; j < 3; ++j) g[a][j] = ld_stream(gp + (a * 3 + j) * TE);
+            for (int j = 0; j < 3; ++j) g[a][j] = ld_stream(gp + grad_slot<R>(a, j, t));
         const R dv = ld_stream(A.dv + ((size_t)tile * NQP + q) * TE + t);
 
         R P[3][3];
@@ -726,8 +785,6 @@ struct tlfea_element_s {
     double *x = nullptr, *y = nullptr, *z = nullptr;
     double *xj = nullptr, *yj = nullptr, *zj = nullptr;
     double *X0x = nullptr, *X0y = nullptr, *X0z = nullptr;
-    float *ux = nullptr, *uy = nullptr, *uz = nullptr;
-    bool u_dirty = true;
     int* d_conn = nullptr;
     double* f_int = nullptr;
     double* f_ext = nullptr;
@@ -773,7 +830,6 @@ struct tlfea_element_s {
 namespace tlfea {
 // Implemented in element.cu, used by the solvers.
 int element_build_pattern(tlfea_element_s* h);
-int element_refresh_u32(tlfea_element_s* h);
 int element_force(tlfea_element_s* h, const double* d_v, bool fp32);
 
 // Barycentric coordinates of the element's quadrature points.

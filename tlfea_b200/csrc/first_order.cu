@@ -39,7 +39,6 @@ struct FOArgs {
     const double *xj, *yj, *zj;
     double *x, *y, *z;
     const double *X0x, *X0y, *X0z;
-    float *ux, *uy, *uz;
     const int* m_off;
     const int* m_col;
     const double* m_val;
@@ -84,18 +83,12 @@ __device__ __forceinline__ void write_partial(const FOArgs& S, int k, double v, 
     if (threadIdx.x == 0) S.red[(size_t)k * S.red_stride + blockIdx.x] = s;
 }
 
-// x = x_prev + dt * v (and the FP32 displacement when forces run in FP32)
+// x = x_prev + dt * v (FP32 force mode stages x - X0 per tile from these)
 template <typename R>
 __device__ __forceinline__ void set_node_positions(const FOArgs& S, int i, double v0, double v1, double v2) {
-    const double nx = S.xp[i] + S.dt * v0, ny = S.yp[i] + S.dt * v1, nz = S.zp[i] + S.dt * v2;
-    S.x[i] = nx;
-    S.y[i] = ny;
-    S.z[i] = nz;
-    if (sizeof(R) == 4) {
-        S.ux[i] = (float)(nx - S.X0x[i]);
-        S.uy[i] = (float)(ny - S.X0y[i]);
-        S.uz[i] = (float)(nz - S.X0z[i]);
-    }
+    S.x[i] = S.xp[i] + S.dt * v0;
+    S.y[i] = S.yp[i] + S.dt * v1;
+    S.z[i] = S.zp[i] + S.dt * v2;
 }
 
 // Internal force of node i (boundary nodes: sum of the tile partials in tile
@@ -474,7 +467,6 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
         if ((st = tlfea_element_build_constraint_jact_csr(el))) return st;
     }
     const bool fp32 = (el->precision == TLFEA_PRECISION_FP32);
-    if (fp32 && (st = element_refresh_u32(el))) return st;
     FOArgs S;
     memset(&S, 0, sizeof(S));
     S.kind = s->kind;
@@ -487,7 +479,6 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     S.xj = el->xj; S.yj = el->yj; S.zj = el->zj;
     S.x = el->x; S.y = el->y; S.z = el->z;
     S.X0x = el->X0x; S.X0y = el->X0y; S.X0z = el->X0z;
-    S.ux = el->ux; S.uy = el->uy; S.uz = el->uz;
     S.m_off = el->pat_off; S.m_col = el->pat_col; S.m_val = el->m_val;
     S.f_ext = el->f_ext;
     S.f_int64 = el->f_int;
@@ -543,7 +534,8 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     A32.kappa = A64.kappa = el->kappa;
     A32.ji = el->tl.ji32;
     A64.ji = el->tl.ji64;
-    A32.grad = el->tl.grad32; A32.dv = el->tl.dv32; A32.px = el->ux; A32.py = el->uy; A32.pz = el->uz;
+    A32.grad = el->tl.grad32; A32.dv = el->tl.dv32; A32.px = A32.py = A32.pz = nullptr;
+    A32.x64 = el->x; A32.y64 = el->y; A32.z64 = el->z; A32.X0x = el->X0x; A32.X0y = el->X0y; A32.X0z = el->X0z;
     A32.f_out = el->f_int32; A32.partial = el->tl.partial32;
     A32.lambda = (float)el->lambda; A32.mu = (float)el->mu; A32.eta = (float)el->eta_d; A32.lamd = (float)el->lambda_d;
     A64.grad = el->tl.grad64; A64.dv = el->tl.dv64; A64.px = el->x; A64.py = el->y; A64.pz = el->z;
@@ -655,7 +647,6 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     s->stats.stop_rule_met = hl[8];
     s->stats.kernel_ms = ms;
     el->f_int_from32 = fp32;
-    el->u_dirty = !fp32;  // the kernel keeps u in step with x in FP32 mode
     if (status == TLFEA_NONFINITE) {
         set_error("non-finite gradient norm");
         return TLFEA_NONFINITE;

@@ -99,19 +99,38 @@ inline size_t pipe_smem_bytes(int max_local, bool damp) {
     return b;
 }
 
-// Issue the cp.async copies of tile `tile`'s node positions (and velocities).
+// Stage tile `tile`'s node positions (and velocities): FP64 by cp.async copies;
+// FP32 as displacements relative to the tile's anchor node (stage_pos), which
+// takes FP64 arithmetic, so those are plain loads.
 template <typename R, bool DAMP>
 __device__ __forceinline__ void prefetch_nodes(const TileArgs<R>& A, int tile, R* xs, R* ys, R* zs, double* vs) {
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
+    double u0[3], v0[3] = {0.0, 0.0, 0.0};
+    tile_anchor(A, A.ln_gid[lb], u0);
+    if (DAMP && sizeof(R) == 4) {
+        const int g0 = A.ln_gid[lb];
+        v0[0] = A.v[3 * g0 + 0];
+        v0[1] = A.v[3 * g0 + 1];
+        v0[2] = A.v[3 * g0 + 2];
+    }
     for (int ln = threadIdx.x; ln < nl; ln += TILE_ELEMS) {
         const int gid = A.ln_gid[lb + ln];
-        cp_async<sizeof(R)>(xs + ln, A.px + gid);
-        cp_async<sizeof(R)>(ys + ln, A.py + gid);
-        cp_async<sizeof(R)>(zs + ln, A.pz + gid);
-        if (DAMP) {
-            cp_async<8>(vs + 3 * ln + 0, A.v + 3 * gid + 0);
-            cp_async<8>(vs + 3 * ln + 1, A.v + 3 * gid + 1);
-            cp_async<8>(vs + 3 * ln + 2, A.v + 3 * gid + 2);
+        if constexpr (sizeof(R) == 8) {
+            cp_async<sizeof(R)>(xs + ln, A.px + gid);
+            cp_async<sizeof(R)>(ys + ln, A.py + gid);
+            cp_async<sizeof(R)>(zs + ln, A.pz + gid);
+            if (DAMP) {
+                cp_async<8>(vs + 3 * ln + 0, A.v + 3 * gid + 0);
+                cp_async<8>(vs + 3 * ln + 1, A.v + 3 * gid + 1);
+                cp_async<8>(vs + 3 * ln + 2, A.v + 3 * gid + 2);
+            }
+        } else {
+            stage_pos(A, gid, u0, xs[ln], ys[ln], zs[ln]);
+            if (DAMP) {
+                vs[3 * ln + 0] = A.v[3 * gid + 0] - v0[0];
+                vs[3 * ln + 1] = A.v[3 * gid + 1] - v0[1];
+                vs[3 * ln + 2] = A.v[3 * gid + 2] - v0[2];
+            }
         }
     }
 }
@@ -212,7 +231,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2) k_force_pipe(TileArgs<R> A, i
 #pragma unroll
                 for (int a = 0; a < G::PART_NODES; ++a)
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) g[p * G::PART_NODES + a][j] = gs[(a * 3 + j) * TE + t];
+                    for (int j = 0; j < 3; ++j) g[p * G::PART_NODES + a][j] = gs[grad_slot<R>(a, j, t)];
                 if (p == G::PARTS - 1) dv = reinterpret_cast<const R*>(st + G::GRAD_BYTES)[t];
                 // The producer refills this stage with a bulk copy (async proxy) once
                 // every consumer has arrived; order this thread's generic-proxy
@@ -407,7 +426,7 @@ inline size_t tile_tma_smem_bytes(int max_local, bool damp) {
 }
 
 template <typename R, int NPE, int NQP, bool DAMP>
-__global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, int* err) {
+__global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 1) k_tile_force_tma(TileArgs<R> A, int* err) {
     using G = TileTmaGeom<R, NPE>;
     constexpr int TE = TILE_ELEMS;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -447,158 +466,193 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_tma(TileArgs<R> A, in
         if (NQP > 1) issue(1);
     }
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
+    double u0[3], v0[3] = {0.0, 0.0, 0.0};
+    tile_anchor(A, A.ln_gid[lb], u0);
+    if (DAMP && sizeof(R) == 4) {  // FP32: velocities relative to the anchor too
+        const int g0 = A.ln_gid[lb];
+        v0[0] = A.v[3 * g0 + 0];
+        v0[1] = A.v[3 * g0 + 1];
+        v0[2] = A.v[3 * g0 + 2];
+    }
     for (int ln = t; ln < nl; ln += TE) {
         const int gid = A.ln_gid[lb + ln];
         const int ps = A.ln_pslot[lb + ln];
         iends[ln] = A.ln_inc_end[lb + ln];
         dsts[ln] = (ps < 0) ? gid : -(ps + 1);
-        xs[ln] = A.px[gid];
-        ys[ln] = A.py[gid];
-        zs[ln] = A.pz[gid];
+        stage_pos(A, gid, u0, xs[ln], ys[ln], zs[ln]);
         if (DAMP) {
-            vs[3 * ln + 0] = A.v[3 * gid + 0];
-            vs[3 * ln + 1] = A.v[3 * gid + 1];
-            vs[3 * ln + 2] = A.v[3 * gid + 2];
+            vs[3 * ln + 0] = A.v[3 * gid + 0] - v0[0];
+            vs[3 * ln + 1] = A.v[3 * gid + 1] - v0[1];
+            vs[3 * ln + 2] = A.v[3 * gid + 2] - v0[2];
         }
     }
     __syncthreads();  // positions and node tables staged; barriers initialised
 
-    int lc[NPE];
-    R f[NPE][3];
+    if constexpr (sizeof(R) == 4) {
+        // FP32: paired arithmetic (two nodes per instruction, __ffma2_rn).  The
+        // element's node displacements are gathered from shared memory once per tile
+        // into registers, node pairs side by side; each QP slice is read as node
+        // pairs (grad_slot<float>), H = sum_a u_a (x) gradN_a and the element forces
+        // f_a += (P dV) gradN_a accumulate two nodes per instruction.
+        constexpr int NP = NPE / 2;
+        if (!mbar_wait(bar0, 0)) atomicExch(err, 3);  // stage 0 brings lconn and the incidence
+        int lc[NPE];
 #pragma unroll
-    for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
+        for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
+        float2 up[NP][3], f2[NP][3];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            up[p][0] = make_float2(xs[lc[2 * p]], xs[lc[2 * p + 1]]);
+            up[p][1] = make_float2(ys[lc[2 * p]], ys[lc[2 * p + 1]]);
+            up[p][2] = make_float2(zs[lc[2 * p]], zs[lc[2 * p + 1]]);
+            f2[p][0] = f2[p][1] = f2[p][2] = make_float2(0.f, 0.f);
+        }
 #pragma unroll 1
-    for (int q = 0; q < NQP; ++q) {
-        if (!mbar_wait(bar0 + 8 * (q & 1), (q >> 1) & 1)) atomicExch(err, 3);
-        const unsigned char* st = stage0 + (size_t)(q & 1) * G::STAGE_BYTES;
-        const R* gs = reinterpret_cast<const R*>(st);
-        if (q == 0) {
-#pragma unroll
-            for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
-        }
-        R g[NPE][3];
-#pragma unroll
-        for (int a = 0; a < NPE; ++a)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) g[a][j] = gs[(a * 3 + j) * TE + t];
-        const R dv = reinterpret_cast<const R*>(st + G::GRAD_BYTES)[t];
-        if (q + 2 < NQP) {
-            // every thread's generic reads of this stage precede the bulk refill
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            if (t == 0) issue(q + 2);
-        }
-        R P[3][3];
-        if constexpr (sizeof(R) == 8) {
-            double F[3][3];
+        for (int q = 0; q < NQP; ++q) {
+            if (q > 0 && !mbar_wait(bar0 + 8 * (q & 1), (q >> 1) & 1)) atomicExch(err, 3);
+            const unsigned char* st = stage0 + (size_t)(q & 1) * G::STAGE_BYTES;
+            const float2* gs2 = reinterpret_cast<const float2*>(st);
+            const float dv = reinterpret_cast<const float*>(st + G::GRAD_BYTES)[t];
+            float2 h2[3][3], fd2[3][3];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int j = 0; j < 3; ++j) F[i][j] = 0.0;
+                for (int j = 0; j < 3; ++j) h2[i][j] = fd2[i][j] = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int a = 0; a < NPE; ++a) {
-                const double xa[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+            for (int p = 0; p < NP; ++p) {
+                float2 g[3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) g[j] = gs2[(p * 3 + j) * TE + t];
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) F[i][j] += xa[i] * g[a][j];
+                    for (int j = 0; j < 3; ++j) h2[i][j] = __ffma2_rn(up[p][i], g[j], h2[i][j]);
+                if (DAMP) {
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const float2 va = make_float2((float)vs[3 * lc[2 * p] + i], (float)vs[3 * lc[2 * p + 1] + i]);
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) fd2[i][j] = __ffma2_rn(va, g[j], fd2[i][j]);
+                    }
+                }
             }
-            svk_p_reference(F, A.lambda, A.mu, P);
-            if (DAMP) {
-                double Fd[3][3], Pv[3][3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) Fd[i][j] = 0.0;
-#pragma unroll
-                for (int a = 0; a < NPE; ++a)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc[a] + i] * g[a][j];
-                kelvin_voigt<double>(F, Fd, A.eta, A.lamd, Pv);
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
-            }
-        } else {
-            R H[3][3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) H[i][j] = R(0);
-#pragma unroll
-            for (int a = 0; a < NPE; ++a) {
-                const R ua[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) H[i][j] += ua[i] * g[a][j];
-            }
-            R Em[3][3];
+            float H[3][3], Fd[3][3], P[3][3];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
-                    R sm = H[i][j] + H[j][i];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) sm += H[k][i] * H[k][j];
-                    Em[i][j] = R(0.5) * sm;
+                    H[i][j] = h2[i][j].x + h2[i][j].y;
+                    Fd[i][j] = fd2[i][j].x + fd2[i][j].y;
                 }
-            const R trE = Em[0][0] + Em[1][1] + Em[2][2];
-            R Sm[3][3];
+            tile_stress<float, DAMP, false>(H, Fd, reinterpret_cast<const TileArgs<float>&>(A), P);
+            // f_a += (P dV) grad_a   (FEAT10DataFunc.cuh:417-449), two nodes per instruction
 #pragma unroll
-            for (int i = 0; i < 3; ++i)
+            for (int p = 0; p < NP; ++p) {
+                float2 g[3];
 #pragma unroll
-                for (int j = 0; j < 3; ++j) Sm[i][j] = R(2) * A.mu * Em[i][j] + (i == j ? A.lambda * trE : R(0));
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    R sm = Sm[i][j];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) sm += H[i][k] * Sm[k][j];
-                    P[i][j] = sm;
-                }
-            if (DAMP) {
-                R F[3][3], Fd[3][3], Pv[3][3];
+                for (int j = 0; j < 3; ++j) g[j] = gs2[(p * 3 + j) * TE + t];
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
                     for (int j = 0; j < 3; ++j) {
-                        F[i][j] = H[i][j] + (i == j ? R(1) : R(0));
-                        Fd[i][j] = R(0);
+                        const float pij = P[i][j] * dv;
+                        f2[p][i] = __ffma2_rn(make_float2(pij, pij), g[j], f2[p][i]);
                     }
-#pragma unroll
-                for (int a = 0; a < NPE; ++a)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) Fd[i][j] += R(vs[3 * lc[a] + i]) * g[a][j];
-                kelvin_voigt<R>(F, Fd, A.eta, A.lamd, Pv);
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
+            }
+            if (q + 2 < NQP) {
+                // every thread's generic reads of this stage precede the bulk refill
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncthreads();
+                if (t == 0) issue(q + 2);
             }
         }
-        // f_a += (P dV) grad_a   (FEAT10DataFunc.cuh:417-449)
+        __syncthreads();  // every thread is done with the stages the force table reuses
 #pragma unroll
-        for (int i = 0; i < 3; ++i)
+        for (int p = 0; p < NP; ++p)
 #pragma unroll
-            for (int j = 0; j < 3; ++j) P[i][j] *= dv;
-#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                fe[((2 * p) * 3 + d) * TE + t] = f2[p][d].x;
+                fe[((2 * p + 1) * 3 + d) * TE + t] = f2[p][d].y;
+            }
+        __syncthreads();
+    } else {
+        int lc[NPE];
+        R f[NPE][3];
+    #pragma unroll
+        for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
+    #pragma unroll 1
+        for (int q = 0; q < NQP; ++q) {
+            if (!mbar_wait(bar0 + 8 * (q & 1), (q >> 1) & 1)) atomicExch(err, 3);
+            const unsigned char* st = stage0 + (size_t)(q & 1) * G::STAGE_BYTES;
+            const R* gs = reinterpret_cast<const R*>(st);
+            if (q == 0) {
+    #pragma unroll
+                for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
+            }
+            R g[NPE][3];
+    #pragma unroll
+            for (int a = 0; a < NPE; ++a)
+    #pragma unroll
+                for (int j = 0; j < 3; ++j) g[a][j] = gs[grad_slot<R>(a, j, t)];
+            const R dv = reinterpret_cast<const R*>(st + G::GRAD_BYTES)[t];
+            if (q + 2 < NQP) {
+                // every thread's generic reads of this stage precede the bulk refill
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncthreads();
+                if (t == 0) issue(q + 2);
+            }
+            R P[3][3];
+            {
+                double F[3][3];
+    #pragma unroll
+                for (int i = 0; i < 3; ++i)
+    #pragma unroll
+                    for (int j = 0; j < 3; ++j) F[i][j] = 0.0;
+    #pragma unroll
+                for (int a = 0; a < NPE; ++a) {
+                    const double xa[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+    #pragma unroll
+                    for (int i = 0; i < 3; ++i)
+    #pragma unroll
+                        for (int j = 0; j < 3; ++j) F[i][j] += xa[i] * g[a][j];
+                }
+                svk_p_reference(F, A.lambda, A.mu, P);
+                if (DAMP) {
+                    double Fd[3][3], Pv[3][3];
+    #pragma unroll
+                    for (int i = 0; i < 3; ++i)
+    #pragma unroll
+                        for (int j = 0; j < 3; ++j) Fd[i][j] = 0.0;
+    #pragma unroll
+                    for (int a = 0; a < NPE; ++a)
+    #pragma unroll
+                        for (int i = 0; i < 3; ++i)
+    #pragma unroll
+                            for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc[a] + i] * g[a][j];
+                    kelvin_voigt<double>(F, Fd, A.eta, A.lamd, Pv);
+    #pragma unroll
+                    for (int i = 0; i < 3; ++i)
+    #pragma unroll
+                        for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
+                }
+            }
+            // f_a += (P dV) grad_a   (FEAT10DataFunc.cuh:417-449)
+    #pragma unroll
+            for (int i = 0; i < 3; ++i)
+    #pragma unroll
+                for (int j = 0; j < 3; ++j) P[i][j] *= dv;
+    #pragma unroll
+            for (int a = 0; a < NPE; ++a)
+    #pragma unroll
+                for (int i = 0; i < 3; ++i) f[a][i] += P[i][0] * g[a][0] + P[i][1] * g[a][1] + P[i][2] * g[a][2];
+        }
+        __syncthreads();  // every thread is done with the stages the force table reuses
+    #pragma unroll
         for (int a = 0; a < NPE; ++a)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) f[a][i] += P[i][0] * g[a][0] + P[i][1] * g[a][1] + P[i][2] * g[a][2];
+    #pragma unroll
+            for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
+        __syncthreads();
     }
-    __syncthreads();  // every thread is done with the stages the force table reuses
-#pragma unroll
-    for (int a = 0; a < NPE; ++a)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
-    __syncthreads();
 
     for (int ln = t; ln < nl; ln += TE) {
         const int beg = ln ? iends[ln - 1] : 0;
@@ -709,18 +763,24 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, in
         if (NQP > 1) issue(1);
     }
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
+    double u0[3], v0[3] = {0.0, 0.0, 0.0};
+    tile_anchor(A, A.ln_gid[lb], u0);
+    if (DAMP && sizeof(R) == 4) {  // FP32: velocities relative to the anchor too
+        const int g0 = A.ln_gid[lb];
+        v0[0] = A.v[3 * g0 + 0];
+        v0[1] = A.v[3 * g0 + 1];
+        v0[2] = A.v[3 * g0 + 2];
+    }
     for (int ln = t; ln < nl; ln += TE) {
         const int gid = A.ln_gid[lb + ln];
         const int ps = A.ln_pslot[lb + ln];
         iends[ln] = A.ln_inc_end[lb + ln];
         dsts[ln] = (ps < 0) ? gid : -(ps + 1);
-        xs[ln] = A.px[gid];
-        ys[ln] = A.py[gid];
-        zs[ln] = A.pz[gid];
+        stage_pos(A, gid, u0, xs[ln], ys[ln], zs[ln]);
         if (DAMP) {
-            vs[3 * ln + 0] = A.v[3 * gid + 0];
-            vs[3 * ln + 1] = A.v[3 * gid + 1];
-            vs[3 * ln + 2] = A.v[3 * gid + 2];
+            vs[3 * ln + 0] = A.v[3 * gid + 0] - v0[0];
+            vs[3 * ln + 1] = A.v[3 * gid + 1] - v0[1];
+            vs[3 * ln + 2] = A.v[3 * gid + 2] - v0[2];
         }
     }
     __syncthreads();  // positions and node tables staged; barriers initialised

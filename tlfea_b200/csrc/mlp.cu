@@ -555,7 +555,7 @@ int tlfea_mlp_create(int n_layers, const int* dims, int max_batch, unsigned long
 
 int tlfea_mlp_destroy(tlfea_mlp m) {
     CHECK_MLP(m);
-    cudaSetDevice(m->device);
+    TLFEA_CUDA(cudaSetDevice(m->device));
     if (m->stream) cudaStreamSynchronize(m->stream);
     for (auto* v : {&m->W, &m->b, &m->mW, &m->vW, &m->mb, &m->vb, &m->gW, &m->gb, &m->Z})
         for (auto& p : *v) dfree(p);

@@ -38,7 +38,7 @@ static int zero_first_order(tlfea_solver_s* s, bool all) {
 static int create_first_order(tlfea_element e, int n_constraints, int kind, tlfea_solver* out) {
     if (!e || !out || n_constraints < 0) return TLFEA_INVALID_ARG;
     *out = nullptr;
-    cudaSetDevice(e->device);
+    TLFEA_CUDA(cudaSetDevice(e->device));
     tlfea_solver_s* s = new tlfea_solver_s();
     s->kind = kind;
     s->el = e;
@@ -88,7 +88,7 @@ int tlfea_linear_static_create(tlfea_element e, double tol, int max_iter, tlfea_
 
 int tlfea_solver_destroy(tlfea_solver s) {
     if (!s) return TLFEA_INVALID_ARG;
-    cudaSetDevice(s->device);
+    TLFEA_CUDA(cudaSetDevice(s->device));
     if (s->kind == KIND_LINEAR_STATIC)
         linear_static_free(s);
     else
@@ -99,14 +99,14 @@ int tlfea_solver_destroy(tlfea_solver s) {
 
 int tlfea_solver_setup(tlfea_solver s) {
     if (!s) return TLFEA_INVALID_ARG;
-    cudaSetDevice(s->device);
+    TLFEA_CUDA(cudaSetDevice(s->device));
     if (s->kind == KIND_LINEAR_STATIC) return TLFEA_OK;
     return zero_first_order(s, true);
 }
 
 int tlfea_solver_set_parameters(tlfea_solver s, const void* params) {
     if (!s) return TLFEA_INVALID_ARG;
-    cudaSetDevice(s->device);
+    TLFEA_CUDA(cudaSetDevice(s->device));
     if (s->kind == KIND_LINEAR_STATIC) return TLFEA_OK;
     if (!params) return TLFEA_INVALID_ARG;
     if (s->kind == KIND_NESTEROV)
@@ -119,7 +119,7 @@ int tlfea_solver_set_parameters(tlfea_solver s, const void* params) {
 
 int tlfea_solver_solve(tlfea_solver s) {
     if (!s) return TLFEA_INVALID_ARG;
-    cudaSetDevice(s->device);
+    TLFEA_CUDA(cudaSetDevice(s->device));
     if (s->kind == KIND_LINEAR_STATIC) return linear_static_solve(s);
     return first_order_solve(s);
 }
@@ -131,7 +131,7 @@ int tlfea_solver_run_steps(tlfea_solver s, int n_steps, double t0, const double*
         set_error("run_steps: the linear static solver has no time steps");
         return TLFEA_INVALID_ARG;
     }
-    cudaSetDevice(s->device);
+    TLFEA_CUDA(cudaSetDevice(s->device));
     if (!s->el->is_setup) {
         set_error("element must be set up first");
         return TLFEA_NOT_SETUP;
@@ -170,7 +170,7 @@ int tlfea_linear_static_last(tlfea_solver s, int* iters, double* rel_residual) {
 
 int tlfea_linear_static_retrieve_k(tlfea_solver s, long long* nnz, int* offsets, int* columns, double* values) {
     if (!s || s->kind != KIND_LINEAR_STATIC) return TLFEA_INVALID_ARG;
-    cudaSetDevice(s->device);
+    TLFEA_CUDA(cudaSetDevice(s->device));
     return linear_static_retrieve_k(s, nnz, offsets, columns, values);
 }
 
@@ -182,14 +182,14 @@ int tlfea_linear_static_set_preconditioner(tlfea_solver s, int kind) {
 
 int tlfea_linear_static_apply(tlfea_solver s, const double* d_x, double* d_y) {
     if (!s || s->kind != KIND_LINEAR_STATIC || !d_x || !d_y) return TLFEA_INVALID_ARG;
-    cudaSetDevice(s->device);
+    TLFEA_CUDA(cudaSetDevice(s->device));
     return linear_static_apply(s, d_x, d_y);
 }
 
 int tlfea_solver_get_velocity(tlfea_solver s, double* v_guess, double* v_prev, int n) {
     if (!s || s->kind == KIND_LINEAR_STATIC) return TLFEA_INVALID_ARG;
     if (n != 3 * s->el->N) return TLFEA_SIZE_MISMATCH;
-    cudaSetDevice(s->device);
+    TLFEA_CUDA(cudaSetDevice(s->device));
     TLFEA_CUDA(cudaStreamSynchronize(s->el->stream));
     if (v_guess) TLFEA_CUDA(cudaMemcpy(v_guess, s->v_guess, sizeof(double) * n, cudaMemcpyDeviceToHost));
     if (v_prev) TLFEA_CUDA(cudaMemcpy(v_prev, s->v_prev, sizeof(double) * n, cudaMemcpyDeviceToHost));
@@ -199,7 +199,7 @@ int tlfea_solver_get_velocity(tlfea_solver s, double* v_guess, double* v_prev, i
 int tlfea_solver_set_velocity(tlfea_solver s, const double* v_guess, const double* v_prev, int n) {
     if (!s || s->kind == KIND_LINEAR_STATIC) return TLFEA_INVALID_ARG;
     if (n != 3 * s->el->N) return TLFEA_SIZE_MISMATCH;
-    cudaSetDevice(s->device);
+    TLFEA_CUDA(cudaSetDevice(s->device));
     TLFEA_CUDA(cudaStreamSynchronize(s->el->stream));
     cudaStream_t st = s->el->stream;
     if (v_guess) TLFEA_CUDA(cudaMemcpyAsync(s->v_guess, v_guess, sizeof(double) * n, cudaMemcpyHostToDevice, st));
@@ -212,7 +212,7 @@ int tlfea_solver_get_multipliers(tlfea_solver s, double* lam, int n) {
     if (!s || s->kind == KIND_LINEAR_STATIC || !lam) return TLFEA_INVALID_ARG;
     if (n != s->n_constraints) return TLFEA_SIZE_MISMATCH;
     if (n == 0) return TLFEA_OK;
-    cudaSetDevice(s->device);
+    TLFEA_CUDA(cudaSetDevice(s->device));
     TLFEA_CUDA(cudaStreamSynchronize(s->el->stream));
     TLFEA_CUDA(cudaMemcpy(lam, s->lam, sizeof(double) * n, cudaMemcpyDeviceToHost));
     return TLFEA_OK;
