@@ -376,6 +376,51 @@ int tlfea_mlp_adamw_step(tlfea_mlp m, float lr, float beta1, float beta2, float 
 int tlfea_mlp_train_step(tlfea_mlp m, const float* d_x, const float* d_target, int batch, float lr, float beta1,
                          float beta2, float eps, float weight_decay, float* loss);
 int tlfea_mlp_sync(tlfea_mlp m);
+/* ------------------------------------------- batched time-stepping sequences
+ *
+ * New, no reference counterpart in this form: B sequences of implicit time steps on
+ * one mesh, each step solved by SyncedNesterov's iteration (SyncedNesterov.cu:97-360:
+ * the outer augmented-Lagrangian loop around the inner Nesterov loop, with the
+ * inertia M (v - v_prev) / dt), all sequences in the same kernels.  The mesh element
+ * (Setup, CalcDnDuPre, CalcMassMatrix, SetNodalFixed, SVK, density, damping and its
+ * external force -- e.g. gravity via add_gravity -- already set) is shared; each
+ * sequence has its own E, nu, step size and state, starting at rest in the reference
+ * configuration.  A sequence's inner loop ends when ||g_free|| / ||f_ext|| < rel_tol
+ * (g: the step's gradient, inertia + internal - external force + constraint terms;
+ * free = not fixed) or after max_inner iterations (rel_tol = 0: always max_inner, the
+ * reference's iteration with zero inner tolerance); its outer loop ends when the rule
+ * was met or ||c|| < outer_tol, or after max_outer iterations. */
+typedef struct tlfea_dynbatch_s* tlfea_dynbatch;
+int tlfea_dynbatch_create(tlfea_element mesh, int n_seq, tlfea_dynbatch* out);
+int tlfea_dynbatch_destroy(tlfea_dynbatch b);
+/* Per-sequence E and nu (n_seq each); mu and lambda as SetSVK(E, nu) (FEAT10Data.cuh:553-569). */
+int tlfea_dynbatch_set_material(tlfea_dynbatch b, const double* E, const double* nu);
+/* SyncedNesterovParams (inner_tol unused: the stop rule above ends the inner loop). */
+int tlfea_dynbatch_set_parameters(tlfea_dynbatch b, const tlfea_nesterov_params* p, double rel_tol);
+/* Per-sequence step sizes alpha (n_seq, each > 0), after set_parameters (which gives
+ * every sequence p->alpha). */
+int tlfea_dynbatch_set_step_sizes(tlfea_dynbatch b, const double* alpha);
+/* Time-varying load: f_ext(t) = f_base + amp * sin(omega * t + phase) * f_var at the end
+ * time t = k dt of step k, computed on the device; f_base = the element's f_ext when the
+ * batch was created.  f_var: host, n = 3N (NULL: zero). */
+int tlfea_dynbatch_set_load(tlfea_dynbatch b, const double* f_var, int n, double amp, double omega, double phase);
+/* Inner iterations per CUDA-graph replay (default 8). */
+int tlfea_dynbatch_set_chunk(tlfea_dynbatch b, int chunk);
+/* Every sequence back to rest in the reference configuration, t = 0. */
+int tlfea_dynbatch_reset(tlfea_dynbatch b);
+/* One implicit step of every sequence.  warm_start: 0 = the previous step's velocity
+ * (the reference's behaviour), 1 = linear extrapolation 2 v_n - v_(n-1), 2 = d_v_guess
+ * (device, n_seq x 3N interleaved).  iters, rel, converged: host arrays of n_seq (or
+ * NULL): inner iterations of the step, the last relative residual, 1 if the stop rule
+ * ended it. */
+int tlfea_dynbatch_step(tlfea_dynbatch b, int warm_start, const double* d_v_guess, int* iters, double* rel,
+                        int* converged);
+/* Device pointers of the state: positions (n_seq x N per component), the velocity
+ * (n_seq x 3N) and the previous step's velocity. */
+int tlfea_dynbatch_device_ptrs(tlfea_dynbatch b, double** x, double** y, double** z, double** v, double** v_hist);
+int tlfea_dynbatch_retrieve_positions(tlfea_dynbatch b, int seq, double* x, double* y, double* z);
+int tlfea_dynbatch_retrieve_velocity(tlfea_dynbatch b, int seq, double* v);
+
 /* The MLP's tensor-core product on its own: d_d[M x N] (FP32, leading dim ldd)
  * = d_a[M x K] (BF16, lda) * d_b[N x K]^T (BF16, ldb) + d_bias[N] (or NULL).
  * N and K multiples of 16, lda and ldb multiples of 8. */

@@ -1,0 +1,152 @@
+"""Batched time-stepping sequences (tlfea_dynbatch_*, BatchedDynamics): B sequences on
+one mesh, each implicit step solved by the SyncedNesterov iteration, against the
+oracle's SyncedNesterov restatement run sequence by sequence.
+
+With zero tolerances both run the same number of iterations (max_outer x max_inner per
+step), so each sequence's trajectory compares at the FP64 parity tolerance (the
+multipliers, rho = 1e14, amplify rounding into the velocities as in the single-solver
+tests).  With the stop rule on, the residual each sequence reports is checked against one
+recomputed from the oracle's mass matrix and internal force at its final state."""
+import numpy as np
+import pytest
+
+import tlfea_b200 as T
+from oracle import oracle as O
+from tlfea_b200 import mesh as M
+
+from .helpers import box, make_element, rel
+
+pytestmark = pytest.mark.gpu
+
+RHO = 1000.0
+FIXED = (1.0e-8, 1e14, 0.0, 0.0, 2, 40, 1.0e-3)
+
+
+def _mesh(cells=(10, 2, 2), order=10, load=(0.0, 0.0, -100.0)):
+    x, y, z, conn = box(*cells, order)
+    fixed, f, tip = M.cantilever_loads(x, y, z, load)
+    return x, y, z, conn, fixed, f, tip
+
+
+def _batch(x, y, z, conn, fixed, f, E, nu, params, rel_tol=0.0, lamd=0.0):
+    el = make_element(x, y, z, conn, E_mod=float(E[0]), nu=float(nu[0]), rho=RHO, fixed=fixed, f_ext=f, lamd=lamd)
+    b = T.BatchedDynamics(el, len(E))
+    b.SetMaterial(E, nu)
+    b.SetParameters(T.SyncedNesterovParams(*params), rel_tol)
+    return el, b
+
+
+@pytest.mark.parametrize("lamd", [0.0, 0.1])
+def test_fixed_iterations_match_the_oracle_per_sequence(lamd):
+    x, y, z, conn, fixed, f, _ = _mesh()
+    E = np.array([1e7, 3e6, 2.5e7])
+    nu = np.array([0.3, 0.25, 0.4])
+    el, b = _batch(x, y, z, conn, fixed, f, E, nu, FIXED, lamd=lamd)
+    models = [O.OracleModel(x, y, z, conn, E[s], nu[s], RHO, fixed, f, 0.0, lamd) for s in range(len(E))]
+    for m in models:
+        m.set_parameters()
+    X0 = np.stack([x, y, z])
+    for step in range(2):
+        it, res, conv = b.Step(T.BatchedDynamics.WARM_PREVIOUS)
+        assert list(it) == [80, 80, 80] and not conv.any()
+        for s, m in enumerate(models):
+            m.nesterov_solve(*FIXED)
+            pos = np.stack(b.RetrievePositions(s))
+            ref = np.stack([m.x, m.y, m.z])
+            assert rel(pos - X0, ref - X0) < 1e-11, (step, s, rel(pos - X0, ref - X0))
+            assert rel(b.RetrieveVelocity(s), m.v_guess) < 1e-8
+    b.Destroy()
+    el.Destroy()
+
+
+def test_time_varying_load_matches_the_oracle():
+    """f_ext(t_k) = f_base + amp sin(omega t_k + phase) f_var, evaluated on the device at
+    t_k = k dt, against the same load set on the oracle step by step (TET4 mesh)."""
+    x, y, z, conn, fixed, f0, tip = _mesh(order=4)
+    f_var = np.zeros(3 * len(x))
+    f_var[3 * tip + 2] = -50.0 / len(tip)
+    E, nu = np.array([1e7, 5e6]), np.array([0.3, 0.35])
+    el, b = _batch(x, y, z, conn, fixed, f0, E, nu, FIXED)
+    amp, omega, phase = 1.0, 2 * np.pi * 5.0, 0.3
+    b.SetLoad(f_var, amp, omega, phase)
+    models = [O.OracleModel(x, y, z, conn, E[s], nu[s], RHO, fixed, f0) for s in range(2)]
+    for m in models:
+        m.set_parameters()
+    X0 = np.stack([x, y, z])
+    for k in range(1, 4):
+        b.Step(0)
+        fk = f0 + (amp * np.sin(omega * (k * FIXED[6]) + phase)) * f_var
+        for s, m in enumerate(models):
+            m.f_ext[:] = fk
+            m.nesterov_solve(*FIXED)
+            pos = np.stack(b.RetrievePositions(s))
+            assert rel(pos - X0, np.stack([m.x, m.y, m.z]) - X0) < 1e-11
+    b.Destroy()
+    el.Destroy()
+
+
+def _hessian_lmax(x, y, z, conn, fixed, E, nu, dt, rho_alm, iters=200):
+    """Largest eigenvalue of the step's Hessian M/dt + dt K (+ dt^2 rho on fixed DOFs)."""
+    import scipy.sparse as sp
+
+    m = O.OracleModel(x, y, z, conn, E, nu, RHO, fixed, np.zeros(3 * len(x)))
+    off, cols, vals = O.stiffness(x, y, z, conn, m.grad, m.detJ, m.lam, m.mu)
+    K = sp.csr_matrix((vals, cols, off))
+    Mf = sp.kron(sp.csr_matrix((m.m_val, m.m_col, m.m_off)), sp.identity(3)).tocsr()
+    d = np.zeros(3 * len(x))
+    for n in fixed:
+        d[3 * n:3 * n + 3] = dt * dt * rho_alm
+    H = Mf / dt + dt * K + sp.diags(d)
+    v = np.random.default_rng(0).standard_normal(H.shape[0])
+    for _ in range(iters):
+        v = H @ v
+        v /= np.linalg.norm(v)
+    return float(v @ (H @ v))
+
+
+def _step_residual(x, y, z, conn, fixed, f, E, nu, xs, v, v_prev, dt):
+    """||g_free|| / ||f_ext|| of a step from the oracle's pieces: g = M (v - v_prev) / dt +
+    f_int(x) - f_ext (the constraint term is zero on free DOFs)."""
+    import scipy.sparse as sp
+
+    m = O.OracleModel(x, y, z, conn, E, nu, RHO, fixed, f)
+    fi = O.force(*xs, conn, m.grad, m.detJ, m.lam, m.mu)
+    Mn = sp.csr_matrix((m.m_val, m.m_col, m.m_off))
+    g = (Mn @ (v - v_prev).reshape(-1, 3)).ravel() / dt + fi - f
+    free = np.ones(len(x), bool)
+    free[fixed] = False
+    return np.linalg.norm(g.reshape(-1, 3)[free]) / np.linalg.norm(f)
+
+
+def test_stop_rule_ends_each_sequence_at_a_checked_residual():
+    x, y, z, conn, fixed, f, _ = _mesh()
+    E, nu = np.array([1e7, 2e6]), np.array([0.3, 0.3])
+    dt, rho_alm = 1e-3, 1e8
+    alphas = [0.9 / _hessian_lmax(x, y, z, conn, fixed, E[s], nu[s], dt, rho_alm) for s in range(2)]
+    params = (alphas[0], rho_alm, 0.0, 1e-300, 1, 20000, dt)
+    el, b = _batch(x, y, z, conn, fixed, f, E, nu, params, rel_tol=1e-6)
+    b.SetStepSizes(alphas)
+    vprev = [np.zeros(3 * len(x)) for _ in E]
+    for step in range(2):
+        it, res, conv = b.Step(T.BatchedDynamics.WARM_LINEAR if step else 0)
+        assert conv.all() and (res < 1e-6).all() and (it < 20000).all(), (it, res, conv)
+        for s in range(len(E)):
+            xs = b.RetrievePositions(s)
+            vs = b.RetrieveVelocity(s)
+            r = _step_residual(x, y, z, conn, fixed, f, E[s], nu[s], xs, vs, vprev[s], dt)
+            assert abs(r - res[s]) <= 1e-6 * r + 1e-13, (r, res[s])
+            vprev[s] = vs
+    # a given warm start: the converged first-step velocities end a fresh first step at its
+    # first residual evaluation
+    import torch
+
+    b.Reset()
+    b.Step(0)
+    v1 = np.concatenate([b.RetrieveVelocity(s) for s in range(len(E))])
+    guess = torch.tensor(v1, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    b.Reset()
+    it, res, conv = b.Step(T.BatchedDynamics.WARM_GIVEN, guess.data_ptr())
+    assert conv.all() and list(it) == [1] * len(E), (it, res)
+    b.Destroy()
+    el.Destroy()

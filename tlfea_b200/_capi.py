@@ -143,6 +143,18 @@ _SIGS = {
     "tlfea_batch_create_shared": [C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, _D, _D, C.c_int, _D, _D, _D, _I,
                                   C.POINTER(_P)],
     "tlfea_batch_destroy": [_P],
+    "tlfea_dynbatch_create": [_P, C.c_int, C.POINTER(_P)],
+    "tlfea_dynbatch_destroy": [_P],
+    "tlfea_dynbatch_set_material": [_P, _D, _D],
+    "tlfea_dynbatch_set_parameters": [_P, _P, C.c_double],
+    "tlfea_dynbatch_set_step_sizes": [_P, _D],
+    "tlfea_dynbatch_set_load": [_P, _D, C.c_int, C.c_double, C.c_double, C.c_double],
+    "tlfea_dynbatch_set_chunk": [_P, C.c_int],
+    "tlfea_dynbatch_reset": [_P],
+    "tlfea_dynbatch_step": [_P, C.c_int, _P, _I, _D, _I],
+    "tlfea_dynbatch_device_ptrs": [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)],
+    "tlfea_dynbatch_retrieve_positions": [_P, C.c_int, _D, _D, _D],
+    "tlfea_dynbatch_retrieve_velocity": [_P, C.c_int, _D],
     "tlfea_batch_get_counts": [_P, _I, _I, _I, _I],
     "tlfea_batch_get_stream": [_P, C.POINTER(_P)],
     "tlfea_batch_set_material": [_P, _D, _D],

@@ -664,6 +664,84 @@ class BatchedLinearStaticSolver:
 
 # -------------------------------------------------------------------- manager
 
+class BatchedDynamics:
+    """New: B sequences of implicit time steps on one mesh, each step solved by the
+    SyncedNesterov iteration (SyncedNesterov.cu:97-360) in the same kernels for all
+    sequences (tlfea_dynbatch_* in include/tlfea_b200.h).  `mesh` is a set-up element
+    (Setup, CalcDnDuPre, CalcMassMatrix, fixed nodes, density, damping, external force
+    such as gravity); each sequence has its own E and nu."""
+
+    WARM_PREVIOUS, WARM_LINEAR, WARM_GIVEN = 0, 1, 2
+
+    def __init__(self, mesh: _TetData, n_seq: int):
+        self.mesh = mesh
+        self.n_seq = int(n_seq)
+        self.N = mesh.n_coef
+        h = C.c_void_p()
+        capi.call("tlfea_dynbatch_create", mesh._handle(), self.n_seq, C.byref(h))
+        self._h = h
+
+    def SetMaterial(self, E, nu):
+        E = _f64(E, self.n_seq, "E")
+        nu = _f64(nu, self.n_seq, "nu")
+        capi.call("tlfea_dynbatch_set_material", self._h, capi.dptr(E), capi.dptr(nu))
+
+    def SetParameters(self, params: SyncedNesterovParams, rel_tol: float = 0.0):
+        p = capi.NesterovParams(*astuple(params))
+        capi.call("tlfea_dynbatch_set_parameters", self._h, C.cast(C.byref(p), C.c_void_p), float(rel_tol))
+
+    def SetStepSizes(self, alpha):
+        a = _f64(alpha, self.n_seq, "alpha")
+        capi.call("tlfea_dynbatch_set_step_sizes", self._h, capi.dptr(a))
+
+    def SetLoad(self, f_var=None, amp: float = 0.0, omega: float = 0.0, phase: float = 0.0):
+        fv = None if f_var is None else _f64(f_var, 3 * self.N, "f_var")
+        capi.call("tlfea_dynbatch_set_load", self._h, capi.dptr(fv) if fv is not None else None, 3 * self.N,
+                  float(amp), float(omega), float(phase))
+
+    def SetChunk(self, chunk: int):
+        capi.call("tlfea_dynbatch_set_chunk", self._h, int(chunk))
+
+    def Reset(self):
+        capi.call("tlfea_dynbatch_reset", self._h)
+
+    def Step(self, warm_start: int = 0, d_v_guess: int | None = None):
+        """One step of every sequence; returns (iterations, relative residual, converged) per sequence."""
+        it = np.zeros(self.n_seq, np.int32)
+        rel = np.zeros(self.n_seq)
+        conv = np.zeros(self.n_seq, np.int32)
+        capi.call("tlfea_dynbatch_step", self._h, int(warm_start),
+                  C.c_void_p(d_v_guess) if d_v_guess is not None else None, capi.iptr(it), capi.dptr(rel),
+                  capi.iptr(conv))
+        return it, rel, conv
+
+    def DevicePtrs(self) -> dict:
+        ptrs = [C.c_void_p() for _ in range(5)]
+        capi.call("tlfea_dynbatch_device_ptrs", self._h, *[C.byref(p) for p in ptrs])
+        return dict(zip(("x", "y", "z", "v", "v_hist"), (p.value for p in ptrs)))
+
+    def RetrievePositions(self, seq: int):
+        x, y, z = (np.zeros(self.N) for _ in range(3))
+        capi.call("tlfea_dynbatch_retrieve_positions", self._h, int(seq), capi.dptr(x), capi.dptr(y), capi.dptr(z))
+        return x, y, z
+
+    def RetrieveVelocity(self, seq: int):
+        v = np.zeros(3 * self.N)
+        capi.call("tlfea_dynbatch_retrieve_velocity", self._h, int(seq), capi.dptr(v))
+        return v
+
+    def Destroy(self):
+        if getattr(self, "_h", None):
+            capi.call("tlfea_dynbatch_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.Destroy()
+        except Exception:
+            pass
+
+
 class FEASolver:
     """FEASolver (FEASolver.h:35-138): name -> non-owning element / solver registry."""
 
