@@ -564,6 +564,172 @@ def dynamics_leg(args, T):
             "tip_deflection_min_z": tip_z}
 
 
+def config5_leg(args, T):
+    """Configuration 5: 64 sequences on the 100x10x10 TET10 cantilever (60,000 elements,
+    88,641 nodes; SVK, rho = 1000, seeded E log-uniform in [3e6, 3e7] Pa and nu in
+    [0.25, 0.4]), clamped at x = 0, gravity 9.81 m/s^2 (consistent-mass row sums) plus a
+    50 sin(2 pi 5 t) N tip load in -z, implicit steps dt = 1e-3 each solved by the
+    SyncedNesterov iteration to ||g_free|| / ||f_ext|| < 1e-6, all 64 sequences batched in
+    the same kernels (BatchedDynamics).  Warm starts of each step compared from rest over
+    the same steps: the previous velocity (the reference's behaviour), linear
+    extrapolation, and the learned step predictor (an MLP correction of the linear
+    extrapolation, trained on the solver's own steps of 16 other seeded sequences).
+    Step size per sequence: 0.9 / lambda_max of the step Hessian M/dt + dt K_s
+    (+ dt^2 rho on fixed DOFs), lambda_max by a batched power iteration with this
+    library's K x and mass matrix."""
+    import torch
+    from tlfea_b200 import mesh as M
+    from tlfea_b200 import warmstart as W
+
+    dt, rho_alm, tol, omega = 1e-3, 1e8, 1e-6, 2 * np.pi * 5.0
+    n_eval, n_train = args.dyn_batch, 16
+    steps_eval, steps_train = args.dyn_eval_steps, args.dyn_train_steps
+    x, y, z, conn = M.box_mesh(100, 10, 10, 10, 1.0, 0.1, 0.1)
+    fixed, f_tip, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -50.0))
+    N, dof = len(x), 3 * len(x)
+    r = np.random.default_rng(5)
+    E_all = np.exp(r.uniform(np.log(3e6), np.log(3e7), n_eval + n_train))
+    nu_all = r.uniform(0.25, 0.4, n_eval + n_train)
+    el = T.GPU_FEAT10_Data(conn.shape[0], N)
+    el.Initialize()
+    el.SetNodalFixed(fixed)
+    el.SetExternalForce(np.zeros(dof))
+    el.Setup(*T.Quadrature.t10(), x, y, z, conn)
+    el.SetDensity(1000.0)
+    el.SetDamping(0.0, 0.0)
+    el.SetSVK(1e7, 0.3)
+    el.CalcDnDuPre()
+    el.CalcMassMatrix()
+    el.CalcConstraintData()
+    el.ConvertToCSR_ConstraintJacT()
+    el.AddGravity(0.0, 0.0, -9.81)
+
+    # lambda_max of M/dt + dt K_s over the free DOFs, every sequence at once
+    t0 = time.perf_counter()
+    moff, mcol, mval = el.RetrieveMassCSRToCPU()
+    Mn = torch.sparse_csr_tensor(torch.as_tensor(moff, dtype=torch.int64), torch.as_tensor(mcol, dtype=torch.int64),
+                                 torch.as_tensor(mval), size=(N, N)).to("cuda")
+    nb = n_eval + n_train
+    kb = T.BatchedLinearStaticSolver([(x, y, z, conn)] * nb, T.TYPE_T10, shared=True)
+    kb.SetMaterial(E_all, nu_all)
+    kb.SetNodalFixed([fixed] * nb)
+    free = torch.ones(N, 3, dtype=torch.float64, device="cuda")
+    free[torch.as_tensor(fixed, device="cuda")] = 0.0
+    free = free.reshape(-1)
+    X = torch.randn(nb, dof, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+    Y = torch.empty_like(X)
+    lmax = None
+    for _ in range(60):
+        X *= free
+        X /= X.norm(dim=1, keepdim=True)
+        torch.cuda.synchronize()
+        kb.Apply(int(X.data_ptr()), int(Y.data_ptr()))
+        MX = (Mn @ X.reshape(nb, N, 3).permute(1, 0, 2).reshape(N, nb * 3)).reshape(N, nb, 3).permute(1, 0, 2)
+        HX = (MX.reshape(nb, dof) / dt + dt * Y) * free
+        lmax = (HX * X).sum(1)
+        X = HX
+    kb.Destroy()
+    alpha_all = 0.9 / (lmax.cpu().numpy() + dt * dt * rho_alm)
+    t_alpha = time.perf_counter() - t0
+
+    params = T.SyncedNesterovParams(float(alpha_all.min()), rho_alm, 0.0, 1e-6, 3, 20000, dt)
+
+    def make(seqs):
+        b = T.BatchedDynamics(el, len(seqs))
+        b.SetMaterial(E_all[seqs], nu_all[seqs])
+        b.SetParameters(params, tol)
+        b.SetStepSizes(alpha_all[seqs])
+        f_var = np.zeros(dof)
+        f_var[:] = f_tip
+        b.SetLoad(f_var, 1.0, omega, 0.0)
+        b.SetChunk(16)
+        return b
+
+    def load_factors(n):  # (sin at t_(n-1), t_n, t_(n+1)), t_k = k dt
+        return np.array([[np.sin(omega * (n - 1 + j) * dt) for j in range(3)]])
+
+    X0 = torch.as_tensor(np.stack([x, y, z], 1).reshape(-1), device="cuda")
+
+    def state(b, B):
+        p = b.DevicePtrs()
+        v = W.device_view(p["v"], (B, dof))
+        vh = W.device_view(p["v_hist"], (B, dof))
+        xs = [W.device_view(p[k], (B, N)) for k in ("x", "y", "z")]
+        u = torch.stack(xs, 2).reshape(B, dof) - X0
+        return v, vh, u
+
+    # training data: the solver's own steps (linear extrapolation) on 16 other sequences
+    t0 = time.perf_counter()
+    tr = np.arange(n_eval, n_eval + n_train)
+    bt = make(tr)
+    V = torch.empty(n_train, steps_train, dof, dtype=torch.float64, device="cuda")
+    U = torch.empty_like(V)
+    it_train = []
+    for k in range(steps_train):
+        it, res, conv = bt.Step(T.BatchedDynamics.WARM_LINEAR)
+        it_train.append(it)
+        v, _, u = state(bt, n_train)
+        V[:, k] = v
+        U[:, k] = u
+    bt.Destroy()
+    loads_tr = np.concatenate([load_factors(n) for n in range(1, steps_train + 1)])
+    sp = W.StepPredictor(k_in=16, k_out=32, hidden=(256, 256), max_batch=128, seed=0, E_range=(3e6, 3e7),
+                         nu_range=(0.25, 0.4))
+    mats = sp.material_features(E_all, nu_all)
+    hist = sp.fit(V, U, loads_tr, mats[tr], epochs=args.dyn_epochs, batch=128)
+    del V, U
+    t_train = time.perf_counter() - t0
+
+    # evaluation: the 64 sequences from rest, the same steps with each warm start
+    ev = np.arange(n_eval)
+    b = make(ev)
+    out = {}
+    for name in ("previous", "linear", "learned"):
+        b.Reset()
+        torch.cuda.synchronize()
+        its, conv_all, t_guess = [], [], 0.0
+        t0 = time.perf_counter()
+        for n in range(1, steps_eval + 1):
+            if name == "previous":
+                it, res, conv = b.Step(T.BatchedDynamics.WARM_PREVIOUS)
+            elif name == "linear" or n == 1:
+                it, res, conv = b.Step(T.BatchedDynamics.WARM_LINEAR)
+            else:
+                tg = time.perf_counter()
+                v, vh, u = state(b, n_eval)
+                g = sp.predict(v, vh, u, np.repeat(load_factors(n - 1), n_eval, 0), mats[ev])
+                t_guess += time.perf_counter() - tg
+                it, res, conv = b.Step(T.BatchedDynamics.WARM_GIVEN, int(g.data_ptr()))
+            its.append(it)
+            conv_all.append(conv)
+        torch.cuda.synchronize()
+        dt_run = time.perf_counter() - t0
+        its = np.array(its)
+        out[name] = {"steps_per_s": round(steps_eval / dt_run, 3),
+                     "sequence_steps_per_s": round(n_eval * steps_eval / dt_run, 2),
+                     "inner_iters_mean": float(its.mean()), "inner_iters_per_step": its.mean(1).round(1).tolist(),
+                     "converged_fraction": float(np.mean(conv_all)), "seconds": round(dt_run, 3),
+                     "guess_seconds": round(t_guess, 3)}
+    b.Destroy()
+    sp.destroy()
+    el.Destroy()
+    base = out["previous"]["inner_iters_mean"]
+    return {"workload": f"configuration 5: {n_eval} sequences, 100x10x10 TET10 (60,000 elements, 88,641 nodes), "
+                        f"gravity + 50 sin(2 pi 5 t) N tip load, dt 1e-3, SyncedNesterov per step to rel. residual "
+                        f"{tol:g}, steps 1..{steps_eval} from rest with each warm start",
+            "value": out["learned"]["sequence_steps_per_s"], "unit": "sequence-steps/s",
+            "warm_starts": out,
+            "iteration_ratio_previous_over_linear": round(base / out["linear"]["inner_iters_mean"], 3),
+            "iteration_ratio_previous_over_learned": round(base / out["learned"]["inner_iters_mean"], 3),
+            "iteration_ratio_linear_over_learned": round(out["linear"]["inner_iters_mean"] /
+                                                         out["learned"]["inner_iters_mean"], 3),
+            "training": {"sequences": n_train, "steps": steps_train, "samples": n_train * (steps_train - 1),
+                         "epochs": args.dyn_epochs, "final_loss": float(hist[-1]), "seconds": round(t_train, 2),
+                         "train_inner_iters_mean": float(np.mean(it_train))},
+            "step_size": {"alpha_min": float(alpha_all.min()), "alpha_max": float(alpha_all.max()),
+                          "power_iteration_s": round(t_alpha, 2), "rho": rho_alm}}
+
+
 def learned_leg(args, T):
     """Learned warm start on the fixed 40 x 8 x 8 TET10 cantilever (1.0 x 0.1 x
     0.1 m): 4096 solver-generated training cases (E log-uniform 1e6..1e8, nu
@@ -695,6 +861,11 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
     ap.add_argument("--no-dynamics", action="store_true", help="skip the time-stepping leg")
     ap.add_argument("--dyn-steps", type=int, default=50, help="implicit steps of the time-stepping leg")
+    ap.add_argument("--no-config5", action="store_true", help="skip the configuration-5 batched sequences leg")
+    ap.add_argument("--dyn-batch", type=int, default=64, help="sequences of the configuration-5 leg")
+    ap.add_argument("--dyn-eval-steps", type=int, default=8, help="steps per warm start in the configuration-5 leg")
+    ap.add_argument("--dyn-train-steps", type=int, default=24, help="training steps of the step predictor")
+    ap.add_argument("--dyn-epochs", type=int, default=400, help="training epochs of the step predictor")
     ap.add_argument("--batch-size", type=int, default=512)
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "fp32"],
                     help="element work of the batched solves (the CG and its stop test stay FP64)")
@@ -855,6 +1026,8 @@ def main():
         out["learned"] = learned_leg(args, T)
     if not args.no_dynamics:
         out["dynamics"] = dynamics_leg(args, T)
+    if not args.no_config5:
+        out["config5"] = config5_leg(args, T)
     if rank == 0 and world == 1 and not args.no_gpu_ref:
         from oracle import ref_lib as R
 

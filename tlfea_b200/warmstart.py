@@ -133,7 +133,8 @@ class PCA:
         self.k = k
         self.coef_scale = coef_scale
 
-    def fit(self, W: np.ndarray):
+    def fit(self, W):
+        """W: snapshots (n, dof), numpy or a torch tensor on the GPU."""
         import torch
 
         Wd = torch.as_tensor(W, dtype=torch.float64, device="cuda")
@@ -158,6 +159,10 @@ class PCA:
 
         Wd = torch.as_tensor(W, dtype=torch.float64, device="cuda")
         return (((Wd - self.mean) @ self.modes - self.c_mean) / self.c_std).cpu().numpy()
+
+    def coefficients_t(self, Wd):
+        """Standardised coefficients of device rows (torch, FP64), kept on the GPU."""
+        return ((Wd - self.mean) @ self.modes - self.c_mean) / self.c_std
 
     def reconstruct(self, Cstd):
         """Standardised coefficients (n, k) -> normalised displacements (n, dof), on the GPU."""
@@ -300,3 +305,128 @@ class GalerkinWarmStart:
         u = c @ self.B
         torch.cuda.synchronize()
         return u
+
+
+# ---------------------------------------------------------------- time stepping
+
+class DeviceArray:
+    """A raw device pointer seen as a CUDA array (``__cuda_array_interface__``), so
+    torch can view the library's state without a copy."""
+
+    def __init__(self, ptr: int, shape, typestr: str = "<f8"):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def device_view(ptr: int, shape, dtype="float64"):
+    import torch
+
+    return torch.as_tensor(DeviceArray(ptr, shape, "<f8" if dtype == "float64" else "<f4"), device="cuda")
+
+
+class StepPredictor:
+    """Learned step predictor for batched time-stepping sequences (new): the next
+    step's velocity as the linear extrapolation of the last two plus a learned
+    correction,
+
+        v_(n+1) ~ 2 v_n - v_(n-1) + dv,   dv = mean + modes (c_std * MLP(features)),
+
+    where the modes are a PCA basis of the corrections the solver itself produced
+    on training sequences (its converged steps), and the MLP (WarmStartMLP: this
+    library's BF16 tcgen05 kernels, FP32 accumulation) maps per-sequence features
+    to the standardised coefficients.  Features: the coefficients of v_n, v_(n-1)
+    and the displacement u_n in PCA bases of the velocity and displacement
+    snapshots, the load factor at the last, this and the next step end times, and
+    the material (log10 E and nu, scaled to about [-1, 1]).  The guess only starts
+    the step's Nesterov iteration: the residual tolerance decides the answer."""
+
+    def __init__(self, k_in=16, k_out=32, hidden=(256, 256), max_batch=128, seed=0, E_range=(1e6, 1e8),
+                 nu_range=(0.2, 0.45)):
+        import torch
+
+        self.k_in, self.k_out = k_in, k_out
+        self.E_range, self.nu_range = E_range, nu_range
+        self.pca_v = PCA(k_in)
+        self.pca_u = PCA(k_in)
+        self.pca_d = PCA(k_out)
+        self.n_feat = 3 * k_in + 5
+        self.dims = [self.n_feat, *hidden, k_out]
+        self.net = WarmStartMLP(self.dims, max_batch=max_batch, seed=seed)
+        self.max_batch = max_batch
+        self.stream = torch.cuda.ExternalStream(self.net.GetStream())
+
+    def material_features(self, E, nu):
+        lo, hi = np.log10(self.E_range[0]), np.log10(self.E_range[1])
+        fe = 2.0 * (np.log10(E) - lo) / (hi - lo) - 1.0
+        fn = 2.0 * (np.asarray(nu) - self.nu_range[0]) / (self.nu_range[1] - self.nu_range[0]) - 1.0
+        return np.column_stack([fe, fn])
+
+    def _features(self, v_n, v_nm1, u_n, loads, mat):
+        """torch (B, n_feat) FP32 from FP64 device tensors (B, dof) and host arrays."""
+        import torch
+
+        a = torch.as_tensor(self.pca_v.coefficients_t(v_n))
+        b = torch.as_tensor(self.pca_v.coefficients_t(v_nm1))
+        c = torch.as_tensor(self.pca_u.coefficients_t(u_n))
+        extra = torch.as_tensor(np.column_stack([loads, mat]), dtype=torch.float64, device="cuda")
+        return torch.cat([a, b, c, extra], 1).float().contiguous()
+
+    def fit(self, V, U, loads, mats, epochs=600, batch=128, lr=1e-3, lr_final=1e-5, seed=0):
+        """V: (S, T, dof) velocities after steps 1..T of S training sequences (v_0 = 0),
+        U: (S, T, dof) displacements, loads: (T, 3) load factors at (t_(n-1), t_n, t_(n+1))
+        of the sample predicting step n+1, mats: (S, 2) material features.  Samples are the
+        steps n = 1..T-1 (v_(n-1) = 0 for n = 1).  Returns the training-loss history."""
+        import torch
+
+        S, Tn, dof = V.shape
+        Vd = torch.as_tensor(V, device="cuda")
+        Ud = torch.as_tensor(U, device="cuda")
+        Vprev = torch.cat([torch.zeros_like(Vd[:, :1]), Vd[:, :-1]], 1)
+        self.pca_v.fit(Vd.reshape(-1, dof))
+        self.pca_u.fit(Ud.reshape(-1, dof))
+        vn, vnm1, un = Vd[:, :-1], Vprev[:, :-1], Ud[:, :-1]
+        d = Vd[:, 1:] - 2.0 * vn + vnm1  # the correction to the linear extrapolation
+        Y = torch.as_tensor(self.pca_d.fit(d.reshape(-1, dof)), dtype=torch.float32, device="cuda")
+        L = np.repeat(loads[None, :-1], S, 0).reshape(-1, loads.shape[1])
+        Mt = np.repeat(mats[:, None, :], Tn - 1, 1).reshape(-1, mats.shape[1])
+        X = self._features(vn.reshape(-1, dof), vnm1.reshape(-1, dof), un.reshape(-1, dof), L, Mt)
+        n = X.shape[0] - X.shape[0] % batch
+        if n == 0:
+            raise ValueError("fewer training samples than one batch")
+        r = np.random.default_rng(seed)
+        hist, steps, k = [], epochs * (n // batch), 0
+        torch.cuda.synchronize()
+        with torch.cuda.stream(self.stream):
+            for ep in range(epochs):
+                perm = torch.as_tensor(r.permutation(X.shape[0])[:n], device="cuda")
+                Xs, Ys = X[perm].contiguous(), Y[perm].contiguous()
+                tot = 0.0
+                for b in range(n // batch):
+                    a = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / max(steps, 1)))
+                    want = (b == n // batch - 1)
+                    l = self.net.TrainStep(Xs[b * batch:(b + 1) * batch].data_ptr(),
+                                           Ys[b * batch:(b + 1) * batch].data_ptr(), batch, lr=float(a),
+                                           want_loss=want)
+                    if want:
+                        tot = l
+                    k += 1
+                hist.append(tot)
+        self.stream.synchronize()
+        return hist
+
+    def predict(self, v_n, v_nm1, u_n, loads, mat):
+        """Velocity guesses (B, dof) FP64 on the GPU for the next step, complete on return."""
+        import torch
+
+        with torch.cuda.stream(self.stream):
+            X = self._features(v_n, v_nm1, u_n, loads, mat)
+            out = torch.empty(X.shape[0], self.k_out, device="cuda")
+            for b in range(0, X.shape[0], self.max_batch):
+                m = min(self.max_batch, X.shape[0] - b)
+                self.net.Forward(X[b:b + m].data_ptr(), m, out[b:b + m].data_ptr())
+            g = 2.0 * v_n - v_nm1 + self.pca_d.reconstruct(out.double())
+        self.stream.synchronize()
+        return g.contiguous()
+
+    def destroy(self):
+        self.net.Destroy()
