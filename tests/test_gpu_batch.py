@@ -278,3 +278,24 @@ def test_shared_mesh_single_instance_and_fp32_refinement():
         assert rel(bs.RetrieveDisplacement(split=False), ug) < 1e-6
         bs.Destroy()
         bg.Destroy()
+
+
+def test_configuration3_batch_sample_matches_oracle_inside_the_full_launch():
+    """The benchmark's 512 seeded uneven cantilevers (nx ~ U{8..64}, ny = nz ~ U{2..8})
+    in one launch, stopped after exactly 25 CG iterations; 8 instances spread over the
+    batch (the largest among them) against the oracle CG at the same count."""
+    insts = [M.random_beam(s) for s in range(512)]
+    b = _batch(insts)
+    b.Solve(1e-300, 25)
+    it, res, st = b.GetResults()
+    assert np.all(it == 25)
+    us = b.RetrieveDisplacement()
+    sizes = np.array([len(d["x"]) for d in insts])
+    picks = sorted(set(np.linspace(0, 511, 7).astype(int).tolist() + [int(np.argmax(sizes))]))
+    for k in picks:
+        d = insts[k]
+        off, cols, kv, fb = _oracle_kbc(d)
+        u_ref, it_ref, res_ref, rc = O.cg(off, cols, kv, fb, 0.0, 25)
+        assert it_ref == 25
+        assert rel(us[k], u_ref) < 1e-9, (k, rel(us[k], u_ref))
+    b.Destroy()

@@ -151,3 +151,45 @@ def test_solver_requires_parameters_and_mass():
     with pytest.raises(T.TLFEAError):
         s.Solve()  # no CalcMassMatrix
     el.Destroy()
+
+
+def test_configuration5_mesh_first_order_steps_match_oracle():
+    """The 100x10x10 TET10 cantilever of configuration 5 (88,641 nodes): two
+    SyncedNesterov and two SyncedAdamW steps at fixed iteration counts against the oracle,
+    in FP64 (and the batched sequences' kernels on two sequences)."""
+    x, y, z, conn = box(100, 10, 10, 10)
+    fixed, f, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -50.0))
+    X0 = np.stack([x, y, z])
+    nes = (1.0e-8, 1e14, 0.0, 0.0, 1, 6, 1.0e-3)
+    adw = list(ADAMW)
+    adw[3], adw[6], adw[7], adw[8], adw[9], adw[10] = 1.0, 0.0, 0.0, 1e4, 1, 6
+    for kind, params in (("nesterov", nes), ("adamw", tuple(adw))):
+        el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
+        s = (T.SyncedNesterovSolver if kind == "nesterov" else T.SyncedAdamWSolver)(el, el.get_n_constraint())
+        s.Setup()
+        s.SetParameters(T.SyncedNesterovParams(*params) if kind == "nesterov" else T.SyncedAdamWParams(*params))
+        m = O.OracleModel(x, y, z, conn, E_MOD, NU, RHO, fixed, f)
+        m.set_parameters()
+        for _ in range(2):
+            s.Solve()
+            m.nesterov_solve(*params) if kind == "nesterov" else m.adamw_solve(*params)
+        pos = np.stack(el.RetrievePositionToCPU())
+        assert rel(pos - X0, np.stack([m.x, m.y, m.z]) - X0) < 1e-10, kind
+        del s
+        el.Destroy()
+    el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
+    b = T.BatchedDynamics(el, 2)
+    b.SetMaterial([E_MOD, 2 * E_MOD], [NU, NU])
+    b.SetParameters(T.SyncedNesterovParams(*nes), 0.0)
+    ms = [O.OracleModel(x, y, z, conn, e, NU, RHO, fixed, f) for e in (E_MOD, 2 * E_MOD)]
+    for m in ms:
+        m.set_parameters()
+    for _ in range(2):
+        b.Step(0)
+        for m in ms:
+            m.nesterov_solve(*nes)
+    for k, m in enumerate(ms):
+        pos = np.stack(b.RetrievePositions(k))
+        assert rel(pos - X0, np.stack([m.x, m.y, m.z]) - X0) < 1e-10
+    b.Destroy()
+    el.Destroy()
