@@ -8,10 +8,12 @@ constraint arrays, the stiffness with Dirichlet BCs, CG iterates after 25 iterat
 at convergence, and SyncedNesterov / SyncedAdamW / SyncedAdamWNocoop trajectories; for
 the configuration-2 meshes, norms, seeded projections and samples of the long vectors.
 
-Bars: FP64 rel 1e-10 for results (1e-12 for element arrays, which differ only by the
-reference's atomicAdd summation order); FP32 force mode rel 1e-5; integer patterns
-bit-exact.  Converged CG solutions (two different rounding sequences stopped at the same
-relative residual) compare at 1e-7, iteration counts within 1%.
+Bars: FP64 rel 1e-12 for forces, mass and stiffness (they differ only by summation
+order), 1e-11 for P (small-strain cancellation); FP32 force mode rel 1e-5; integer
+patterns bit-exact.  Iterative results use the bars of ``test_ref_fixtures.py``, calibrated
+on each case: max(1e-10, 3 x the oracle's own sensitivity to a 1e-15 input perturbation)
+(the 1e-10 of the parity contract wherever the iteration does not amplify rounding beyond
+it); converged CG solutions compare at 1e-7 with iteration counts within 5%.
 """
 import sys
 from pathlib import Path
@@ -26,7 +28,9 @@ sys.path.insert(0, str(HERE / "golden"))
 import ref_cases as RC  # noqa: E402
 
 from .helpers import make_element, rel  # noqa: E402
-from .test_ref_fixtures import first_order_runs, load  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+from .test_ref_fixtures import (cg25_bar, cg_iteration_bar, first_order_bars, first_order_runs, load,  # noqa: E402
+                                run_inputs)
 
 pytestmark = pytest.mark.gpu
 TOL32 = 1e-5
@@ -71,7 +75,7 @@ def test_force_matches_reference(name):
     check_long(name, "f_int", el.RetrieveInternalForceToCPU(), fx, 1e-12)
     if "P" in fx:
         P = el.RetrievePFromFToCPU()  # (E, QP, 3, 3) -> reference layout i + 3j
-        assert rel(P.transpose(0, 1, 3, 2).ravel(), fx["P"]) < 1e-13
+        assert rel(P.transpose(0, 1, 3, 2).ravel(), fx["P"]) < 1e-11
     el.Destroy()
 
 
@@ -103,6 +107,14 @@ def test_linear_static_matches_reference(name):
     c = RC.case(name)
     tol = 1e-6 if name in RC.LARGE else 1e-10
     X0 = np.stack([c["x"], c["y"], c["z"]])
+    bar25 = 1e-10
+    if name in RC.SMALL:
+        lam = c["E"] * c["nu"] / ((1 + c["nu"]) * (1 - 2 * c["nu"]))
+        mu = c["E"] / (2 * (1 + c["nu"]))
+        g, dj = O.dndu_pre(c["x"], c["y"], c["z"], c["conn"])
+        off, cols, vals = O.stiffness(c["x"], c["y"], c["z"], c["conn"], g, dj, lam, mu)
+        kv, fb = O.apply_bcs(off, cols, vals, c["f"], c["fixed"])
+        bar25 = cg25_bar(off, cols, kv, fb)
     el = element(c, mass=False)
     for tag, max_iter in (("cg25", 25), ("cg", 200000)):
         el.ResetPositions()
@@ -113,14 +125,14 @@ def test_linear_static_matches_reference(name):
         it_ref = int(fx[f"{tag}_iters"][0])
         if tag == "cg25":
             assert it == it_ref == 25
-            check_long(name, "u_cg25", u, fx, 1e-10)
+            check_long(name, "u_cg25", u, fx, bar25)
             if "K_val" in fx:
                 off, cols, vals = s.RetrieveStiffnessCSRToCPU()
                 assert np.array_equal(off, fx["K_off"]) and np.array_equal(cols, fx["K_col"])
                 assert rel(vals, fx["K_val"]) < 1e-12
         else:
-            assert abs(it - it_ref) <= max(2, 0.01 * it_ref), (it, it_ref)
             check_long(name, "u_cg", u, fx, 1e-7 if name not in RC.LARGE else 1e-5)
+            assert abs(it - it_ref) <= cg_iteration_bar(it_ref), (it, it_ref)
         del s
     el.Destroy()
 
@@ -130,12 +142,9 @@ def test_first_order_solvers_match_reference(name):
     fx = load(name)
     c = RC.case(name)
     X0 = np.stack([c["x"], c["y"], c["z"]])
-    for tag, kind, params, steps, load_kind, tol_x, tol_v in first_order_runs(name):
-        fixed, f, lamd = c["fixed"], c["f"], 0.0
-        if load_kind == "generic":
-            fixed, f = RC.generic_load(c)
-        elif load_kind == "damped":
-            lamd = 0.1
+    for tag, kind, params, steps, load_kind in first_order_runs(name):
+        fixed, f, lamd = run_inputs(c, load_kind)
+        tol_x, tol_v = first_order_bars(c, kind, params, steps, fixed, f, lamd)
         el = element(c, fixed=fixed, f=f, lamd=lamd)
         cls = {"nesterov": T.SyncedNesterovSolver, "adamw": T.SyncedAdamWSolver,
                "nocoop": T.SyncedAdamWNocoopSolver}[kind]
@@ -147,8 +156,7 @@ def test_first_order_solvers_match_reference(name):
             s.Solve()
             pos = np.stack(el.RetrievePositionToCPU())
             assert rel(pos - X0, ref[k] - X0) < tol_x, (tag, k, rel(pos - X0, ref[k] - X0))
-        if tol_v is not None:
-            vg, _ = s.GetVelocity()
-            assert rel(vg, fx[f"{tag}_v"]) < tol_v, (tag, rel(vg, fx[f"{tag}_v"]))
+        vg, _ = s.GetVelocity()
+        assert rel(vg, fx[f"{tag}_v"]) < tol_v, (tag, rel(vg, fx[f"{tag}_v"]), tol_v)
         del s
         el.Destroy()

