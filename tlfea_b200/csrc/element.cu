@@ -213,6 +213,17 @@ __global__ void k_add_gravity(int N, const int* __restrict__ off, const double* 
     f[3 * i + 2] += s * gz;
 }
 
+// u64[3i + d] = x_d[i] - X0_d[i], node order (coalesced).
+__global__ void k_disp64(int n, const double* __restrict__ x, const double* __restrict__ y,
+                         const double* __restrict__ z, const double* __restrict__ X0x, const double* __restrict__ X0y,
+                         const double* __restrict__ X0z, double* __restrict__ u) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    u[3 * i + 0] = x[i] - X0x[i];
+    u[3 * i + 1] = y[i] - X0y[i];
+    u[3 * i + 2] = z[i] - X0z[i];
+}
+
 __global__ void k_f32_to_f64(long long n, const float* __restrict__ a, double* b) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = (double)a[i];
@@ -587,6 +598,7 @@ static TileArgs<R> make_args(tlfea_element_s* h, bool fp32) {
         A.px = (const R*)h->x;
         A.py = (const R*)h->y;
         A.pz = (const R*)h->z;
+        A.u64 = A.x64 = A.y64 = A.z64 = A.X0x = A.X0y = A.X0z = nullptr;
         A.f_out = (R*)h->f_int;
         A.partial = (R*)tl.partial64;
     } else {
@@ -594,6 +606,7 @@ static TileArgs<R> make_args(tlfea_element_s* h, bool fp32) {
         A.ji = (const R*)tl.ji32;
         A.dv = (const R*)tl.dv32;
         A.px = A.py = A.pz = nullptr;  // staged from x64 - X0 relative to each tile's anchor
+        A.u64 = h->u64;
         A.x64 = h->x;
         A.y64 = h->y;
         A.z64 = h->z;
@@ -729,9 +742,20 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
 
 // f_int (FP64) or f_int32 (FP32) = internal force at the current positions.
 // Asynchronous on h->stream (the solvers call it inside their loops).
+// The interleaved FP64 displacement the FP32 force stages from, after a change of positions.
+int element_refresh_u64(tlfea_element_s* h) {
+    if (!h->u_dirty) return TLFEA_OK;
+    const int n = h->N;
+    k_disp64<<<(n + 255) / 256, 256, 0, h->stream>>>(n, h->x, h->y, h->z, h->X0x, h->X0y, h->X0z, h->u64);
+    TLFEA_CHECK_LAUNCH();
+    h->u_dirty = false;
+    return TLFEA_OK;
+}
+
 int element_force(tlfea_element_s* h, const double* d_v, bool fp32) {
     int st;
     if (fp32) {
+        if ((st = element_refresh_u64(h))) return st;
         st = (h->npe == 10) ? force_dispatch<float, 10, 5>(h, d_v, true) : force_dispatch<float, 4, 1>(h, d_v, true);
     } else {
         st = (h->npe == 10) ? force_dispatch<double, 10, 5>(h, d_v, false)
@@ -904,7 +928,7 @@ int tlfea_element_create(int type, int n_elem, int n_nodes, tlfea_element* out) 
     int st = TLFEA_OK;
     st |= dalloc(&h->x, N) | dalloc(&h->y, N) | dalloc(&h->z, N);
     st |= dalloc(&h->xj, N) | dalloc(&h->yj, N) | dalloc(&h->zj, N);
-    st |= dalloc(&h->X0x, N) | dalloc(&h->X0y, N) | dalloc(&h->X0z, N);
+    st |= dalloc(&h->X0x, N) | dalloc(&h->X0y, N) | dalloc(&h->X0z, N) | dalloc(&h->u64, 3 * (size_t)N);
     st |= dalloc(&h->d_conn, (size_t)n_elem * h->npe);
     st |= dalloc(&h->f_int, 3 * N) | dalloc(&h->f_ext, 3 * N) | dalloc(&h->f_int32, 3 * N);
     st |= dalloc(&h->detJ, (size_t)n_elem * h->nqp);
@@ -928,7 +952,7 @@ int tlfea_element_destroy(tlfea_element h) {
     TLFEA_CUDA(cudaSetDevice(h->device));
     dfree(h->x); dfree(h->y); dfree(h->z);
     dfree(h->xj); dfree(h->yj); dfree(h->zj);
-    dfree(h->X0x); dfree(h->X0y); dfree(h->X0z);
+    dfree(h->X0x); dfree(h->X0y); dfree(h->X0z); dfree(h->u64);
     dfree(h->d_conn); dfree(h->f_int); dfree(h->f_ext); dfree(h->f_int32);
     dfree(h->detJ); dfree(h->Pst); dfree(h->d_err);
     free_tiling(h->tl);
@@ -967,6 +991,7 @@ int tlfea_element_set_blocking(tlfea_element h, int blocking) {
 int tlfea_element_reset_positions(tlfea_element h) {
     CHECK_HANDLE(h);
     REQUIRE_SETUP(h);
+    h->u_dirty = true;
     const size_t nb = (size_t)h->N * sizeof(double);
     TLFEA_CUDA(cudaMemcpyAsync(h->x, h->X0x, nb, cudaMemcpyDeviceToDevice, h->stream));
     TLFEA_CUDA(cudaMemcpyAsync(h->y, h->X0y, nb, cudaMemcpyDeviceToDevice, h->stream));
@@ -1028,6 +1053,7 @@ int tlfea_element_setup(tlfea_element h, const double* qx, const double* qy, con
     if (st) return st;
     if ((st = build_incidence(h))) return st;
     SYNC(h);
+    h->u_dirty = true;
     h->is_setup = true;
     return TLFEA_OK;
 }
@@ -1152,6 +1178,7 @@ static int copy_positions(tlfea_element h, double* dx, double* dy, double* dz, c
 
 int tlfea_element_update_positions(tlfea_element h, const double* x, const double* y, const double* z, int n) {
     CHECK_HANDLE(h);
+    h->u_dirty = true;
     return copy_positions(h, h->x, h->y, h->z, x, y, z, n);
 }
 
@@ -1186,6 +1213,7 @@ int tlfea_element_calc_dndu_pre(tlfea_element h) {
     TLFEA_CUDA(cudaMemcpyAsync(h->X0x, h->x, nb, cudaMemcpyDeviceToDevice, h->stream));
     TLFEA_CUDA(cudaMemcpyAsync(h->X0y, h->y, nb, cudaMemcpyDeviceToDevice, h->stream));
     TLFEA_CUDA(cudaMemcpyAsync(h->X0z, h->z, nb, cudaMemcpyDeviceToDevice, h->stream));
+    h->u_dirty = true;
     h->precomputed = true;
     SYNC(h);
     return TLFEA_OK;

@@ -83,8 +83,10 @@ struct TileArgs {
     const R* px;  // FP64 mode: positions x (null in FP32 mode)
     const R* py;
     const R* pz;
-    // FP32 mode: FP64 positions and reference positions; each tile stages its nodes'
-    // displacements relative to its first local node (tile_anchor / stage_pos)
+    // FP32 mode: each tile stages its nodes' displacements relative to its first local
+    // node (tile_anchor / stage_pos), from the interleaved FP64 displacement u64 = x - X0
+    // when it is given, else from the FP64 positions and reference positions
+    const double* u64;
     const double* x64;
     const double* y64;
     const double* z64;
@@ -127,9 +129,15 @@ __host__ __device__ __forceinline__ size_t grad_slot(int a, int j, int t) {
 template <typename R>
 __device__ __forceinline__ void tile_anchor(const TileArgs<R>& A, int gid0, double u0[3]) {
     if constexpr (sizeof(R) == 4) {
-        u0[0] = A.x64[gid0] - A.X0x[gid0];
-        u0[1] = A.y64[gid0] - A.X0y[gid0];
-        u0[2] = A.z64[gid0] - A.X0z[gid0];
+        if (A.u64) {
+            u0[0] = A.u64[3 * gid0 + 0];
+            u0[1] = A.u64[3 * gid0 + 1];
+            u0[2] = A.u64[3 * gid0 + 2];
+        } else {
+            u0[0] = A.x64[gid0] - A.X0x[gid0];
+            u0[1] = A.y64[gid0] - A.X0y[gid0];
+            u0[2] = A.z64[gid0] - A.X0z[gid0];
+        }
     } else {
         u0[0] = u0[1] = u0[2] = 0.0;
     }
@@ -138,9 +146,15 @@ __device__ __forceinline__ void tile_anchor(const TileArgs<R>& A, int gid0, doub
 template <typename R>
 __device__ __forceinline__ void stage_pos(const TileArgs<R>& A, int gid, const double u0[3], R& x, R& y, R& z) {
     if constexpr (sizeof(R) == 4) {
-        x = (float)((A.x64[gid] - A.X0x[gid]) - u0[0]);
-        y = (float)((A.y64[gid] - A.X0y[gid]) - u0[1]);
-        z = (float)((A.z64[gid] - A.X0z[gid]) - u0[2]);
+        if (A.u64) {
+            x = (float)(A.u64[3 * gid + 0] - u0[0]);
+            y = (float)(A.u64[3 * gid + 1] - u0[1]);
+            z = (float)(A.u64[3 * gid + 2] - u0[2]);
+        } else {
+            x = (float)((A.x64[gid] - A.X0x[gid]) - u0[0]);
+            y = (float)((A.y64[gid] - A.X0y[gid]) - u0[1]);
+            z = (float)((A.z64[gid] - A.X0z[gid]) - u0[2]);
+        }
     } else {
         x = A.px[gid];
         y = A.py[gid];
@@ -785,6 +799,8 @@ struct tlfea_element_s {
     double *x = nullptr, *y = nullptr, *z = nullptr;
     double *xj = nullptr, *yj = nullptr, *zj = nullptr;
     double *X0x = nullptr, *X0y = nullptr, *X0z = nullptr;
+    double* u64 = nullptr;  // interleaved x - X0 for the FP32 force (refreshed when positions change)
+    bool u_dirty = true;
     int* d_conn = nullptr;
     double* f_int = nullptr;
     double* f_ext = nullptr;
@@ -831,6 +847,7 @@ namespace tlfea {
 // Implemented in element.cu, used by the solvers.
 int element_build_pattern(tlfea_element_s* h);
 int element_force(tlfea_element_s* h, const double* d_v, bool fp32);
+int element_refresh_u64(tlfea_element_s* h);
 
 // Barycentric coordinates of the element's quadrature points.
 inline QpBary qp_bary(const tlfea_element_s* h) {

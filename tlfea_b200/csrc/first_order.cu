@@ -647,6 +647,7 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     s->stats.stop_rule_met = hl[8];
     s->stats.kernel_ms = ms;
     el->f_int_from32 = fp32;
+    el->u_dirty = true;  // the solve moved the positions
     if (status == TLFEA_NONFINITE) {
         set_error("non-finite gradient norm");
         return TLFEA_NONFINITE;
