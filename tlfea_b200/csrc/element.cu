@@ -182,7 +182,7 @@ __global__ void k_combine(int nb, const int* __restrict__ bgid, const int* __res
                           const R* __restrict__ partial, R* f_out) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
-    R s0 = R(0), s1 = R(0), s2 = R(0);
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;  // node sums in FP64 (near equilibrium they cancel)
     for (int k = boff[b]; k < boff[b + 1]; ++k) {
         s0 += partial[3 * k + 0];
         s1 += partial[3 * k + 1];

@@ -731,7 +731,7 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
     for (int ln = t; ln < nl; ln += TE) {
         const int beg = ln ? A.ln_inc_end[lb + ln - 1] : 0;
         const int end = A.ln_inc_end[lb + ln];
-        R s0 = R(0), s1 = R(0), s2 = R(0);
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;  // node sums in FP64 (near equilibrium they cancel)
         for (int k = beg; k < end; ++k) {
             const int ent = inc[k];
             const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));

@@ -101,7 +101,7 @@ __device__ __forceinline__ void node_force(const FOArgs& S, const TileArgs<R>& A
         f[1] = (double)A.f_out[3 * i + 1];
         f[2] = (double)A.f_out[3 * i + 2];
     } else {
-        R s0 = R(0), s1 = R(0), s2 = R(0);
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;  // node sums in FP64 (near equilibrium they cancel)
         for (int k = S.bnode_off[b]; k < S.bnode_off[b + 1]; ++k) {
             const int p = S.bnode_slots[k];
             s0 += A.partial[3 * p + 0];

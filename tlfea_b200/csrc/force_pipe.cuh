@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2) k_force_pipe(TileArgs<R> A, i
         for (int ln = t; ln < nl; ln += TE) {
             const int beg = ln ? A.ln_inc_end[lb + ln - 1] : 0;
             const int end = A.ln_inc_end[lb + ln];
-            R s0 = R(0), s1 = R(0), s2 = R(0);
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0;  // node sums in FP64 (near equilibrium they cancel)
             for (int k = beg; k < end; ++k) {
                 const int ent = inc[k];
                 const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
@@ -657,7 +657,7 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 1) k_tile_for
     for (int ln = t; ln < nl; ln += TE) {
         const int beg = ln ? iends[ln - 1] : 0;
         const int end = iends[ln];
-        R s0 = R(0), s1 = R(0), s2 = R(0);
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;  // node sums in FP64 (near equilibrium they cancel)
         for (int k = beg; k < end; ++k) {
             const int ent = incs[k];
             const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
@@ -835,7 +835,7 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, in
     for (int ln = t; ln < nl; ln += TE) {
         const int beg = ln ? iends[ln - 1] : 0;
         const int end = iends[ln];
-        R s0 = R(0), s1 = R(0), s2 = R(0);
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;  // node sums in FP64 (near equilibrium they cancel)
         for (int k = beg; k < end; ++k) {
             const int ent = incs[k];
             const int base = (ent >> TILE_SHIFT) * 3 * TE + (ent & (TE - 1));
