@@ -564,6 +564,98 @@ def dynamics_leg(args, T):
             "tip_deflection_min_z": tip_z}
 
 
+def config2_more_legs(args, T, cfg):
+    """Configuration 2's other legs.
+    * SyncedNesterov on the 200x20x20 TET10 mesh (2,022,243 DOF), one implicit step with
+      the parameters of the reference's Nesterov example (test_feat10_nesterov.cc:189:
+      alpha 1e-8, rho 1e14, tolerances 1e-6, 5 x 300 iterations, dt 1e-3) from the
+      reference configuration under the seeded tip load, FP64 and FP32 element forces.
+      Reported per inner iteration (the unit of the method's work).  The reference's own
+      Nesterov kernel is not timed: at this size it clamps its grid to the co-resident
+      blocks and never updates the DOFs beyond it (SyncedNesterov.cu:391-397).
+    * The TET4 variant: the same beam with corner nodes only (201x21x21 = 88,641 nodes,
+      480,000 TET4 elements), linear static CG to 1e-6, beside the reference's own CUDA
+      build on the same GPU."""
+    import torch
+    from tlfea_b200 import mesh as M
+
+    out = {}
+    x, y, z, conn, fixed, f = build_mesh(cfg)
+    el = setup_element(T, cfg, x, y, z, conn, fixed, f)
+    el.CalcMassMatrix()
+    el.CalcConstraintData()
+    el.ConvertToCSR_ConstraintJacT()
+    nes = {}
+    for prec in ("fp64", "fp32"):
+        el.SetForcePrecision(prec)
+        s = T.SyncedNesterovSolver(el, el.get_n_constraint())
+        s.Setup()
+        s.SetParameters(T.SyncedNesterovParams(1.0e-8, 1e14, 1.0e-6, 1.0e-6, 5, 300, 1.0e-3))
+        el.ResetPositions()
+        s.Solve()  # warm-up (first launch)
+        s.SetParameters(T.SyncedNesterovParams(1.0e-8, 1e14, 1.0e-6, 1.0e-6, 5, 300, 1.0e-3))
+        el.ResetPositions()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.Solve()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        st = s.GetStats()
+        it = max(1, st["inner_iters_total"])
+        nes[prec] = {"step_s": round(dt, 4), "inner_iters": st["inner_iters_total"], "outer_iters": st["outer_iters"],
+                     "ms_per_inner_iteration": round(1e3 * dt / it, 4),
+                     "inner_iterations_per_s": round(it / dt, 1), "kernel_ms": round(st["kernel_ms"], 3)}
+        del s
+    el.SetForcePrecision("fp64")
+    el.Destroy()
+    out["nesterov_200x20x20_t10"] = {
+        "workload": "SyncedNesterov, one implicit step from rest, the reference example's parameters",
+        **nes, "reference": "not timed: its cooperative kernel leaves DOFs beyond the co-resident grid un-updated"}
+    # TET4 CG
+    c4 = dict(cfg, order=4)
+    x4, y4, z4, conn4 = M.box_mesh(c4["nx"], c4["ny"], c4["nz"], 4, c4["lx"], c4["ly"], c4["lz"])
+    fixed4, f4, _ = M.cantilever_loads(x4, y4, z4, (0.0, 0.0, -load_magnitude(c4["seed"])))
+    el = T.GPU_FEAT4_Data(conn4.shape[0], len(x4))
+    el.Initialize()
+    el.SetNodalFixed(fixed4)
+    el.SetExternalForce(f4)
+    el.Setup(*T.Quadrature.t4(), x4, y4, z4, conn4)
+    el.SetDensity(c4["rho"])
+    el.SetDamping(0.0, 0.0)
+    el.SetSVK(c4["E"], c4["nu"])
+    el.CalcDnDuPre()
+    solver = T.LinearStaticSolver(el, c4["tol"], 1000000)
+    stream = el.GetStream()
+
+    def step():
+        el.ResetPositions()
+        solver.Solve()
+
+    for _ in range(2):
+        step()
+    ms = time_stream(torch, stream, step, max(1, args.steps))
+    t4 = {"value": round(1e3 / ms, 3), "unit": "solves/s", "ms_per_step": round(ms, 3),
+          "cg_iters_per_solve": solver.GetLastIterCount(), "final_rel_residual": solver.GetLastResidual(),
+          "elements": int(conn4.shape[0]), "nodes": int(len(x4))}
+    for _ in range(3):
+        el.ComputeInternalForce()
+    ms_f = time_stream(torch, stream, el.ComputeInternalForce, args.kernel_reps)
+    b = elem_force_bytes(conn4.shape[0], len(x4), 4, 1, 8)
+    hbm, _ = peaks()
+    t4["elem_force_fp64"] = {"ms": round(ms_f, 4), "achieved_gbs": round(b / (ms_f / 1e3) / 1e9, 1),
+                             "frac": round(b / (ms_f / 1e3) / 1e9 / hbm, 4), "algorithmic_bytes": int(b)}
+    del solver
+    el.Destroy()
+    from oracle import ref_lib as R
+
+    if R.available() and not args.no_gpu_ref:
+        g = gpu_reference_leg(c4, x4, y4, z4, conn4, fixed4, f4, steps=2, warmup=1)
+        t4["gpu_reference"] = {k: g[k] for k in ("value", "ms_per_step", "cg_iters_per_solve", "elem_force_fp64")}
+        t4["speedup_vs_reference"] = round(t4["value"] / g["value"], 3)
+    out["cg_200x20x20_t4"] = t4
+    return out
+
+
 def config5_leg(args, T):
     """Configuration 5: 64 sequences on the 100x10x10 TET10 cantilever (60,000 elements,
     88,641 nodes; SVK, rho = 1000, seeded E log-uniform in [3e6, 3e7] Pa and nu in
@@ -862,6 +954,8 @@ def main():
     ap.add_argument("--no-dynamics", action="store_true", help="skip the time-stepping leg")
     ap.add_argument("--dyn-steps", type=int, default=50, help="implicit steps of the time-stepping leg")
     ap.add_argument("--no-config5", action="store_true", help="skip the configuration-5 batched sequences leg")
+    ap.add_argument("--no-config2-more", action="store_true",
+                    help="skip configuration 2's Nesterov and TET4 legs")
     ap.add_argument("--dyn-batch", type=int, default=64, help="sequences of the configuration-5 leg")
     ap.add_argument("--dyn-eval-steps", type=int, default=8, help="steps per warm start in the configuration-5 leg")
     ap.add_argument("--dyn-train-steps", type=int, default=24, help="training steps of the step predictor")
@@ -1020,6 +1114,8 @@ def main():
            "roofline": roofline, "elem_force": ef, "gpu_launches": int(launches), "clocks": clk.summary(),
            "pcg": pcg}
     el.Destroy()
+    if not args.no_config2_more:
+        out["config2_more"] = config2_more_legs(args, T, cfg)
     if not args.no_batch:
         out["batched"] = batched_leg(args, T)
     if not args.no_learned:
