@@ -150,3 +150,79 @@ def test_stop_rule_ends_each_sequence_at_a_checked_residual():
     assert conv.all() and list(it) == [1] * len(E), (it, res)
     b.Destroy()
     el.Destroy()
+
+
+def test_learned_step_predictor_reduces_iterations():
+    """What the trained network gains (configuration-5 style, small mesh): a StepPredictor
+    trained on the solver's own steps of other sequences warm-starts each step; to the same
+    residual tolerance it needs fewer Nesterov iterations than the reference's start (the
+    previous velocity), and its residuals are checked by the same stop rule."""
+    import torch
+    from tlfea_b200 import warmstart as W
+
+    x, y, z, conn, fixed, _, tip = _mesh(cells=(10, 2, 2))
+    N = len(x)
+    el = make_element(x, y, z, conn, E_mod=1e7, nu=0.3, rho=RHO, fixed=fixed, f_ext=np.zeros(3 * N))
+    el.AddGravity(0.0, 0.0, -9.81)
+    f_var = np.zeros(3 * N)
+    f_var[3 * tip + 2] = -50.0 / len(tip)
+    omega, dt, rho_alm = 2 * np.pi * 5.0, 1e-3, 1e8
+    r = np.random.default_rng(3)
+    E = np.exp(r.uniform(np.log(5e6), np.log(2e7), 8))
+    nu = r.uniform(0.25, 0.35, 8)
+    alphas = np.array([0.9 / (_hessian_lmax(x, y, z, conn, fixed, E[s], nu[s], dt, rho_alm, 100)) for s in range(8)])
+    params = T.SyncedNesterovParams(float(alphas.min()), rho_alm, 0.0, 1e-6, 3, 20000, dt)
+    X0 = torch.as_tensor(np.stack([x, y, z], 1).reshape(-1), device="cuda")
+
+    def make(seqs):
+        b = T.BatchedDynamics(el, len(seqs))
+        b.SetMaterial(E[seqs], nu[seqs])
+        b.SetParameters(params, 1e-6)
+        b.SetStepSizes(alphas[seqs])
+        b.SetLoad(f_var, 1.0, omega, 0.0)
+        return b
+
+    def state(b, B):
+        p = b.DevicePtrs()
+        v = W.device_view(p["v"], (B, 3 * N))
+        vh = W.device_view(p["v_hist"], (B, 3 * N))
+        u = torch.stack([W.device_view(p[k], (B, N)) for k in ("x", "y", "z")], 2).reshape(B, 3 * N) - X0
+        return v, vh, u
+
+    def lf(n):
+        return np.array([[np.sin(omega * (n - 1 + j) * dt) for j in range(3)]])
+
+    tr, ev, steps = np.arange(4, 8), np.arange(4), 12
+    bt = make(tr)
+    V = torch.empty(4, steps, 3 * N, dtype=torch.float64, device="cuda")
+    U = torch.empty_like(V)
+    for k in range(steps):
+        bt.Step(T.BatchedDynamics.WARM_LINEAR)
+        v, _, u = state(bt, 4)
+        V[:, k], U[:, k] = v, u
+    bt.Destroy()
+    sp = W.StepPredictor(k_in=8, k_out=16, hidden=(128, 128), max_batch=128, seed=0, E_range=(5e6, 2e7),
+                         nu_range=(0.25, 0.35))
+    mats = sp.material_features(E, nu)
+    sp.fit(V, U, np.concatenate([lf(n) for n in range(1, steps + 1)]), mats[tr], epochs=300, batch=32)
+    b = make(ev)
+    totals = {}
+    for name in ("previous", "learned"):
+        b.Reset()
+        tot = 0
+        for n in range(1, 7):
+            if name == "previous":
+                it, res, conv = b.Step(T.BatchedDynamics.WARM_PREVIOUS)
+            elif n == 1:
+                it, res, conv = b.Step(T.BatchedDynamics.WARM_LINEAR)
+            else:
+                v, vh, u = state(b, 4)
+                g = sp.predict(v, vh, u, np.repeat(lf(n - 1), 4, 0), mats[ev])
+                it, res, conv = b.Step(T.BatchedDynamics.WARM_GIVEN, int(g.data_ptr()))
+            assert conv.all() and (res < 1e-6).all()
+            tot += int(it.sum())
+        totals[name] = tot
+    assert totals["learned"] < totals["previous"], totals
+    b.Destroy()
+    sp.destroy()
+    el.Destroy()
