@@ -396,13 +396,17 @@ struct TileTmaGeom {
     static constexpr uint32_t STAGE_BYTES = GRAD_BYTES + DV_BYTES;
     static constexpr uint32_t LCONN_BYTES = NPE * TILE_ELEMS * sizeof(uint16_t);
     static constexpr uint32_t INC_BYTES = NPE * TILE_ELEMS * sizeof(uint16_t);
-    // element forces of the scatter reuse the two stages once the QP loop is done
-    static_assert(3 * NPE * TILE_ELEMS * sizeof(R) <= 2 * STAGE_BYTES, "force table must fit in the stages");
+    // QP-slice stages: FP64 copies a slice into registers before computing it, so one
+    // stage suffices (refilled as soon as it is read); FP32 reads a slice twice (H, then
+    // the forces) and double-buffers
+    static constexpr int STAGES = sizeof(R) == 8 ? 1 : 2;
+    // element forces of the scatter reuse the stages once the QP loop is done
+    static_assert(3 * NPE * TILE_ELEMS * sizeof(R) <= STAGES * STAGE_BYTES, "force table must fit in the stages");
     static_assert(LCONN_BYTES % 16 == 0 && INC_BYTES % 16 == 0 && STAGE_BYTES % 16 == 0, "bulk sizes");
 };
 
 // Byte offsets of the regions of k_tile_force_tma's shared memory, each
-// 16-byte aligned: [stage 0 | stage 1, later the element forces][lconn][incidence]
+// 16-byte aligned: [stage(s), later the element forces][lconn][incidence]
 // [x y z][node destination][incidence end][velocities][2 mbarriers].
 template <typename R, int NPE>
 struct TileTmaLayout {
@@ -410,7 +414,7 @@ struct TileTmaLayout {
     __host__ __device__ TileTmaLayout(int max_local, bool damp) {
         using G = TileTmaGeom<R, NPE>;
         auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
-        inc = 2 * (size_t)G::STAGE_BYTES + G::LCONN_BYTES;
+        inc = G::STAGES * (size_t)G::STAGE_BYTES + G::LCONN_BYTES;
         pos = inc + G::INC_BYTES;
         dst = al(pos + 3 * (size_t)max_local * sizeof(R));
         iend = al(dst + (size_t)max_local * sizeof(int));
@@ -426,15 +430,16 @@ inline size_t tile_tma_smem_bytes(int max_local, bool damp) {
 }
 
 template <typename R, int NPE, int NQP, bool DAMP>
-__global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 1) k_tile_force_tma(TileArgs<R> A, int* err) {
+__global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_force_tma(TileArgs<R> A, int* err) {
     using G = TileTmaGeom<R, NPE>;
+    constexpr int S = G::STAGES;
     constexpr int TE = TILE_ELEMS;
     extern __shared__ __align__(128) unsigned char smem[];
     const int tile = blockIdx.x, t = threadIdx.x;
     const int ML = A.max_local;
     const TileTmaLayout<R, NPE> L(ML, DAMP);
     unsigned char* stage0 = smem;
-    const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + 2 * G::STAGE_BYTES);
+    const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + S * G::STAGE_BYTES);
     const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
     R* xs = reinterpret_cast<R*>(smem + L.pos);
     R* ys = xs + ML;
@@ -445,9 +450,10 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 1) k_tile_for
     R* fe = reinterpret_cast<R*>(smem);  // aliases the stages after the QP loop
     const uint32_t bar0 = smem_u32(smem + L.bar);
 
+    // slice q goes to stage q % S, completing phase (q / S) of that stage's barrier
     auto issue = [&](int q) {  // thread 0 only
-        const uint32_t bar = bar0 + 8 * (q & 1);
-        const uint32_t dst = smem_u32(stage0 + (size_t)(q & 1) * G::STAGE_BYTES);
+        const uint32_t bar = bar0 + 8 * (q % S);
+        const uint32_t dst = smem_u32(stage0 + (size_t)(q % S) * G::STAGE_BYTES);
         const uint32_t extra = (q == 0) ? G::LCONN_BYTES + G::INC_BYTES : 0;
         mbar_expect_tx(bar, G::STAGE_BYTES + extra);
         bulk_g2s(dst, A.grad + ((size_t)tile * NQP + q) * (NPE * 3) * TE, G::GRAD_BYTES, bar);
@@ -463,7 +469,7 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 1) k_tile_for
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         issue(0);
-        if (NQP > 1) issue(1);
+        if (S > 1 && NQP > 1) issue(1);
     }
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
     double u0[3], v0[3] = {0.0, 0.0, 0.0};
@@ -509,8 +515,8 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 1) k_tile_for
         }
 #pragma unroll 1
         for (int q = 0; q < NQP; ++q) {
-            if (q > 0 && !mbar_wait(bar0 + 8 * (q & 1), (q >> 1) & 1)) atomicExch(err, 3);
-            const unsigned char* st = stage0 + (size_t)(q & 1) * G::STAGE_BYTES;
+            if (q > 0 && !mbar_wait(bar0 + 8 * (q % S), (q / S) & 1)) atomicExch(err, 3);
+            const unsigned char* st = stage0 + (size_t)(q % S) * G::STAGE_BYTES;
             const float2* gs2 = reinterpret_cast<const float2*>(st);
             const float dv = reinterpret_cast<const float*>(st + G::GRAD_BYTES)[t];
             float2 h2[3][3], fd2[3][3];
@@ -559,11 +565,11 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 1) k_tile_for
                         f2[p][i] = __ffma2_rn(make_float2(pij, pij), g[j], f2[p][i]);
                     }
             }
-            if (q + 2 < NQP) {
+            if (q + S < NQP) {
                 // every thread's generic reads of this stage precede the bulk refill
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncthreads();
-                if (t == 0) issue(q + 2);
+                if (t == 0) issue(q + S);
             }
         }
         __syncthreads();  // every thread is done with the stages the force table reuses
@@ -582,8 +588,8 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 1) k_tile_for
         for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
     #pragma unroll 1
         for (int q = 0; q < NQP; ++q) {
-            if (!mbar_wait(bar0 + 8 * (q & 1), (q >> 1) & 1)) atomicExch(err, 3);
-            const unsigned char* st = stage0 + (size_t)(q & 1) * G::STAGE_BYTES;
+            if (!mbar_wait(bar0 + 8 * (q % S), (q / S) & 1)) atomicExch(err, 3);
+            const unsigned char* st = stage0 + (size_t)(q % S) * G::STAGE_BYTES;
             const R* gs = reinterpret_cast<const R*>(st);
             if (q == 0) {
     #pragma unroll
@@ -595,11 +601,11 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 1) k_tile_for
     #pragma unroll
                 for (int j = 0; j < 3; ++j) g[a][j] = gs[grad_slot<R>(a, j, t)];
             const R dv = reinterpret_cast<const R*>(st + G::GRAD_BYTES)[t];
-            if (q + 2 < NQP) {
+            if (q + S < NQP) {
                 // every thread's generic reads of this stage precede the bulk refill
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncthreads();
-                if (t == 0) issue(q + 2);
+                if (t == 0) issue(q + S);
             }
             R P[3][3];
             {
