@@ -180,6 +180,9 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force(TileArgs<R> A) {
 template <typename R, bool ACCUM>
 __global__ void k_combine(int nb, const int* __restrict__ bgid, const int* __restrict__ boff,
                           const R* __restrict__ partial, R* f_out) {
+    // launched as a programmatic dependent of the force kernel: its blocks may be
+    // scheduled while the force kernel drains, and wait here until it has completed
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;  // node sums in FP64 (near equilibrium they cancel)
@@ -643,8 +646,18 @@ template <typename R, bool ACCUM>
 static int launch_combine(tlfea_element_s* h, const R* partial, R* f_out) {
     const int nb = h->tl.n_bnodes;
     if (nb == 0) return TLFEA_OK;
-    k_combine<R, ACCUM><<<(nb + 255) / 256, 256, 0, h->stream>>>(nb, h->tl.bnode_gid, h->tl.bnode_off, partial,
-                                                                 f_out);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((nb + 255) / 256));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TLFEA_CUDA(cudaLaunchKernelEx(&cfg, k_combine<R, ACCUM>, nb, (const int*)h->tl.bnode_gid,
+                                  (const int*)h->tl.bnode_off, partial, f_out));
     TLFEA_CHECK_LAUNCH();
     return TLFEA_OK;
 }

@@ -683,6 +683,8 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_for
             A.partial[3 * ps + 2] = s2;
         }
     }
+    // outputs written: the combine kernel (a programmatic dependent) may be scheduled
+    asm volatile("griddepcontrol.launch_dependents;");
 }
 
 // ---------------------------------------------------------------------------
@@ -861,6 +863,8 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, in
             A.partial[3 * ps + 2] = s2;
         }
     }
+    // outputs written: the combine kernel (a programmatic dependent) may be scheduled
+    asm volatile("griddepcontrol.launch_dependents;");
 }
 
 }  // namespace tlfea
