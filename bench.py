@@ -478,7 +478,19 @@ def batched_leg(args, T):
         its.append(itp)
     plain = k / tot
     value = n / (ms / 1e3)
+    # roofline of the batched CG: per iteration an instance streams its compact geometry
+    # (J^-1 and dV per element and QP, FP64) and makes ~14 passes over 3N-vectors (the
+    # matrix-free K p reads p and writes q; p.Kp, u/r update with r.r, p update); summed
+    # over the iterations each instance ran, over the batch's time
+    hbm, _ = peaks()
+    per_iter = np.array([d["conn"].shape[0] * 5 * 10 * 8 + 3 * len(d["x"]) * 8 * 14 for d in insts], np.float64)
+    moved = float(np.sum(per_iter * np.asarray(it, np.float64)))
+    ach = moved / (ms / 1e3) / 1e9
+    roof = {"kernel": "k_batch_cg (whole solve)", "bound": "hbm", "achieved": round(ach, 1), "peak": hbm,
+            "unit": "GB/s", "frac": round(ach / hbm, 4), "algorithmic_bytes": int(moved),
+            "model": "per instance and iteration: E*5*10*8 (J^-1 + dV stream) + 3N*8*14 (vector passes)"}
     return {"workload": f"{n} uneven TET10 cantilevers, linear static CG to 1e-6 (one persistent launch)",
+            "roofline": roof,
             "elements": counts["elements"], "nodes": counts["nodes"], "dof": 3 * counts["nodes"],
             "precision": args.batch_precision, "value": round(value, 2), "unit": "solves/s",
             "ms_per_batch": round(ms, 3), "iters_mean": float(np.mean(it)), "iters_max": int(np.max(it)),
