@@ -780,7 +780,9 @@ def config5_leg(args, T):
     sp = W.StepPredictor(k_in=16, k_out=32, hidden=(256, 256), max_batch=128, seed=0, E_range=(3e6, 3e7),
                          nu_range=(0.25, 0.4))
     mats = sp.material_features(E_all, nu_all)
-    hist = sp.fit(V, U, loads_tr, mats[tr], epochs=args.dyn_epochs, batch=128)
+    # samples: steps 1..T-1 of each training sequence; a batch is a multiple of 16 rows
+    n_samples = n_train * (steps_train - 1)
+    hist = sp.fit(V, U, loads_tr, mats[tr], epochs=args.dyn_epochs, batch=min(128, n_samples // 16 * 16))
     del V, U
     t_train = time.perf_counter() - t0
 

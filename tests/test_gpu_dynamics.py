@@ -3,9 +3,11 @@ one mesh, each implicit step solved by the SyncedNesterov iteration, against the
 oracle's SyncedNesterov restatement run sequence by sequence.
 
 With zero tolerances both run the same number of iterations (max_outer x max_inner per
-step), so each sequence's trajectory compares at the FP64 parity tolerance (the
-multipliers, rho = 1e14, amplify rounding into the velocities as in the single-solver
-tests).  With the stop rule on, the residual each sequence reports is checked against one
+step), so each sequence's trajectory compares within a bar calibrated on the case:
+max(1e-10, 3 s), s being how far the oracle's own displacements move when its reference
+positions are perturbed by 1e-15 (relative).  The multipliers (rho = 1e14) amplify rounding
+to s ~ 3e-9 on these meshes; the oracle and the reference's own CUDA build differ by
+1.2e-9 on the same kind of run.  With the stop rule on, the residual each sequence reports is checked against one
 recomputed from the oracle's mass matrix and internal force at its final state."""
 import numpy as np
 import pytest
@@ -28,6 +30,35 @@ def _mesh(cells=(10, 2, 2), order=10, load=(0.0, 0.0, -100.0)):
     return x, y, z, conn, fixed, f, tip
 
 
+def _oracle_steps(x, y, z, conn, E, nu, fixed, loads, params, lamd=0.0, pert=0.0, seed=1):
+    """The oracle's displacements (from the reference positions it was given) and velocity
+    guess after each SyncedNesterov step, one external force per step."""
+    xp = x if pert == 0.0 else x * (1.0 + pert * np.random.default_rng(seed).standard_normal(len(x)))
+    m = O.OracleModel(xp, y, z, conn, E, nu, RHO, fixed, loads[0], 0.0, lamd)
+    m.set_parameters()
+    X0 = np.stack([xp, y, z])
+    disp, vel = [], []
+    for fk in loads:
+        m.f_ext[:] = fk
+        m.nesterov_solve(*params)
+        disp.append(np.stack([m.x, m.y, m.z]) - X0)
+        vel.append(m.v_guess[:3 * len(x)].copy())
+    return disp, vel
+
+
+def _oracle_with_bar(x, y, z, conn, E, nu, fixed, loads, params, lamd=0.0):
+    """(displacements, velocities, displacement bar, velocity bar): each bar is
+    max(1e-10, 3 s) over two perturbation seeds, s the largest relative change of a step's
+    displacement (or velocity)."""
+    d0, v0 = _oracle_steps(x, y, z, conn, E, nu, fixed, loads, params, lamd)
+    sx = sv = 0.0
+    for seed in (1, 2):
+        d1, v1 = _oracle_steps(x, y, z, conn, E, nu, fixed, loads, params, lamd, 1e-15, seed)
+        sx = max(sx, max(rel(a, b) for a, b in zip(d1, d0)))
+        sv = max(sv, max(rel(a, b) for a, b in zip(v1, v0)))
+    return d0, v0, max(1e-10, 3.0 * sx), max(1e-10, 3.0 * sv)
+
+
 def _batch(x, y, z, conn, fixed, f, E, nu, params, rel_tol=0.0, lamd=0.0):
     el = make_element(x, y, z, conn, E_mod=float(E[0]), nu=float(nu[0]), rho=RHO, fixed=fixed, f_ext=f, lamd=lamd)
     b = T.BatchedDynamics(el, len(E))
@@ -42,19 +73,16 @@ def test_fixed_iterations_match_the_oracle_per_sequence(lamd):
     E = np.array([1e7, 3e6, 2.5e7])
     nu = np.array([0.3, 0.25, 0.4])
     el, b = _batch(x, y, z, conn, fixed, f, E, nu, FIXED, lamd=lamd)
-    models = [O.OracleModel(x, y, z, conn, E[s], nu[s], RHO, fixed, f, 0.0, lamd) for s in range(len(E))]
-    for m in models:
-        m.set_parameters()
+    refs = [_oracle_with_bar(x, y, z, conn, E[s], nu[s], fixed, [f, f], FIXED, lamd) for s in range(len(E))]
     X0 = np.stack([x, y, z])
     for step in range(2):
         it, res, conv = b.Step(T.BatchedDynamics.WARM_PREVIOUS)
         assert list(it) == [80, 80, 80] and not conv.any()
-        for s, m in enumerate(models):
-            m.nesterov_solve(*FIXED)
-            pos = np.stack(b.RetrievePositions(s))
-            ref = np.stack([m.x, m.y, m.z])
-            assert rel(pos - X0, ref - X0) < 1e-11, (step, s, rel(pos - X0, ref - X0))
-            assert rel(b.RetrieveVelocity(s), m.v_guess) < 1e-8
+        for s, (disp, vel, bx, bv) in enumerate(refs):
+            e = rel(np.stack(b.RetrievePositions(s)) - X0, disp[step])
+            assert e < bx, (step, s, e, bx)
+            e = rel(b.RetrieveVelocity(s), vel[step])
+            assert e < bv, (step, s, e, bv)
     b.Destroy()
     el.Destroy()
 
@@ -69,18 +97,14 @@ def test_time_varying_load_matches_the_oracle():
     el, b = _batch(x, y, z, conn, fixed, f0, E, nu, FIXED)
     amp, omega, phase = 1.0, 2 * np.pi * 5.0, 0.3
     b.SetLoad(f_var, amp, omega, phase)
-    models = [O.OracleModel(x, y, z, conn, E[s], nu[s], RHO, fixed, f0) for s in range(2)]
-    for m in models:
-        m.set_parameters()
+    loads = [f0 + (amp * np.sin(omega * (k * FIXED[6]) + phase)) * f_var for k in range(1, 4)]
+    refs = [_oracle_with_bar(x, y, z, conn, E[s], nu[s], fixed, loads, FIXED) for s in range(2)]
     X0 = np.stack([x, y, z])
-    for k in range(1, 4):
+    for k in range(3):
         b.Step(0)
-        fk = f0 + (amp * np.sin(omega * (k * FIXED[6]) + phase)) * f_var
-        for s, m in enumerate(models):
-            m.f_ext[:] = fk
-            m.nesterov_solve(*FIXED)
-            pos = np.stack(b.RetrievePositions(s))
-            assert rel(pos - X0, np.stack([m.x, m.y, m.z]) - X0) < 1e-11
+        for s, (disp, _, bar, _) in enumerate(refs):
+            e = rel(np.stack(b.RetrievePositions(s)) - X0, disp[k])
+            assert e < bar, (k, s, e, bar)
     b.Destroy()
     el.Destroy()
 

@@ -156,40 +156,55 @@ def test_solver_requires_parameters_and_mass():
 def test_configuration5_mesh_first_order_steps_match_oracle():
     """The 100x10x10 TET10 cantilever of configuration 5 (88,641 nodes): two
     SyncedNesterov and two SyncedAdamW steps at fixed iteration counts against the oracle,
-    in FP64 (and the batched sequences' kernels on two sequences)."""
+    in FP64 (and the batched sequences' kernels on two sequences), each within a bar
+    calibrated on the oracle's own sensitivity to a 1e-15 input perturbation."""
     x, y, z, conn = box(100, 10, 10, 10)
     fixed, f, _ = M.cantilever_loads(x, y, z, (0.0, 0.0, -50.0))
     X0 = np.stack([x, y, z])
-    nes = (1.0e-8, 1e14, 0.0, 0.0, 1, 6, 1.0e-3)
+    # step size 6e-4 below 1 / lambda_max of the step Hessian M/dt + dt K (787 at E = 1e7,
+    # about 1500 at 2E), rho = 1e8 as in the batched sequences: 60 iterations per step move
+    # the tip by 3.6e-5, far above the rounding of the positions it is read from
+    nes = (6.0e-4, 1e8, 0.0, 0.0, 2, 30, 1.0e-3)
     adw = list(ADAMW)
-    adw[3], adw[6], adw[7], adw[8], adw[9], adw[10] = 1.0, 0.0, 0.0, 1e4, 1, 6
+    adw[0], adw[3], adw[6], adw[7], adw[8], adw[9], adw[10] = 1e-3, 1.0, 0.0, 0.0, 1e4, 2, 30
     for kind, params in (("nesterov", nes), ("adamw", tuple(adw))):
         el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
         s = (T.SyncedNesterovSolver if kind == "nesterov" else T.SyncedAdamWSolver)(el, el.get_n_constraint())
         s.Setup()
         s.SetParameters(T.SyncedNesterovParams(*params) if kind == "nesterov" else T.SyncedAdamWParams(*params))
-        m = O.OracleModel(x, y, z, conn, E_MOD, NU, RHO, fixed, f)
-        m.set_parameters()
         for _ in range(2):
             s.Solve()
-            m.nesterov_solve(*params) if kind == "nesterov" else m.adamw_solve(*params)
-        pos = np.stack(el.RetrievePositionToCPU())
-        assert rel(pos - X0, np.stack([m.x, m.y, m.z]) - X0) < 1e-10, kind
+        disp, bar = _oracle_displacement_with_bar(x, y, z, conn, E_MOD, fixed, f, kind, params, 2)
+        e = rel(np.stack(el.RetrievePositionToCPU()) - X0, disp)
+        assert e < bar, (kind, e, bar)
         del s
         el.Destroy()
     el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
     b = T.BatchedDynamics(el, 2)
     b.SetMaterial([E_MOD, 2 * E_MOD], [NU, NU])
     b.SetParameters(T.SyncedNesterovParams(*nes), 0.0)
-    ms = [O.OracleModel(x, y, z, conn, e, NU, RHO, fixed, f) for e in (E_MOD, 2 * E_MOD)]
-    for m in ms:
-        m.set_parameters()
     for _ in range(2):
         b.Step(0)
-        for m in ms:
-            m.nesterov_solve(*nes)
-    for k, m in enumerate(ms):
-        pos = np.stack(b.RetrievePositions(k))
-        assert rel(pos - X0, np.stack([m.x, m.y, m.z]) - X0) < 1e-10
+    for k, e_mod in enumerate((E_MOD, 2 * E_MOD)):
+        disp, bar = _oracle_displacement_with_bar(x, y, z, conn, e_mod, fixed, f, "nesterov", nes, 2)
+        e = rel(np.stack(b.RetrievePositions(k)) - X0, disp)
+        assert e < bar, (k, e, bar)
     b.Destroy()
     el.Destroy()
+
+
+def _oracle_displacement_with_bar(x, y, z, conn, e_mod, fixed, f, kind, params, steps):
+    """The oracle's displacement after `steps` solves and the bar max(1e-10, 3 s), s the
+    largest relative change of that displacement when the reference positions are
+    perturbed by 1e-15 (relative; two seeds)."""
+    def run(pert, seed):
+        xp = x if pert == 0.0 else x * (1.0 + pert * np.random.default_rng(seed).standard_normal(len(x)))
+        m = O.OracleModel(xp, y, z, conn, e_mod, NU, RHO, fixed, f)
+        m.set_parameters()
+        for _ in range(steps):
+            m.nesterov_solve(*params) if kind == "nesterov" else m.adamw_solve(*params)
+        return np.stack([m.x - xp, m.y - y, m.z - z])
+
+    d0 = run(0.0, 0)
+    s = max(rel(run(1e-15, seed), d0) for seed in (1, 2))
+    return d0, max(1e-10, 3.0 * s)

@@ -83,9 +83,9 @@ struct TileArgs {
     const R* px;  // FP64 mode: positions x (null in FP32 mode)
     const R* py;
     const R* pz;
-    // FP32 mode: each tile stages its nodes' displacements relative to its first local
-    // node (tile_anchor / stage_pos), from the interleaved FP64 displacement u64 = x - X0
-    // when it is given, else from the FP64 positions and reference positions
+    // FP32 mode: each tile stages its nodes' FP64 displacements (stage_pos), from the
+    // interleaved record u64 = x - X0 when it is given, else from the FP64 positions and
+    // reference positions
     const double* u64;
     const double* x64;
     const double* y64;
@@ -118,48 +118,65 @@ __host__ __device__ __forceinline__ size_t grad_slot(int a, int j, int t) {
         return (size_t)(a * 3 + j) * TILE_ELEMS + t;
 }
 
-// Node values staged for a tile.  FP64 mode: the positions themselves (F =
-// sum_a x_a (x) gradN_a, the reference's formula).  FP32 mode: the displacement
-// relative to the tile's first local node ("anchor"), differenced in FP64 and
-// rounded once, u_a - u_0 = (x_a - X0_a) - (x_0 - X0_0).  The shape-function
-// gradients sum to zero, so H = sum_a (u_a - u_0) (x) gradN_a exactly; with the
-// anchor both roundings -- of u_a and of the FP32 gradients -- scale with how much
-// u varies across the tile instead of with |u|, which keeps the FP32 force
-// accurate at large displacements.
+// Node values staged for a tile, always FP64 in shared memory.  FP64 mode: the
+// positions themselves (F = sum_a x_a (x) gradN_a, the reference's formula).  FP32
+// mode: the displacements u = x - X0, from the interleaved FP64 record u64 when it is
+// given, else differenced from the FP64 positions and reference positions.
 template <typename R>
-__device__ __forceinline__ void tile_anchor(const TileArgs<R>& A, int gid0, double u0[3]) {
+__device__ __forceinline__ void stage_pos(const TileArgs<R>& A, int gid, double& x, double& y, double& z) {
     if constexpr (sizeof(R) == 4) {
         if (A.u64) {
-            u0[0] = A.u64[3 * gid0 + 0];
-            u0[1] = A.u64[3 * gid0 + 1];
-            u0[2] = A.u64[3 * gid0 + 2];
+            x = A.u64[3 * gid + 0];
+            y = A.u64[3 * gid + 1];
+            z = A.u64[3 * gid + 2];
         } else {
-            u0[0] = A.x64[gid0] - A.X0x[gid0];
-            u0[1] = A.y64[gid0] - A.X0y[gid0];
-            u0[2] = A.z64[gid0] - A.X0z[gid0];
-        }
-    } else {
-        u0[0] = u0[1] = u0[2] = 0.0;
-    }
-}
-
-template <typename R>
-__device__ __forceinline__ void stage_pos(const TileArgs<R>& A, int gid, const double u0[3], R& x, R& y, R& z) {
-    if constexpr (sizeof(R) == 4) {
-        if (A.u64) {
-            x = (float)(A.u64[3 * gid + 0] - u0[0]);
-            y = (float)(A.u64[3 * gid + 1] - u0[1]);
-            z = (float)(A.u64[3 * gid + 2] - u0[2]);
-        } else {
-            x = (float)((A.x64[gid] - A.X0x[gid]) - u0[0]);
-            y = (float)((A.y64[gid] - A.X0y[gid]) - u0[1]);
-            z = (float)((A.z64[gid] - A.X0z[gid]) - u0[2]);
+            x = A.x64[gid] - A.X0x[gid];
+            y = A.y64[gid] - A.X0y[gid];
+            z = A.z64[gid] - A.X0z[gid];
         }
     } else {
         x = A.px[gid];
         y = A.py[gid];
         z = A.pz[gid];
     }
+}
+
+// One element's node values for the force arithmetic, from the tile's staged FP64
+// values (xs/ys/zs, or interleaved for `element_velocities`).  FP64 mode: the values
+// as staged.  FP32 mode: relative to the element's first node, differenced in FP64
+// and rounded once, u_a - u_0.  The shape-function gradients sum to zero, so
+// H = sum_a (u_a - u_0) (x) gradN_a exactly; both roundings -- of the node values and
+// of the FP32 gradients -- then scale with how much u varies across the element
+// instead of with |u|, which keeps the FP32 force accurate at large displacements
+// and rotations.
+template <typename R, int NPE>
+__device__ __forceinline__ void element_nodes(const double* xs, const double* ys, const double* zs, const int* lc,
+                                              R xa[NPE][3]) {
+    double b0 = 0.0, b1 = 0.0, b2 = 0.0;
+    if constexpr (sizeof(R) == 4) {
+        b0 = xs[lc[0]];
+        b1 = ys[lc[0]];
+        b2 = zs[lc[0]];
+    }
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+        xa[a][0] = R(xs[lc[a]] - b0);
+        xa[a][1] = R(ys[lc[a]] - b1);
+        xa[a][2] = R(zs[lc[a]] - b2);
+    }
+}
+
+template <typename R, int NPE>
+__device__ __forceinline__ void element_velocities(const double* vs, const int* lc, R va[NPE][3]) {
+    double b[3] = {0.0, 0.0, 0.0};
+    if constexpr (sizeof(R) == 4) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) b[d] = vs[3 * lc[0] + d];
+    }
+#pragma unroll
+    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) va[a][d] = R(vs[3 * lc[a] + d] - b[d]);
 }
 
 // Tile routine modes.
@@ -583,31 +600,24 @@ template <typename R, int NPE, int NQP, int MODE, bool DAMP, bool MR = false, bo
 __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, unsigned char* smem_raw) {
     constexpr int TE = TILE_ELEMS;
     const int t = threadIdx.x;
-    R* xs = reinterpret_cast<R*>(smem_raw);
-    R* ys = xs + A.max_local;
-    R* zs = ys + A.max_local;
-    R* vs = zs + A.max_local;
-    R* ws = DAMP ? vs + 3 * A.max_local : vs;
+    // [x y z (FP64)][velocities (FP64, DAMP)][mass term (MASS)][element forces]
+    double* xs = reinterpret_cast<double*>(smem_raw);
+    double* ys = xs + A.max_local;
+    double* zs = ys + A.max_local;
+    double* vs = zs + A.max_local;
+    R* ws = reinterpret_cast<R*>(DAMP ? vs + 3 * A.max_local : vs);
     R* fe = MASS ? ws + 3 * A.max_local : ws;
 
     const int lb = A.node_off[tile];
     const int nl = A.node_off[tile + 1] - lb;
     if (MODE != TILE_FORCE_FROM_P) {
-        double u0[3], v0[3] = {0.0, 0.0, 0.0};
-        tile_anchor(A, A.ln_gid[lb], u0);
-        if (DAMP && sizeof(R) == 4) {  // FP32: velocities relative to the anchor too (Fdot = sum v_a (x) gradN_a)
-            const int g0 = A.ln_gid[lb];
-            v0[0] = A.v[3 * g0 + 0];
-            v0[1] = A.v[3 * g0 + 1];
-            v0[2] = A.v[3 * g0 + 2];
-        }
         for (int ln = t; ln < nl; ln += TE) {
             const int gid = A.ln_gid[lb + ln];
-            stage_pos(A, gid, u0, xs[ln], ys[ln], zs[ln]);
+            stage_pos(A, gid, xs[ln], ys[ln], zs[ln]);
             if (DAMP) {
-                vs[3 * ln + 0] = R(A.v[3 * gid + 0] - v0[0]);
-                vs[3 * ln + 1] = R(A.v[3 * gid + 1] - v0[1]);
-                vs[3 * ln + 2] = R(A.v[3 * gid + 2] - v0[2]);
+                vs[3 * ln + 0] = A.v[3 * gid + 0];
+                vs[3 * ln + 1] = A.v[3 * gid + 1];
+                vs[3 * ln + 2] = A.v[3 * gid + 2];
             }
             if (MASS) {
 #pragma unroll
@@ -624,6 +634,9 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
     R f[NPE][3];
 #pragma unroll
     for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
+    // the element's node values: FP32 reads them once per tile (element-relative, so
+    // the FP64 differences are taken once); FP64 re-reads them per QP (registers)
+    R xa[NPE][3], va[NPE][3];
 
 #pragma unroll 1
     for (int q = 0; q < NQP && MODE == TILE_FORCE; ++q) {
@@ -634,16 +647,9 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
         for (int m = 0; m < 9; ++m) ji[m] = ld_stream(jp + m * TE);
         const R dv = ld_stream(A.dv + ((size_t)tile * NQP + q) * TE + t);
         const R Lq[4] = {R(A.qb.L[q][0]), R(A.qb.L[q][1]), R(A.qb.L[q][2]), R(A.qb.L[q][3])};
-        R xa[NPE][3], va[NPE][3];
-#pragma unroll
-        for (int a = 0; a < NPE; ++a) {
-            xa[a][0] = xs[lc[a]];
-            xa[a][1] = ys[lc[a]];
-            xa[a][2] = zs[lc[a]];
-            if (DAMP) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d) va[a][d] = vs[3 * lc[a] + d];
-            }
+        if (q == 0 || sizeof(R) == 8) {
+            element_nodes<R, NPE>(xs, ys, zs, lc, xa);
+            if (DAMP) element_velocities<R, NPE>(vs, lc, va);
         }
         compact_qp<R, NPE, DAMP, false, MR>(A, xa, va, ji, dv, Lq, f);
         if constexpr (MASS) {
@@ -680,21 +686,23 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
             for (int i = 0; i < 3; ++i)
 #pragma unroll
                 for (int j = 0; j < 3; ++j) H[i][j] = Fd[i][j] = R(0);
+            if (q == 0 || sizeof(R) == 8) {
+                element_nodes<R, NPE>(xs, ys, zs, lc, xa);
+                if (DAMP) element_velocities<R, NPE>(vs, lc, va);
+            }
 #pragma unroll
-            for (int a = 0; a < NPE; ++a) {
-                const R xa[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+            for (int a = 0; a < NPE; ++a)
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) H[i][j] += xa[i] * g[a][j];
-            }
+                    for (int j = 0; j < 3; ++j) H[i][j] += xa[a][i] * g[a][j];
             if (DAMP) {
 #pragma unroll
                 for (int a = 0; a < NPE; ++a)
 #pragma unroll
                     for (int i = 0; i < 3; ++i)
 #pragma unroll
-                        for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc[a] + i] * g[a][j];
+                        for (int j = 0; j < 3; ++j) Fd[i][j] += va[a][i] * g[a][j];
             }
             tile_stress<R, DAMP, MR>(H, Fd, A, P);
         }
@@ -763,7 +771,8 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
 // Shared memory bytes of one tile block.
 template <typename R>
 inline size_t tile_smem_bytes(int npe, int max_local, bool damp, bool mass = false) {
-    return sizeof(R) * ((size_t)max_local * (3 + (damp ? 3 : 0) + (mass ? 3 : 0)) + (size_t)3 * npe * TILE_ELEMS);
+    return sizeof(double) * (size_t)max_local * (3 + (damp ? 3 : 0)) +
+           sizeof(R) * ((size_t)max_local * (mass ? 3 : 0) + (size_t)3 * npe * TILE_ELEMS);
 }
 
 }  // namespace tlfea

@@ -91,7 +91,7 @@ template <typename R, int NPE>
 inline size_t pipe_smem_bytes(int max_local, bool damp) {
     using G = PipeGeom<R, NPE>;
     size_t b = (size_t)G::STAGES * G::STAGE_BYTES;        // ring
-    b += 2 * 3 * (size_t)max_local * sizeof(R);           // positions, double-buffered
+    b += 2 * 3 * (size_t)max_local * sizeof(double);      // positions (FP64), double-buffered
     if (damp) b += 2 * 3 * (size_t)max_local * sizeof(double);  // velocities, double-buffered
     b += (size_t)3 * NPE * TILE_ELEMS * sizeof(R);        // element forces
     b = (b + 15) & ~size_t(15);
@@ -99,38 +99,25 @@ inline size_t pipe_smem_bytes(int max_local, bool damp) {
     return b;
 }
 
-// Stage tile `tile`'s node positions (and velocities): FP64 by cp.async copies;
-// FP32 as displacements relative to the tile's anchor node (stage_pos), which
-// takes FP64 arithmetic, so those are plain loads.
+// Stage tile `tile`'s node values (and velocities) in FP64: FP64 mode the positions
+// by cp.async copies; FP32 mode the displacements (stage_pos), plain loads.
 template <typename R, bool DAMP>
-__device__ __forceinline__ void prefetch_nodes(const TileArgs<R>& A, int tile, R* xs, R* ys, R* zs, double* vs) {
+__device__ __forceinline__ void prefetch_nodes(const TileArgs<R>& A, int tile, double* xs, double* ys, double* zs,
+                                               double* vs) {
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
-    double u0[3], v0[3] = {0.0, 0.0, 0.0};
-    tile_anchor(A, A.ln_gid[lb], u0);
-    if (DAMP && sizeof(R) == 4) {
-        const int g0 = A.ln_gid[lb];
-        v0[0] = A.v[3 * g0 + 0];
-        v0[1] = A.v[3 * g0 + 1];
-        v0[2] = A.v[3 * g0 + 2];
-    }
     for (int ln = threadIdx.x; ln < nl; ln += TILE_ELEMS) {
         const int gid = A.ln_gid[lb + ln];
         if constexpr (sizeof(R) == 8) {
-            cp_async<sizeof(R)>(xs + ln, A.px + gid);
-            cp_async<sizeof(R)>(ys + ln, A.py + gid);
-            cp_async<sizeof(R)>(zs + ln, A.pz + gid);
-            if (DAMP) {
-                cp_async<8>(vs + 3 * ln + 0, A.v + 3 * gid + 0);
-                cp_async<8>(vs + 3 * ln + 1, A.v + 3 * gid + 1);
-                cp_async<8>(vs + 3 * ln + 2, A.v + 3 * gid + 2);
-            }
+            cp_async<8>(xs + ln, A.px + gid);
+            cp_async<8>(ys + ln, A.py + gid);
+            cp_async<8>(zs + ln, A.pz + gid);
         } else {
-            stage_pos(A, gid, u0, xs[ln], ys[ln], zs[ln]);
-            if (DAMP) {
-                vs[3 * ln + 0] = A.v[3 * gid + 0] - v0[0];
-                vs[3 * ln + 1] = A.v[3 * gid + 1] - v0[1];
-                vs[3 * ln + 2] = A.v[3 * gid + 2] - v0[2];
-            }
+            stage_pos(A, gid, xs[ln], ys[ln], zs[ln]);
+        }
+        if (DAMP) {
+            cp_async<8>(vs + 3 * ln + 0, A.v + 3 * gid + 0);
+            cp_async<8>(vs + 3 * ln + 1, A.v + 3 * gid + 1);
+            cp_async<8>(vs + 3 * ln + 2, A.v + 3 * gid + 2);
         }
     }
 }
@@ -142,12 +129,12 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2) k_force_pipe(TileArgs<R> A, i
     constexpr int S = G::STAGES;
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char* ring = smem;
-    R* pos = reinterpret_cast<R*>(smem + (size_t)S * G::STAGE_BYTES);
+    double* pos = reinterpret_cast<double*>(smem + (size_t)S * G::STAGE_BYTES);
     const int ML = A.max_local;
-    double* vel = reinterpret_cast<double*>(pos + 6 * ML);
+    double* vel = pos + 6 * ML;
     R* fe = reinterpret_cast<R*>(DAMP ? reinterpret_cast<unsigned char*>(vel + 6 * ML)
                                       : reinterpret_cast<unsigned char*>(vel));
-    size_t bar_off = (size_t)S * G::STAGE_BYTES + 2 * 3 * (size_t)ML * sizeof(R) +
+    size_t bar_off = (size_t)S * G::STAGE_BYTES + 2 * 3 * (size_t)ML * sizeof(double) +
                      (DAMP ? 2 * 3 * (size_t)ML * sizeof(double) : 0) + (size_t)3 * NPE * TE * sizeof(R);
     bar_off = (bar_off + 15) & ~size_t(15);
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + bar_off);
@@ -201,16 +188,17 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2) k_force_pipe(TileArgs<R> A, i
         consumer_sync();  // positions of this tile visible; previous tile's reduction done
         const int next = tile + gridDim.x;
         if (next < n_tiles) {
-            R* nx = pos + (buf ^ 1) * 3 * ML;
+            double* nx = pos + (buf ^ 1) * 3 * ML;
             prefetch_nodes<R, DAMP>(A, next, nx, nx + ML, nx + 2 * ML, vel + (DAMP ? (buf ^ 1) * 3 * ML : 0));
         }
-        const R* xs = pos + buf * 3 * ML;
-        const R* ys = xs + ML;
-        const R* zs = ys + ML;
+        const double* xs = pos + buf * 3 * ML;
+        const double* ys = xs + ML;
+        const double* zs = ys + ML;
         const double* vs = vel + (DAMP ? buf * 3 * ML : 0);
 
         int lc[NPE];
         R f[NPE][3];
+        R ua[NPE][3], va[NPE][3];  // FP32: the element's node values, read once per tile
 #pragma unroll
         for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
 #pragma unroll 1
@@ -281,14 +269,16 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2) k_force_pipe(TileArgs<R> A, i
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
                     for (int j = 0; j < 3; ++j) H[i][j] = R(0);
+                if (q == 0) {
+                    element_nodes<R, NPE>(xs, ys, zs, lc, ua);
+                    if (DAMP) element_velocities<R, NPE>(vs, lc, va);
+                }
 #pragma unroll
-                for (int a = 0; a < NPE; ++a) {
-                    const R ua[3] = {xs[lc[a]], ys[lc[a]], zs[lc[a]]};
+                for (int a = 0; a < NPE; ++a)
 #pragma unroll
                     for (int i = 0; i < 3; ++i)
 #pragma unroll
-                        for (int j = 0; j < 3; ++j) H[i][j] += ua[i] * g[a][j];
-                }
+                        for (int j = 0; j < 3; ++j) H[i][j] += ua[a][i] * g[a][j];
                 R Em[3][3];
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
@@ -328,7 +318,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2) k_force_pipe(TileArgs<R> A, i
 #pragma unroll
                         for (int i = 0; i < 3; ++i)
 #pragma unroll
-                            for (int j = 0; j < 3; ++j) Fd[i][j] += R(vs[3 * lc[a] + i]) * g[a][j];
+                            for (int j = 0; j < 3; ++j) Fd[i][j] += va[a][i] * g[a][j];
                     kelvin_voigt<R>(F, Fd, A.eta, A.lamd, Pv);
 #pragma unroll
                     for (int i = 0; i < 3; ++i)
@@ -389,6 +379,67 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2) k_force_pipe(TileArgs<R> A, i
 // always in flight while the CTA computes.  The node positions are gathered by
 // the threads while the first two slices land.
 
+// Stage one tile's local nodes into shared memory: destination (global id, or
+// -(partial slot + 1) for a node shared with other tiles), incidence end, and the node
+// values in FP64 (stage_pos: positions, or displacements in FP32 mode), plus
+// velocities for the Kelvin-Voigt term.  The loads are dependent gathers (local node
+// -> global id -> values), so each thread first issues the table loads of up to
+// STAGE_NODES of its nodes, then their value loads, and only then stores: the
+// latencies overlap instead of adding up node by node.
+constexpr int STAGE_NODES = 4;
+
+template <typename R, bool DAMP>
+__device__ __forceinline__ void stage_tile_nodes(const TileArgs<R>& A, int lb, int nl, double* xs, double* ys,
+                                                 double* zs, int* dsts, uint16_t* iends, double* vs) {
+    constexpr int TE = TILE_ELEMS;
+    const int t = threadIdx.x;
+    int gid[STAGE_NODES], ps[STAGE_NODES];
+    uint16_t ie[STAGE_NODES];
+#pragma unroll
+    for (int k = 0; k < STAGE_NODES; ++k) {
+        const int ln = t + k * TE;
+        gid[k] = 0;
+        ps[k] = -1;
+        ie[k] = 0;
+        if (ln < nl) {
+            gid[k] = A.ln_gid[lb + ln];
+            ps[k] = A.ln_pslot[lb + ln];
+            ie[k] = A.ln_inc_end[lb + ln];
+        }
+    }
+    double vx[STAGE_NODES], vy[STAGE_NODES], vz[STAGE_NODES];
+#pragma unroll
+    for (int k = 0; k < STAGE_NODES; ++k)
+        if (t + k * TE < nl) stage_pos(A, gid[k], vx[k], vy[k], vz[k]);
+#pragma unroll
+    for (int k = 0; k < STAGE_NODES; ++k) {
+        const int ln = t + k * TE;
+        if (ln < nl) {
+            iends[ln] = ie[k];
+            dsts[ln] = (ps[k] < 0) ? gid[k] : -(ps[k] + 1);
+            xs[ln] = vx[k];
+            ys[ln] = vy[k];
+            zs[ln] = vz[k];
+        }
+    }
+    // tiles with more local nodes than STAGE_NODES per thread: the rest one by one
+    for (int ln = t + STAGE_NODES * TE; ln < nl; ln += TE) {
+        const int g = A.ln_gid[lb + ln];
+        const int p = A.ln_pslot[lb + ln];
+        iends[ln] = A.ln_inc_end[lb + ln];
+        dsts[ln] = (p < 0) ? g : -(p + 1);
+        stage_pos(A, g, xs[ln], ys[ln], zs[ln]);
+    }
+    if (DAMP) {
+        for (int ln = t; ln < nl; ln += TE) {
+            const int g = A.ln_gid[lb + ln];
+            vs[3 * ln + 0] = A.v[3 * g + 0];
+            vs[3 * ln + 1] = A.v[3 * g + 1];
+            vs[3 * ln + 2] = A.v[3 * g + 2];
+        }
+    }
+}
+
 template <typename R, int NPE>
 struct TileTmaGeom {
     static constexpr uint32_t GRAD_BYTES = NPE * 3 * TILE_ELEMS * sizeof(R);
@@ -416,7 +467,7 @@ struct TileTmaLayout {
         auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
         inc = G::STAGES * (size_t)G::STAGE_BYTES + G::LCONN_BYTES;
         pos = inc + G::INC_BYTES;
-        dst = al(pos + 3 * (size_t)max_local * sizeof(R));
+        dst = al(pos + 3 * (size_t)max_local * sizeof(double));
         iend = al(dst + (size_t)max_local * sizeof(int));
         vel = al(iend + (size_t)max_local * sizeof(uint16_t));
         bar = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
@@ -441,9 +492,9 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_for
     unsigned char* stage0 = smem;
     const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + S * G::STAGE_BYTES);
     const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
-    R* xs = reinterpret_cast<R*>(smem + L.pos);
-    R* ys = xs + ML;
-    R* zs = ys + ML;
+    double* xs = reinterpret_cast<double*>(smem + L.pos);
+    double* ys = xs + ML;
+    double* zs = ys + ML;
     int* dsts = reinterpret_cast<int*>(smem + L.dst);  // global node id, or -(partial slot + 1)
     uint16_t* iends = reinterpret_cast<uint16_t*>(smem + L.iend);
     double* vs = reinterpret_cast<double*>(smem + L.vel);
@@ -472,26 +523,7 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_for
         if (S > 1 && NQP > 1) issue(1);
     }
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
-    double u0[3], v0[3] = {0.0, 0.0, 0.0};
-    tile_anchor(A, A.ln_gid[lb], u0);
-    if (DAMP && sizeof(R) == 4) {  // FP32: velocities relative to the anchor too
-        const int g0 = A.ln_gid[lb];
-        v0[0] = A.v[3 * g0 + 0];
-        v0[1] = A.v[3 * g0 + 1];
-        v0[2] = A.v[3 * g0 + 2];
-    }
-    for (int ln = t; ln < nl; ln += TE) {
-        const int gid = A.ln_gid[lb + ln];
-        const int ps = A.ln_pslot[lb + ln];
-        iends[ln] = A.ln_inc_end[lb + ln];
-        dsts[ln] = (ps < 0) ? gid : -(ps + 1);
-        stage_pos(A, gid, u0, xs[ln], ys[ln], zs[ln]);
-        if (DAMP) {
-            vs[3 * ln + 0] = A.v[3 * gid + 0] - v0[0];
-            vs[3 * ln + 1] = A.v[3 * gid + 1] - v0[1];
-            vs[3 * ln + 2] = A.v[3 * gid + 2] - v0[2];
-        }
-    }
+    stage_tile_nodes<R, DAMP>(A, lb, nl, xs, ys, zs, dsts, iends, vs);
     __syncthreads();  // positions and node tables staged; barriers initialised
 
     if constexpr (sizeof(R) == 4) {
@@ -506,12 +538,23 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_for
 #pragma unroll
         for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
         float2 up[NP][3], f2[NP][3];
+        {
+            float ua[NPE][3];
+            element_nodes<float, NPE>(xs, ys, zs, lc, ua);
 #pragma unroll
-        for (int p = 0; p < NP; ++p) {
-            up[p][0] = make_float2(xs[lc[2 * p]], xs[lc[2 * p + 1]]);
-            up[p][1] = make_float2(ys[lc[2 * p]], ys[lc[2 * p + 1]]);
-            up[p][2] = make_float2(zs[lc[2 * p]], zs[lc[2 * p + 1]]);
-            f2[p][0] = f2[p][1] = f2[p][2] = make_float2(0.f, 0.f);
+            for (int p = 0; p < NP; ++p)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    up[p][d] = make_float2(ua[2 * p][d], ua[2 * p + 1][d]);
+                    f2[p][d] = make_float2(0.f, 0.f);
+                }
+        }
+        // velocities relative to the element's first node, differenced per QP (keeping
+        // them in registers would spill)
+        double vb[3] = {0.0, 0.0, 0.0};
+        if constexpr (DAMP) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) vb[d] = vs[3 * lc[0] + d];
         }
 #pragma unroll 1
         for (int q = 0; q < NQP; ++q) {
@@ -536,9 +579,10 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_for
                 if (DAMP) {
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
-                        const float2 va = make_float2((float)vs[3 * lc[2 * p] + i], (float)vs[3 * lc[2 * p + 1] + i]);
+                        const float2 v2 = make_float2(float(vs[3 * lc[2 * p] + i] - vb[i]),
+                                                      float(vs[3 * lc[2 * p + 1] + i] - vb[i]));
 #pragma unroll
-                        for (int j = 0; j < 3; ++j) fd2[i][j] = __ffma2_rn(va, g[j], fd2[i][j]);
+                        for (int j = 0; j < 3; ++j) fd2[i][j] = __ffma2_rn(v2, g[j], fd2[i][j]);
                     }
                 }
             }
@@ -717,7 +761,7 @@ struct TileGeoLayout {
         lconn = G::REGION0;
         inc = lconn + G::LCONN_BYTES;
         pos = inc + G::INC_BYTES;
-        dst = al(pos + 3 * (size_t)max_local * sizeof(R));
+        dst = al(pos + 3 * (size_t)max_local * sizeof(double));
         iend = al(dst + (size_t)max_local * sizeof(int));
         vel = al(iend + (size_t)max_local * sizeof(uint16_t));
         bar = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
@@ -741,9 +785,9 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, in
     unsigned char* stage0 = smem;
     const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + L.lconn);
     const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
-    R* xs = reinterpret_cast<R*>(smem + L.pos);
-    R* ys = xs + ML;
-    R* zs = ys + ML;
+    double* xs = reinterpret_cast<double*>(smem + L.pos);
+    double* ys = xs + ML;
+    double* zs = ys + ML;
     int* dsts = reinterpret_cast<int*>(smem + L.dst);  // global node id, or -(partial slot + 1)
     uint16_t* iends = reinterpret_cast<uint16_t*>(smem + L.iend);
     double* vs = reinterpret_cast<double*>(smem + L.vel);
@@ -771,30 +815,11 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, in
         if (NQP > 1) issue(1);
     }
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
-    double u0[3], v0[3] = {0.0, 0.0, 0.0};
-    tile_anchor(A, A.ln_gid[lb], u0);
-    if (DAMP && sizeof(R) == 4) {  // FP32: velocities relative to the anchor too
-        const int g0 = A.ln_gid[lb];
-        v0[0] = A.v[3 * g0 + 0];
-        v0[1] = A.v[3 * g0 + 1];
-        v0[2] = A.v[3 * g0 + 2];
-    }
-    for (int ln = t; ln < nl; ln += TE) {
-        const int gid = A.ln_gid[lb + ln];
-        const int ps = A.ln_pslot[lb + ln];
-        iends[ln] = A.ln_inc_end[lb + ln];
-        dsts[ln] = (ps < 0) ? gid : -(ps + 1);
-        stage_pos(A, gid, u0, xs[ln], ys[ln], zs[ln]);
-        if (DAMP) {
-            vs[3 * ln + 0] = A.v[3 * gid + 0] - v0[0];
-            vs[3 * ln + 1] = A.v[3 * gid + 1] - v0[1];
-            vs[3 * ln + 2] = A.v[3 * gid + 2] - v0[2];
-        }
-    }
+    stage_tile_nodes<R, DAMP>(A, lb, nl, xs, ys, zs, dsts, iends, vs);
     __syncthreads();  // positions and node tables staged; barriers initialised
 
     int lc[NPE];
-    R f[NPE][3];
+    R f[NPE][3], xa[NPE][3], va[NPE][3];
 #pragma unroll 1
     for (int q = 0; q < NQP; ++q) {
         if (!mbar_wait(bar0 + 8 * (q & 1), (q >> 1) & 1)) atomicExch(err, 3);
@@ -815,16 +840,9 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, in
             if (t == 0) issue(q + 2);
         }
         const R Lq[4] = {R(A.qb.L[q][0]), R(A.qb.L[q][1]), R(A.qb.L[q][2]), R(A.qb.L[q][3])};
-        R xa[NPE][3], va[NPE][3];
-#pragma unroll
-        for (int a = 0; a < NPE; ++a) {
-            xa[a][0] = xs[lc[a]];
-            xa[a][1] = ys[lc[a]];
-            xa[a][2] = zs[lc[a]];
-            if (DAMP) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d) va[a][d] = R(vs[3 * lc[a] + d]);
-            }
+        if (q == 0 || sizeof(R) == 8) {  // FP32 keeps the element-relative values in registers
+            element_nodes<R, NPE>(xs, ys, zs, lc, xa);
+            if (DAMP) element_velocities<R, NPE>(vs, lc, va);
         }
         // F (FP64) or H (FP32), the stress, f_a (+)= (dV P J^-T) dN_a/dxi
         // (FEAT10DataFunc.cuh:417-449 with gradN = J^-T dN/dxi)
