@@ -181,6 +181,10 @@ int tlfea_element_set_force_precision(tlfea_element h, int precision);
  * geometry stream (J^-1 and dV per QP, gradients formed in registers);
  * grid_limit caps the persistent grid (0 = all resident blocks). */
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit);
+/* L2 prefetch of the one-tile-per-block force kernels (force_kernel 0 and 3; new):
+ * each tile prefetches into L2 the streams of the tile one wave of resident blocks
+ * later, so the next wave's bulk copies hit L2.  On (1) by default; 0 turns it off. */
+int tlfea_element_set_l2_prefetch(tlfea_element h, int on);
 
 /* Allocation-free internal force.  No counterpart in the reference.
  *
@@ -339,12 +343,18 @@ int tlfea_batch_set_initial_guess(tlfea_batch b, const double* u0, long long n, 
  * The residual and status reported are the FP64 ones, the iterations the sum
  * over passes.  FP32 solves are not graph-captured. */
 int tlfea_batch_set_precision(tlfea_batch b, int precision);
-/* Launch shape: resident blocks per SM of the persistent kernel (0 = occupancy
- * maximum) and nodes per reduction chunk (0 = keep). */
+/* Launch mode: 0 (default) = one kernel per CG phase (element tiles, p.q, update,
+ * direction) at the occupancy each allows, chunks of iterations replayed as CUDA
+ * graphs until every instance is done; 1 = the whole solve in one persistent
+ * cooperative launch with grid barriers between the phases. */
+int tlfea_batch_set_mode(tlfea_batch b, int mode);
+/* Launch shape: resident blocks per SM of the persistent kernel (mode 1; 0 =
+ * occupancy maximum) and nodes per reduction chunk (0 = keep). */
 int tlfea_batch_set_launch(tlfea_batch b, int blocks_per_sm, int chunk_nodes);
 int tlfea_batch_get_launch(tlfea_batch b, int* blocks_per_sm, int* chunk_nodes, int* grid);
-/* Times trial_iters CG iterations per (blocks per SM, chunk size) candidate and
- * keeps the fastest; overwrites the solution vectors. */
+/* Times trial_iters CG iterations per candidate and keeps the fastest: chunk sizes
+ * (mode 0; best_blocks_per_sm = 0), or (blocks per SM, chunk size) pairs (mode 1).
+ * Overwrites the solution vectors. */
 int tlfea_batch_autotune(tlfea_batch b, int trial_iters, int* best_blocks_per_sm, int* best_chunk, float* best_ms);
 /* Solves every instance; per-instance iterations, ||r||/||f_free|| and status
  * (0 converged, 1 non-positive p.Kp, 2 max_iter reached). */

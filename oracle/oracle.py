@@ -2,8 +2,9 @@
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this module, and only as the checker / reported CPU baseline.  Layouts are the
-reference's device layouts (see tlfea_oracle.h).  Parity status: unpinned by
-reference-run data; pinned by analytic known-answer tests (tests/test_oracle.py).
+reference's device layouts (see tlfea_oracle.h).  Parity status: pinned to fixtures
+written by the reference's own CUDA build (tests/golden/ref_*.npz, checked by
+tests/test_ref_fixtures.py) and by analytic known-answer tests (tests/test_oracle.py).
 """
 from __future__ import annotations
 

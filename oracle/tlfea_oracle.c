@@ -8,8 +8,9 @@
  * reference scatters element forces and stiffness blocks with atomicAdd in an
  * unspecified order; here they are added in element order (deterministic).
  *
- * Parity: unpinned by reference-run data (the reference ships none and cannot
- * be built here); pinned by analytic known-answer tests in tests/.
+ * Parity: pinned to fixtures written by the reference's own CUDA build
+ * (tests/golden/ref_*.npz, checked by tests/test_ref_fixtures.py) and by analytic
+ * known-answer tests in tests/.
  */
 #include "tlfea_oracle.h"
 

@@ -14,12 +14,16 @@
  *   detJ(e,q)          detJ[e*QP+q]
  *   nodal vectors      SoA x/y/z (length N); forces/velocities interleaved [3*node+d]
  *
- * Parity status: the reference ships no golden vectors, known-answer tests or
- * fixtures for this path, and its own build needs Eigen3 and the un-vendored
- * MoPhiEssentials submodule.  The restatement is pinned by analytic
- * known-answer tests (rigid motion, patch tests, mass = rho*V, stiffness rigid
- * modes and symmetry, CG vs a direct solve) and by the reference's own mesh
- * fixtures, not by reference outputs: parity unpinned by reference-run data.
+ * Parity status: pinned to the reference's own CUDA build.  The reference ships no
+ * golden vectors for this path, and its own build system needs Eigen3 and the
+ * un-vendored MoPhiEssentials submodule; oracle/build_ref.py compiles its unchanged
+ * element and solver sources for sm_100a against project-written stand-ins for those
+ * two headers (oracle/refshim), and tests/golden/make_ref_fixtures.py ran that build
+ * on a B200 to write tests/golden/ref_*.npz (geometry, mass, forces, P, stiffness,
+ * CG, SyncedNesterov / SyncedAdamW trajectories, constraint arrays).
+ * tests/test_ref_fixtures.py checks this restatement against those fixtures; the
+ * analytic known-answer tests (rigid motion, patch tests, mass = rho*V, stiffness
+ * rigid modes and symmetry, CG vs a direct solve) stay beside them.
  */
 #ifndef TLFEA_ORACLE_H
 #define TLFEA_ORACLE_H

@@ -190,10 +190,14 @@ def test_batch_fp32_elements_with_fp64_refinement():
 def test_batch_autotune_and_replay_determinism():
     insts = _instances(8)
     b = _batch(insts)
+    b.SetMode("persistent")
     cfg = b.Autotune(4)
     assert cfg["blocks_per_sm"] >= 1 and cfg["chunk_nodes"] in (128, 256, 512, 1024)
     L = b.GetLaunch()
     assert L["blocks_per_sm"] == cfg["blocks_per_sm"] and L["grid"] > 0
+    b.SetMode("phased")  # per-phase launches tune the chunk size only
+    cfg = b.Autotune(4)
+    assert cfg["blocks_per_sm"] == 0 and cfg["chunk_nodes"] in (128, 256, 512, 1024)
     b.Solve(1e-9, 20000)
     u1 = b.RetrieveDisplacement(split=False)
     r1 = b.GetResults()
@@ -205,6 +209,52 @@ def test_batch_autotune_and_replay_determinism():
     b.Solve(1e-9, 20000)
     u3 = b.RetrieveDisplacement(split=False)
     assert rel(u3, u1) < 1e-7
+    b.Destroy()
+
+
+@pytest.mark.parametrize("shared", [False, True])
+def test_phased_and_persistent_launches_agree_bitwise(shared):
+    """The per-phase kernels (default) and the persistent cooperative launch run the
+    same phase code with the same fixed summation orders: bitwise the same solution,
+    iteration counts and residuals, cold and warm, and the same FP32-refined answer."""
+    if shared:
+        d0 = M.random_beam(5, order=10, **SMALL)
+        r = np.random.default_rng(4)
+        n = 11
+        b = T.BatchedLinearStaticSolver([(d0["x"], d0["y"], d0["z"], d0["conn"])] * n, T.TYPE_T10, shared=True)
+        b.SetMaterial(np.exp(r.uniform(np.log(1e6), np.log(1e9), n)), r.uniform(0.2, 0.45, n))
+        b.SetNodalFixed([d0["fixed"]] * n)
+        b.SetExternalForce([d0["f"] * s for s in r.uniform(0.5, 2.0, n)])
+    else:
+        b = _batch(_instances(9))
+    out = {}
+    for mode in ("persistent", "phased"):
+        b.SetMode(mode)
+        b.SetInitialGuess(None)
+        b.Solve(1e-9, 20000)
+        u = b.RetrieveDisplacement(split=False)
+        res = b.GetResults()
+        b.SetInitialGuess(0.9 * u)
+        b.Solve(1e-9, 20000)
+        uw = b.RetrieveDisplacement(split=False)
+        resw = b.GetResults()
+        b.SetInitialGuess(None)
+        b.SetPrecision("fp32")
+        b.Solve(1e-8, 20000)
+        u32 = b.RetrieveDisplacement(split=False)
+        b.SetPrecision("fp64")
+        b.Solve(1e-12, 7)  # the iteration cap ends every instance with status 2
+        capped = b.GetResults()
+        out[mode] = (u, res, uw, resw, u32, capped)
+    a, c = out["persistent"], out["phased"]
+    assert np.all(a[1][2] == 0) and np.all(a[3][2] == 0)
+    assert np.all(c[5][0] == 7) and np.all(c[5][2] == 2)
+    for x, y in zip(a, c):
+        if isinstance(x, tuple):
+            for xx, yy in zip(x, y):
+                assert np.array_equal(xx, yy)
+        else:
+            assert np.array_equal(x, y)
     b.Destroy()
 
 

@@ -107,6 +107,7 @@ _SIGS = {
     "tlfea_element_compute_internal_force": [_P, _P],
     "tlfea_element_set_force_precision": [_P, C.c_int],
     "tlfea_element_set_launch_config": [_P, C.c_int, C.c_int],
+    "tlfea_element_set_l2_prefetch": [_P, C.c_int],
     "tlfea_element_compute_internal_force_noalloc": [_P, _P, _P],
     "tlfea_element_get_mass_nnz": [_P, C.POINTER(_LL)],
     "tlfea_element_retrieve_mass_csr": [_P, _I, _I, _D],
@@ -163,6 +164,7 @@ _SIGS = {
     "tlfea_batch_set_initial_guess": [_P, _P, _LL, C.c_int],
     "tlfea_batch_set_precision": [_P, C.c_int],
     "tlfea_batch_set_launch": [_P, C.c_int, C.c_int],
+    "tlfea_batch_set_mode": [_P, C.c_int],
     "tlfea_batch_get_launch": [_P, _I, _I, _I],
     "tlfea_batch_autotune": [_P, C.c_int, _I, _I, C.POINTER(C.c_float)],
     "tlfea_batch_solve": [_P, C.c_double, C.c_int],

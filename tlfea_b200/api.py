@@ -182,6 +182,11 @@ class _TetData(ElementBase):
         k = self.FORCE_KERNELS[force_kernel] if isinstance(force_kernel, str) else int(force_kernel)
         capi.call("tlfea_element_set_launch_config", self._handle(), k, int(grid_limit))
 
+    def SetL2Prefetch(self, on: bool = True):
+        """New: whether the one-tile-per-block force kernels ("tma", "compact") prefetch
+        into L2 the streams of the tile one wave of resident blocks later (default on)."""
+        capi.call("tlfea_element_set_l2_prefetch", self._handle(), 1 if on else 0)
+
     # -- retrieval ---------------------------------------------------------------
     def RetrieveMassCSRToCPU(self):
         nnz = C.c_longlong()
@@ -611,6 +616,13 @@ class BatchedLinearStaticSolver:
 
     def SetLaunch(self, blocks_per_sm: int = 0, chunk_nodes: int = 0):
         capi.call("tlfea_batch_set_launch", self._h, int(blocks_per_sm), int(chunk_nodes))
+
+    MODES = {"phased": 0, "persistent": 1}
+
+    def SetMode(self, mode: str = "phased"):
+        """New: "phased" (default) -- one kernel per CG phase, chunks of iterations
+        replayed as CUDA graphs -- or "persistent" (one cooperative launch)."""
+        capi.call("tlfea_batch_set_mode", self._h, self.MODES[mode])
 
     def GetLaunch(self) -> dict:
         a, b, c = C.c_int(), C.c_int(), C.c_int()

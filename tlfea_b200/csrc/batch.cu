@@ -31,6 +31,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -63,19 +64,28 @@ struct tlfea_batch_s {
     double *u = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *f = nullptr, *u0 = nullptr;
     double *cpa = nullptr, *cpb = nullptr;  // per-chunk partials
     double *rr = nullptr, *fnorm = nullptr, *rel = nullptr;  // rr: 2 * n_inst (iteration parity)
-    int *iters = nullptr, *status = nullptr, *done = nullptr, *n_done = nullptr;
+    int *iters = nullptr, *status = nullptr, *done = nullptr;
+    int* n_done = nullptr;  // [0] instances done, [1] the per-phase launches' iteration counter
     double *alpha = nullptr, *beta = nullptr;  // per instance, folded once per phase
     int *flag = nullptr, *ticket = nullptr;    // per instance: 0 go, 1 converged, 2 broke down; fold tickets
     bool warm = false;
     bool material_set = false;
     // launch
-    int blocks_per_sm = 0;  // 0 = occupancy maximum
+    int mode = 0;           // 0 = per-phase kernels, 1 = one persistent cooperative launch
+    int blocks_per_sm = 0;  // persistent launch: 0 = occupancy maximum
     cudaGraphExec_t graph = nullptr;  // the captured cold-start solve
     cudaGraphExec_t graph_w = nullptr;  // the captured warm-start solve
     double graph_tol = -1.0;
     int graph_max_iter = -1;
     int graph_grid = -1;
     int graph_precision = -1;
+    // per-phase launches: captured chunks of iterations, keyed by what they bake in
+    struct PhaseGraph {
+        int precision, max_iter, iters;
+        double tol;
+        cudaGraphExec_t exec;
+    };
+    std::vector<PhaseGraph> phase_graphs;
     // FP32 element work: iterations summed over the refinement passes
     std::vector<int> iters_total;
     bool refined = false;
@@ -87,6 +97,8 @@ static void drop_graphs(tlfea_batch_s* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     if (b->graph_w) cudaGraphExecDestroy(b->graph_w);
     b->graph = b->graph_w = nullptr;
+    for (auto& g : b->phase_graphs) cudaGraphExecDestroy(g.exec);
+    b->phase_graphs.clear();
 }
 
 namespace tlfea {
@@ -127,6 +139,7 @@ struct BatchArgs {
     int *iters, *status, *done, *n_done;
     double *alpha, *beta;
     int *flag, *ticket;
+    int* it_dev;  // per-phase launches: the device-side iteration counter
     QpBary qb;
 };
 
@@ -494,15 +507,18 @@ __device__ __forceinline__ void apply_all_tiles(const BatchArgs<R>& A, const dou
     }
 }
 
-// The whole batched solve.  mode: 0 = solve, 1 = y = K_bc x only (x in p, y in q).
-template <typename R, int NPE, int NQP, bool SH>
-__global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double tol, int max_iter, int warm) {
-    cg::grid_group grid = cg::this_grid();
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double red[32];
-    const int t = threadIdx.x;
+// ---------------------------------------------------------------------------
+// The phases of the batched CG.  Each is a grid-stride loop, so the persistent
+// kernel (one cooperative launch, grid barriers between phases) and the
+// per-phase kernels (one launch per phase, stream order between them) run the
+// same code.  Chunk phases run one block per chunk; node phases of an iteration
+// run one warp per chunk (no block barriers): a chunk's partial is the warp's
+// lane-strided sum folded by shuffles, so its bits are fixed.
 
-    // ---- prologue: u = u0, r = f_free, ||f_free|| per chunk
+// u = u0 (warm) or 0, r = f_free, p = u; ||f_free||^2 per chunk into cpa.
+template <typename R>
+__device__ __forceinline__ void bcg_start(const BatchArgs<R>& A, int warm, double* red) {
+    const int t = threadIdx.x;
     for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
         double sf = 0.0;
         for (int i = A.chunk_beg[c] + t; i < A.chunk_beg[c + 1]; i += blockDim.x) {
@@ -520,11 +536,12 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
         const double s = block_sum(sf, red);
         if (t == 0) A.cpa[c] = s;
     }
-    grid.sync();
-    if (warm) {
-        apply_all_tiles<R, NPE, NQP, SH>(A, A.p, A.q, smem, false);
-        grid.sync();
-    }
+}
+
+// r -= K u0 (warm: q holds K p with p = u0), p = r; ||r||^2 per chunk into cpb.
+template <typename R>
+__device__ __forceinline__ void bcg_start_residual(const BatchArgs<R>& A, int warm, double* red) {
+    const int t = threadIdx.x;
     for (int c = blockIdx.x; c < A.n_chunks; c += gridDim.x) {
         double sr = 0.0;
         for (int i = A.chunk_beg[c] + t; i < A.chunk_beg[c + 1]; i += blockDim.x) {
@@ -541,7 +558,12 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
         const double s = block_sum(sr, red);
         if (t == 0) A.cpb[c] = s;
     }
-    grid.sync();
+}
+
+// Per instance: ||f_free||, rr_0, the initial relative residual and the start state.
+template <typename R>
+__device__ __forceinline__ void bcg_init(const BatchArgs<R>& A, double tol) {
+    const int t = threadIdx.x;
     for (int b = blockIdx.x; b < A.n_inst; b += gridDim.x) {
         if (t < 32) {
             const double ff = inst_sum(A.cpa, A.inst_chunk, b);
@@ -562,186 +584,294 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double 
             }
         }
     }
-    grid.sync();
+}
 
-    // ---- CG iterations.  The per-instance scalars are folded once per phase, by
-    // the chunk-block of the instance that posts its partial last (a ticket per
-    // instance; the fold runs in chunk order, so its bits do not depend on which
-    // block it is): alpha in the p.q phase, then rr_new, the convergence test and
-    // beta in the r.r phase.  The next phase reads them after the grid barrier.
-    // done[] changes only in the last phase of an iteration, so every other
-    // phase branches on it uniformly.
-    // Node phases run one warp per chunk (no block barriers): a chunk's partial
-    // is the warp's lane-strided sum folded by shuffles, so its bits are fixed.
-    const int lane = t & 31;
-    const int gw = blockIdx.x * (TILE_ELEMS / 32) + (t >> 5), n_warps = gridDim.x * (TILE_ELEMS / 32);
-    auto post_last = [&](double* part, int c, int b, double s) -> bool {  // s: the warp's sum (all lanes)
-        int last = 0;
-        if (lane == 0) {
-            part[c] = s;
-            __threadfence();
-            const int nch = A.inst_chunk[b + 1] - A.inst_chunk[b];
-            const int tk = atomicAdd(A.ticket + b, 1);
-            last = (tk == nch - 1);
-            if (last) A.ticket[b] = 0;  // every ticket of this phase is taken
-        }
-        last = __shfl_sync(0xffffffffu, last, 0);
-        if (last) __threadfence();
-        return last != 0;
-    };
-    for (int it = 0; it < max_iter; ++it) {
-        if (atomicAdd(A.n_done, 0) >= A.n_inst) break;  // uniform: read after a grid barrier
-        const double* rr_old = A.rr + (size_t)(it & 1) * A.n_inst;
-        double* rr_new_out = A.rr + (size_t)((it + 1) & 1) * A.n_inst;
-        // q = K p
-        apply_all_tiles<R, NPE, NQP, SH>(A, A.p, A.q, smem, true);
-        grid.sync();
-        // complete q, p.q per chunk; alpha = rr / p.q
-        for (int c = gw; c < A.n_chunks; c += n_warps) {
-            const int b = A.chunk_inst[c];
-            const int i_end = A.chunk_beg[c + 1];
-            if (__ldcg(A.done + b)) continue;
-            double s = 0.0;
-            // two nodes per lane per step: every load of both is issued before
-            // the first use (the chunk's nodes all belong to instance b)
-            const int noff = A.tiles_per_inst ? b * A.nodes_per_inst : 0;
-            const int poff = A.tiles_per_inst ? b * A.pslots_per_inst : 0;
-            for (int i0 = A.chunk_beg[c] + lane; i0 < i_end; i0 += 64) {
-                double pv[2][3], qv[2][3];
-                int fx[2], bi[2];
+// Post a chunk's partial; true (in every lane) for the warp whose post completes the
+// instance.  The per-instance scalars of a phase are folded once, in chunk order, by
+// that warp (a ticket per instance), so their bits do not depend on which warp it is.
+template <typename R>
+__device__ __forceinline__ bool bcg_post_last(const BatchArgs<R>& A, double* part, int c, int b, double s) {
+    const int lane = threadIdx.x & 31;
+    int last = 0;
+    if (lane == 0) {
+        part[c] = s;
+        __threadfence();
+        const int nch = A.inst_chunk[b + 1] - A.inst_chunk[b];
+        const int tk = atomicAdd(A.ticket + b, 1);
+        last = (tk == nch - 1);
+        if (last) A.ticket[b] = 0;  // every ticket of this phase is taken
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) __threadfence();
+    return last != 0;
+}
+
+// Complete q = K p at the nodes (partials of shared nodes, zero at fixed ones), p.q
+// per chunk; alpha = rr / p.q per instance (iteration `it`).
+template <typename R>
+__device__ __forceinline__ void bcg_pq(const BatchArgs<R>& A, int it) {
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), n_warps = gridDim.x * (blockDim.x / 32);
+    const double* rr_old = A.rr + (size_t)(it & 1) * A.n_inst;
+    for (int c = gw; c < A.n_chunks; c += n_warps) {
+        const int b = A.chunk_inst[c];
+        const int i_end = A.chunk_beg[c + 1];
+        if (__ldcg(A.done + b)) continue;
+        double s = 0.0;
+        // two nodes per lane per step: every load of both is issued before
+        // the first use (the chunk's nodes all belong to instance b)
+        const int noff = A.tiles_per_inst ? b * A.nodes_per_inst : 0;
+        const int poff = A.tiles_per_inst ? b * A.pslots_per_inst : 0;
+        for (int i0 = A.chunk_beg[c] + lane; i0 < i_end; i0 += 64) {
+            double pv[2][3], qv[2][3];
+            int fx[2], bi[2];
 #pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    const int i = i0 + 32 * k;
-                    const bool ok = i < i_end;
-                    fx[k] = ok ? A.fixed[i] : 1;
-                    bi[k] = ok ? A.node_bidx[i - noff] : -1;
+            for (int k = 0; k < 2; ++k) {
+                const int i = i0 + 32 * k;
+                const bool ok = i < i_end;
+                fx[k] = ok ? A.fixed[i] : 1;
+                bi[k] = ok ? A.node_bidx[i - noff] : -1;
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        pv[k][d] = ok ? __ldcg(A.p + 3 * i + d) : 0.0;
-                        qv[k][d] = ok ? __ldcg(A.q + 3 * i + d) : 0.0;
-                    }
-                }
-                int kb[2], ke[2];
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    kb[k] = (bi[k] >= 0) ? A.bnode_off[bi[k]] : 0;
-                    ke[k] = (bi[k] >= 0) ? A.bnode_off[bi[k] + 1] : 0;
-                }
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    const int i = i0 + 32 * k;
-                    if (bi[k] >= 0) {
-                        R s0 = R(0), s1 = R(0), s2 = R(0);
-                        for (int m = kb[k]; m < ke[k]; ++m) {
-                            const R* pt = A.partial + 3 * (size_t)(poff + m);
-                            s0 += __ldcg(pt + 0);
-                            s1 += __ldcg(pt + 1);
-                            s2 += __ldcg(pt + 2);
-                        }
-                        qv[k][0] = double(s0);
-                        qv[k][1] = double(s1);
-                        qv[k][2] = double(s2);
-                    }
-                    if (fx[k]) qv[k][0] = qv[k][1] = qv[k][2] = 0.0;
-                    if (i < i_end) {
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) A.q[3 * i + d] = qv[k][d];
-                    }
-                    s += pv[k][0] * qv[k][0] + pv[k][1] * qv[k][1] + pv[k][2] * qv[k][2];
+                for (int d = 0; d < 3; ++d) {
+                    pv[k][d] = ok ? __ldcg(A.p + 3 * i + d) : 0.0;
+                    qv[k][d] = ok ? __ldcg(A.q + 3 * i + d) : 0.0;
                 }
             }
-            s = warp_sum(s);
-            if (post_last(A.cpa, c, b, s)) {
-                const double pq = inst_sum(A.cpa, A.inst_chunk, b);
-                if (lane == 0) {
-                    // non-positive p.Kp: the reference aborts this solve (flag 2)
-                    A.alpha[b] = (pq > 0.0) ? __ldcg(rr_old + b) / pq : 0.0;
-                    A.flag[b] = (pq > 0.0) ? 0 : 2;
+            int kb[2], ke[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                kb[k] = (bi[k] >= 0) ? A.bnode_off[bi[k]] : 0;
+                ke[k] = (bi[k] >= 0) ? A.bnode_off[bi[k] + 1] : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int i = i0 + 32 * k;
+                if (bi[k] >= 0) {
+                    R s0 = R(0), s1 = R(0), s2 = R(0);
+                    for (int m = kb[k]; m < ke[k]; ++m) {
+                        const R* pt = A.partial + 3 * (size_t)(poff + m);
+                        s0 += __ldcg(pt + 0);
+                        s1 += __ldcg(pt + 1);
+                        s2 += __ldcg(pt + 2);
+                    }
+                    qv[k][0] = double(s0);
+                    qv[k][1] = double(s1);
+                    qv[k][2] = double(s2);
                 }
+                if (fx[k]) qv[k][0] = qv[k][1] = qv[k][2] = 0.0;
+                if (i < i_end) {
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) A.q[3 * i + d] = qv[k][d];
+                }
+                s += pv[k][0] * qv[k][0] + pv[k][1] * qv[k][1] + pv[k][2] * qv[k][2];
             }
         }
-        grid.sync();
-        // u += alpha p; r -= alpha q; r.r per chunk; then rr_new, the test, beta
-        for (int c = gw; c < A.n_chunks; c += n_warps) {
-            const int b = A.chunk_inst[c];
-            const int dn = __ldcg(A.done + b), fl = __ldcg(A.flag + b);  // loads issued together
-            const double alpha = __ldcg(A.alpha + b);
-            if (dn || fl == 2) continue;
-            double s = 0.0;
-            // flat over the chunk's 3n values, four per lane per step with every
-            // load issued before the first store
+        s = warp_sum(s);
+        if (bcg_post_last(A, A.cpa, c, b, s)) {
+            const double pq = inst_sum(A.cpa, A.inst_chunk, b);
+            if (lane == 0) {
+                // non-positive p.Kp: the reference aborts this solve (flag 2)
+                A.alpha[b] = (pq > 0.0) ? __ldcg(rr_old + b) / pq : 0.0;
+                A.flag[b] = (pq > 0.0) ? 0 : 2;
+            }
+        }
+    }
+}
+
+// u += alpha p; r -= alpha q; r.r per chunk; then rr_new, the test and beta.
+template <typename R>
+__device__ __forceinline__ void bcg_update(const BatchArgs<R>& A, int it, double tol, int max_iter) {
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), n_warps = gridDim.x * (blockDim.x / 32);
+    const double* rr_old = A.rr + (size_t)(it & 1) * A.n_inst;
+    double* rr_new_out = A.rr + (size_t)((it + 1) & 1) * A.n_inst;
+    for (int c = gw; c < A.n_chunks; c += n_warps) {
+        const int b = A.chunk_inst[c];
+        const int dn = __ldcg(A.done + b), fl = __ldcg(A.flag + b);  // loads issued together
+        const double alpha = __ldcg(A.alpha + b);
+        if (dn || fl == 2) continue;
+        double s = 0.0;
+        // flat over the chunk's 3n values, eight per lane per step with every
+        // load issued before the first store
+        const int j1 = 3 * A.chunk_beg[c + 1];
+        for (int j0 = 3 * A.chunk_beg[c] + lane; j0 < j1; j0 += 256) {
+            double uv[8], pv[8], rv[8], qv[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int j = j0 + 32 * k;
+                const bool ok = j < j1;
+                uv[k] = ok ? __ldcg(A.u + j) : 0.0;
+                pv[k] = ok ? __ldcg(A.p + j) : 0.0;
+                rv[k] = ok ? __ldcg(A.r + j) : 0.0;
+                qv[k] = ok ? __ldcg(A.q + j) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int j = j0 + 32 * k;
+                const double rj = rv[k] - alpha * qv[k];
+                if (j < j1) {
+                    A.u[j] = uv[k] + alpha * pv[k];
+                    A.r[j] = rj;
+                }
+                s += rj * rj;
+            }
+        }
+        s = warp_sum(s);
+        if (bcg_post_last(A, A.cpb, c, b, s)) {
+            const double rrn = inst_sum(A.cpb, A.inst_chunk, b);
+            if (lane == 0) {
+                const double rel = sqrt(rrn) / __ldcg(A.fnorm + b);
+                const bool conv = rel < tol;
+                rr_new_out[b] = rrn;
+                A.beta[b] = rrn / __ldcg(rr_old + b);
+                A.iters[b] = it + 1;
+                A.rel[b] = rel;
+                A.flag[b] = conv ? 1 : 0;
+                if (!conv && it + 1 >= max_iter) A.status[b] = 2;
+            }
+        }
+    }
+}
+
+// p = r + beta p; instances that converged or broke down retire (their first chunk
+// sets done; every warp skips them either way).
+template <typename R>
+__device__ __forceinline__ void bcg_direction(const BatchArgs<R>& A) {
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), n_warps = gridDim.x * (blockDim.x / 32);
+    for (int c = gw; c < A.n_chunks; c += n_warps) {
+        const int b = A.chunk_inst[c];
+        const int dn = __ldcg(A.done + b), fl = __ldcg(A.flag + b);  // loads issued together
+        const double beta = __ldcg(A.beta + b);
+        if (dn) continue;
+        if (fl == 0) {
             const int j1 = 3 * A.chunk_beg[c + 1];
             for (int j0 = 3 * A.chunk_beg[c] + lane; j0 < j1; j0 += 256) {
-                double uv[8], pv[8], rv[8], qv[8];
+                double pv[8], rv[8];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const int j = j0 + 32 * k;
-                    const bool ok = j < j1;
-                    uv[k] = ok ? __ldcg(A.u + j) : 0.0;
-                    pv[k] = ok ? __ldcg(A.p + j) : 0.0;
-                    rv[k] = ok ? __ldcg(A.r + j) : 0.0;
-                    qv[k] = ok ? __ldcg(A.q + j) : 0.0;
+                    pv[k] = (j < j1) ? __ldcg(A.p + j) : 0.0;
+                    rv[k] = (j < j1) ? __ldcg(A.r + j) : 0.0;
                 }
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const int j = j0 + 32 * k;
-                    const double rj = rv[k] - alpha * qv[k];
-                    if (j < j1) {
-                        A.u[j] = uv[k] + alpha * pv[k];
-                        A.r[j] = rj;
-                    }
-                    s += rj * rj;
+                    if (j < j1) A.p[j] = rv[k] + beta * pv[k];
                 }
             }
-            s = warp_sum(s);
-            if (post_last(A.cpb, c, b, s)) {
-                const double rrn = inst_sum(A.cpb, A.inst_chunk, b);
-                if (lane == 0) {
-                    const double rel = sqrt(rrn) / __ldcg(A.fnorm + b);
-                    const bool conv = rel < tol;
-                    rr_new_out[b] = rrn;
-                    A.beta[b] = rrn / __ldcg(rr_old + b);
-                    A.iters[b] = it + 1;
-                    A.rel[b] = rel;
-                    A.flag[b] = conv ? 1 : 0;
-                    if (!conv && it + 1 >= max_iter) A.status[b] = 2;
-                }
-            }
+        } else if (lane == 0 && c == A.inst_chunk[b]) {
+            if (fl == 2) A.status[b] = 1;
+            A.done[b] = 1;
+            atomicAdd(A.n_done, 1);
         }
-        grid.sync();
-        // p = r + beta p; instances that converged or broke down retire (their
-        // first chunk sets done; every warp skips them either way)
-        for (int c = gw; c < A.n_chunks; c += n_warps) {
-            const int b = A.chunk_inst[c];
-            const int dn = __ldcg(A.done + b), fl = __ldcg(A.flag + b);  // loads issued together
-            const double beta = __ldcg(A.beta + b);
-            if (dn) continue;
-            if (fl == 0) {
-                const int j1 = 3 * A.chunk_beg[c + 1];
-                for (int j0 = 3 * A.chunk_beg[c] + lane; j0 < j1; j0 += 256) {
-                    double pv[8], rv[8];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const int j = j0 + 32 * k;
-                        pv[k] = (j < j1) ? __ldcg(A.p + j) : 0.0;
-                        rv[k] = (j < j1) ? __ldcg(A.r + j) : 0.0;
-                    }
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const int j = j0 + 32 * k;
-                        if (j < j1) A.p[j] = rv[k] + beta * pv[k];
-                    }
-                }
-            } else if (lane == 0 && c == A.inst_chunk[b]) {
-                if (fl == 2) A.status[b] = 1;
-                A.done[b] = 1;
-                atomicAdd(A.n_done, 1);
-            }
-        }
+    }
+}
+
+// Instances still running when the iteration cap is reached end with status 2.
+template <typename R>
+__device__ __forceinline__ void bcg_finish(const BatchArgs<R>& A) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < A.n_inst; b += gridDim.x * blockDim.x)
+        if (!A.done[b] && A.status[b] == 0) A.status[b] = 2;
+}
+
+// The whole batched solve in one persistent cooperative launch (launch mode 1).
+template <typename R, int NPE, int NQP, bool SH>
+__global__ void __launch_bounds__(TILE_ELEMS) k_batch_cg(BatchArgs<R> A, double tol, int max_iter, int warm) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double red[32];
+    bcg_start<R>(A, warm, red);
+    grid.sync();
+    if (warm) {
+        apply_all_tiles<R, NPE, NQP, SH>(A, A.p, A.q, smem, false);
         grid.sync();
     }
-    for (int b = blockIdx.x * blockDim.x + t; b < A.n_inst; b += gridDim.x * blockDim.x)
-        if (!A.done[b] && A.status[b] == 0) A.status[b] = 2;
+    bcg_start_residual<R>(A, warm, red);
+    grid.sync();
+    bcg_init<R>(A, tol);
+    grid.sync();
+    // done[] changes only in the last phase of an iteration, so every other phase
+    // branches on it uniformly
+    for (int it = 0; it < max_iter; ++it) {
+        if (atomicAdd(A.n_done, 0) >= A.n_inst) break;  // uniform: read after a grid barrier
+        apply_all_tiles<R, NPE, NQP, SH>(A, A.p, A.q, smem, true);
+        grid.sync();
+        bcg_pq<R>(A, it);
+        grid.sync();
+        bcg_update<R>(A, it, tol, max_iter);
+        grid.sync();
+        bcg_direction<R>(A);
+        grid.sync();
+    }
+    bcg_finish<R>(A);
+}
+
+// ---------------------------------------------------------------------------
+// Per-phase kernels (launch mode 0, the default): each phase one launch at the
+// occupancy its own registers allow -- the element tiles one item per block, the
+// node phases one warp per chunk -- and an iteration is five launches: tiles,
+// p.q, update, direction, and a one-thread kernel that advances the device-side
+// iteration counter.  Chunks of iterations are captured in a CUDA graph and
+// replayed until every instance is done or the cap is reached; a kernel whose
+// iteration is past the cap, or that finds every instance done, returns at entry,
+// so a replay that overshoots costs a few empty launches.
+template <typename R>
+__global__ void __launch_bounds__(TILE_ELEMS) k_bcg_start(BatchArgs<R> A, int warm) {
+    __shared__ double red[32];
+    bcg_start<R>(A, warm, red);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(TILE_ELEMS) k_bcg_start_residual(BatchArgs<R> A, int warm) {
+    __shared__ double red[32];
+    bcg_start_residual<R>(A, warm, red);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(TILE_ELEMS) k_bcg_init(BatchArgs<R> A, double tol) {
+    bcg_init<R>(A, tol);
+}
+
+__device__ __forceinline__ bool bcg_idle(const int* it_dev, const int* n_done, int n_inst, int max_iter) {
+    return __ldcg(n_done) >= n_inst || __ldcg(it_dev) >= max_iter;
+}
+
+// skip_done = 0: the warm start's K u0, before the iterations
+template <typename R, int NPE, int NQP, bool SH>
+__global__ void __launch_bounds__(TILE_ELEMS) k_bcg_tiles(BatchArgs<R> A, int skip_done, int max_iter) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (skip_done && bcg_idle(A.it_dev, A.n_done, A.n_inst, max_iter)) return;
+    apply_all_tiles<R, NPE, NQP, SH>(A, A.p, A.q, smem, skip_done != 0);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(TILE_ELEMS) k_bcg_pq(BatchArgs<R> A, int max_iter) {
+    if (bcg_idle(A.it_dev, A.n_done, A.n_inst, max_iter)) return;
+    bcg_pq<R>(A, __ldcg(A.it_dev));
+}
+
+template <typename R>
+__global__ void __launch_bounds__(TILE_ELEMS) k_bcg_update(BatchArgs<R> A, double tol, int max_iter) {
+    if (bcg_idle(A.it_dev, A.n_done, A.n_inst, max_iter)) return;
+    bcg_update<R>(A, __ldcg(A.it_dev), tol, max_iter);
+}
+
+// n_done may reach n_inst while this kernel runs (its own retirements); a block that
+// then returns at entry has nothing left to retire
+template <typename R>
+__global__ void __launch_bounds__(TILE_ELEMS) k_bcg_direction(BatchArgs<R> A, int max_iter) {
+    if (bcg_idle(A.it_dev, A.n_done, A.n_inst, max_iter)) return;
+    bcg_direction<R>(A);
+}
+
+__global__ void k_bcg_next(int* it_dev, const int* n_done, int n_inst, int max_iter) {
+    if (*n_done < n_inst && *it_dev < max_iter) ++*it_dev;
+}
+
+template <typename R>
+__global__ void k_bcg_finish(BatchArgs<R> A) {
+    bcg_finish<R>(A);
 }
 
 // y = K_bc x for the whole batch: fixed rows are identity rows and fixed
@@ -827,6 +957,7 @@ static BatchArgs<R> batch_args(tlfea_batch_s* b) {
     A.beta = b->beta;
     A.flag = b->flag;
     A.ticket = b->ticket;
+    A.it_dev = b->n_done + 1;
     return A;
 }
 
@@ -898,6 +1029,138 @@ static int batch_launch(tlfea_batch_s* b, int grid, double tol, int max_iter, bo
                    : launch_batch_cg<double, 10, 5>(b, grid, tol, max_iter, warm, st);
     return f32 ? launch_batch_cg<float, 4, 1>(b, grid, tol, max_iter, warm, st)
                : launch_batch_cg<double, 4, 1>(b, grid, tol, max_iter, warm, st);
+}
+
+// ---- per-phase launches (mode 0)
+
+// Work items of the tile kernel (one per block): tiles, or (tile, instance group)
+// pairs in shared-mesh mode.
+static int bcg_items(const tlfea_batch_s* b) {
+    const int T = b->el->tl.n_tiles;
+    return b->shared ? T * ((b->n_inst + SHARED_GROUP - 1) / SHARED_GROUP) : T;
+}
+
+template <typename R, int NPE, int NQP>
+static int bcg_prepare(const tlfea_batch_s* b) {
+    const size_t smem = batch_smem<R>(b);
+    if (smem > 200 * 1024) {
+        set_error("batch: a tile touches too many nodes for shared memory");
+        return TLFEA_UNSUPPORTED;
+    }
+    const void* kern = b->shared ? (const void*)k_bcg_tiles<R, NPE, NQP, true> : (const void*)k_bcg_tiles<R, NPE, NQP, false>;
+    TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return TLFEA_OK;
+}
+
+template <typename R, int NPE, int NQP>
+static void bcg_enqueue_tiles(const tlfea_batch_s* b, const BatchArgs<R>& A, int skip_done, int max_iter,
+                              cudaStream_t st) {
+    const size_t smem = batch_smem<R>(b);
+    if (b->shared)
+        k_bcg_tiles<R, NPE, NQP, true><<<bcg_items(b), TILE_ELEMS, smem, st>>>(A, skip_done, max_iter);
+    else
+        k_bcg_tiles<R, NPE, NQP, false><<<bcg_items(b), TILE_ELEMS, smem, st>>>(A, skip_done, max_iter);
+}
+
+// One CG iteration: five launches in stream order.
+template <typename R, int NPE, int NQP>
+static void bcg_enqueue_iteration(const tlfea_batch_s* b, const BatchArgs<R>& A, double tol, int max_iter,
+                                  cudaStream_t st) {
+    const int warps_grid = (b->n_chunks + TILE_ELEMS / 32 - 1) / (TILE_ELEMS / 32);  // one warp per chunk
+    bcg_enqueue_tiles<R, NPE, NQP>(b, A, 1, max_iter, st);
+    k_bcg_pq<R><<<warps_grid, TILE_ELEMS, 0, st>>>(A, max_iter);
+    k_bcg_update<R><<<warps_grid, TILE_ELEMS, 0, st>>>(A, tol, max_iter);
+    k_bcg_direction<R><<<warps_grid, TILE_ELEMS, 0, st>>>(A, max_iter);
+    k_bcg_next<<<1, 1, 0, st>>>(A.it_dev, A.n_done, A.n_inst, max_iter);
+}
+
+// The graph of `iters` iterations for (precision, tol, max_iter), captured once.
+template <typename R, int NPE, int NQP>
+static int bcg_graph(tlfea_batch_s* b, const BatchArgs<R>& A, double tol, int max_iter, int iters, cudaStream_t st,
+                     cudaGraphExec_t* out) {
+    const int prec = sizeof(R) == 4 ? TLFEA_PRECISION_FP32 : TLFEA_PRECISION_FP64;
+    for (auto& g : b->phase_graphs)
+        if (g.precision == prec && g.tol == tol && g.max_iter == max_iter && g.iters == iters) {
+            *out = g.exec;
+            return TLFEA_OK;
+        }
+    cudaGraph_t g = nullptr;
+    TLFEA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < iters; ++k) bcg_enqueue_iteration<R, NPE, NQP>(b, A, tol, max_iter, st);
+    const cudaError_t e1 = cudaGetLastError();
+    const cudaError_t e2 = cudaStreamEndCapture(st, &g);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        set_error("batch_solve: capture of the iteration chunk failed");
+        return TLFEA_CUDA_ERROR;
+    }
+    cudaGraphExec_t ge = nullptr;
+    const cudaError_t e3 = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e3 != cudaSuccess) {
+        set_error(std::string("batch_solve: cudaGraphInstantiate: ") + cudaGetErrorString(e3));
+        return TLFEA_CUDA_ERROR;
+    }
+    b->phase_graphs.push_back({prec, max_iter, iters, tol, ge});
+    *out = ge;
+    return TLFEA_OK;
+}
+
+// The whole solve in per-phase launches: the start (u, r, p, the initial residual),
+// then chunks of iterations replayed until every instance is done or max_iter is
+// reached (the host reads the two control words after each chunk), then the final
+// status.  f_over / u0_over replace the batch's load and initial guess.
+template <typename R, int NPE, int NQP>
+static int run_phased(tlfea_batch_s* b, double tol, int max_iter, bool warm, cudaStream_t st,
+                      const double* f_over = nullptr, const double* u0_over = nullptr) {
+    int s = bcg_prepare<R, NPE, NQP>(b);
+    if (s) return s;
+    BatchArgs<R> A = batch_args<R>(b);
+    if (f_over) A.f = f_over;
+    if (u0_over) A.u0 = u0_over;
+    const int w = warm ? 1 : 0;
+    const int chunk_grid = std::min(b->n_chunks, 148 * 16);  // one block per chunk, grid-stride beyond
+    TLFEA_CUDA(cudaMemsetAsync(b->n_done, 0, 2 * sizeof(int), st));
+    k_bcg_start<R><<<chunk_grid, TILE_ELEMS, 0, st>>>(A, w);
+    if (warm) bcg_enqueue_tiles<R, NPE, NQP>(b, A, 0, max_iter, st);
+    k_bcg_start_residual<R><<<chunk_grid, TILE_ELEMS, 0, st>>>(A, w);
+    k_bcg_init<R><<<std::min(b->n_inst, 65535), 32, 0, st>>>(A, tol);
+    TLFEA_CUDA(cudaGetLastError());
+    TLFEA_LAUNCHED(warm ? 4 : 3);
+    int ctl[2] = {0, 0};
+    for (int chunk = 16; max_iter > 0; chunk = 64) {
+        cudaGraphExec_t ge = nullptr;
+        if ((s = bcg_graph<R, NPE, NQP>(b, A, tol, max_iter, chunk, st, &ge))) return s;
+        TLFEA_CUDA(cudaGraphLaunch(ge, st));
+        TLFEA_LAUNCHED(5 * chunk);
+        TLFEA_CUDA(cudaMemcpyAsync(ctl, b->n_done, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        TLFEA_CUDA(cudaStreamSynchronize(st));
+        if (ctl[0] >= b->n_inst || ctl[1] >= max_iter) break;
+    }
+    k_bcg_finish<R><<<(b->n_inst + 127) / 128, 128, 0, st>>>(A);
+    TLFEA_CUDA(cudaGetLastError());
+    TLFEA_LAUNCHED(1);
+    return TLFEA_OK;
+}
+
+// Dispatch on precision and element type; mode 1 keeps the persistent launch.
+static int bcg_run(tlfea_batch_s* b, bool f32, int grid, double tol, int max_iter, bool warm, cudaStream_t st,
+                   const double* f_over = nullptr, const double* u0_over = nullptr) {
+    const bool t10 = (b->el->npe == 10);
+    if (b->mode == 0) {
+        if (t10)
+            return f32 ? run_phased<float, 10, 5>(b, tol, max_iter, warm, st, f_over, u0_over)
+                       : run_phased<double, 10, 5>(b, tol, max_iter, warm, st, f_over, u0_over);
+        return f32 ? run_phased<float, 4, 1>(b, tol, max_iter, warm, st, f_over, u0_over)
+                   : run_phased<double, 4, 1>(b, tol, max_iter, warm, st, f_over, u0_over);
+    }
+    TLFEA_CUDA(cudaMemsetAsync(b->n_done, 0, sizeof(int), st));
+    if (t10)
+        return f32 ? launch_batch_cg<float, 10, 5>(b, grid, tol, max_iter, warm, st, f_over, u0_over)
+                   : launch_batch_cg<double, 10, 5>(b, grid, tol, max_iter, warm, st, f_over, u0_over);
+    return f32 ? launch_batch_cg<float, 4, 1>(b, grid, tol, max_iter, warm, st, f_over, u0_over)
+               : launch_batch_cg<double, 4, 1>(b, grid, tol, max_iter, warm, st, f_over, u0_over);
 }
 
 // Node chunks of at most `chunk_nodes` nodes that never straddle instances.
@@ -1004,7 +1267,7 @@ static int batch_alloc_state(tlfea_batch_s* b) {
         (st = dalloc(&b->f, n3)) || (st = dalloc(&b->u0, n3)) || (st = dalloc(&b->rr, 2 * (size_t)n_inst)) ||
         (st = dalloc(&b->fnorm, (size_t)n_inst)) || (st = dalloc(&b->rel, (size_t)n_inst)) ||
         (st = dalloc(&b->iters, (size_t)n_inst)) || (st = dalloc(&b->status, (size_t)n_inst)) ||
-        (st = dalloc(&b->done, (size_t)n_inst)) || (st = dalloc(&b->n_done, 1)) ||
+        (st = dalloc(&b->done, (size_t)n_inst)) || (st = dalloc(&b->n_done, 2)) ||
         (st = dalloc(&b->alpha, (size_t)n_inst)) || (st = dalloc(&b->beta, (size_t)n_inst)) ||
         (st = dalloc(&b->flag, (size_t)n_inst)) || (st = dalloc(&b->ticket, (size_t)n_inst)))
         return st;
@@ -1307,6 +1570,14 @@ int tlfea_batch_set_launch(tlfea_batch b, int blocks_per_sm, int chunk_nodes) {
     return TLFEA_OK;
 }
 
+int tlfea_batch_set_mode(tlfea_batch b, int mode) {
+    CHECK_BATCH(b);
+    if (mode != 0 && mode != 1) return TLFEA_INVALID_ARG;
+    if (mode != b->mode) drop_graphs(b);
+    b->mode = mode;
+    return TLFEA_OK;
+}
+
 int tlfea_batch_get_launch(tlfea_batch b, int* blocks_per_sm, int* chunk_nodes, int* grid) {
     CHECK_BATCH(b);
     if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
@@ -1380,12 +1651,13 @@ int tlfea_batch_solve(tlfea_batch b, double tol, int max_iter) {
     }
     if (!(tol > 0.0) || max_iter < 0) return TLFEA_INVALID_ARG;
     cudaStream_t st = b->el->stream;
-    int grid = 0;
-    int s = batch_dispatch_grid(b, b->blocks_per_sm, &grid);
-    if (s) return s;
+    int grid = 0, s = 0;
+    if (b->mode == 1 && (s = batch_dispatch_grid(b, b->blocks_per_sm, &grid))) return s;
     b->refined = false;
     if (b->precision != TLFEA_PRECISION_FP32) {
-        if ((s = run_captured(b, grid, tol, max_iter, b->warm))) return s;
+        if ((s = (b->mode == 1) ? run_captured(b, grid, tol, max_iter, b->warm)
+                                : bcg_run(b, false, 0, tol, max_iter, b->warm, st)))
+            return s;
         TLFEA_CUDA(cudaStreamSynchronize(st));
         return TLFEA_OK;
     }
@@ -1401,13 +1673,12 @@ int tlfea_batch_solve(tlfea_batch b, double tol, int max_iter) {
     std::vector<int> it(n);
     b->iters_total.assign(n, 0);
     int grid64 = 0;
-    s = (b->el->npe == 10) ? batch_grid<double, 10, 5>(b, 0, &grid64) : batch_grid<double, 4, 1>(b, 0, &grid64);
-    if (s) return s;
-    const bool t10 = (b->el->npe == 10);
+    if (b->mode == 1) {
+        s = (b->el->npe == 10) ? batch_grid<double, 10, 5>(b, 0, &grid64) : batch_grid<double, 4, 1>(b, 0, &grid64);
+        if (s) return s;
+    }
     auto eval64 = [&](bool at_u, const double* u_at) -> int {  // FP64 residual at u_at (or at 0)
-        TLFEA_CUDA(cudaMemsetAsync(b->n_done, 0, sizeof(int), st));
-        return t10 ? launch_batch_cg<double, 10, 5>(b, grid64, tol, 0, at_u, st, nullptr, u_at)
-                   : launch_batch_cg<double, 4, 1>(b, grid64, tol, 0, at_u, st, nullptr, u_at);
+        return bcg_run(b, false, grid64, tol, 0, at_u, st, nullptr, u_at);
     };
     const double tau = std::max(tol, std::min(0.1, std::max(1e-4, 0.5 * std::sqrt(tol))));
     constexpr int MAX_PASSES = 8;
@@ -1423,10 +1694,7 @@ int tlfea_batch_solve(tlfea_batch b, double tol, int max_iter) {
                                                                  b->r, b->rhs);
         TLFEA_CUDA(cudaGetLastError());
         TLFEA_LAUNCHED(1);
-        TLFEA_CUDA(cudaMemsetAsync(b->n_done, 0, sizeof(int), st));
-        s = t10 ? launch_batch_cg<float, 10, 5>(b, grid, tau, max_iter, false, st, b->rhs, nullptr)
-                : launch_batch_cg<float, 4, 1>(b, grid, tau, max_iter, false, st, b->rhs, nullptr);
-        if (s) return s;
+        if ((s = bcg_run(b, true, grid, tau, max_iter, false, st, b->rhs, nullptr))) return s;
         TLFEA_CUDA(cudaMemcpyAsync(it.data(), b->iters, n * sizeof(int), cudaMemcpyDeviceToHost, st));
         TLFEA_CUDA(cudaStreamSynchronize(st));
         for (size_t i = 0; i < n; ++i) b->iters_total[i] += it[i];
@@ -1520,13 +1788,41 @@ int tlfea_batch_autotune(tlfea_batch b, int trial_iters, int* best_blocks_per_sm
     }
     if (trial_iters <= 0) trial_iters = 8;
     cudaStream_t st = b->el->stream;
+    const int chunks[] = {128, 256, 512, 1024};
+    int s = 0;
+    if (b->mode == 0) {
+        // per-phase launches: every kernel takes the occupancy its registers allow, so
+        // the chunk size is the one knob; time trial_iters iterations of each
+        const bool f32 = b->precision == TLFEA_PRECISION_FP32;
+        float best = 1e30f;
+        int bc = b->chunk_nodes;
+        for (int c : chunks) {
+            if ((s = build_chunks(b, c))) return s;
+            float ms = 0.f;
+            for (int rep = 0; rep < 2 && !s; ++rep) {  // first run warms up (and captures)
+                const auto t0 = std::chrono::steady_clock::now();
+                s = bcg_run(b, f32, 0, 1e-300, trial_iters, false, st);
+                if (!s && cudaStreamSynchronize(st) != cudaSuccess) s = TLFEA_CUDA_ERROR;
+                ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            }
+            if (s) return s;
+            if (ms < best) {
+                best = ms;
+                bc = c;
+            }
+        }
+        if ((s = build_chunks(b, bc))) return s;
+        if (best_blocks_per_sm) *best_blocks_per_sm = 0;
+        if (best_chunk) *best_chunk = bc;
+        if (best_ms) *best_ms = best;
+        return TLFEA_OK;
+    }
     int max_grid = 0;
-    int s = batch_dispatch_grid(b, 0, &max_grid);
+    s = batch_dispatch_grid(b, 0, &max_grid);
     if (s) return s;
     int sms = 0;
     TLFEA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->el->device));
     const int max_per_sm = std::max(1, max_grid / std::max(sms, 1));
-    const int chunks[] = {128, 256, 512, 1024};
     cudaEvent_t e0, e1;
     TLFEA_CUDA(cudaEventCreate(&e0));
     TLFEA_CUDA(cudaEventCreate(&e1));
