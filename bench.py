@@ -61,6 +61,11 @@ SPMV_TRAFFIC_RATIO = 1.026
 FORCE_FP32_TRAFFIC_BYTES = 357.03e6
 
 
+def progress(msg):
+    """One progress line on stderr (the JSON result goes to stdout)."""
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -357,6 +362,22 @@ def kernels_only(args):
         torch.cuda.synchronize()
         print(json.dumps({"kernels_only": "batch", "cases": 64, "iterations": 10}))
         fm.destroy()
+        return
+    if args.kernels_only == "batch-uneven":
+        # the batched CG of the uneven batch (general tiling): the first 64 seeded
+        # cantilevers of the 512-instance batch, 10 iterations
+        from tlfea_b200 import mesh as M
+
+        insts = [M.random_beam(s) for s in range(64)]
+        b = T.BatchedLinearStaticSolver([(d["x"], d["y"], d["z"], d["conn"]) for d in insts], T.TYPE_T10)
+        b.SetMaterial([d["E"] for d in insts], [d["nu"] for d in insts])
+        b.SetNodalFixed([d["fixed"] for d in insts])
+        b.SetExternalForce(np.concatenate([d["f"] for d in insts]))
+        b.Solve(1e-12, 10)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernels_only": "batch-uneven", "cases": 64, "iterations": 10,
+                          "nodes": b.GetCounts()["nodes"]}))
+        b.Destroy()
         return
     cfg = dict(CFG)
     x, y, z, conn, fixed, f = build_mesh(cfg)
@@ -747,6 +768,7 @@ def config5_leg(args, T):
     kb.Destroy()
     alpha_all = 0.9 / (lmax.cpu().numpy() + dt * dt * rho_alm)
     t_alpha = time.perf_counter() - t0
+    progress(f"config5: step sizes {alpha_all.min():.3e}..{alpha_all.max():.3e} in {t_alpha:.1f} s")
 
     params = T.SyncedNesterovParams(float(alpha_all.min()), rho_alm, 0.0, 1e-6, 3, 20000, dt)
 
@@ -784,6 +806,8 @@ def config5_leg(args, T):
     for k in range(steps_train):
         it, res, conv = bt.Step(T.BatchedDynamics.WARM_LINEAR)
         it_train.append(it)
+        progress(f"config5: training step {k + 1}: inner iterations mean {np.mean(it):.0f} max {np.max(it)}, "
+                 f"converged {np.mean(conv):.2f}, {time.perf_counter() - t0:.1f} s")
         v, _, u = state(bt, n_train)
         V[:, k] = v
         U[:, k] = u
@@ -820,6 +844,8 @@ def config5_leg(args, T):
                 it, res, conv = b.Step(T.BatchedDynamics.WARM_GIVEN, int(g.data_ptr()))
             its.append(it)
             conv_all.append(conv)
+            progress(f"config5: {name} step {n}: inner iterations mean {np.mean(it):.0f} max {np.max(it)}, "
+                     f"converged {np.mean(conv):.2f}, {time.perf_counter() - t0:.1f} s")
         torch.cuda.synchronize()
         dt_run = time.perf_counter() - t0
         its = np.array(its)
@@ -972,7 +998,7 @@ def main():
     ap.add_argument("--no-gpu-ref", action="store_true", help="skip the reference's own CUDA build leg")
     ap.add_argument("--kernel-reps", type=int, default=20)
     ap.add_argument("--cg-iters", type=int, default=120, help="iteration cap of --kernels-only cg")
-    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg", "batch", "steps"], default=None,
+    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg", "batch", "batch-uneven", "steps"], default=None,
                     help="profiling case: set up, then launch only the named kernel a few times")
     ap.add_argument("--mesh", default=None, help="cells NXxNYxNZ (default 200x20x20)")
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")
