@@ -36,10 +36,17 @@ def test_learned_warm_start_beats_cold_start():
     assert np.all(st_cold == 0) and np.all(st_warm == 0)
     assert np.all(res_warm < 1e-6)
     # What the network gives the solver: the displacement to within a few percent
-    # (the cold start's error is 100%), checked above.  Its high-frequency error
-    # leaves a starting residual of the order of the cold start's, and unpreconditioned CG
-    # on this small mesh needs about as many iterations as it has DOFs either way,
-    # so for CG the assertion is non-regression.
+    # (the cold start's error is 100%), checked above, and a lower starting residual
+    # ||f - K u_guess|| / ||f|| than the cold start's 1 (max_iter = 0 reports it).  Its
+    # high-frequency error still leaves CG most of its iterations: unpreconditioned CG on
+    # this small mesh needs about as many iterations as it has DOFs either way, so the
+    # iteration count is only checked not to grow.  (The network earns its keep in the
+    # batched SyncedNesterov steps, tests/test_gpu_dynamics.py, where it cuts the
+    # iterations against linear extrapolation.)
+    _, _, r0_warm, _ = fm.solve(test, tol=1e-6, max_iter=0, u0=g)
+    _, _, r0_cold, _ = fm.solve(test, tol=1e-6, max_iter=0)
+    assert np.allclose(r0_cold, 1.0)
+    assert np.median(r0_warm) < 0.8, np.median(r0_warm)
     assert it_warm.mean() <= 1.02 * it_cold.mean()
     for k in range(0, 256, 37):
         assert rel(u_warm[k], u_cold[k]) < 1e-4

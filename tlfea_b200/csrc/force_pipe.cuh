@@ -457,7 +457,9 @@ __device__ __forceinline__ void prefetch_next_tile(const TileArgs<R>& A, const R
     const int nt = blockIdx.x + A.pf_ahead;
     if (nt >= (int)gridDim.x) return;
     const int lane = threadIdx.x & 31;
-    if (lane < NQP) bulk_prefetch_l2(slices + ((size_t)nt * NQP + lane) * slice_elems, slice_elems * TE * sizeof(R));
+    // slice q of tile nt starts (nt * NQP + q) * slice_elems * TE values into the stream
+    if (lane < NQP)
+        bulk_prefetch_l2(slices + ((size_t)nt * NQP + lane) * slice_elems * TE, slice_elems * TE * sizeof(R));
     if (lane == NQP) bulk_prefetch_l2(A.dv + (size_t)nt * NQP * TE, NQP * TE * sizeof(R));
     if (lane == NQP + 1) bulk_prefetch_l2(A.lconn + (size_t)nt * NPE * TE, NPE * TE * sizeof(uint16_t));
     if (lane == NQP + 2) bulk_prefetch_l2(A.inc + (size_t)nt * NPE * TE, NPE * TE * sizeof(uint16_t));
