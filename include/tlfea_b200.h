@@ -280,6 +280,12 @@ int tlfea_solver_get_stats(tlfea_solver s, tlfea_solve_stats* st);
  * positions the internal force was computed at, and the solve ends -- keeping
  * those positions -- once it is below rel_tol.  0 turns it off (default). */
 int tlfea_solver_set_stop_rule(tlfea_solver s, double rel_tol);
+/* New: launch mode of the Nesterov / AdamW solvers.  0 (default) = one kernel per
+ * phase (velocity guess, forces, gradient, update, outer update) with the loop state
+ * on the device, chunks of iterations replayed as CUDA graphs until the solve ends;
+ * 1 = the whole Solve() in one persistent cooperative launch.  The iterations are the
+ * same; with fixed iteration counts so are the trajectories, bit for bit. */
+int tlfea_solver_set_mode(tlfea_solver s, int mode);
 
 /* New, no reference counterpart: n_steps implicit steps of a first-order solver
  * in one call -- the loop a reference driver writes around SetExternalForce +

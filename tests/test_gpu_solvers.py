@@ -208,3 +208,62 @@ def _oracle_displacement_with_bar(x, y, z, conn, e_mod, fixed, f, kind, params, 
     d0 = run(0.0, 0)
     s = max(rel(run(1e-15, seed), d0) for seed in (1, 2))
     return d0, max(1e-10, 3.0 * s)
+
+
+@pytest.mark.parametrize("kind,params,case,steps", [
+    ("nesterov", (1.0e-8, 1e14, 0.0, 0.0, 2, 40, 1.0e-3), "cfg1", 3),
+    ("nesterov", NESTEROV, "cube", 3),
+    ("adamw", ADAMW, "cube", 2),
+    ("nocoop", ADAMW, "cube", 2),
+])
+def test_phased_and_persistent_launches_agree(kind, params, case, steps):
+    """The per-phase launches (default) and the persistent cooperative launch run the
+    same per-node and per-tile arithmetic: with fixed iteration counts the trajectories
+    are bitwise the same; with the reference examples' tolerances (decisions taken on
+    norms whose partials group differently) the iteration counts and positions agree."""
+    res = {}
+    for mode in ("persistent", "phased"):
+        x, y, z, conn, fixed, f = _cube() if case == "cube" else _cfg1()
+        el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
+        cls = {"nesterov": T.SyncedNesterovSolver, "adamw": T.SyncedAdamWSolver,
+               "nocoop": T.SyncedAdamWNocoopSolver}[kind]
+        s = cls(el, el.get_n_constraint())
+        s.Setup()
+        s.SetParameters(T.SyncedNesterovParams(*params) if kind == "nesterov" else T.SyncedAdamWParams(*params))
+        s.SetMode(mode)
+        pos, its = [], []
+        for _ in range(steps):
+            s.Solve()
+            pos.append(np.stack(el.RetrievePositionToCPU()))
+            st = s.GetStats()
+            its.append((st["outer_iters"], st["inner_iters_total"], st["last_inner_iters"]))
+        res[mode] = (np.stack(pos), its, s.GetVelocity()[0])
+        del s
+        el.Destroy()
+    a, b = res["persistent"], res["phased"]
+    assert a[1] == b[1], (a[1], b[1])
+    if params[2] == 0.0 and params[3] == 0.0:  # zero tolerances: fixed counts
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2])
+    else:
+        X0 = np.stack(_cube()[:3])
+        assert rel(b[0][-1] - X0, a[0][-1] - X0) < 1e-9
+
+
+def test_phased_run_steps_match_the_persistent_launch():
+    x, y, z, conn, fixed, f = _cfg1()
+    params = (1.0e-8, 1e14, 0.0, 0.0, 1, 12, 1.0e-3)
+    out = {}
+    for mode in ("persistent", "phased"):
+        el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
+        s = T.SyncedNesterovSolver(el, el.get_n_constraint())
+        s.Setup()
+        s.SetParameters(T.SyncedNesterovParams(*params))
+        s.SetMode(mode)
+        f_var = np.zeros_like(f)
+        f_var[2::3] = -1.0
+        its = s.RunSteps(5, f_var, 3.0, 2 * np.pi * 5.0, 0.2)
+        out[mode] = (np.stack(el.RetrievePositionToCPU()), list(its))
+        del s
+        el.Destroy()
+    assert out["persistent"][1] == out["phased"][1] == [12] * 5
+    assert np.array_equal(out["persistent"][0], out["phased"][0])

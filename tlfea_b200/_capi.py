@@ -139,6 +139,7 @@ _SIGS = {
     "tlfea_solver_get_multipliers": [_P, _D, C.c_int],
     "tlfea_solver_get_stats": [_P, C.POINTER(SolveStats)],
     "tlfea_solver_set_stop_rule": [_P, C.c_double],
+    "tlfea_solver_set_mode": [_P, C.c_int],
     "tlfea_solver_run_steps": [_P, C.c_int, C.c_double, _D, C.c_double, C.c_double, C.c_double, _I],
     "tlfea_batch_create": [C.c_int, C.c_int, _I, _I, _D, _D, _D, _D, C.c_int, _D, _D, _D, _I, C.POINTER(_P)],
     "tlfea_batch_create_shared": [C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, _D, _D, C.c_int, _D, _D, _D, _I,

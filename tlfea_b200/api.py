@@ -401,6 +401,12 @@ class _FirstOrder(SolverBase):
         (FP64, evaluated every inner iteration); 0 turns the rule off."""
         capi.call("tlfea_solver_set_stop_rule", self._h, float(rel_tol))
 
+    def SetMode(self, mode: str = "phased"):
+        """New: "phased" (default) -- one kernel per phase, the loop state on the
+        device, chunks of iterations replayed as CUDA graphs -- or "persistent" (the
+        whole Solve() in one cooperative launch)."""
+        capi.call("tlfea_solver_set_mode", self._h, {"phased": 0, "persistent": 1}[mode])
+
     def RunSteps(self, n_steps: int, f_var=None, amp: float = 1.0, omega: float = 0.0, phase: float = 0.0,
                  t0: float = 0.0):
         """New: n_steps calls of Solve() in one launch (one CUDA graph), the loop

@@ -388,6 +388,391 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_first_order(FOArgs S, TileArgs<R
     }
 }
 
+// ---------------------------------------------------------------------------
+// Per-phase solve (mode 0, the default).  The persistent kernel above holds 2
+// blocks (8 warps) per SM -- its registers are the force tile routine's -- so its
+// node phases run latency-bound.  Here every phase is its own launch at the
+// occupancy its code allows, and the control flow of the reference's loops
+// (inner stop tests, outer multiplier updates, the stop rule) lives in a small
+// device-side state record, FOCtl, advanced by the last block to finish each
+// phase (a ticket; the norms are folded in block order, so deterministically).
+// A slot of launches -- outer start, velocity guess, forces, gradient, Nesterov
+// update, outer update (two), final positions -- covers every state; each kernel
+// returns at entry unless the state is its own, so a CUDA graph of a chunk of
+// slots is replayed until the state reads FO_DONE.  Per node and per tile the
+// arithmetic is the persistent kernel's, so with fixed iteration counts the
+// trajectories are bitwise the same; norms group their partials per launch grid.
+enum { FO_OUTER_START = 0, FO_INNER = 1, FO_OUTER = 2, FO_FINAL = 3, FO_DONE = 4 };
+
+struct FOCtl {
+    int mode, outer, inner, inner_flag, outer_flag, status, n_outer, inner_total, last_inner, rule_met;
+    unsigned int ticket;
+    int pad;
+    double t, lr, prev_norm_g, norm_g, norm_g0, last_norm, last_rel, fext_norm;
+    double beta, lr_cur, b1t, b2t;  // scalars of the current inner iteration
+};
+
+constexpr int FO_NODE_THREADS = 256;
+
+__device__ __forceinline__ int fo_eff_outer(const FOArgs& S) {
+    return (S.kind == KIND_ADAMW_NOCOOP && S.nc == 0) ? 1 : S.max_outer;
+}
+
+// True in every thread of the block that finishes the phase last (all other blocks'
+// partials and writes are visible to it).
+__device__ __forceinline__ bool fo_last_block(FOCtl* C, int* flag_sh) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int tk = atomicAdd(&C->ticket, 1u);
+        const int last = (tk == gridDim.x - 1) ? 1 : 0;
+        if (last) {
+            C->ticket = 0u;
+            __threadfence();
+        }
+        *flag_sh = last;
+    }
+    __syncthreads();
+    return *flag_sh != 0;
+}
+
+// The scalars of inner iteration C->inner, as the persistent kernel forms them at
+// the top of its inner loop (one thread).
+__device__ __forceinline__ void fo_scalars(const FOArgs& S, FOCtl* C) {
+    if (S.kind == KIND_NESTEROV) {
+        const double t_next = 0.5 * (1.0 + sqrt(1.0 + 4.0 * C->t * C->t));
+        C->beta = (C->t - 1.0) / t_next;
+        C->t = t_next;
+    } else if (S.kind == KIND_ADAMW_NOCOOP) {
+        C->lr_cur = S.lr * pow(S.lr_decay, C->inner + 1);
+        const double tc = (double)(C->inner + 2);
+        C->b1t = 1.0 / (1.0 - pow(S.beta1, tc));
+        C->b2t = 1.0 / (1.0 - pow(S.beta2, tc));
+    } else {
+        C->lr = C->lr * S.lr_decay;
+        C->t += 1;
+        C->lr_cur = C->lr;
+        C->b1t = 1 - pow(S.beta1, C->t);
+        C->b2t = 1 - pow(S.beta2, C->t);
+    }
+}
+
+// End of inner iteration C->inner (one thread): leave the inner loop on a flag, a
+// non-finite norm or the iteration cap, else set up the next iteration.
+__device__ __forceinline__ void fo_end_inner(const FOArgs& S, FOCtl* C) {
+    const int count = C->inner + 1;
+    if (C->status || C->inner_flag || count >= S.max_inner) {
+        C->inner_total += count;
+        C->last_inner = count;
+        C->last_norm = C->norm_g;
+        C->mode = C->status ? FO_FINAL : FO_OUTER;
+    } else {
+        C->inner = count;
+        fo_scalars(S, C);
+    }
+}
+
+// x_prev = x, ||f_ext||^2 (stop rule), the start state.
+__global__ void __launch_bounds__(FO_NODE_THREADS) k_fo_start(FOArgs S, FOCtl* C) {
+    __shared__ double red_sh[32];
+    __shared__ double fold_sh;
+    __shared__ int flag_sh;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    const bool rule = S.rel_tol > 0.0;
+    double sf = 0.0;
+    for (int i = gt; i < S.N; i += gs) {
+        S.xp[i] = S.x[i];
+        S.yp[i] = S.y[i];
+        S.zp[i] = S.z[i];
+        if (rule)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) sf += S.f_ext[3 * i + d] * S.f_ext[3 * i + d];
+    }
+    if (rule) write_partial(S, 5, sf, red_sh);
+    if (!fo_last_block(C, &flag_sh)) return;
+    const double fn = rule ? sqrt(fold_partials(S, 5, &fold_sh)) : 0.0;
+    if (threadIdx.x == 0) {
+        C->fext_norm = fn;
+        C->outer = C->inner = C->inner_flag = C->outer_flag = C->status = 0;
+        C->n_outer = C->inner_total = C->last_inner = C->rule_met = 0;
+        C->norm_g = C->last_norm = 0.0;
+        C->last_rel = -1.0;
+        C->mode = (fo_eff_outer(S) > 0) ? FO_OUTER_START : FO_FINAL;
+    }
+}
+
+// Start of an outer iteration: the inner loop's vectors and scalars.
+__global__ void __launch_bounds__(FO_NODE_THREADS) k_fo_outer_start(FOArgs S, FOCtl* C) {
+    __shared__ int flag_sh;
+    if (__ldcg(&C->mode) != FO_OUTER_START) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    const bool nesterov = (S.kind == KIND_NESTEROV);
+    for (int i = gt; i < 3 * S.N; i += gs) {
+        if (nesterov) {
+            S.vk[i] = S.vg[i];
+            S.vkm1[i] = S.vg[i];
+        } else {
+            S.g[i] = 0.0;
+            S.m[i] = 0.0;
+            S.va[i] = 0.0;
+        }
+    }
+    if (!fo_last_block(C, &flag_sh) || threadIdx.x != 0) return;
+    C->n_outer += 1;
+    C->t = 1.0;
+    C->prev_norm_g = 0.0;
+    C->norm_g = 0.0;
+    C->norm_g0 = -1.0;
+    C->lr = S.lr;
+    C->inner_flag = 0;
+    C->inner = 0;
+    if (S.max_inner > 0) {
+        fo_scalars(S, C);
+        C->mode = FO_INNER;
+    } else {
+        C->last_inner = 0;
+        C->last_norm = C->norm_g;
+        C->mode = FO_OUTER;
+    }
+}
+
+// P1: the inner iteration's velocity guess and positions.
+template <typename R>
+__global__ void __launch_bounds__(FO_NODE_THREADS) k_fo_guess(FOArgs S, const FOCtl* C) {
+    if (__ldcg(&C->mode) != FO_INNER) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    if (S.kind == KIND_NESTEROV) {
+        const double beta = __ldcg(&C->beta);
+        for (int i = gt; i < S.N; i += gs) {
+            double v[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double vk = S.vk[3 * i + d];
+                v[d] = vk + beta * (vk - S.vkm1[3 * i + d]);
+                S.vg[3 * i + d] = v[d];
+            }
+            set_node_positions<R>(S, i, v[0], v[1], v[2]);
+        }
+        return;
+    }
+    const bool nocoop = (S.kind == KIND_ADAMW_NOCOOP);
+    const double lr_cur = __ldcg(&C->lr_cur), b1t = __ldcg(&C->b1t), b2t = __ldcg(&C->b2t);
+    for (int i = gt; i < S.N; i += gs) {
+        double v[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int k = 3 * i + d;
+            const double gk = S.g[k], vgk = S.vg[k];
+            const double mt = S.beta1 * S.m[k] + (1 - S.beta1) * gk;
+            const double vt = S.beta2 * S.va[k] + (1 - S.beta2) * gk * gk;
+            double mh, vh;
+            if (nocoop) {
+                mh = mt * b1t;
+                vh = vt * b2t;
+            } else {
+                mh = mt / b1t;
+                vh = vt / b2t;
+            }
+            v[d] = vgk - lr_cur * (mh / (sqrt(vh) + S.eps) + S.wd * vgk);
+            S.m[k] = mt;
+            S.va[k] = vt;
+            S.vg[k] = v[d];
+        }
+        set_node_positions<R>(S, i, v[0], v[1], v[2]);
+    }
+}
+
+// P2: internal force, one tile per block (the fused tile routine), and the
+// constraint values at the new positions.
+template <typename R, int NPE, int NQP, bool DAMP, bool MR, bool MASS>
+__global__ void __launch_bounds__(TILE_ELEMS) k_fo_force(FOArgs S, TileArgs<R> A, const FOCtl* C) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (__ldcg(&C->mode) != FO_INNER) return;
+    process_tile<R, NPE, NQP, TILE_FORCE, DAMP, MR, MASS>(A, blockIdx.x, smem);
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    for (int k = gt; k < S.n_fixed; k += gs) {
+        const int n = S.fixed[k];
+        S.c[3 * k + 0] = S.x[n] - S.xj[n];
+        S.c[3 * k + 1] = S.y[n] - S.yj[n];
+        S.c[3 * k + 2] = S.z[n] - S.zj[n];
+    }
+}
+
+// P3: the gradient per node and its norm partials; the last block applies the
+// stop tests (AdamW: all of them; Nesterov: the stop rule, which skips the update,
+// and the ||g|| test).
+template <typename R, bool MASS>
+__global__ void __launch_bounds__(FO_NODE_THREADS) k_fo_grad(FOArgs S, TileArgs<R> A, FOCtl* C) {
+    __shared__ double red_sh[32];
+    __shared__ double fold_sh;
+    __shared__ int flag_sh;
+    if (__ldcg(&C->mode) != FO_INNER) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    const bool nesterov = (S.kind == KIND_NESTEROV);
+    const bool rule = S.rel_tol > 0.0;
+    const int check = S.check > 0 ? S.check : 1;
+    const int inner = __ldcg(&C->inner);
+    const bool do_check = nesterov || (inner % check == 0);
+    double sg = 0.0, sv = 0.0, sr = 0.0;
+    for (int i = gt; i < S.N; i += gs) {
+        double f[3], gi[3];
+        node_force<R>(S, A, i, f);
+        grad_node<MASS>(S, i, f, gi);
+        const bool free_node = rule && !S.node_fixed[i];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            S.g[3 * i + d] = gi[d];
+            sg += gi[d] * gi[d];
+            if (!nesterov) sv += S.vg[3 * i + d] * S.vg[3 * i + d];
+            if (free_node) {
+                const double rd = f[d] - S.f_ext[3 * i + d];
+                sr += rd * rd;
+            }
+        }
+    }
+    if (do_check) {
+        write_partial(S, 0, sg, red_sh);
+        if (!nesterov) write_partial(S, 1, sv, red_sh);
+        if (rule) write_partial(S, 4, sr, red_sh);
+    }
+    if (!fo_last_block(C, &flag_sh)) return;
+    bool rule_now = false;
+    double rr = 0.0, norm_g = 0.0, nv = 0.0;
+    if (rule && do_check) rr = sqrt(fold_partials(S, 4, &fold_sh));
+    if (nesterov || do_check) norm_g = sqrt(fold_partials(S, 0, &fold_sh));
+    if (!nesterov && do_check) nv = sqrt(fold_partials(S, 1, &fold_sh));
+    if (threadIdx.x != 0) return;
+    if (rule && do_check) {
+        C->last_rel = C->fext_norm > 0.0 ? rr / C->fext_norm : rr;
+        rule_now = C->last_rel < S.rel_tol;
+    }
+    if (nesterov) {
+        C->norm_g = norm_g;
+        if (!isfinite(norm_g)) C->status = TLFEA_NONFINITE;
+        if (rule_now) {
+            // stop at the positions the residual was measured at (v = y)
+            C->inner_flag = 1;
+            C->rule_met = 1;
+            fo_end_inner(S, C);
+            return;
+        }
+        if (inner > 0 && fabs(norm_g - C->prev_norm_g) < S.inner_tol) C->inner_flag = 1;
+        return;  // the update and the rest of the tests follow in k_fo_nesterov
+    }
+    if (do_check) {
+        C->norm_g = norm_g;
+        if (!isfinite(norm_g)) C->status = TLFEA_NONFINITE;
+        if (C->norm_g0 < 0.0) C->norm_g0 = norm_g;
+        const double tol_abs = S.inner_tol * (1.0 + nv);
+        const double tol_rel = (S.rtol > 0.0 && C->norm_g0 > 0.0) ? (S.rtol * C->norm_g0) : 0.0;
+        if (norm_g <= tol_abs || (tol_rel > 0.0 && norm_g <= tol_rel)) C->inner_flag = 1;
+        if (rule_now) {
+            C->inner_flag = 1;
+            C->rule_met = 1;
+        }
+    }
+    fo_end_inner(S, C);
+}
+
+// P4 (Nesterov): v_next = y - alpha g, and the ||v_next|| - ||v_k|| test.
+__global__ void __launch_bounds__(FO_NODE_THREADS) k_fo_nesterov(FOArgs S, FOCtl* C) {
+    __shared__ double red_sh[32];
+    __shared__ double fold_sh;
+    __shared__ int flag_sh;
+    if (__ldcg(&C->mode) != FO_INNER) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    double snv = 0.0, snk = 0.0;
+    for (int i = gt; i < 3 * S.N; i += gs) {
+        const double vn = S.vg[i] - S.alpha * S.g[i];
+        const double vk = S.vk[i];
+        snv += vn * vn;
+        snk += vk * vk;
+        S.vkm1[i] = vk;
+        S.vk[i] = vn;
+        S.vg[i] = vn;
+    }
+    write_partial(S, 1, snv, red_sh);
+    write_partial(S, 2, snk, red_sh);
+    if (!fo_last_block(C, &flag_sh)) return;
+    const double nvn = sqrt(fold_partials(S, 1, &fold_sh));
+    const double nvk = sqrt(fold_partials(S, 2, &fold_sh));
+    if (threadIdx.x != 0) return;
+    if (C->inner > 0 && fabs(nvn - nvk) < S.inner_tol) C->inner_flag = 1;
+    C->prev_norm_g = C->norm_g;
+    fo_end_inner(S, C);
+}
+
+// Outer update, part 1: v_prev = v and x = x_prev + dt v.
+template <typename R>
+__global__ void __launch_bounds__(FO_NODE_THREADS) k_fo_outer_positions(FOArgs S, const FOCtl* C) {
+    if (__ldcg(&C->mode) != FO_OUTER) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    for (int i = gt; i < S.N; i += gs) {
+        double v[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            v[d] = S.vg[3 * i + d];
+            S.vp[3 * i + d] = v[d];
+        }
+        set_node_positions<R>(S, i, v[0], v[1], v[2]);
+    }
+}
+
+// Outer update, part 2: constraints, multipliers and the outer stop test.
+__global__ void __launch_bounds__(FO_NODE_THREADS) k_fo_outer_multipliers(FOArgs S, FOCtl* C) {
+    __shared__ double red_sh[32];
+    __shared__ double fold_sh;
+    __shared__ int flag_sh;
+    if (__ldcg(&C->mode) != FO_OUTER) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    double sc = 0.0;
+    for (int k = gt; k < S.n_fixed; k += gs) {
+        const int n = S.fixed[k];
+        const double cc[3] = {S.x[n] - S.xj[n], S.y[n] - S.yj[n], S.z[n] - S.zj[n]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            S.c[3 * k + d] = cc[d];
+            S.lam[3 * k + d] += S.rho * S.dt * cc[d];
+            sc += cc[d] * cc[d];
+        }
+    }
+    write_partial(S, 3, sc, red_sh);
+    if (!fo_last_block(C, &flag_sh)) return;
+    const double norm_c = sqrt(fold_partials(S, 3, &fold_sh));
+    if (threadIdx.x != 0) return;
+    if (C->rule_met) {
+        C->outer_flag = 1;
+    } else if (S.kind == KIND_ADAMW_NOCOOP) {
+        if (S.nc > 0 && norm_c < S.outer_tol && C->inner_flag) C->outer_flag = 1;
+    } else if (fabs(norm_c) < S.outer_tol) {
+        C->outer_flag = 1;
+    }
+    if (C->outer_flag || C->outer + 1 >= fo_eff_outer(S)) {
+        C->mode = FO_FINAL;
+    } else {
+        C->outer += 1;
+        C->mode = FO_OUTER_START;
+    }
+}
+
+// Final positions x = x_prev + dt v and the statistics.
+template <typename R>
+__global__ void __launch_bounds__(FO_NODE_THREADS) k_fo_final(FOArgs S, FOCtl* C) {
+    __shared__ int flag_sh;
+    if (__ldcg(&C->mode) != FO_FINAL) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    for (int i = gt; i < S.N; i += gs) set_node_positions<R>(S, i, S.vg[3 * i], S.vg[3 * i + 1], S.vg[3 * i + 2]);
+    if (!fo_last_block(C, &flag_sh) || threadIdx.x != 0) return;
+    S.stat[0] = C->n_outer;
+    S.stat[1] = C->inner_total;
+    S.stat[2] = C->last_inner;
+    S.stat[3] = C->status;
+    *S.stat_norm = C->last_norm;
+    *S.stat_rel = C->last_rel;
+    S.stat[8] = C->rule_met;
+    C->mode = FO_DONE;
+}
+
 template <typename R, int NPE, int NQP, bool DAMP, bool MR, bool MASS>
 static int launch_first_order(tlfea_solver_s* s, FOArgs& S, TileArgs<R>& A) {
     tlfea_element_s* el = s->el;
@@ -410,6 +795,86 @@ static int launch_first_order(tlfea_solver_s* s, FOArgs& S, TileArgs<R>& A) {
     return TLFEA_OK;
 }
 
+void first_order_drop_graphs(tlfea_solver_s* s);
+
+// One slot of per-phase launches (every state's kernels, each a no-op unless the
+// state is its own).
+template <typename R, int NPE, int NQP, bool DAMP, bool MR, bool MASS>
+static void fo_enqueue_slot(const tlfea_solver_s* s, const FOArgs& S, const TileArgs<R>& A, FOCtl* C,
+                            cudaStream_t st) {
+    const int gn = std::max(1, std::min(s->max_blocks, (S.N + FO_NODE_THREADS - 1) / FO_NODE_THREADS));
+    const size_t smem = tile_smem_bytes<R>(NPE, A.max_local, DAMP, MASS);
+    k_fo_outer_start<<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
+    k_fo_guess<R><<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
+    k_fo_force<R, NPE, NQP, DAMP, MR, MASS><<<S.n_tiles, TILE_ELEMS, smem, st>>>(S, A, C);
+    k_fo_grad<R, MASS><<<gn, FO_NODE_THREADS, 0, st>>>(S, A, C);
+    if (S.kind == KIND_NESTEROV) k_fo_nesterov<<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
+    k_fo_outer_positions<R><<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
+    k_fo_outer_multipliers<<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
+    k_fo_final<R><<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
+}
+
+// One Solve() in per-phase launches: the start kernel, then graph chunks of slots
+// (8, then 32) until the state reads FO_DONE.  The chunks are captured once per
+// (arguments, kernel variant) and kept.
+template <typename R, int NPE, int NQP, bool DAMP, bool MR, bool MASS>
+static int run_phased(tlfea_solver_s* s, const FOArgs& S, const TileArgs<R>& A, cudaStream_t st) {
+    auto kern = k_fo_force<R, NPE, NQP, DAMP, MR, MASS>;
+    const size_t smem = tile_smem_bytes<R>(NPE, A.max_local, DAMP, MASS);
+    if (smem > 48 * 1024) TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FOCtl* C = static_cast<FOCtl*>(s->fo_ctl);
+    // the chunks bake in S, A and the kernel variant: recapture when any differs
+    const int variant = (sizeof(R) == 4 ? 1 : 0) | (NPE == 10 ? 2 : 0) | (DAMP ? 4 : 0) | (MR ? 8 : 0) | (MASS ? 16 : 0);
+    std::vector<unsigned char> key(sizeof(int) + sizeof(FOArgs) + sizeof(TileArgs<R>));
+    memcpy(key.data(), &variant, sizeof(int));
+    memcpy(key.data() + sizeof(int), &S, sizeof(FOArgs));
+    memcpy(key.data() + sizeof(int) + sizeof(FOArgs), &A, sizeof(TileArgs<R>));
+    if (key != s->fo_graph_key) {
+        first_order_drop_graphs(s);
+        const int slots[2] = {8, 32};
+        for (int k = 0; k < 2; ++k) {
+            cudaGraph_t g = nullptr;
+            TLFEA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            for (int j = 0; j < slots[k]; ++j) fo_enqueue_slot<R, NPE, NQP, DAMP, MR, MASS>(s, S, A, C, st);
+            const cudaError_t e1 = cudaGetLastError();
+            const cudaError_t e2 = cudaStreamEndCapture(st, &g);
+            cudaGraphExec_t ge = nullptr;
+            const cudaError_t e3 = (e1 == cudaSuccess && e2 == cudaSuccess) ? cudaGraphInstantiate(&ge, g, 0) : e2;
+            if (g) cudaGraphDestroy(g);
+            if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+                cudaGetLastError();
+                first_order_drop_graphs(s);
+                set_error("first-order solve: capture of the per-phase chunk failed");
+                return TLFEA_CUDA_ERROR;
+            }
+            s->fo_graph[k] = ge;
+        }
+        s->fo_graph_key = key;
+    }
+    const int gn = std::max(1, std::min(s->max_blocks, (S.N + FO_NODE_THREADS - 1) / FO_NODE_THREADS));
+    k_fo_start<<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
+    TLFEA_CUDA(cudaGetLastError());
+    TLFEA_LAUNCHED(1);
+    // every slot advances the state by at least one phase: a bound on the replays
+    const long long max_slots = 4 + (long long)std::max(S.max_outer, 1) * ((long long)std::max(S.max_inner, 0) + 2);
+    long long slots = 0;
+    const int per_slot = (S.kind == KIND_NESTEROV) ? 8 : 7;
+    for (int k = 0;; k = 1) {
+        TLFEA_CUDA(cudaGraphLaunch(s->fo_graph[k], st));
+        TLFEA_LAUNCHED(per_slot * (k ? 32 : 8));
+        slots += k ? 32 : 8;
+        int mode = 0;
+        TLFEA_CUDA(cudaMemcpyAsync(&mode, &C->mode, sizeof(int), cudaMemcpyDeviceToHost, st));
+        TLFEA_CUDA(cudaStreamSynchronize(st));
+        if (mode == FO_DONE) break;
+        if (slots > max_slots) {
+            set_error("first-order solve: the per-phase loop did not finish within its iteration bounds");
+            return TLFEA_CUDA_ERROR;
+        }
+    }
+    return TLFEA_OK;
+}
+
 int first_order_alloc(tlfea_solver_s* s) {
     tlfea_element_s* el = s->el;
     const size_t n3 = 3 * (size_t)el->N, N = el->N;
@@ -424,8 +889,18 @@ int first_order_alloc(tlfea_solver_s* s) {
     st |= dalloc(&s->red, (size_t)6 * s->max_blocks);
     st |= dalloc(&s->dstat, 16);
     st |= dalloc(&s->node_fixed, N);
+    if (cudaMalloc(&s->fo_ctl, sizeof(FOCtl)) != cudaSuccess) st = 1;
+    else if (cudaMemset(s->fo_ctl, 0, sizeof(FOCtl)) != cudaSuccess) st = 1;
     if (st) return TLFEA_CUDA_ERROR;
     return TLFEA_OK;
+}
+
+void first_order_drop_graphs(tlfea_solver_s* s) {
+    for (auto& g : s->fo_graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    s->fo_graph_key.clear();
 }
 
 void first_order_free(tlfea_solver_s* s) {
@@ -433,6 +908,9 @@ void first_order_free(tlfea_solver_s* s) {
     dfree(s->g); dfree(s->m); dfree(s->va); dfree(s->lam);
     dfree(s->xp); dfree(s->yp); dfree(s->zp);
     dfree(s->red); dfree(s->dstat); dfree(s->node_fixed);
+    first_order_drop_graphs(s);
+    if (s->fo_ctl) cudaFree(s->fo_ctl);
+    s->fo_ctl = nullptr;
 }
 
 // f_ext = f_base + a * f_var, rounded multiply then rounded add (no fused
@@ -442,6 +920,9 @@ __global__ void k_step_load(int n3, const double* __restrict__ f_base, const dou
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n3) f_ext[i] = __dadd_rn(f_base[i], __dmul_rn(a, f_var[i]));
 }
+
+static int first_order_finish(tlfea_solver_s* s, const std::vector<int>& hs, int n_steps, int* inner_iters,
+                              float ms, bool fp32);
 
 // One Solve(), or n implicit steps with a time-varying load (new).
 int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* inner_iters) {
@@ -561,6 +1042,50 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     };
     cudaStream_t stream = el->stream;
     const int n_steps = std::max(1, steps);
+    st = TLFEA_OK;
+    if (s->fo_mode == 0) {
+        // per-phase launches: each step's load, then its solve, then its statistics
+        auto run_one = [&]() -> int {
+#define TLFEA_FO_PHASED(R_, NPE_, NQP_, AA)                                                              \
+    (mr ? (damp ? run_phased<R_, NPE_, NQP_, true, true, false>(s, S, AA, stream)                        \
+                : run_phased<R_, NPE_, NQP_, false, true, false>(s, S, AA, stream))                      \
+        : mass ? (damp ? run_phased<R_, NPE_, NQP_, true, false, true>(s, S, AA, stream)                 \
+                       : run_phased<R_, NPE_, NQP_, false, false, true>(s, S, AA, stream))               \
+               : (damp ? run_phased<R_, NPE_, NQP_, true, false, false>(s, S, AA, stream)                \
+                       : run_phased<R_, NPE_, NQP_, false, false, false>(s, S, AA, stream)))
+            if (fp32) return (el->npe == 10) ? TLFEA_FO_PHASED(float, 10, 5, A32) : TLFEA_FO_PHASED(float, 4, 1, A32);
+            return (el->npe == 10) ? TLFEA_FO_PHASED(double, 10, 5, A64) : TLFEA_FO_PHASED(double, 4, 1, A64);
+#undef TLFEA_FO_PHASED
+        };
+        std::vector<int> hs(16 * (size_t)n_steps);
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, stream);
+        for (int k = 0; k < n_steps && !st; ++k) {
+            if (load) {
+                const double tk = load->t0 + (k + 1) * S.dt;
+                const double a = load->amp * sin(load->omega * tk + load->phase);
+                const int n3 = 3 * el->N;
+                k_step_load<<<(n3 + 255) / 256, 256, 0, stream>>>(n3, load->f_base, load->f_var, a, el->f_ext);
+                if (cudaGetLastError() != cudaSuccess) st = TLFEA_CUDA_ERROR;
+            }
+            if (!st) st = run_one();
+            if (!st && cudaMemcpy(hs.data() + 16 * (size_t)k, s->dstat, 16 * sizeof(int), cudaMemcpyDeviceToHost) !=
+                           cudaSuccess) {
+                set_error("first-order solve: statistics read-back failed");
+                st = TLFEA_CUDA_ERROR;
+            }
+        }
+        cudaEventRecord(e1, stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st) return st;
+        return first_order_finish(s, hs, n_steps, inner_iters, ms, fp32);
+    }
     int* stat_steps = s->dstat;
     if (n_steps > 1 && (st = dalloc(&stat_steps, 16 * (size_t)n_steps))) return st;
     auto release = [&]() {
@@ -631,6 +1156,13 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
         return TLFEA_CUDA_ERROR;
     }
     release();
+    return first_order_finish(s, hs, n_steps, inner_iters, ms, fp32);
+}
+
+// Statistics of the last step (and inner iterations of every step) into the solver.
+static int first_order_finish(tlfea_solver_s* s, const std::vector<int>& hs, int n_steps, int* inner_iters,
+                              float ms, bool fp32) {
+    tlfea_element_s* el = s->el;
     int status = TLFEA_OK;
     for (int k = 0; k < n_steps; ++k) {
         const int* h = hs.data() + 16 * k;

@@ -2,6 +2,8 @@
 // linear static (CG) solvers.
 #pragma once
 
+#include <vector>
+
 #include "element.cuh"
 
 namespace tlfea {
@@ -45,6 +47,10 @@ struct tlfea_solver_s {
     unsigned char* node_fixed = nullptr;  // N, for the stop rule's free-DOF norm
     int max_blocks = 0;
     int* dstat = nullptr;    // device diagnostics (tlfea_solve_stats fields)
+    int fo_mode = 0;         // 0 = per-phase kernels and graph chunks, 1 = one persistent launch
+    void* fo_ctl = nullptr;  // per-phase mode: the device-side loop state
+    cudaGraphExec_t fo_graph[2] = {nullptr, nullptr};  // per-phase mode: chunks of 8 and 32 slots
+    std::vector<unsigned char> fo_graph_key;             // what the captured chunks bake in
     tlfea_nesterov_params np{};
     tlfea_adamw_params ap{};
     bool params_set = false;

@@ -234,4 +234,14 @@ int tlfea_solver_set_stop_rule(tlfea_solver s, double rel_tol) {
     return TLFEA_OK;
 }
 
+int tlfea_solver_set_mode(tlfea_solver s, int mode) {
+    if (!s || (mode != 0 && mode != 1)) return TLFEA_INVALID_ARG;
+    if (s->kind == tlfea::KIND_LINEAR_STATIC) {
+        tlfea::set_error("the launch mode applies to the Nesterov / AdamW solvers");
+        return TLFEA_UNSUPPORTED;
+    }
+    s->fo_mode = mode;
+    return TLFEA_OK;
+}
+
 }  // extern "C"
