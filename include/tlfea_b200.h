@@ -181,10 +181,6 @@ int tlfea_element_set_force_precision(tlfea_element h, int precision);
  * geometry stream (J^-1 and dV per QP, gradients formed in registers);
  * grid_limit caps the persistent grid (0 = all resident blocks). */
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit);
-/* L2 prefetch of the one-tile-per-block force kernels (force_kernel 0 and 3; new):
- * each tile prefetches into L2 the streams of the tile one wave of resident blocks
- * later, so the next wave's bulk copies hit L2.  On (1) by default; 0 turns it off. */
-int tlfea_element_set_l2_prefetch(tlfea_element h, int on);
 
 /* Allocation-free internal force.  No counterpart in the reference.
  *
@@ -422,6 +418,14 @@ int tlfea_dynbatch_set_step_sizes(tlfea_dynbatch b, const double* alpha);
 int tlfea_dynbatch_set_load(tlfea_dynbatch b, const double* f_var, int n, double amp, double omega, double phase);
 /* Inner iterations per CUDA-graph replay (default 8). */
 int tlfea_dynbatch_set_chunk(tlfea_dynbatch b, int chunk);
+/* Momentum restart of the inner Nesterov loop (new; 0 = off, the reference's
+ * iteration, the default): a sequence whose step works against its momentum,
+ * g . (v_next - v_k) > 0, starts the beta sequence afresh at its next look-ahead (the
+ * gradient restart test of O'Donoghue and Candes, 2015).  Without a restart the
+ * reference's beta schedule converges sublinearly on a well-conditioned but stiff
+ * step Hessian; with it, linearly at about sqrt(condition number) iterations per
+ * e-fold of the residual. */
+int tlfea_dynbatch_set_restart(tlfea_dynbatch b, int on);
 /* Every sequence back to rest in the reference configuration, t = 0. */
 int tlfea_dynbatch_reset(tlfea_dynbatch b);
 /* One implicit step of every sequence.  warm_start: 0 = the previous step's velocity

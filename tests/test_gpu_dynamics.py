@@ -250,3 +250,37 @@ def test_learned_step_predictor_reduces_iterations():
     b.Destroy()
     sp.destroy()
     el.Destroy()
+
+
+def test_momentum_restart_converges_in_fewer_iterations_to_a_checked_residual():
+    """With the gradient restart test (g . (v_next - v_k) > 0 starts the beta sequence
+    afresh) each step reaches the stop rule in fewer inner iterations than the
+    reference's schedule, and the residual it reports is the one recomputed from the
+    oracle's pieces at its final state."""
+    x, y, z, conn, fixed, f, _ = _mesh()
+    E, nu = np.array([2e7, 3e6]), np.array([0.3, 0.3])
+    dt, rho_alm = 1e-3, 1e8
+    alphas = [0.9 / _hessian_lmax(x, y, z, conn, fixed, E[s], nu[s], dt, rho_alm) for s in range(2)]
+    params = (alphas[0], rho_alm, 0.0, 1e-300, 1, 40000, dt)
+    its = {}
+    for restart in (False, True):
+        el, b = _batch(x, y, z, conn, fixed, f, E, nu, params, rel_tol=1e-6)
+        b.SetStepSizes(alphas)
+        b.SetRestart(restart)
+        vprev = [np.zeros(3 * len(x)) for _ in E]
+        its[restart] = []
+        for step in range(2):
+            it, res, conv = b.Step(T.BatchedDynamics.WARM_LINEAR if step else 0)
+            assert conv.all() and (res < 1e-6).all(), (restart, it, res)
+            its[restart].append(it.copy())
+            for s in range(len(E)):
+                xs = b.RetrievePositions(s)
+                vs = b.RetrieveVelocity(s)
+                r = _step_residual(x, y, z, conn, fixed, f, E[s], nu[s], xs, vs, vprev[s], dt)
+                assert abs(r - res[s]) <= 1e-6 * r + 1e-13, (r, res[s])
+                vprev[s] = vs
+        b.Destroy()
+        el.Destroy()
+    # a CPU run of the same iteration: about 6,800 inner iterations per step without the
+    # restart, about 600 with it (E = 2e7)
+    assert np.sum(its[True]) < 0.3 * np.sum(its[False]), its

@@ -35,18 +35,30 @@ def test_learned_warm_start_beats_cold_start():
     u_warm, it_warm, res_warm, st_warm = fm.solve(test, tol=1e-6, u0=g)
     assert np.all(st_cold == 0) and np.all(st_warm == 0)
     assert np.all(res_warm < 1e-6)
-    # What the network gives the solver: the displacement to within a few percent
-    # (the cold start's error is 100%), checked above, and a lower starting residual
-    # ||f - K u_guess|| / ||f|| than the cold start's 1 (max_iter = 0 reports it).  Its
-    # high-frequency error still leaves CG most of its iterations: unpreconditioned CG on
-    # this small mesh needs about as many iterations as it has DOFs either way, so the
-    # iteration count is only checked not to grow.  (The network earns its keep in the
-    # batched SyncedNesterov steps, tests/test_gpu_dynamics.py, where it cuts the
-    # iterations against linear extrapolation.)
-    _, _, r0_warm, _ = fm.solve(test, tol=1e-6, max_iter=0, u0=g)
-    _, _, r0_cold, _ = fm.solve(test, tol=1e-6, max_iter=0)
-    assert np.allclose(r0_cold, 1.0)
-    assert np.median(r0_warm) < 0.8, np.median(r0_warm)
+    # What the network gives the solver: the displacement to within a few percent (the
+    # cold start's error is 100%), checked above, and an energy-norm error
+    # ||u_guess - u||_K / ||u||_K -- the error CG minimises -- well below the cold start's
+    # 1.  It does not lower the starting residual ||f - K u_guess|| / ||f||: the guess's
+    # high-frequency error, which K amplifies, leaves it above the cold start's 1 on this
+    # mesh (3.6, median), and unpreconditioned CG needs about as many iterations as the
+    # mesh has DOFs either way, so the iteration count is only checked not to grow.  The
+    # network earns its keep in the batched SyncedNesterov steps
+    # (tests/test_gpu_dynamics.py), where it cuts the iterations against linear
+    # extrapolation.
+    import torch
+
+    fixed_dofs = (3 * fm.fixed[:, None] + np.arange(3)[None, :]).ravel()
+    e = torch.zeros(256, g.shape[1], dtype=torch.float64, device="cuda")
+    e[:] = torch.as_tensor(g - u_cold)
+    e[:, torch.as_tensor(fixed_dofs, device="cuda")] = 0.0
+    uc = torch.as_tensor(u_cold, device="cuda").contiguous()
+    Ke, Ku = torch.empty_like(e), torch.empty_like(uc)
+    torch.cuda.synchronize()
+    fm.solver.Apply(e.data_ptr(), Ke.data_ptr())
+    fm.solver.Apply(uc.data_ptr(), Ku.data_ptr())
+    torch.cuda.synchronize()
+    energy = torch.sqrt((e * Ke).sum(1) / (uc * Ku).sum(1)).cpu().numpy()
+    assert np.median(energy) < 0.5, np.median(energy)
     assert it_warm.mean() <= 1.02 * it_cold.mean()
     for k in range(0, 256, 37):
         assert rel(u_warm[k], u_cold[k]) < 1e-4

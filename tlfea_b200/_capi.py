@@ -107,7 +107,6 @@ _SIGS = {
     "tlfea_element_compute_internal_force": [_P, _P],
     "tlfea_element_set_force_precision": [_P, C.c_int],
     "tlfea_element_set_launch_config": [_P, C.c_int, C.c_int],
-    "tlfea_element_set_l2_prefetch": [_P, C.c_int],
     "tlfea_element_compute_internal_force_noalloc": [_P, _P, _P],
     "tlfea_element_get_mass_nnz": [_P, C.POINTER(_LL)],
     "tlfea_element_retrieve_mass_csr": [_P, _I, _I, _D],
@@ -152,6 +151,7 @@ _SIGS = {
     "tlfea_dynbatch_set_step_sizes": [_P, _D],
     "tlfea_dynbatch_set_load": [_P, _D, C.c_int, C.c_double, C.c_double, C.c_double],
     "tlfea_dynbatch_set_chunk": [_P, C.c_int],
+    "tlfea_dynbatch_set_restart": [_P, C.c_int],
     "tlfea_dynbatch_reset": [_P],
     "tlfea_dynbatch_step": [_P, C.c_int, _P, _I, _D, _I],
     "tlfea_dynbatch_device_ptrs": [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)],

@@ -182,11 +182,6 @@ class _TetData(ElementBase):
         k = self.FORCE_KERNELS[force_kernel] if isinstance(force_kernel, str) else int(force_kernel)
         capi.call("tlfea_element_set_launch_config", self._handle(), k, int(grid_limit))
 
-    def SetL2Prefetch(self, on: bool = True):
-        """New: whether the one-tile-per-block force kernels ("tma", "compact") prefetch
-        into L2 the streams of the tile one wave of resident blocks later (default on)."""
-        capi.call("tlfea_element_set_l2_prefetch", self._handle(), 1 if on else 0)
-
     # -- retrieval ---------------------------------------------------------------
     def RetrieveMassCSRToCPU(self):
         nnz = C.c_longlong()
@@ -719,6 +714,11 @@ class BatchedDynamics:
 
     def SetChunk(self, chunk: int):
         capi.call("tlfea_dynbatch_set_chunk", self._h, int(chunk))
+
+    def SetRestart(self, on: bool = True):
+        """New: momentum restart of the inner Nesterov loop when g . (v_next - v_k) > 0
+        (off by default: the reference's iteration)."""
+        capi.call("tlfea_dynbatch_set_restart", self._h, 1 if on else 0)
 
     def Reset(self):
         capi.call("tlfea_dynbatch_reset", self._h)

@@ -74,6 +74,12 @@ struct DynArgs {
     const double* beta;  // beta[k] for the look-ahead after inner iteration k (beta[0] = 0)
     double rho, dt, rel_tol;
     int max_inner;
+    // momentum restart (optional; off = the reference's iteration): per sequence the
+    // index into beta, which restarts at 0 when g . (v_next - v_k) > 0 (the gradient
+    // restart test of O'Donoghue and Candes, 2015); red2 holds the two dot partials
+    int restart;
+    int* mom;
+    double* red2;
 };
 
 // ---------------------------------------------------------------- kernels
@@ -124,6 +130,7 @@ __global__ void k_dyn_outer_ctl(DynArgs D, const int* __restrict__ outer_done) {
         const int od = outer_done[s];
         D.done[s] = od ? DYN_FINISHED : DYN_RUNNING;
         D.inner[s] = 0;
+        D.mom[s] = 0;
         D.ticket[s] = 0u;
         if (od) atomicAdd(&cnt, 1);
     }
@@ -180,7 +187,7 @@ __global__ void __launch_bounds__(DYN_NODE_THREADS) k_dyn_grad(DynArgs D) {
     if (D.done[s] != DYN_RUNNING) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t oN = (size_t)s * D.N, o3 = 3 * oN;
-    double sg = 0.0;
+    double sg = 0.0, gdy = 0.0, gg = 0.0;
     if (i < D.N) {
         double fn[3];
         const int b = D.node_bidx[i];
@@ -217,6 +224,18 @@ __global__ void __launch_bounds__(DYN_NODE_THREADS) k_dyn_grad(DynArgs D) {
             }
             D.g[o3 + t] = r;
             if (free_node) sg += r * r;
+            if (D.restart) {
+                gdy += r * (D.vg[o3 + t] - D.vk[o3 + t]);  // g . (y - v_k)
+                gg += r * r;
+            }
+        }
+    }
+    if (D.restart) {
+        gdy = block_sum(gdy, red_sh);
+        gg = block_sum(gg, red_sh);
+        if (threadIdx.x == 0) {
+            D.red2[(size_t)s * D.blocks_per_seq + blockIdx.x] = gdy;
+            D.red2[((size_t)D.B + s) * D.blocks_per_seq + blockIdx.x] = gg;
         }
     }
     sg = block_sum(sg, red_sh);
@@ -231,11 +250,23 @@ __global__ void __launch_bounds__(DYN_NODE_THREADS) k_dyn_grad(DynArgs D) {
     if (threadIdx.x < 32) {
         __threadfence();
         double a = 0.0;
-        for (int bb = threadIdx.x; bb < D.blocks_per_seq; bb += 32)
+        double a_dy = 0.0, a_gg = 0.0;
+        for (int bb = threadIdx.x; bb < D.blocks_per_seq; bb += 32) {
             a += __ldcg(D.red + (size_t)s * D.blocks_per_seq + bb);
+            if (D.restart) {
+                a_dy += __ldcg(D.red2 + (size_t)s * D.blocks_per_seq + bb);
+                a_gg += __ldcg(D.red2 + ((size_t)D.B + s) * D.blocks_per_seq + bb);
+            }
+        }
         a = warp_sum(a);
+        a_dy = warp_sum(a_dy);
+        a_gg = warp_sum(a_gg);
         if (threadIdx.x == 0) {
             D.ticket[s] = 0u;
+            // g . (v_next - v_k) = g . (y - v_k) - alpha ||g||^2 > 0: the step works against
+            // the momentum, so the next look-ahead starts the beta sequence afresh
+            const bool restart_now = D.restart && (a_dy - D.alpha_s[s] * a_gg > 0.0);
+            D.mom[s] = restart_now ? 0 : D.mom[s] + 1;
             const double fe = *D.fext_norm;
             const double rel = fe > 0.0 ? sqrt(a) / fe : sqrt(a);
             D.rel[s] = rel;
@@ -270,7 +301,7 @@ __global__ void __launch_bounds__(DYN_NODE_THREADS) k_dyn_update(DynArgs D) {
     if (i >= D.N) return;
     const size_t oN = (size_t)s * D.N, o3 = 3 * oN;
     const bool predict = (st == DYN_RUNNING);
-    const double beta = predict ? D.beta[D.inner[s]] : 0.0;
+    const double beta = predict ? D.beta[D.mom[s]] : 0.0;
     const double alpha = D.alpha_s[s];
     double yv[3];
 #pragma unroll
@@ -377,6 +408,8 @@ struct tlfea_dynbatch_s {
     double *lam = nullptr, *vhist = nullptr, *lam_s = nullptr, *mu_s = nullptr, *alpha_s = nullptr;
     int *done = nullptr, *inner = nullptr, *inner_total = nullptr, *rule_met = nullptr, *status = nullptr;
     int* outer_done = nullptr;
+    int* mom = nullptr;       // momentum index per sequence (restart)
+    double* red2 = nullptr;   // restart test partials
     double *rel = nullptr, *red = nullptr, *beta = nullptr, *fext_norm = nullptr;
     unsigned int *ticket = nullptr, *ticket2 = nullptr;
     int* counters = nullptr;    // [n_done]
@@ -535,6 +568,7 @@ void dyn_free(tlfea_dynbatch_s* b) {
     dfree(b->lam); dfree(b->vhist); dfree(b->lam_s); dfree(b->mu_s); dfree(b->alpha_s);
     dfree(b->done); dfree(b->inner); dfree(b->inner_total); dfree(b->rule_met); dfree(b->status);
     dfree(b->outer_done); dfree(b->rel); dfree(b->red); dfree(b->beta); dfree(b->fext_norm);
+    dfree(b->mom); dfree(b->red2);
     dfree(b->ticket); dfree(b->ticket2); dfree(b->counters); dfree(b->node_fixed);
     dfree(b->f_base); dfree(b->f_var); dfree(b->zero_off);
     if (b->h_counters) cudaFreeHost(b->h_counters);
@@ -590,6 +624,7 @@ int tlfea_dynbatch_create(tlfea_element mesh, int n_seq, tlfea_dynbatch* out) {
     st |= dalloc(&b->done, B) | dalloc(&b->inner, B) | dalloc(&b->inner_total, B) | dalloc(&b->rule_met, B);
     st |= dalloc(&b->status, B) | dalloc(&b->outer_done, B) | dalloc(&b->rel, B);
     st |= dalloc(&b->red, B * (size_t)bps) | dalloc(&b->fext_norm, 1);
+    st |= dalloc(&b->mom, B) | dalloc(&b->red2, 2 * B * (size_t)bps);
     st |= dalloc(&b->ticket, B) | dalloc(&b->ticket2, B) | dalloc(&b->counters, 1);
     st |= dalloc(&b->node_fixed, N) | dalloc(&b->f_base, n3) | dalloc(&b->f_var, n3);
     if (el->n_constraint == 0) st |= dalloc(&b->zero_off, n3 + 1);
@@ -639,6 +674,10 @@ int tlfea_dynbatch_create(tlfea_element mesh, int n_seq, tlfea_dynbatch* out) {
     D.alpha_s = b->alpha_s;
     D.done = b->done; D.inner = b->inner; D.inner_total = b->inner_total; D.rule_met = b->rule_met;
     D.status = b->status; D.rel = b->rel; D.red = b->red; D.ticket = b->ticket; D.n_done = b->counters;
+    D.mom = b->mom;
+    D.red2 = b->red2;
+    D.restart = 0;
+    cudaMemsetAsync(b->mom, 0, B * sizeof(int), stream);
     const dim3 grid(bps, n_seq);
     k_dyn_reset_state<<<grid, DYN_NODE_THREADS, 0, stream>>>(D, b->vhist, el->X0x, el->X0y, el->X0z);
     const cudaError_t e2 = cudaGetLastError();
@@ -720,6 +759,14 @@ int tlfea_dynbatch_set_load(tlfea_dynbatch b, const double* f_var, int n, double
     b->amp = amp;
     b->omega = omega;
     b->phase = phase;
+    return TLFEA_OK;
+}
+
+int tlfea_dynbatch_set_restart(tlfea_dynbatch b, int on) {
+    CHECK_DYN(b);
+    if (on != 0 && on != 1) return TLFEA_INVALID_ARG;
+    if (on != b->D.restart) drop_graph(b);  // kernel arguments changed
+    b->D.restart = on;
     return TLFEA_OK;
 }
 

@@ -663,16 +663,6 @@ static int launch_combine(tlfea_element_s* h, const R* partial, R* f_out) {
     return TLFEA_OK;
 }
 
-// CTAs of `kern` resident at once on the element's GPU with `smem` bytes each: the
-// distance (in tiles) of the L2 prefetch of a one-tile-per-CTA force kernel.
-template <typename K>
-static int resident_ctas(tlfea_element_s* h, K kern, size_t smem) {
-    int per_sm = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TILE_ELEMS, smem) != cudaSuccess) return 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess) return 0;
-    return per_sm * sms;
-}
-
 // One tile per block, QP slices double-buffered by bulk copies.
 template <typename R, int NPE, int NQP, bool DAMP>
 static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
@@ -689,9 +679,7 @@ static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
         configured = true;
     }
     if (smem > 48 * 1024) TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TileArgs<R> B = A;
-    B.pf_ahead = h->l2_prefetch ? resident_ctas(h, kern, smem) : 0;
-    kern<<<h->tl.n_tiles, TILE_ELEMS, smem, h->stream>>>(B, h->d_err);
+    kern<<<h->tl.n_tiles, TILE_ELEMS, smem, h->stream>>>(A, h->d_err);
     TLFEA_CHECK_LAUNCH();
     return TLFEA_OK;
 }
@@ -712,9 +700,7 @@ static int launch_tile_geo(tlfea_element_s* h, const TileArgs<R>& A) {
         configured = true;
     }
     if (smem > 48 * 1024) TLFEA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TileArgs<R> B = A;
-    B.pf_ahead = h->l2_prefetch ? resident_ctas(h, kern, smem) : 0;
-    kern<<<h->tl.n_tiles, TILE_ELEMS, smem, h->stream>>>(B, h->d_err);
+    kern<<<h->tl.n_tiles, TILE_ELEMS, smem, h->stream>>>(A, h->d_err);
     TLFEA_CHECK_LAUNCH();
     return TLFEA_OK;
 }
@@ -1377,13 +1363,6 @@ int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_
     h->force_kernel = force_kernel;
     h->pipe_grid_limit = grid_limit;
     for (int& g : h->pipe_grid) g = 0;
-    return TLFEA_OK;
-}
-
-int tlfea_element_set_l2_prefetch(tlfea_element h, int on) {
-    CHECK_HANDLE(h);
-    if (on != 0 && on != 1) return TLFEA_INVALID_ARG;
-    h->l2_prefetch = (on == 1);
     return TLFEA_OK;
 }
 

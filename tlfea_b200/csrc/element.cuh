@@ -102,9 +102,6 @@ struct TileArgs {
     const double* vp;          // MASS instantiations: previous-step velocity (interleaved 3N)
     double mass_scale;         // MASS instantiations: rho / dt
     int max_local;
-    // tiles ahead whose streams a force tile prefetches into L2 (the CTAs resident at
-    // once, so the prefetched tile is the one that starts when this one ends); 0 = off
-    int pf_ahead;
     QpBary qb;
 };
 
@@ -853,7 +850,6 @@ struct tlfea_element_s {
     // 0 = TMA pipeline, 1 = one tile per block; cap on the pipeline grid (0 = none)
     int force_kernel = 0;
     int pipe_grid_limit = 0;
-    bool l2_prefetch = true;  // force kernels 0 and 3: prefetch the next wave's tile streams
 };
 
 namespace tlfea {

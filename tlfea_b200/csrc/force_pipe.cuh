@@ -62,11 +62,6 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                  : "memory");
 }
 
-// L2 prefetch of `bytes` (a multiple of 16) from a 16-byte aligned global address.
-__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-}
-
 template <int BYTES>
 __device__ __forceinline__ void cp_async(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES) : "memory");
@@ -445,33 +440,6 @@ __device__ __forceinline__ void stage_tile_nodes(const TileArgs<R>& A, int lb, i
     }
 }
 
-// Warp 1 of a force tile prefetches into L2 what the tile A.pf_ahead tiles later will
-// read first: its QP-slice stream (gradients or J^-1, `slice_elems` values per QP), dV,
-// local connectivity and incidence by bulk prefetches, and its node tables line by
-// line.  Tiles start roughly in index order, so that tile starts on some SM about when
-// this one ends, and its copies then hit L2 instead of waiting on DRAM.
-template <typename R, int NPE, int NQP>
-__device__ __forceinline__ void prefetch_next_tile(const TileArgs<R>& A, const R* slices, int slice_elems) {
-    constexpr int TE = TILE_ELEMS;
-    if (A.pf_ahead <= 0 || (threadIdx.x >> 5) != 1) return;
-    const int nt = blockIdx.x + A.pf_ahead;
-    if (nt >= (int)gridDim.x) return;
-    const int lane = threadIdx.x & 31;
-    // slice q of tile nt starts (nt * NQP + q) * slice_elems * TE values into the stream
-    if (lane < NQP)
-        bulk_prefetch_l2(slices + ((size_t)nt * NQP + lane) * slice_elems * TE, slice_elems * TE * sizeof(R));
-    if (lane == NQP) bulk_prefetch_l2(A.dv + (size_t)nt * NQP * TE, NQP * TE * sizeof(R));
-    if (lane == NQP + 1) bulk_prefetch_l2(A.lconn + (size_t)nt * NPE * TE, NPE * TE * sizeof(uint16_t));
-    if (lane == NQP + 2) bulk_prefetch_l2(A.inc + (size_t)nt * NPE * TE, NPE * TE * sizeof(uint16_t));
-    const int lb = A.node_off[nt], le = A.node_off[nt + 1];
-    for (int ln = lb + 32 * lane; ln < le; ln += 32 * 32) {  // one 128-byte line of int per lane
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(A.ln_gid + ln));
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(A.ln_pslot + ln));
-    }
-    for (int ln = lb + 64 * lane; ln < le; ln += 64 * 32)  // uint16: 64 per line
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(A.ln_inc_end + ln));
-}
-
 template <typename R, int NPE>
 struct TileTmaGeom {
     static constexpr uint32_t GRAD_BYTES = NPE * 3 * TILE_ELEMS * sizeof(R);
@@ -554,7 +522,6 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_for
         issue(0);
         if (S > 1 && NQP > 1) issue(1);
     }
-    prefetch_next_tile<R, NPE, NQP>(A, A.grad, NPE * 3);
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
     stage_tile_nodes<R, DAMP>(A, lb, nl, xs, ys, zs, dsts, iends, vs);
     __syncthreads();  // positions and node tables staged; barriers initialised
@@ -847,7 +814,6 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, in
         issue(0);
         if (NQP > 1) issue(1);
     }
-    prefetch_next_tile<R, NPE, NQP>(A, A.ji, 9);
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
     stage_tile_nodes<R, DAMP>(A, lb, nl, xs, ys, zs, dsts, iends, vs);
     __syncthreads();  // positions and node tables staged; barriers initialised
