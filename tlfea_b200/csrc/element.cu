@@ -664,9 +664,9 @@ static int launch_combine(tlfea_element_s* h, const R* partial, R* f_out) {
 }
 
 // One tile per block, QP slices double-buffered by bulk copies.
-template <typename R, int NPE, int NQP, bool DAMP>
+template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false>
 static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
-    auto kern = k_tile_force_tma<R, NPE, NQP, DAMP>;
+    auto kern = k_tile_force_tma<R, NPE, NQP, DAMP, LEAN && sizeof(R) == 8>;
     const size_t smem = tile_tma_smem_bytes<R, NPE>(h->tl.max_local, DAMP);
     if (smem > 227 * 1024) {
         set_error("force kernel shared memory exceeds 227 KB (tile touches too many nodes)");
@@ -748,6 +748,8 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
         st = damp ? launch_pipe<R, NPE, NQP, true>(h, A) : launch_pipe<R, NPE, NQP, false>(h, A);
     else if (h->force_kernel == 3)
         st = damp ? launch_tile_geo<R, NPE, NQP, true>(h, A) : launch_tile_geo<R, NPE, NQP, false>(h, A);
+    else if (h->force_kernel == 4)
+        st = damp ? launch_tile_tma<R, NPE, NQP, true, true>(h, A) : launch_tile_tma<R, NPE, NQP, false, true>(h, A);
     else
         st = damp ? launch_tile_tma<R, NPE, NQP, true>(h, A) : launch_tile_tma<R, NPE, NQP, false>(h, A);
     if (st) return st;
@@ -1359,7 +1361,7 @@ int tlfea_element_compute_internal_force(tlfea_element h, const double* d_v) {
 
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit) {
     CHECK_HANDLE(h);
-    if (force_kernel < 0 || force_kernel > 3 || grid_limit < 0) return TLFEA_INVALID_ARG;
+    if (force_kernel < 0 || force_kernel > 4 || grid_limit < 0) return TLFEA_INVALID_ARG;
     h->force_kernel = force_kernel;
     h->pipe_grid_limit = grid_limit;
     for (int& g : h->pipe_grid) g = 0;

@@ -480,8 +480,8 @@ inline size_t tile_tma_smem_bytes(int max_local, bool damp) {
     return TileTmaLayout<R, NPE>(max_local, damp).total;
 }
 
-template <typename R, int NPE, int NQP, bool DAMP>
-__global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_force_tma(TileArgs<R> A, int* err) {
+template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false>
+__global__ void __launch_bounds__(TILE_ELEMS, (sizeof(R) == 4 || LEAN) ? 4 : 3) k_tile_force_tma(TileArgs<R> A, int* err) {
     using G = TileTmaGeom<R, NPE>;
     constexpr int S = G::STAGES;
     constexpr int TE = TILE_ELEMS;
@@ -624,6 +624,84 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_for
                 fe[((2 * p) * 3 + d) * TE + t] = f2[p][d].x;
                 fe[((2 * p + 1) * 3 + d) * TE + t] = f2[p][d].y;
             }
+        __syncthreads();
+    } else if constexpr (LEAN) {
+        // FP64, register-lean: the QP slice is read from shared memory twice (F, then
+        // the forces) instead of being copied into registers, so a thread holds only
+        // its element forces and F / P; the single stage is refilled after the force
+        // pass (4 CTAs per SM interleave the loads instead)
+        // local node indices are read from shared memory where used (a register copy
+        // indexed in the partly unrolled F loop would live in local memory)
+        auto lc = [&](int a) -> int { return lcs[a * TE + t]; };
+        R f[NPE][3];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
+#pragma unroll 1
+        for (int q = 0; q < NQP; ++q) {
+            if (!mbar_wait(bar0 + 8 * (q % S), (q / S) & 1)) atomicExch(err, 3);
+            const unsigned char* st = stage0 + (size_t)(q % S) * G::STAGE_BYTES;
+            const R* gs = reinterpret_cast<const R*>(st);
+            const R dv = reinterpret_cast<const R*>(st + G::GRAD_BYTES)[t];
+            R P[3][3];
+            {
+                double F[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) F[i][j] = 0.0;
+#pragma unroll 2
+                for (int a = 0; a < NPE; ++a) {
+                    const double xa[3] = {xs[lc(a)], ys[lc(a)], zs[lc(a)]};
+                    const double ga[3] = {gs[grad_slot<R>(a, 0, t)], gs[grad_slot<R>(a, 1, t)],
+                                          gs[grad_slot<R>(a, 2, t)]};
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) F[i][j] += xa[i] * ga[j];
+                }
+                svk_p_reference(F, A.lambda, A.mu, P);
+                if (DAMP) {
+                    double Fd[3][3], Pv[3][3];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) Fd[i][j] = 0.0;
+#pragma unroll 2
+                    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc(a) + i] * gs[grad_slot<R>(a, j, t)];
+                    kelvin_voigt<double>(F, Fd, A.eta, A.lamd, Pv);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
+                }
+            }
+            // f_a += (P dV) grad_a   (FEAT10DataFunc.cuh:417-449)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) P[i][j] *= dv;
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) {
+                const R ga[3] = {gs[grad_slot<R>(a, 0, t)], gs[grad_slot<R>(a, 1, t)], gs[grad_slot<R>(a, 2, t)]};
+#pragma unroll
+                for (int i = 0; i < 3; ++i) f[a][i] += P[i][0] * ga[0] + P[i][1] * ga[1] + P[i][2] * ga[2];
+            }
+            if (q + S < NQP) {
+                // every thread's generic reads of this stage precede the bulk refill
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncthreads();
+                if (t == 0) issue(q + S);
+            }
+        }
+        __syncthreads();  // every thread is done with the stages the force table reuses
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
         __syncthreads();
     } else {
         int lc[NPE];
