@@ -385,8 +385,8 @@ def kernels_only(args):
     r = np.random.default_rng(1)
     el.UpdatePositions(*(v + 1e-4 * r.standard_normal(v.shape) for v in (x, y, z)))
     if args.kernels_only == "force":
-        # gradient-stream kernel, then the compact-geometry kernel
-        for kern in ("tma", "compact"):
+        # gradient-stream kernel, the compact-geometry kernel, the register-lean FP64 variant
+        for kern in ("tma", "compact", "tma-lean"):
             el.SetLaunchConfig(kern)
             for prec in ("fp32", "fp32", "fp64", "fp64"):
                 el.SetForcePrecision(prec)
@@ -650,6 +650,25 @@ def config2_more_legs(args, T, cfg):
         nes[prec] = {"step_s": round(dt, 4), "inner_iters": st["inner_iters_total"], "outer_iters": st["outer_iters"],
                      "ms_per_inner_iteration": round(1e3 * dt / it, 4),
                      "inner_iterations_per_s": round(it / dt, 1), "kernel_ms": round(st["kernel_ms"], 3)}
+        # the cost of one inner iteration: 60 iterations at zero tolerances (2 outer x 30
+        # inner), in both launch modes
+        fixed_it = {}
+        for mode in ("phased", "persistent"):
+            s.SetMode(mode)
+            s.SetParameters(T.SyncedNesterovParams(1.0e-8, 1e14, 0.0, 0.0, 2, 30, 1.0e-3))
+            el.ResetPositions()
+            s.Solve()
+            s.SetParameters(T.SyncedNesterovParams(1.0e-8, 1e14, 0.0, 0.0, 2, 30, 1.0e-3))
+            el.ResetPositions()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.Solve()
+            torch.cuda.synchronize()
+            dtf = time.perf_counter() - t0
+            itf = max(1, s.GetStats()["inner_iters_total"])
+            fixed_it[mode] = {"inner_iters": itf, "ms_per_inner_iteration": round(1e3 * dtf / itf, 4)}
+        s.SetMode("phased")
+        nes[prec]["fixed_60_iterations"] = fixed_it
         del s
     el.SetForcePrecision("fp64")
     el.Destroy()
