@@ -230,7 +230,11 @@ int tlfea_element_retrieve_constraint_jac_csr(tlfea_element h, int which, int* o
                                               double* values);
 /* WriteOutputVTK (FEAT10Data.cu:759-794): legacy ASCII VTK of the current mesh. */
 int tlfea_element_write_vtk(tlfea_element h, const char* filename);
-/* Get{X,Y,Z}12DevicePtr, GetExternalForceDevicePtr (FEAT10Data.cuh:599-621). */
+/* Get{X,Y,Z}12DevicePtr, GetExternalForceDevicePtr (FEAT10Data.cuh:599-621).  Pass NULL
+ * for pointers not wanted.  Once a position pointer has been handed out, the caller may
+ * write the positions at any time, so the element rebuilds the records it derives from
+ * them (the tile-ordered node values, FP32 mode's displacements) before every force
+ * evaluation from then on. */
 int tlfea_element_device_ptrs(tlfea_element h, double** x, double** y, double** z, double** f_ext, double** f_int);
 
 /* ------------------------------------------------------------- solvers */

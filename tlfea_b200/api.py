@@ -250,25 +250,30 @@ class _TetData(ElementBase):
     def WriteOutputVTK(self, filename: str):
         capi.call("tlfea_element_write_vtk", self._handle(), str(filename).encode())
 
-    def _ptrs(self):
-        ps = [C.c_void_p() for _ in range(5)]
-        capi.call("tlfea_element_device_ptrs", self._handle(), *[C.byref(p) for p in ps])
-        return [p.value for p in ps]
+    def _ptr(self, k):
+        """Device pointer k of (x, y, z, f_ext, f_int); only that one is requested (taking a
+        position pointer makes the element rebuild its derived position records before
+        every force evaluation, since the caller may write the positions directly)."""
+        p = C.c_void_p()
+        args = [None] * 5
+        args[k] = C.byref(p)
+        capi.call("tlfea_element_device_ptrs", self._handle(), *args)
+        return p.value
 
     def GetX12DevicePtr(self):
-        return self._ptrs()[0]
+        return self._ptr(0)
 
     def GetY12DevicePtr(self):
-        return self._ptrs()[1]
+        return self._ptr(1)
 
     def GetZ12DevicePtr(self):
-        return self._ptrs()[2]
+        return self._ptr(2)
 
     def GetExternalForceDevicePtr(self):
-        return self._ptrs()[3]
+        return self._ptr(3)
 
     def GetInternalForceDevicePtr(self):
-        return self._ptrs()[4]
+        return self._ptr(4)
 
     def SetBlocking(self, blocking: bool):
         """New: False makes compute calls return after enqueueing on GetStream()."""

@@ -22,6 +22,9 @@ constexpr int T4_NQP = 1;
 // incidence code packs slot*TE + element).
 constexpr int TILE_ELEMS = 128;
 constexpr int TILE_SHIFT = 7;
+// a tile's block in the tile-ordered node record holds a multiple of this many entries:
+// 8 doubles, ints or uint16 are each a multiple of 16 bytes (bulk-copy granularity)
+constexpr int TILE_NODE_PAD = 8;
 
 // Number of kernels this library has launched (the bench reports launches
 // inside its timed region from the difference of two reads).

@@ -312,6 +312,13 @@ static void free_tiling(Tiling& tl) {
     dfree(tl.bnode_off);
     dfree(tl.bnode_slots);
     dfree(tl.node_bidx);
+    dfree(tl.pad_off);
+    dfree(tl.pad_gid);
+    dfree(tl.pad_dst);
+    dfree(tl.pad_iend);
+    dfree(tl.sx);
+    dfree(tl.sy);
+    dfree(tl.sz);
     dfree(tl.grad64);
     dfree(tl.dv64);
     dfree(tl.grad32);
@@ -485,7 +492,40 @@ static int build_tiling(tlfea_element_s* h, const double* x, const double* y, co
     tl.n_bnodes = (int)bgid.size();
     tl.h_tile_elem = tile_elem;
 
+    // the tile-ordered node record, each tile's block padded to TILE_NODE_PAD entries
+    std::vector<int> pad_off((size_t)n_tiles + 1, 0), pad_gid, pad_dst;
+    std::vector<uint16_t> pad_iend;
+    int max_pad = 0;
+    for (int tile = 0; tile < n_tiles; ++tile) {
+        const int b = node_off[tile], nl = node_off[tile + 1] - b;
+        const int np = (nl + TILE_NODE_PAD - 1) / TILE_NODE_PAD * TILE_NODE_PAD;
+        max_pad = std::max(max_pad, np);
+        for (int l = 0; l < np; ++l) {
+            if (l < nl) {
+                const int g = ln_gid[(size_t)b + l], ps = ln_pslot[(size_t)b + l];
+                pad_gid.push_back(g);
+                pad_dst.push_back(ps < 0 ? g : -(ps + 1));
+                pad_iend.push_back(ln_inc_end[(size_t)b + l]);
+            } else {
+                pad_gid.push_back(-1);
+                pad_dst.push_back(0);
+                pad_iend.push_back(0);
+            }
+        }
+        pad_off[tile + 1] = pad_off[tile] + np;
+    }
+    tl.n_pad = (long long)pad_gid.size();
+    tl.max_local_pad = std::max(max_pad, TILE_NODE_PAD);
+
     int st;
+    if ((st = upload(&tl.pad_off, pad_off, h->stream))) return st;
+    if ((st = upload(&tl.pad_gid, pad_gid, h->stream))) return st;
+    if ((st = upload(&tl.pad_dst, pad_dst, h->stream))) return st;
+    if ((st = upload(&tl.pad_iend, pad_iend, h->stream))) return st;
+    if ((st = dalloc(&tl.sx, (size_t)tl.n_pad)) || (st = dalloc(&tl.sy, (size_t)tl.n_pad)) ||
+        (st = dalloc(&tl.sz, (size_t)tl.n_pad)))
+        return st;
+    h->stage_content = 0;
     if ((st = upload(&tl.node_off, node_off, h->stream))) return st;
     if ((st = upload(&tl.ln_gid, ln_gid, h->stream))) return st;
     if ((st = upload(&tl.ln_pslot, ln_pslot, h->stream))) return st;
@@ -594,7 +634,14 @@ static TileArgs<R> make_args(tlfea_element_s* h, bool fp32) {
     A.mu = (R)h->mu;
     A.eta = (R)h->eta_d;
     A.lamd = (R)h->lambda_d;
-    A.max_local = tl.max_local;
+    A.max_local = tl.max_local_pad;  // staging regions hold a tile's padded record block
+    A.pad_off = tl.pad_off;
+    A.pad_dst = tl.pad_dst;
+    A.pad_iend = tl.pad_iend;
+    A.pad_gid = tl.pad_gid;
+    A.sx = tl.sx;
+    A.sy = tl.sy;
+    A.sz = tl.sz;
     if constexpr (sizeof(R) == 8) {
         A.grad = (const R*)tl.grad64;
         A.ji = (const R*)tl.ji64;
@@ -630,7 +677,7 @@ static TileArgs<R> make_args(tlfea_element_s* h, bool fp32) {
 
 template <typename R, int NPE, int NQP, int MODE, bool DAMP, bool MR = false>
 static int launch_tiles(tlfea_element_s* h, const TileArgs<R>& A) {
-    const size_t smem = tile_smem_bytes<R>(NPE, h->tl.max_local, DAMP);
+    const size_t smem = tile_smem_bytes<R>(NPE, h->tl.max_local_pad, DAMP);
     if (smem > 200 * 1024) {
         set_error("tile shared memory exceeds 200 KB");
         return TLFEA_UNSUPPORTED;
@@ -667,7 +714,7 @@ static int launch_combine(tlfea_element_s* h, const R* partial, R* f_out) {
 template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false>
 static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
     auto kern = k_tile_force_tma<R, NPE, NQP, DAMP, LEAN && sizeof(R) == 8>;
-    const size_t smem = tile_tma_smem_bytes<R, NPE>(h->tl.max_local, DAMP);
+    const size_t smem = tile_tma_smem_bytes<R, NPE>(h->tl.max_local_pad, DAMP);
     if (smem > 227 * 1024) {
         set_error("force kernel shared memory exceeds 227 KB (tile touches too many nodes)");
         return TLFEA_UNSUPPORTED;
@@ -688,7 +735,7 @@ static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
 template <typename R, int NPE, int NQP, bool DAMP, bool MR = false>
 static int launch_tile_geo(tlfea_element_s* h, const TileArgs<R>& A) {
     auto kern = k_tile_force_geo<R, NPE, NQP, DAMP, MR>;
-    const size_t smem = tile_geo_smem_bytes<R, NPE>(h->tl.max_local, DAMP);
+    const size_t smem = tile_geo_smem_bytes<R, NPE>(h->tl.max_local_pad, DAMP);
     if (smem > 227 * 1024) {
         set_error("force kernel shared memory exceeds 227 KB (tile touches too many nodes)");
         return TLFEA_UNSUPPORTED;
@@ -709,7 +756,7 @@ static int launch_tile_geo(tlfea_element_s* h, const TileArgs<R>& A) {
 template <typename R, int NPE, int NQP, bool DAMP>
 static int launch_pipe(tlfea_element_s* h, const TileArgs<R>& A) {
     auto kern = k_force_pipe<R, NPE, NQP, DAMP>;
-    const size_t smem = pipe_smem_bytes<R, NPE>(h->tl.max_local, DAMP);
+    const size_t smem = pipe_smem_bytes<R, NPE>(h->tl.max_local_pad, DAMP);
     int& grid = h->pipe_grid[(sizeof(R) == 4 ? 2 : 0) + (DAMP ? 1 : 0)];
     if (grid == 0) {
         if (smem > 227 * 1024) {
@@ -756,11 +803,51 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
     return launch_combine<R, false>(h, A.partial, A.f_out);
 }
 
+// The tile-ordered node record's values: FP64 positions (disp = 0) or displacements
+// x - X0 (disp = 1, FP32 mode, the same difference as k_disp64); padding entries 0.
+__global__ void k_stage_refresh(long long n, const int* __restrict__ gid, const double* __restrict__ x,
+                                const double* __restrict__ y, const double* __restrict__ z,
+                                const double* __restrict__ X0x, const double* __restrict__ X0y,
+                                const double* __restrict__ X0z, int disp, double* __restrict__ sx,
+                                double* __restrict__ sy, double* __restrict__ sz) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int g = gid[k];
+        double a = 0.0, b = 0.0, c = 0.0;
+        if (g >= 0) {
+            a = x[g];
+            b = y[g];
+            c = z[g];
+            if (disp) {
+                a -= X0x[g];
+                b -= X0y[g];
+                c -= X0z[g];
+            }
+        }
+        sx[k] = a;
+        sy[k] = b;
+        sz[k] = c;
+    }
+}
+
+// Rebuild the tile-ordered node record for the precision about to be evaluated, after
+// a change of positions (or every time, once the positions' pointers are exposed).
+static int element_refresh_record(tlfea_element_s* h, bool fp32) {
+    const int want = fp32 ? 2 : 1;
+    if (h->stage_content == want && !h->positions_exposed) return TLFEA_OK;
+    const long long n = h->tl.n_pad;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
+    k_stage_refresh<<<blocks, 256, 0, h->stream>>>(n, h->tl.pad_gid, h->x, h->y, h->z, h->X0x, h->X0y, h->X0z,
+                                                   fp32 ? 1 : 0, h->tl.sx, h->tl.sy, h->tl.sz);
+    TLFEA_CHECK_LAUNCH();
+    h->stage_content = want;
+    return TLFEA_OK;
+}
+
 // f_int (FP64) or f_int32 (FP32) = internal force at the current positions.
 // Asynchronous on h->stream (the solvers call it inside their loops).
 // The interleaved FP64 displacement the FP32 force stages from, after a change of positions.
 int element_refresh_u64(tlfea_element_s* h) {
-    if (!h->u_dirty) return TLFEA_OK;
+    if (!h->u_dirty && !h->positions_exposed) return TLFEA_OK;
     const int n = h->N;
     k_disp64<<<(n + 255) / 256, 256, 0, h->stream>>>(n, h->x, h->y, h->z, h->X0x, h->X0y, h->X0z, h->u64);
     TLFEA_CHECK_LAUNCH();
@@ -770,6 +857,10 @@ int element_refresh_u64(tlfea_element_s* h) {
 
 int element_force(tlfea_element_s* h, const double* d_v, bool fp32) {
     int st;
+    // the bulk-copy tile kernels (launch options 0, 3, 4, and Mooney-Rivlin's) stage the record
+    if ((h->force_kernel == 0 || h->force_kernel >= 3 || h->material == TLFEA_MATERIAL_MOONEY_RIVLIN) &&
+        (st = element_refresh_record(h, fp32)))
+        return st;
     if (fp32) {
         if ((st = element_refresh_u64(h))) return st;
         st = (h->npe == 10) ? force_dispatch<float, 10, 5>(h, d_v, true) : force_dispatch<float, 4, 1>(h, d_v, true);
@@ -1007,7 +1098,7 @@ int tlfea_element_set_blocking(tlfea_element h, int blocking) {
 int tlfea_element_reset_positions(tlfea_element h) {
     CHECK_HANDLE(h);
     REQUIRE_SETUP(h);
-    h->u_dirty = true;
+    positions_changed(h);
     const size_t nb = (size_t)h->N * sizeof(double);
     TLFEA_CUDA(cudaMemcpyAsync(h->x, h->X0x, nb, cudaMemcpyDeviceToDevice, h->stream));
     TLFEA_CUDA(cudaMemcpyAsync(h->y, h->X0y, nb, cudaMemcpyDeviceToDevice, h->stream));
@@ -1069,7 +1160,7 @@ int tlfea_element_setup(tlfea_element h, const double* qx, const double* qy, con
     if (st) return st;
     if ((st = build_incidence(h))) return st;
     SYNC(h);
-    h->u_dirty = true;
+    positions_changed(h);
     h->is_setup = true;
     return TLFEA_OK;
 }
@@ -1194,7 +1285,7 @@ static int copy_positions(tlfea_element h, double* dx, double* dy, double* dz, c
 
 int tlfea_element_update_positions(tlfea_element h, const double* x, const double* y, const double* z, int n) {
     CHECK_HANDLE(h);
-    h->u_dirty = true;
+    positions_changed(h);
     return copy_positions(h, h->x, h->y, h->z, x, y, z, n);
 }
 
@@ -1229,7 +1320,7 @@ int tlfea_element_calc_dndu_pre(tlfea_element h) {
     TLFEA_CUDA(cudaMemcpyAsync(h->X0x, h->x, nb, cudaMemcpyDeviceToDevice, h->stream));
     TLFEA_CUDA(cudaMemcpyAsync(h->X0y, h->y, nb, cudaMemcpyDeviceToDevice, h->stream));
     TLFEA_CUDA(cudaMemcpyAsync(h->X0z, h->z, nb, cudaMemcpyDeviceToDevice, h->stream));
-    h->u_dirty = true;
+    positions_changed(h);
     h->precomputed = true;
     SYNC(h);
     return TLFEA_OK;
@@ -1586,6 +1677,8 @@ int tlfea_element_write_vtk(tlfea_element h, const char* filename) {
 
 int tlfea_element_device_ptrs(tlfea_element h, double** x, double** y, double** z, double** f_ext, double** f_int) {
     CHECK_HANDLE(h);
+    // a caller holding the positions may write them without telling the element
+    if (x || y || z) h->positions_exposed = true;
     if (x) *x = h->x;
     if (y) *y = h->y;
     if (z) *z = h->z;

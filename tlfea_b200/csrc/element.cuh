@@ -48,6 +48,21 @@ struct Tiling {
     int* bnode_off = nullptr;       // n_bnodes + 1
     int* bnode_slots = nullptr;     // n_pslots
     int* node_bidx = nullptr;       // N, boundary index or -1
+    // Tile-ordered node record: every tile's local nodes in a block padded to a multiple
+    // of TILE_NODE_PAD entries (so each block starts 16-byte aligned for every element
+    // type and one bulk copy moves it).  pad_gid: global node (-1 = padding); pad_dst:
+    // the scatter destination (global id, or -(partial slot + 1)); pad_iend: incidence
+    // end; sx/sy/sz: the node values the force kernels stage (FP64 positions, or FP32
+    // mode's displacements), refreshed from x (and X0) after the positions change.
+    long long n_pad = 0;
+    int max_local_pad = 0;
+    int* pad_off = nullptr;         // n_tiles + 1, in entries
+    int* pad_gid = nullptr;         // n_pad
+    int* pad_dst = nullptr;         // n_pad
+    uint16_t* pad_iend = nullptr;   // n_pad
+    double* sx = nullptr;           // n_pad
+    double* sy = nullptr;
+    double* sz = nullptr;
     double* grad64 = nullptr;
     double* dv64 = nullptr;
     float* grad32 = nullptr;
@@ -102,6 +117,14 @@ struct TileArgs {
     const double* vp;          // MASS instantiations: previous-step velocity (interleaved 3N)
     double mass_scale;         // MASS instantiations: rho / dt
     int max_local;
+    // the tile-ordered node record (Tiling::pad_*), read by bulk copies
+    const int* pad_off;
+    const int* pad_dst;
+    const uint16_t* pad_iend;
+    const int* pad_gid;
+    const double* sx;
+    const double* sy;
+    const double* sz;
     QpBary qb;
 };
 
@@ -810,6 +833,12 @@ struct tlfea_element_s {
     double *X0x = nullptr, *X0y = nullptr, *X0z = nullptr;
     double* u64 = nullptr;  // interleaved x - X0 for the FP32 force (refreshed when positions change)
     bool u_dirty = true;
+    // the tile-ordered node record (Tiling::sx/sy/sz): 0 = stale, 1 = FP64 positions,
+    // 2 = displacements x - X0 (FP32 mode); stale again whenever the positions change
+    int stage_content = 0;
+    // set once a caller has taken the positions' device pointers: it may write them at
+    // any time, so the derived records are rebuilt before every evaluation
+    bool positions_exposed = false;
     int* d_conn = nullptr;
     double* f_int = nullptr;
     double* f_ext = nullptr;
@@ -851,6 +880,13 @@ struct tlfea_element_s {
     int force_kernel = 0;
     int pipe_grid_limit = 0;
 };
+
+// The positions changed: the records derived from them (FP32 mode's displacement u64,
+// the tile-ordered node record) are rebuilt before the next force evaluation.
+inline void positions_changed(tlfea_element_s* h) {
+    h->u_dirty = true;
+    h->stage_content = 0;
+}
 
 namespace tlfea {
 // Implemented in element.cu, used by the solvers.

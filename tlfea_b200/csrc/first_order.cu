@@ -1179,7 +1179,7 @@ static int first_order_finish(tlfea_solver_s* s, const std::vector<int>& hs, int
     s->stats.stop_rule_met = hl[8];
     s->stats.kernel_ms = ms;
     el->f_int_from32 = fp32;
-    el->u_dirty = true;  // the solve moved the positions
+    positions_changed(el);  // the solve moved the positions
     if (status == TLFEA_NONFINITE) {
         set_error("non-finite gradient norm");
         return TLFEA_NONFINITE;

@@ -440,6 +440,35 @@ __device__ __forceinline__ void stage_tile_nodes(const TileArgs<R>& A, int lb, i
     }
 }
 
+// Stage a tile's block of the tile-ordered node record (values, scatter destinations,
+// incidence ends) by bulk copies completing on `bar` (thread 0; `bar` initialised with
+// count 1).  The record holds every tile's nodes contiguously, padded to TILE_NODE_PAD
+// entries, so the staging is three plus two copies instead of dependent gathers
+// (local node -> global id -> value).
+template <typename R>
+__device__ __forceinline__ void issue_node_record(const TileArgs<R>& A, int tile, uint32_t bar, double* xs,
+                                                  double* ys, double* zs, int* dsts, uint16_t* iends) {
+    const int pb = A.pad_off[tile], np = A.pad_off[tile + 1] - pb;
+    mbar_expect_tx(bar, (uint32_t)np * (3 * sizeof(double) + sizeof(int) + sizeof(uint16_t)));
+    bulk_g2s(smem_u32(xs), A.sx + pb, np * sizeof(double), bar);
+    bulk_g2s(smem_u32(ys), A.sy + pb, np * sizeof(double), bar);
+    bulk_g2s(smem_u32(zs), A.sz + pb, np * sizeof(double), bar);
+    bulk_g2s(smem_u32(dsts), A.pad_dst + pb, np * sizeof(int), bar);
+    bulk_g2s(smem_u32(iends), A.pad_iend + pb, np * sizeof(uint16_t), bar);
+}
+
+// Velocities of a tile's local nodes for the Kelvin-Voigt term (gathered).
+template <typename R>
+__device__ __forceinline__ void stage_tile_velocities(const TileArgs<R>& A, int tile, int nl, double* vs) {
+    const int pb = A.pad_off[tile];
+    for (int ln = threadIdx.x; ln < nl; ln += TILE_ELEMS) {
+        const int g = A.pad_gid[pb + ln];
+        vs[3 * ln + 0] = A.v[3 * g + 0];
+        vs[3 * ln + 1] = A.v[3 * g + 1];
+        vs[3 * ln + 2] = A.v[3 * g + 2];
+    }
+}
+
 template <typename R, int NPE>
 struct TileTmaGeom {
     static constexpr uint32_t GRAD_BYTES = NPE * 3 * TILE_ELEMS * sizeof(R);
@@ -471,7 +500,7 @@ struct TileTmaLayout {
         iend = al(dst + (size_t)max_local * sizeof(int));
         vel = al(iend + (size_t)max_local * sizeof(uint16_t));
         bar = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
-        total = bar + 2 * sizeof(unsigned long long);
+        total = bar + 3 * sizeof(unsigned long long);  // two stage barriers, the node record's
     }
 };
 
@@ -517,14 +546,17 @@ __global__ void __launch_bounds__(TILE_ELEMS, (sizeof(R) == 4 || LEAN) ? 4 : 3) 
     if (t == 0) {
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
+        mbar_init(bar0 + 16, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         issue(0);
         if (S > 1 && NQP > 1) issue(1);
+        issue_node_record(A, tile, bar0 + 16, xs, ys, zs, dsts, iends);
     }
-    const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
-    stage_tile_nodes<R, DAMP>(A, lb, nl, xs, ys, zs, dsts, iends, vs);
-    __syncthreads();  // positions and node tables staged; barriers initialised
+    const int nl = A.node_off[tile + 1] - A.node_off[tile];
+    if (DAMP) stage_tile_velocities(A, tile, nl, vs);
+    __syncthreads();  // barriers initialised (velocities staged)
+    if (!mbar_wait(bar0 + 16, 0)) atomicExch(err, 3);  // the node record
 
     if constexpr (sizeof(R) == 4) {
         // FP32: paired arithmetic (two nodes per instruction, __ffma2_rn).  The
@@ -843,7 +875,7 @@ struct TileGeoLayout {
         iend = al(dst + (size_t)max_local * sizeof(int));
         vel = al(iend + (size_t)max_local * sizeof(uint16_t));
         bar = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
-        total = bar + 2 * sizeof(unsigned long long);
+        total = bar + 3 * sizeof(unsigned long long);  // two stage barriers, the node record's
     }
 };
 
@@ -887,14 +919,17 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, in
     if (t == 0) {
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
+        mbar_init(bar0 + 16, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         issue(0);
         if (NQP > 1) issue(1);
+        issue_node_record(A, tile, bar0 + 16, xs, ys, zs, dsts, iends);
     }
-    const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
-    stage_tile_nodes<R, DAMP>(A, lb, nl, xs, ys, zs, dsts, iends, vs);
-    __syncthreads();  // positions and node tables staged; barriers initialised
+    const int nl = A.node_off[tile + 1] - A.node_off[tile];
+    if (DAMP) stage_tile_velocities(A, tile, nl, vs);
+    __syncthreads();  // barriers initialised (velocities staged)
+    if (!mbar_wait(bar0 + 16, 0)) atomicExch(err, 3);  // the node record
 
     int lc[NPE];
     R f[NPE][3], xa[NPE][3], va[NPE][3];

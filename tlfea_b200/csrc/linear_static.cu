@@ -628,7 +628,7 @@ int linear_static_solve(tlfea_solver_s* s) {
     }
     // UpdatePositions
     k_update_positions<<<(N + 255) / 256, 256, 0, stream>>>(N, el->x, el->y, el->z, s->u);
-    el->u_dirty = true;
+    positions_changed(el);
     TLFEA_CHECK_LAUNCH();
     TLFEA_CUDA(cudaStreamSynchronize(stream));
     return TLFEA_OK;
