@@ -1182,6 +1182,16 @@ def main():
                                  "ms": round(ms_f, 4),
                                  "speedup_vs_gradient_stream": round(ef[prec]["ms"] / ms_f, 3)}
     el.SetLaunchConfig("tma")
+    # the same evaluations with the tile-ordered node record rebuilt every time (as after
+    # every change of positions): once a caller holds the positions' device pointer the
+    # element can no longer tell, and refreshes before each evaluation
+    el.GetX12DevicePtr()
+    for prec in ("fp32", "fp64"):
+        el.SetForcePrecision(prec)
+        for _ in range(3):
+            el.ComputeInternalForce()
+        ef[prec]["ms_with_record_refresh"] = round(time_stream(torch, stream, el.ComputeInternalForce,
+                                                               args.kernel_reps), 4)
     el.SetForcePrecision("fp64")
     el.SetBlocking(True)
 

@@ -379,67 +379,6 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2) k_force_pipe(TileArgs<R> A, i
 // always in flight while the CTA computes.  The node positions are gathered by
 // the threads while the first two slices land.
 
-// Stage one tile's local nodes into shared memory: destination (global id, or
-// -(partial slot + 1) for a node shared with other tiles), incidence end, and the node
-// values in FP64 (stage_pos: positions, or displacements in FP32 mode), plus
-// velocities for the Kelvin-Voigt term.  The loads are dependent gathers (local node
-// -> global id -> values), so each thread first issues the table loads of up to
-// STAGE_NODES of its nodes, then their value loads, and only then stores: the
-// latencies overlap instead of adding up node by node.
-constexpr int STAGE_NODES = 4;
-
-template <typename R, bool DAMP>
-__device__ __forceinline__ void stage_tile_nodes(const TileArgs<R>& A, int lb, int nl, double* xs, double* ys,
-                                                 double* zs, int* dsts, uint16_t* iends, double* vs) {
-    constexpr int TE = TILE_ELEMS;
-    const int t = threadIdx.x;
-    int gid[STAGE_NODES], ps[STAGE_NODES];
-    uint16_t ie[STAGE_NODES];
-#pragma unroll
-    for (int k = 0; k < STAGE_NODES; ++k) {
-        const int ln = t + k * TE;
-        gid[k] = 0;
-        ps[k] = -1;
-        ie[k] = 0;
-        if (ln < nl) {
-            gid[k] = A.ln_gid[lb + ln];
-            ps[k] = A.ln_pslot[lb + ln];
-            ie[k] = A.ln_inc_end[lb + ln];
-        }
-    }
-    double vx[STAGE_NODES], vy[STAGE_NODES], vz[STAGE_NODES];
-#pragma unroll
-    for (int k = 0; k < STAGE_NODES; ++k)
-        if (t + k * TE < nl) stage_pos(A, gid[k], vx[k], vy[k], vz[k]);
-#pragma unroll
-    for (int k = 0; k < STAGE_NODES; ++k) {
-        const int ln = t + k * TE;
-        if (ln < nl) {
-            iends[ln] = ie[k];
-            dsts[ln] = (ps[k] < 0) ? gid[k] : -(ps[k] + 1);
-            xs[ln] = vx[k];
-            ys[ln] = vy[k];
-            zs[ln] = vz[k];
-        }
-    }
-    // tiles with more local nodes than STAGE_NODES per thread: the rest one by one
-    for (int ln = t + STAGE_NODES * TE; ln < nl; ln += TE) {
-        const int g = A.ln_gid[lb + ln];
-        const int p = A.ln_pslot[lb + ln];
-        iends[ln] = A.ln_inc_end[lb + ln];
-        dsts[ln] = (p < 0) ? g : -(p + 1);
-        stage_pos(A, g, xs[ln], ys[ln], zs[ln]);
-    }
-    if (DAMP) {
-        for (int ln = t; ln < nl; ln += TE) {
-            const int g = A.ln_gid[lb + ln];
-            vs[3 * ln + 0] = A.v[3 * g + 0];
-            vs[3 * ln + 1] = A.v[3 * g + 1];
-            vs[3 * ln + 2] = A.v[3 * g + 2];
-        }
-    }
-}
-
 // Stage a tile's block of the tile-ordered node record (values, scatter destinations,
 // incidence ends) by bulk copies completing on `bar` (thread 0; `bar` initialised with
 // count 1).  The record holds every tile's nodes contiguously, padded to TILE_NODE_PAD
