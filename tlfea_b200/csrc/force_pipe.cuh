@@ -408,7 +408,7 @@ __device__ __forceinline__ void stage_tile_velocities(const TileArgs<R>& A, int 
     }
 }
 
-template <typename R, int NPE>
+template <typename R, int NPE, int NS = 0>
 struct TileTmaGeom {
     static constexpr uint32_t GRAD_BYTES = NPE * 3 * TILE_ELEMS * sizeof(R);
     static constexpr uint32_t DV_BYTES = TILE_ELEMS * sizeof(R);
@@ -418,7 +418,8 @@ struct TileTmaGeom {
     // QP-slice stages: FP64 copies a slice into registers before computing it, so one
     // stage suffices (refilled as soon as it is read); FP32 reads a slice twice (H, then
     // the forces) and double-buffers
-    static constexpr int STAGES = sizeof(R) == 8 ? 1 : 2;
+    // the double buffer (NS = 0); NS > 0 sets the stage count (a deeper ring, launch option 5)
+    static constexpr int STAGES = NS > 0 ? NS : (sizeof(R) == 8 ? 1 : 2);
     // element forces of the scatter reuse the stages once the QP loop is done
     static_assert(3 * NPE * TILE_ELEMS * sizeof(R) <= STAGES * STAGE_BYTES, "force table must fit in the stages");
     static_assert(LCONN_BYTES % 16 == 0 && INC_BYTES % 16 == 0 && STAGE_BYTES % 16 == 0, "bulk sizes");
@@ -426,12 +427,13 @@ struct TileTmaGeom {
 
 // Byte offsets of the regions of k_tile_force_tma's shared memory, each
 // 16-byte aligned: [stage(s), later the element forces][lconn][incidence]
-// [x y z][node destination][incidence end][velocities][2 mbarriers].
-template <typename R, int NPE>
+// [x y z][node destination][incidence end][velocities][a barrier per stage, the node
+// record's].
+template <typename R, int NPE, int NS = 0>
 struct TileTmaLayout {
     size_t inc, pos, dst, iend, vel, bar, total;
     __host__ __device__ TileTmaLayout(int max_local, bool damp) {
-        using G = TileTmaGeom<R, NPE>;
+        using G = TileTmaGeom<R, NPE, NS>;
         auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
         inc = G::STAGES * (size_t)G::STAGE_BYTES + G::LCONN_BYTES;
         pos = inc + G::INC_BYTES;
@@ -439,24 +441,25 @@ struct TileTmaLayout {
         iend = al(dst + (size_t)max_local * sizeof(int));
         vel = al(iend + (size_t)max_local * sizeof(uint16_t));
         bar = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
-        total = bar + 3 * sizeof(unsigned long long);  // two stage barriers, the node record's
+        total = bar + (G::STAGES + 1) * sizeof(unsigned long long);
     }
 };
 
-template <typename R, int NPE>
+template <typename R, int NPE, int NS = 0>
 inline size_t tile_tma_smem_bytes(int max_local, bool damp) {
-    return TileTmaLayout<R, NPE>(max_local, damp).total;
+    return TileTmaLayout<R, NPE, NS>(max_local, damp).total;
 }
 
-template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false>
-__global__ void __launch_bounds__(TILE_ELEMS, (sizeof(R) == 4 || LEAN) ? 4 : 3) k_tile_force_tma(TileArgs<R> A, int* err) {
-    using G = TileTmaGeom<R, NPE>;
+template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false, int NS = 0>
+__global__ void __launch_bounds__(TILE_ELEMS, NS == 3 ? 3 : ((sizeof(R) == 4 || LEAN) ? 4 : 3))
+    k_tile_force_tma(TileArgs<R> A, int* err) {
+    using G = TileTmaGeom<R, NPE, NS>;
     constexpr int S = G::STAGES;
     constexpr int TE = TILE_ELEMS;
     extern __shared__ __align__(128) unsigned char smem[];
     const int tile = blockIdx.x, t = threadIdx.x;
     const int ML = A.max_local;
-    const TileTmaLayout<R, NPE> L(ML, DAMP);
+    const TileTmaLayout<R, NPE, NS> L(ML, DAMP);
     unsigned char* stage0 = smem;
     const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + S * G::STAGE_BYTES);
     const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
@@ -483,19 +486,16 @@ __global__ void __launch_bounds__(TILE_ELEMS, (sizeof(R) == 4 || LEAN) ? 4 : 3) 
         }
     };
     if (t == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar0 + 8, 1);
-        mbar_init(bar0 + 16, 1);
+        for (int k = 0; k <= S; ++k) mbar_init(bar0 + 8 * k, 1);  // S stages, then the node record
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue(0);
-        if (S > 1 && NQP > 1) issue(1);
-        issue_node_record(A, tile, bar0 + 16, xs, ys, zs, dsts, iends);
+        for (int q = 0; q < S && q < NQP; ++q) issue(q);
+        issue_node_record(A, tile, bar0 + 8 * S, xs, ys, zs, dsts, iends);
     }
     const int nl = A.node_off[tile + 1] - A.node_off[tile];
     if (DAMP) stage_tile_velocities(A, tile, nl, vs);
     __syncthreads();  // barriers initialised (velocities staged)
-    if (!mbar_wait(bar0 + 16, 0)) atomicExch(err, 3);  // the node record
+    if (!mbar_wait(bar0 + 8 * S, 0)) atomicExch(err, 3);  // the node record
 
     if constexpr (sizeof(R) == 4) {
         // FP32: paired arithmetic (two nodes per instruction, __ffma2_rn).  The
