@@ -711,10 +711,10 @@ static int launch_combine(tlfea_element_s* h, const R* partial, R* f_out) {
 }
 
 // One tile per block, QP slices double-buffered by bulk copies.
-template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false, int NS = 0>
+template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false, int NS = 0, bool CSM = false>
 static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
-    auto kern = k_tile_force_tma<R, NPE, NQP, DAMP, LEAN && sizeof(R) == 8, NS>;
-    const size_t smem = tile_tma_smem_bytes<R, NPE, NS>(h->tl.max_local_pad, DAMP);
+    auto kern = k_tile_force_tma<R, NPE, NQP, DAMP, LEAN && sizeof(R) == 8, NS, CSM>;
+    const size_t smem = tile_tma_smem_bytes<R, NPE, NS, CSM>(h->tl.max_local_pad, DAMP);
     if (smem > 227 * 1024) {
         set_error("force kernel shared memory exceeds 227 KB (tile touches too many nodes)");
         return TLFEA_UNSUPPORTED;
@@ -800,6 +800,10 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
     else if (h->force_kernel == 5) {  // a deeper slice ring: 3 stages in FP32, 2 in FP64
         constexpr int NS = sizeof(R) == 4 ? 3 : 2;
         st = damp ? launch_tile_tma<R, NPE, NQP, true, false, NS>(h, A) : launch_tile_tma<R, NPE, NQP, false, false, NS>(h, A);
+    } else if (h->force_kernel == 6 && sizeof(R) == 4 && tile_tma_csm_fits<R, NPE>(h->tl.max_local_pad)) {
+        // FP32 with the node values in the second stage buffer: 5 blocks per SM
+        constexpr bool C = sizeof(R) == 4;
+        st = damp ? launch_tile_tma<R, NPE, NQP, true, false, 0, C>(h, A) : launch_tile_tma<R, NPE, NQP, false, false, 0, C>(h, A);
     }
     else
         st = damp ? launch_tile_tma<R, NPE, NQP, true>(h, A) : launch_tile_tma<R, NPE, NQP, false>(h, A);
@@ -1456,7 +1460,7 @@ int tlfea_element_compute_internal_force(tlfea_element h, const double* d_v) {
 
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit) {
     CHECK_HANDLE(h);
-    if (force_kernel < 0 || force_kernel > 5 || grid_limit < 0) return TLFEA_INVALID_ARG;
+    if (force_kernel < 0 || force_kernel > 6 || grid_limit < 0) return TLFEA_INVALID_ARG;
     h->force_kernel = force_kernel;
     h->pipe_grid_limit = grid_limit;
     for (int& g : h->pipe_grid) g = 0;

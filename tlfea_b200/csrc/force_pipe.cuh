@@ -418,7 +418,7 @@ struct TileTmaGeom {
     // QP-slice stages: FP64 copies a slice into registers before computing it, so one
     // stage suffices (refilled as soon as it is read); FP32 reads a slice twice (H, then
     // the forces) and double-buffers
-    // the double buffer (NS = 0); NS > 0 sets the stage count (a deeper ring, launch option 5)
+    // NS > 0 sets the stage count (a deeper ring, launch option 5)
     static constexpr int STAGES = NS > 0 ? NS : (sizeof(R) == 8 ? 1 : 2);
     // element forces of the scatter reuse the stages once the QP loop is done
     static_assert(3 * NPE * TILE_ELEMS * sizeof(R) <= STAGES * STAGE_BYTES, "force table must fit in the stages");
@@ -428,16 +428,17 @@ struct TileTmaGeom {
 // Byte offsets of the regions of k_tile_force_tma's shared memory, each
 // 16-byte aligned: [stage(s), later the element forces][lconn][incidence]
 // [x y z][node destination][incidence end][velocities][a barrier per stage, the node
-// record's].
-template <typename R, int NPE, int NS = 0>
+// record's].  CSM (compact shared memory, FP32): the node values x y z live in the
+// second stage buffer, whose first slice is copied only once they are in registers.
+template <typename R, int NPE, int NS = 0, bool CSM = false>
 struct TileTmaLayout {
     size_t inc, pos, dst, iend, vel, bar, total;
     __host__ __device__ TileTmaLayout(int max_local, bool damp) {
         using G = TileTmaGeom<R, NPE, NS>;
         auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
         inc = G::STAGES * (size_t)G::STAGE_BYTES + G::LCONN_BYTES;
-        pos = inc + G::INC_BYTES;
-        dst = al(pos + 3 * (size_t)max_local * sizeof(double));
+        pos = CSM ? (size_t)G::STAGE_BYTES : inc + G::INC_BYTES;
+        dst = CSM ? al(inc + G::INC_BYTES) : al(pos + 3 * (size_t)max_local * sizeof(double));
         iend = al(dst + (size_t)max_local * sizeof(int));
         vel = al(iend + (size_t)max_local * sizeof(uint16_t));
         bar = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
@@ -445,21 +446,28 @@ struct TileTmaLayout {
     }
 };
 
-template <typename R, int NPE, int NS = 0>
+template <typename R, int NPE, int NS = 0, bool CSM = false>
 inline size_t tile_tma_smem_bytes(int max_local, bool damp) {
-    return TileTmaLayout<R, NPE, NS>(max_local, damp).total;
+    return TileTmaLayout<R, NPE, NS, CSM>(max_local, damp).total;
 }
 
-template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false, int NS = 0>
-__global__ void __launch_bounds__(TILE_ELEMS, NS == 3 ? 3 : ((sizeof(R) == 4 || LEAN) ? 4 : 3))
+// Whether a tile's node values fit the second stage buffer (the CSM layout).
+template <typename R, int NPE>
+inline bool tile_tma_csm_fits(int max_local) {
+    return 3 * (size_t)max_local * sizeof(double) <= TileTmaGeom<R, NPE>::STAGE_BYTES;
+}
+
+template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false, int NS = 0, bool CSM = false>
+__global__ void __launch_bounds__(TILE_ELEMS, CSM ? 5 : (NS == 3 ? 3 : ((sizeof(R) == 4 || LEAN) ? 4 : 3)))
     k_tile_force_tma(TileArgs<R> A, int* err) {
     using G = TileTmaGeom<R, NPE, NS>;
     constexpr int S = G::STAGES;
+    static_assert(!CSM || (sizeof(R) == 4 && S == 2), "the compact layout is the FP32 double buffer's");
     constexpr int TE = TILE_ELEMS;
     extern __shared__ __align__(128) unsigned char smem[];
     const int tile = blockIdx.x, t = threadIdx.x;
     const int ML = A.max_local;
-    const TileTmaLayout<R, NPE, NS> L(ML, DAMP);
+    const TileTmaLayout<R, NPE, NS, CSM> L(ML, DAMP);
     unsigned char* stage0 = smem;
     const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + S * G::STAGE_BYTES);
     const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
@@ -489,7 +497,7 @@ __global__ void __launch_bounds__(TILE_ELEMS, NS == 3 ? 3 : ((sizeof(R) == 4 || 
         for (int k = 0; k <= S; ++k) mbar_init(bar0 + 8 * k, 1);  // S stages, then the node record
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        for (int q = 0; q < S && q < NQP; ++q) issue(q);
+        for (int q = 0; q < (CSM ? 1 : S) && q < NQP; ++q) issue(q);  // CSM: stage 1 holds x y z first
         issue_node_record(A, tile, bar0 + 8 * S, xs, ys, zs, dsts, iends);
     }
     const int nl = A.node_off[tile + 1] - A.node_off[tile];
@@ -519,6 +527,12 @@ __global__ void __launch_bounds__(TILE_ELEMS, NS == 3 ? 3 : ((sizeof(R) == 4 || 
                     up[p][d] = make_float2(ua[2 * p][d], ua[2 * p + 1][d]);
                     f2[p][d] = make_float2(0.f, 0.f);
                 }
+        }
+        if constexpr (CSM) {
+            // every thread has read x y z out of the second stage buffer: its first slice now
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (t == 0 && NQP > 1) issue(1);
         }
         // velocities relative to the element's first node, differenced per QP (keeping
         // them in registers would spill)
