@@ -386,7 +386,7 @@ def kernels_only(args):
     el.UpdatePositions(*(v + 1e-4 * r.standard_normal(v.shape) for v in (x, y, z)))
     if args.kernels_only == "force":
         # gradient-stream kernel, the compact-geometry kernel, the register-lean FP64 variant
-        for kern in ("tma", "compact", "tma-lean"):
+        for kern in ("tma", "compact", "tma-lean", "tma-compact-smem"):
             el.SetLaunchConfig(kern)
             for prec in ("fp32", "fp32", "fp64", "fp64"):
                 el.SetForcePrecision(prec)

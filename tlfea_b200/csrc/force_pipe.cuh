@@ -518,15 +518,18 @@ __global__ void __launch_bounds__(TILE_ELEMS, CSM ? 5 : (NS == 3 ? 3 : ((sizeof(
         for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
         float2 up[NP][3], f2[NP][3];
         {
-            float ua[NPE][3];
-            element_nodes<float, NPE>(xs, ys, zs, lc, ua);
+            // element_nodes' values (relative to the element's first node, differenced in
+            // FP64, rounded once), formed directly as node pairs
+            const double* sv[3] = {xs, ys, zs};
 #pragma unroll
-            for (int p = 0; p < NP; ++p)
+            for (int d = 0; d < 3; ++d) {
+                const double b = sv[d][lc[0]];
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    up[p][d] = make_float2(ua[2 * p][d], ua[2 * p + 1][d]);
+                for (int p = 0; p < NP; ++p) {
+                    up[p][d] = make_float2(float(sv[d][lc[2 * p]] - b), float(sv[d][lc[2 * p + 1]] - b));
                     f2[p][d] = make_float2(0.f, 0.f);
                 }
+            }
         }
         if constexpr (CSM) {
             // every thread has read x y z out of the second stage buffer: its first slice now
