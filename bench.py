@@ -385,8 +385,8 @@ def kernels_only(args):
     r = np.random.default_rng(1)
     el.UpdatePositions(*(v + 1e-4 * r.standard_normal(v.shape) for v in (x, y, z)))
     if args.kernels_only == "force":
-        # gradient-stream kernel, the compact-geometry kernel, the register-lean FP64 variant
-        for kern in ("tma", "compact", "tma-lean", "tma-compact-smem"):
+        # gradient-stream kernel, then the compact-geometry kernel
+        for kern in ("tma", "compact"):
             el.SetLaunchConfig(kern)
             for prec in ("fp32", "fp32", "fp64", "fp64"):
                 el.SetForcePrecision(prec)

@@ -178,12 +178,7 @@ int tlfea_element_set_force_precision(tlfea_element h, int precision);
  * force_kernel 0 = one tile per block with bulk-copy double-buffered QP
  * slices of the gradient stream (default), 1 = one tile per block with direct
  * loads, 2 = persistent producer/consumer pipeline, 3 = as 0 on the compact
- * geometry stream (J^-1 and dV per QP, gradients formed in registers), 4 = as 0
- * with the FP64 slices read from shared memory twice instead of copied into
- * registers (fewer registers, more resident blocks; FP32 as 0), 5 = as 0 with a
- * deeper slice ring (3 stages in FP32, 2 in FP64), 6 = as 0 with FP32's node values
- * kept in its second stage buffer until they are in registers (less shared memory, 5
- * blocks per SM; FP64, or a tile too large for the buffer: as 0);
+ * geometry stream (J^-1 and dV per QP, gradients formed in registers);
  * grid_limit caps the persistent grid (0 = all resident blocks). */
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit);
 

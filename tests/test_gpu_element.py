@@ -99,7 +99,7 @@ def test_fused_force_with_kelvin_voigt_damping(order):
     el.Destroy()
 
 
-@pytest.mark.parametrize("kernel", ["compact", "direct", "pipeline", "tma-lean", "tma-deep", "tma-compact-smem"])
+@pytest.mark.parametrize("kernel", ["compact", "direct", "pipeline"])
 @pytest.mark.parametrize("order", [10, 4])
 @pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("fp32", TOL32)])
 def test_force_kernel_variants_match_oracle(kernel, order, prec, tol):
@@ -143,7 +143,7 @@ def test_compact_kernel_large_mesh_rigid_motion():
     xs = perturb(x, y, z, 1e-4, 4)
     el.UpdatePositions(*xs)
     out = {}
-    for k in ("compact", "tma", "tma-lean", "tma-deep", "tma-compact-smem"):
+    for k in ("compact", "tma"):
         el.SetLaunchConfig(k)
         for prec in ("fp64", "fp32"):
             el.SetForcePrecision(prec)
@@ -152,10 +152,6 @@ def test_compact_kernel_large_mesh_rigid_motion():
     assert np.abs(f_rigid).max() < 1e-8 * np.abs(out["compact", "fp64"]).max()
     assert rel(out["compact", "fp64"], out["tma", "fp64"]) < 1e-12
     assert rel(out["compact", "fp32"], out["tma", "fp64"]) < TOL32
-    assert rel(out["tma-lean", "fp64"], out["tma", "fp64"]) < 1e-14  # same operations, other schedule
-    assert np.array_equal(out["tma-deep", "fp64"], out["tma", "fp64"])  # same code, more stages
-    assert np.array_equal(out["tma-deep", "fp32"], out["tma", "fp32"])
-    assert np.array_equal(out["tma-compact-smem", "fp32"], out["tma", "fp32"])
     el.Destroy()
 
 

@@ -38,7 +38,7 @@ def test_fp32_force_at_solved_configuration2_deflection(order):
     el.ComputeInternalForce()
     assert rel(el.RetrieveInternalForceToCPU(), f_ref) < TOL64
     el.SetForcePrecision("fp32")
-    for kernel in ("tma", "compact", "pipeline", "tma-deep", "tma-compact-smem"):
+    for kernel in ("tma", "compact", "pipeline"):
         el.SetLaunchConfig(kernel)
         el.ComputeInternalForce()
         err = rel(el.RetrieveInternalForceToCPU(), f_ref)

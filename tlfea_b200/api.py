@@ -173,7 +173,7 @@ class _TetData(ElementBase):
         p = {"fp64": capi.PRECISION_FP64, "fp32": capi.PRECISION_FP32}[precision]
         capi.call("tlfea_element_set_force_precision", self._handle(), p)
 
-    FORCE_KERNELS = {"tma": 0, "direct": 1, "pipeline": 2, "compact": 3, "tma-lean": 4, "tma-deep": 5, "tma-compact-smem": 6}
+    FORCE_KERNELS = {"tma": 0, "direct": 1, "pipeline": 2, "compact": 3}
 
     def SetLaunchConfig(self, force_kernel="tma", grid_limit: int = 0):
         """New: the fused force kernel -- "tma" (gradient stream, bulk-copy double

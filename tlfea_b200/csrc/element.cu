@@ -711,10 +711,10 @@ static int launch_combine(tlfea_element_s* h, const R* partial, R* f_out) {
 }
 
 // One tile per block, QP slices double-buffered by bulk copies.
-template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false, int NS = 0, bool CSM = false>
+template <typename R, int NPE, int NQP, bool DAMP>
 static int launch_tile_tma(tlfea_element_s* h, const TileArgs<R>& A) {
-    auto kern = k_tile_force_tma<R, NPE, NQP, DAMP, LEAN && sizeof(R) == 8, NS, CSM>;
-    const size_t smem = tile_tma_smem_bytes<R, NPE, NS, CSM>(h->tl.max_local_pad, DAMP);
+    auto kern = k_tile_force_tma<R, NPE, NQP, DAMP>;
+    const size_t smem = tile_tma_smem_bytes<R, NPE>(h->tl.max_local_pad, DAMP);
     if (smem > 227 * 1024) {
         set_error("force kernel shared memory exceeds 227 KB (tile touches too many nodes)");
         return TLFEA_UNSUPPORTED;
@@ -795,16 +795,6 @@ static int force_dispatch(tlfea_element_s* h, const double* d_v, bool fp32) {
         st = damp ? launch_pipe<R, NPE, NQP, true>(h, A) : launch_pipe<R, NPE, NQP, false>(h, A);
     else if (h->force_kernel == 3)
         st = damp ? launch_tile_geo<R, NPE, NQP, true>(h, A) : launch_tile_geo<R, NPE, NQP, false>(h, A);
-    else if (h->force_kernel == 4)
-        st = damp ? launch_tile_tma<R, NPE, NQP, true, true>(h, A) : launch_tile_tma<R, NPE, NQP, false, true>(h, A);
-    else if (h->force_kernel == 5) {  // a deeper slice ring: 3 stages in FP32, 2 in FP64
-        constexpr int NS = sizeof(R) == 4 ? 3 : 2;
-        st = damp ? launch_tile_tma<R, NPE, NQP, true, false, NS>(h, A) : launch_tile_tma<R, NPE, NQP, false, false, NS>(h, A);
-    } else if (h->force_kernel == 6 && sizeof(R) == 4 && tile_tma_csm_fits<R, NPE>(h->tl.max_local_pad)) {
-        // FP32 with the node values in the second stage buffer: 5 blocks per SM
-        constexpr bool C = sizeof(R) == 4;
-        st = damp ? launch_tile_tma<R, NPE, NQP, true, false, 0, C>(h, A) : launch_tile_tma<R, NPE, NQP, false, false, 0, C>(h, A);
-    }
     else
         st = damp ? launch_tile_tma<R, NPE, NQP, true>(h, A) : launch_tile_tma<R, NPE, NQP, false>(h, A);
     if (st) return st;
@@ -865,8 +855,8 @@ int element_refresh_u64(tlfea_element_s* h) {
 
 int element_force(tlfea_element_s* h, const double* d_v, bool fp32) {
     int st;
-    // the bulk-copy tile kernels (launch options 0, 3, 4, and Mooney-Rivlin's) stage the record
-    if ((h->force_kernel == 0 || h->force_kernel >= 3 || h->material == TLFEA_MATERIAL_MOONEY_RIVLIN) &&
+    // the bulk-copy tile kernels (launch options 0 and 3, and Mooney-Rivlin's) stage the record
+    if ((h->force_kernel == 0 || h->force_kernel == 3 || h->material == TLFEA_MATERIAL_MOONEY_RIVLIN) &&
         (st = element_refresh_record(h, fp32)))
         return st;
     if (fp32) {
@@ -1460,7 +1450,7 @@ int tlfea_element_compute_internal_force(tlfea_element h, const double* d_v) {
 
 int tlfea_element_set_launch_config(tlfea_element h, int force_kernel, int grid_limit) {
     CHECK_HANDLE(h);
-    if (force_kernel < 0 || force_kernel > 6 || grid_limit < 0) return TLFEA_INVALID_ARG;
+    if (force_kernel < 0 || force_kernel > 3 || grid_limit < 0) return TLFEA_INVALID_ARG;
     h->force_kernel = force_kernel;
     h->pipe_grid_limit = grid_limit;
     for (int& g : h->pipe_grid) g = 0;

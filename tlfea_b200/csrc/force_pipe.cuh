@@ -408,7 +408,7 @@ __device__ __forceinline__ void stage_tile_velocities(const TileArgs<R>& A, int 
     }
 }
 
-template <typename R, int NPE, int NS = 0>
+template <typename R, int NPE>
 struct TileTmaGeom {
     static constexpr uint32_t GRAD_BYTES = NPE * 3 * TILE_ELEMS * sizeof(R);
     static constexpr uint32_t DV_BYTES = TILE_ELEMS * sizeof(R);
@@ -418,8 +418,7 @@ struct TileTmaGeom {
     // QP-slice stages: FP64 copies a slice into registers before computing it, so one
     // stage suffices (refilled as soon as it is read); FP32 reads a slice twice (H, then
     // the forces) and double-buffers
-    // NS > 0 sets the stage count (a deeper ring, launch option 5)
-    static constexpr int STAGES = NS > 0 ? NS : (sizeof(R) == 8 ? 1 : 2);
+    static constexpr int STAGES = sizeof(R) == 8 ? 1 : 2;
     // element forces of the scatter reuse the stages once the QP loop is done
     static_assert(3 * NPE * TILE_ELEMS * sizeof(R) <= STAGES * STAGE_BYTES, "force table must fit in the stages");
     static_assert(LCONN_BYTES % 16 == 0 && INC_BYTES % 16 == 0 && STAGE_BYTES % 16 == 0, "bulk sizes");
@@ -428,17 +427,16 @@ struct TileTmaGeom {
 // Byte offsets of the regions of k_tile_force_tma's shared memory, each
 // 16-byte aligned: [stage(s), later the element forces][lconn][incidence]
 // [x y z][node destination][incidence end][velocities][a barrier per stage, the node
-// record's].  CSM (compact shared memory, FP32): the node values x y z live in the
-// second stage buffer, whose first slice is copied only once they are in registers.
-template <typename R, int NPE, int NS = 0, bool CSM = false>
+// record's].
+template <typename R, int NPE>
 struct TileTmaLayout {
     size_t inc, pos, dst, iend, vel, bar, total;
     __host__ __device__ TileTmaLayout(int max_local, bool damp) {
-        using G = TileTmaGeom<R, NPE, NS>;
+        using G = TileTmaGeom<R, NPE>;
         auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
         inc = G::STAGES * (size_t)G::STAGE_BYTES + G::LCONN_BYTES;
-        pos = CSM ? (size_t)G::STAGE_BYTES : inc + G::INC_BYTES;
-        dst = CSM ? al(inc + G::INC_BYTES) : al(pos + 3 * (size_t)max_local * sizeof(double));
+        pos = inc + G::INC_BYTES;
+        dst = al(pos + 3 * (size_t)max_local * sizeof(double));
         iend = al(dst + (size_t)max_local * sizeof(int));
         vel = al(iend + (size_t)max_local * sizeof(uint16_t));
         bar = al(vel + (damp ? 3 * (size_t)max_local * sizeof(double) : 0));
@@ -446,28 +444,20 @@ struct TileTmaLayout {
     }
 };
 
-template <typename R, int NPE, int NS = 0, bool CSM = false>
-inline size_t tile_tma_smem_bytes(int max_local, bool damp) {
-    return TileTmaLayout<R, NPE, NS, CSM>(max_local, damp).total;
-}
-
-// Whether a tile's node values fit the second stage buffer (the CSM layout).
 template <typename R, int NPE>
-inline bool tile_tma_csm_fits(int max_local) {
-    return 3 * (size_t)max_local * sizeof(double) <= TileTmaGeom<R, NPE>::STAGE_BYTES;
+inline size_t tile_tma_smem_bytes(int max_local, bool damp) {
+    return TileTmaLayout<R, NPE>(max_local, damp).total;
 }
 
-template <typename R, int NPE, int NQP, bool DAMP, bool LEAN = false, int NS = 0, bool CSM = false>
-__global__ void __launch_bounds__(TILE_ELEMS, CSM ? 5 : (NS == 3 ? 3 : ((sizeof(R) == 4 || LEAN) ? 4 : 3)))
-    k_tile_force_tma(TileArgs<R> A, int* err) {
-    using G = TileTmaGeom<R, NPE, NS>;
+template <typename R, int NPE, int NQP, bool DAMP>
+__global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_force_tma(TileArgs<R> A, int* err) {
+    using G = TileTmaGeom<R, NPE>;
     constexpr int S = G::STAGES;
-    static_assert(!CSM || (sizeof(R) == 4 && S == 2), "the compact layout is the FP32 double buffer's");
     constexpr int TE = TILE_ELEMS;
     extern __shared__ __align__(128) unsigned char smem[];
     const int tile = blockIdx.x, t = threadIdx.x;
     const int ML = A.max_local;
-    const TileTmaLayout<R, NPE, NS, CSM> L(ML, DAMP);
+    const TileTmaLayout<R, NPE> L(ML, DAMP);
     unsigned char* stage0 = smem;
     const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + S * G::STAGE_BYTES);
     const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
@@ -497,7 +487,7 @@ __global__ void __launch_bounds__(TILE_ELEMS, CSM ? 5 : (NS == 3 ? 3 : ((sizeof(
         for (int k = 0; k <= S; ++k) mbar_init(bar0 + 8 * k, 1);  // S stages, then the node record
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        for (int q = 0; q < (CSM ? 1 : S) && q < NQP; ++q) issue(q);  // CSM: stage 1 holds x y z first
+        for (int q = 0; q < S && q < NQP; ++q) issue(q);
         issue_node_record(A, tile, bar0 + 8 * S, xs, ys, zs, dsts, iends);
     }
     const int nl = A.node_off[tile + 1] - A.node_off[tile];
@@ -531,12 +521,7 @@ __global__ void __launch_bounds__(TILE_ELEMS, CSM ? 5 : (NS == 3 ? 3 : ((sizeof(
                 }
             }
         }
-        if constexpr (CSM) {
-            // every thread has read x y z out of the second stage buffer: its first slice now
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            if (t == 0 && NQP > 1) issue(1);
-        }
+
         // velocities relative to the element's first node, differenced per QP (keeping
         // them in registers would spill)
         double vb[3] = {0.0, 0.0, 0.0};
@@ -612,84 +597,6 @@ __global__ void __launch_bounds__(TILE_ELEMS, CSM ? 5 : (NS == 3 ? 3 : ((sizeof(
                 fe[((2 * p) * 3 + d) * TE + t] = f2[p][d].x;
                 fe[((2 * p + 1) * 3 + d) * TE + t] = f2[p][d].y;
             }
-        __syncthreads();
-    } else if constexpr (LEAN) {
-        // FP64, register-lean: the QP slice is read from shared memory twice (F, then
-        // the forces) instead of being copied into registers, so a thread holds only
-        // its element forces and F / P; the single stage is refilled after the force
-        // pass (4 CTAs per SM interleave the loads instead)
-        // local node indices are read from shared memory where used (a register copy
-        // indexed in the partly unrolled F loop would live in local memory)
-        auto lc = [&](int a) -> int { return lcs[a * TE + t]; };
-        R f[NPE][3];
-#pragma unroll
-        for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = R(0);
-#pragma unroll 1
-        for (int q = 0; q < NQP; ++q) {
-            if (!mbar_wait(bar0 + 8 * (q % S), (q / S) & 1)) atomicExch(err, 3);
-            const unsigned char* st = stage0 + (size_t)(q % S) * G::STAGE_BYTES;
-            const R* gs = reinterpret_cast<const R*>(st);
-            const R dv = reinterpret_cast<const R*>(st + G::GRAD_BYTES)[t];
-            R P[3][3];
-            {
-                double F[3][3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) F[i][j] = 0.0;
-#pragma unroll 2
-                for (int a = 0; a < NPE; ++a) {
-                    const double xa[3] = {xs[lc(a)], ys[lc(a)], zs[lc(a)]};
-                    const double ga[3] = {gs[grad_slot<R>(a, 0, t)], gs[grad_slot<R>(a, 1, t)],
-                                          gs[grad_slot<R>(a, 2, t)]};
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) F[i][j] += xa[i] * ga[j];
-                }
-                svk_p_reference(F, A.lambda, A.mu, P);
-                if (DAMP) {
-                    double Fd[3][3], Pv[3][3];
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) Fd[i][j] = 0.0;
-#pragma unroll 2
-                    for (int a = 0; a < NPE; ++a)
-#pragma unroll
-                        for (int i = 0; i < 3; ++i)
-#pragma unroll
-                            for (int j = 0; j < 3; ++j) Fd[i][j] += vs[3 * lc(a) + i] * gs[grad_slot<R>(a, j, t)];
-                    kelvin_voigt<double>(F, Fd, A.eta, A.lamd, Pv);
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) P[i][j] += Pv[i][j];
-                }
-            }
-            // f_a += (P dV) grad_a   (FEAT10DataFunc.cuh:417-449)
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) P[i][j] *= dv;
-#pragma unroll
-            for (int a = 0; a < NPE; ++a) {
-                const R ga[3] = {gs[grad_slot<R>(a, 0, t)], gs[grad_slot<R>(a, 1, t)], gs[grad_slot<R>(a, 2, t)]};
-#pragma unroll
-                for (int i = 0; i < 3; ++i) f[a][i] += P[i][0] * ga[0] + P[i][1] * ga[1] + P[i][2] * ga[2];
-            }
-            if (q + S < NQP) {
-                // every thread's generic reads of this stage precede the bulk refill
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                __syncthreads();
-                if (t == 0) issue(q + S);
-            }
-        }
-        __syncthreads();  // every thread is done with the stages the force table reuses
-#pragma unroll
-        for (int a = 0; a < NPE; ++a)
-#pragma unroll
-            for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
         __syncthreads();
     } else {
         int lc[NPE];
