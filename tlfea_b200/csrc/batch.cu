@@ -399,19 +399,12 @@ __device__ __forceinline__ void shared_group_tile(const BatchArgs<R>& A, int til
             r1 = ps[1];
             r2 = ps[2];
         }
-        R f[NPE][3];
-        R xa[NPE][3];
-#pragma unroll
-        for (int a = 0; a < NPE; ++a) {
-            if constexpr (sizeof(R) == 4) {
-                xa[a][0] = R(ps[3 * lc[a] + 0] - r0);
-                xa[a][1] = R(ps[3 * lc[a] + 1] - r1);
-                xa[a][2] = R(ps[3 * lc[a] + 2] - r2);
-            } else {
-#pragma unroll
-                for (int d = 0; d < 3; ++d) xa[a][d] = ps[3 * lc[a] + d];
-            }
-        }
+        // p at the element's nodes is read from the gather buffer where tet_dx_dxi_at uses
+        // it, and the element forces accumulate in this thread's column of the force table
+        // (shared memory): holding either 30-value set in registers halved the resident
+        // blocks
+        const double rr[3] = {r0, r1, r2};
+        auto xa = [&](int a, int d) -> R { return R(ps[3 * lc[a] + d] - rr[d]); };
 #pragma unroll 1
         for (int qp = 0; qp < NQP; ++qp) {
             const R* jp = A.ji + ((size_t)tile * NQP + qp) * 9 * TE + t;
@@ -421,7 +414,7 @@ __device__ __forceinline__ void shared_group_tile(const BatchArgs<R>& A, int til
             const R dv = __ldg(A.dv + ((size_t)tile * NQP + qp) * TE + t);
             const R Lq[4] = {R(A.qb.L[qp][0]), R(A.qb.L[qp][1]), R(A.qb.L[qp][2]), R(A.qb.L[qp][3])};
             R G[3][3], H[3][3];
-            tet_dx_dxi<R, NPE>(xa, Lq, G);
+            tet_dx_dxi_at<R, NPE>(xa, Lq, G);
             mul_jinv(G, ji, H);
             const R tr = lam * (H[0][0] + H[1][1] + H[2][2]);
             R P[3][3], Q[3][3];
@@ -431,14 +424,10 @@ __device__ __forceinline__ void shared_group_tile(const BatchArgs<R>& A, int til
                 for (int j = 0; j < 3; ++j) P[i][j] = (mu * (H[i][j] + H[j][i]) + (i == j ? tr : R(0))) * dv;
             mul_jinv_t(P, ji, Q);
             if (qp == 0)
-                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] = v; });
+                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { fe[(a * 3 + d) * TE + t] = v; });
             else
-                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] += v; });
+                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { fe[(a * 3 + d) * TE + t] += v; });
         }
-#pragma unroll
-        for (int a = 0; a < NPE; ++a)
-#pragma unroll
-            for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
         __syncthreads();  // element forces complete
         const size_t noff = (size_t)cur * A.nodes_per_inst, poff = (size_t)cur * A.pslots_per_inst;
         for (int ln = t; ln < nl; ln += TE) {

@@ -247,6 +247,34 @@ __device__ __forceinline__ void tet_dx_dxi(const R (&xa)[NPE][3], const R L[4], 
     }
 }
 
+// The same dx/dxi with the node values read through x(a, d) where they are used (from
+// shared memory, say), so they need not be held in registers all at once.
+template <typename R, int NPE, typename X>
+__device__ __forceinline__ void tet_dx_dxi_at(X x, const R L[4], R G[3][3]) {
+    if constexpr (NPE == 10) {
+        const R c0 = R(4) * L[0] - R(1), c1 = R(4) * L[1] - R(1), c2 = R(4) * L[2] - R(1), c3 = R(4) * L[3] - R(1);
+        const R l0 = R(4) * L[0], l1 = R(4) * L[1], l2 = R(4) * L[2], l3 = R(4) * L[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const R y0 = c0 * x(0, d) + l1 * x(4, d) + l2 * x(6, d) + l3 * x(7, d);
+            const R y1 = c1 * x(1, d) + l0 * x(4, d) + l2 * x(5, d) + l3 * x(8, d);
+            const R y2 = c2 * x(2, d) + l1 * x(5, d) + l0 * x(6, d) + l3 * x(9, d);
+            const R y3 = c3 * x(3, d) + l0 * x(7, d) + l1 * x(8, d) + l2 * x(9, d);
+            G[d][0] = y1 - y0;
+            G[d][1] = y2 - y0;
+            G[d][2] = y3 - y0;
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const R x0 = x(0, d);
+            G[d][0] = x(1, d) - x0;
+            G[d][1] = x(2, d) - x0;
+            G[d][2] = x(3, d) - x0;
+        }
+    }
+}
+
 // acc(a, d, Q[d][:] . dN_a/dxi) for every node a and component d.
 template <typename R, int NPE, typename Acc>
 __device__ __forceinline__ void tet_scatter(const R Q[3][3], const R L[4], Acc acc) {
