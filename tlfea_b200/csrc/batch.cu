@@ -168,6 +168,16 @@ __device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int item, con
     int* dsts = reinterpret_cast<int*>(fe + 3 * NPE * TE);  // max_local: node id, or -(slot + 1)
     uint16_t* iends = reinterpret_cast<uint16_t*>(dsts + A.max_local);
     uint16_t* incs = iends + A.max_local;  // NPE * TE
+    if (t == 0) {
+        // the tile's J^-1 and dV stream (every QP) into L2 now, so the per-QP loads below
+        // hit L2 instead of each waiting on DRAM (sizes are multiples of 16 bytes)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.ji + (size_t)tile * NQP * 9 * TE),
+                     "r"((uint32_t)(NQP * 9 * TE * sizeof(R)))
+                     : "memory");
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.dv + (size_t)tile * NQP * TE),
+                     "r"((uint32_t)(NQP * TE * sizeof(R)))
+                     : "memory");
+    }
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
     for (int k = t; k < NPE * TE; k += TE) incs[k] = A.inc[(size_t)tile * TE * NPE + k];
     // p relative to the tile's first node, differenced in FP64: the gradients
