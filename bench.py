@@ -167,6 +167,12 @@ def elem_force_bytes_compact(E, N, npe, nqp, s):
     return E * (4 * npe + nqp * 10 * s) + N * 6 * s
 
 
+def mf_apply_bytes(E, N, npe, nqp):
+    """Algorithmic bytes of one matrix-free K p: the FP64 gradient stream and dV per QP,
+    local connectivity (4 B per node slot), and per node its position, p and q (FP64)."""
+    return E * (4 * npe + nqp * npe * 3 * 8 + nqp * 8) + N * 3 * 8 * 3
+
+
 def spmv_bytes(N, nnzb):
     """Bytes one block SpMV must move: every 3x3 node block (72 B values +
     4 B column), the row offsets, p read and q written once."""
@@ -1100,10 +1106,36 @@ def main():
     step()
     pcg_iters = solver.GetLastIterCount()
     ms_pcg = time_stream(torch, stream, step, max(1, args.steps // 2))
-    solver.SetPreconditioner("none")
     pcg = {"value": round(1e3 / ms_pcg, 4), "unit": "solves/s", "ms_per_step": round(ms_pcg, 3),
            "cg_iters_per_solve": pcg_iters, "final_rel_residual": solver.GetLastResidual(),
            "preconditioner": "block Jacobi (3x3 node diagonal blocks)"}
+    hbm, peak_kind = peaks()
+    xin = torch.randn(3 * N, dtype=torch.float64, device="cuda")
+    yout = torch.empty_like(xin)
+    torch.cuda.synchronize()
+    # the assembled K of the last (preconditioned) solve: its SpMV, and the plain CG on it
+    el.SetBlocking(False)
+    for _ in range(3):
+        solver.Apply(xin.data_ptr(), yout.data_ptr())
+    ms_spmv = time_stream(torch, stream, lambda: solver.Apply(xin.data_ptr(), yout.data_ptr()), args.kernel_reps)
+    el.SetBlocking(True)
+    solver.SetPreconditioner("none")
+    off_m, cols_m, _ = el.RetrieveMassCSRToCPU()
+    nnzb = len(cols_m)
+    b_spmv = spmv_bytes(N, nnzb)
+    ach_s = b_spmv / (ms_spmv / 1e3) / 1e9
+    solver.SetOperator("assembled")
+    step()
+    ms_asm = time_stream(torch, stream, step, 1)
+    asm_iters = solver.GetLastIterCount()
+    solver.SetOperator("matrix-free")
+    assembled = {"value": round(1e3 / ms_asm, 4), "unit": "solves/s", "ms_per_step": round(ms_asm, 3),
+                 "cg_iters_per_solve": asm_iters,
+                 "spmv": {"kernel": "k_cg_spmv_dot", "bound": "hbm", "achieved": round(ach_s, 1), "peak": hbm,
+                          "unit": "GB/s", "frac": round(ach_s / hbm, 4), "algorithmic_bytes": int(b_spmv),
+                          "format": "row-planar 3x3 node blocks", "ms": round(ms_spmv, 4),
+                          "traffic": int(SPMV_TRAFFIC_RATIO * b_spmv)},
+                 "path": "the reference's operator: K assembled (3x3 node blocks) once per solve, SpMV per iteration"}
 
     # e2e through the public API with host buffers
     def e2e_step():
@@ -1121,24 +1153,18 @@ def main():
     e2e = {"value": whole_job_rate(world, args.steps, t_e2e), "unit": "solves/s", "h2d_bytes_per_step": 6 * N * 8,
            "d2h_bytes_per_step": 3 * N * 8}
 
-    hbm, peak_kind = peaks()
-    # dominant kernel: the CG SpMV (3x3 node blocks), timed back to back on the element stream
-    xin = torch.randn(3 * N, dtype=torch.float64, device="cuda")
-    yout = torch.empty_like(xin)
-    torch.cuda.synchronize()
+    # dominant kernel: the matrix-free K p of the CG (tile kernel + shared-node combine
+    # with p.q), timed back to back on the element stream at the last solve's positions
     el.SetBlocking(False)
     for _ in range(3):
         solver.Apply(xin.data_ptr(), yout.data_ptr())
-    ms_spmv = time_stream(torch, stream, lambda: solver.Apply(xin.data_ptr(), yout.data_ptr()), args.kernel_reps)
-    off_m, cols_m, _ = el.RetrieveMassCSRToCPU()
-    nnzb = len(cols_m)
-    b_spmv = spmv_bytes(N, nnzb)
-    ach = b_spmv / (ms_spmv / 1e3) / 1e9
-    roofline = {"kernel": "k_cg_spmv_dot", "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": int(b_spmv),
-                "format": "row-planar 3x3 node blocks", "ms": round(ms_spmv, 4),
-                "traffic": int(SPMV_TRAFFIC_RATIO * b_spmv),
-                "full_csr_equivalent_gbs": round(spmv_bytes_full_csr(N, nnzb) / (ms_spmv / 1e3) / 1e9, 1)}
+    ms_mf = time_stream(torch, stream, lambda: solver.Apply(xin.data_ptr(), yout.data_ptr()), args.kernel_reps)
+    b_mf = mf_apply_bytes(E, N, 10, 5)
+    ach = b_mf / (ms_mf / 1e3) / 1e9
+    roofline = {"kernel": "k_mf_tile + k_mf_combine_dot", "bound": "hbm", "achieved": round(ach, 1), "peak": hbm,
+                "unit": "GB/s", "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": int(b_mf),
+                "format": "matrix-free SVK tangent from the FP64 gradient stream", "ms": round(ms_mf, 4),
+                "traffic": None}
     # fused element force, FP32 and FP64
     ef = {}
     f_by_prec = {}
@@ -1203,7 +1229,7 @@ def main():
                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (K 1.35 GB)"},
            "e2e": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in e2e.items()},
            "roofline": roofline, "elem_force": ef, "gpu_launches": int(launches), "clocks": clk.summary(),
-           "pcg": pcg}
+           "pcg": pcg, "assembled_operator": assembled}
     el.Destroy()
     if not args.no_config2_more:
         out["config2_more"] = config2_more_legs(args, T, cfg)

@@ -261,13 +261,20 @@ int tlfea_solver_solve(tlfea_solver s);
  * Jacobi on the 3x3 node diagonal blocks of K (BCs applied).  The stop test
  * stays sqrt(r.r / r0.r0) < tol. */
 int tlfea_linear_static_set_preconditioner(tlfea_solver s, int kind);
+/* How the CG applies K (new).  0 (default) = matrix-free where it applies (SVK, no
+ * damping, no preconditioner): K p from the elements' tangent at the current positions
+ * in each iteration, never assembled (K is assembled on demand, at the positions of the
+ * last solve, for tlfea_linear_static_retrieve_k); otherwise, and with 1, the assembled
+ * K of the reference (3x3 node blocks).  Both are the same operator: the solutions and
+ * iteration counts agree to rounding. */
+int tlfea_linear_static_set_operator(tlfea_solver s, int mode);
 /* GetLastIterCount / GetLastResidual (LinearStaticSolver.cuh:68-72). */
 int tlfea_linear_static_last(tlfea_solver s, int* iters, double* rel_residual);
 /* Retrieve the LinearStaticSolver stiffness (BCs applied) as 3N x 3N CSR
  * (new; the reference keeps K private).  Call with NULL arrays for nnz. */
 int tlfea_linear_static_retrieve_k(tlfea_solver s, long long* nnz, int* offsets, int* columns, double* values);
 /* d_y = K d_x with the stiffness of the last Solve() (device pointers, 3N
- * each); the SpMV kernel of the CG loop (new). */
+ * each); the CG loop's operator (matrix-free or the SpMV kernel; new). */
 int tlfea_linear_static_apply(tlfea_solver s, const double* d_x, double* d_y);
 /* Velocity state of the first-order solvers (v_guess, v_prev: 3N; lambda: n_c). */
 int tlfea_solver_get_velocity(tlfea_solver s, double* v_guess, double* v_prev, int n);

@@ -171,3 +171,43 @@ def test_block_jacobi_pcg_matches_numpy_and_needs_fewer_iterations():
     u20 = np.stack([x3 - x, y3 - y, z3 - z], 1).ravel()
     assert rel(u20, _numpy_pcg(K, fb, None, 20)) < 1e-9
     el.Destroy()
+
+
+@pytest.mark.parametrize("order", [10, 4])
+def test_matrix_free_operator_matches_the_assembled_stiffness(order):
+    """The default matrix-free K p (the SVK tangent applied element by element in every
+    CG iteration) against the assembled K of the reference: K x for random x with fixed
+    components (their columns dropped, their rows identity), at deformed positions (so
+    the tangent's geometric terms are exercised), the CG solution and iteration count, and
+    the stiffness retrieved after a matrix-free solve."""
+    import torch
+
+    x, y, z, conn = box(12, 3, 2, order)
+    fixed, f, _ = M.cantilever_loads(x, y, z, (20.0, -30.0, -100.0))
+    out = {}
+    for mode in ("assembled", "matrix-free"):
+        el = make_element(x, y, z, conn, fixed=fixed, f_ext=f)
+        r = np.random.default_rng(5)
+        xs = [v + 2e-3 * r.standard_normal(v.shape) for v in (x, y, z)]
+        el.UpdatePositions(*xs)
+        s = T.LinearStaticSolver(el, 1e-10, 50000)
+        s.SetOperator(mode)
+        s.Solve()
+        u = np.stack(el.RetrievePositionToCPU()) - np.stack(xs)
+        xv = torch.tensor(r.standard_normal(3 * len(x)), dtype=torch.float64, device="cuda")
+        yv = torch.empty_like(xv)
+        torch.cuda.synchronize()
+        s.Apply(xv.data_ptr(), yv.data_ptr())
+        torch.cuda.synchronize()
+        Kx = yv.cpu().numpy()
+        off, cols, vals = s.RetrieveStiffnessCSRToCPU()
+        out[mode] = (u, s.GetLastIterCount(), s.GetLastResidual(), Kx, vals, xv.cpu().numpy())
+        del s
+        el.Destroy()
+    ua, ia, ra, Ka, va, xa = out["assembled"]
+    um, im, rm, Km, vm, xm = out["matrix-free"]
+    assert np.array_equal(xa, xm)
+    assert rel(Km, Ka) < 1e-12
+    assert np.array_equal(va, vm)  # K assembled on demand at the matrix-free solve's positions
+    assert rm < 1e-10 and abs(im - ia) <= max(2, 0.05 * ia), (im, ia)
+    assert rel(um, ua) < 1e-8

@@ -130,6 +130,7 @@ _SIGS = {
     "tlfea_solver_set_parameters": [_P, _P],
     "tlfea_solver_solve": [_P],
     "tlfea_linear_static_last": [_P, _I, _D],
+    "tlfea_linear_static_set_operator": [_P, C.c_int],
     "tlfea_linear_static_set_preconditioner": [_P, C.c_int],
     "tlfea_linear_static_retrieve_k": [_P, C.POINTER(_LL), _I, _I, _D],
     "tlfea_linear_static_apply": [_P, _P, _P],

@@ -473,6 +473,11 @@ class LinearStaticSolver(SolverBase):
         reference's unpreconditioned CG, the default)."""
         capi.call("tlfea_linear_static_set_preconditioner", self._h, {"none": 0, "block_jacobi": 1}[kind])
 
+    def SetOperator(self, mode: str = "matrix-free"):
+        """New: "matrix-free" (default where it applies: SVK, no damping, no
+        preconditioner) or "assembled" (the reference's assembled K)."""
+        capi.call("tlfea_linear_static_set_operator", self._h, {"matrix-free": 0, "assembled": 1}[mode])
+
     def _last(self):
         it, res = C.c_int(), C.c_double()
         capi.call("tlfea_linear_static_last", self._h, C.byref(it), C.byref(res))

@@ -409,10 +409,11 @@ __device__ __forceinline__ void shared_group_tile(const BatchArgs<R>& A, int til
             r1 = ps[1];
             r2 = ps[2];
         }
+        R f[NPE][3];
         // p at the element's nodes is read from the gather buffer where tet_dx_dxi_at uses
-        // it, and the element forces accumulate in this thread's column of the force table
-        // (shared memory): holding either 30-value set in registers halved the resident
-        // blocks
+        // it (holding those 30 values in registers beside the element forces cost a third
+        // of the resident blocks; accumulating the forces in shared memory instead was
+        // slower still)
         const double rr[3] = {r0, r1, r2};
         auto xa = [&](int a, int d) -> R { return R(ps[3 * lc[a] + d] - rr[d]); };
 #pragma unroll 1
@@ -434,10 +435,14 @@ __device__ __forceinline__ void shared_group_tile(const BatchArgs<R>& A, int til
                 for (int j = 0; j < 3; ++j) P[i][j] = (mu * (H[i][j] + H[j][i]) + (i == j ? tr : R(0))) * dv;
             mul_jinv_t(P, ji, Q);
             if (qp == 0)
-                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { fe[(a * 3 + d) * TE + t] = v; });
+                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] = v; });
             else
-                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { fe[(a * 3 + d) * TE + t] += v; });
+                tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] += v; });
         }
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) fe[(a * 3 + d) * TE + t] = f[a][d];
         __syncthreads();  // element forces complete
         const size_t noff = (size_t)cur * A.nodes_per_inst, poff = (size_t)cur * A.pslots_per_inst;
         for (int ln = t; ln < nl; ln += TE) {

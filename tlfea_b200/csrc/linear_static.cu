@@ -9,6 +9,7 @@
 #include <cstring>
 #include <vector>
 
+#include "mf_tangent.cuh"
 #include "solver.cuh"
 
 namespace tlfea {
@@ -155,6 +156,11 @@ __global__ void k_apply_bcs(int N, const int* __restrict__ off, const int* __res
     }
     for (int d = 0; d < 3; ++d)
         if (fixed[3 * i + d]) f[3 * i + d] = 0.0;
+}
+
+__global__ void k_zero_fixed(int n3, const unsigned char* __restrict__ fixed, double* f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n3 && fixed[i]) f[i] = 0.0;
 }
 
 __global__ void k_mark_fixed(int nf, const int* __restrict__ nodes, unsigned char* fixed) {
@@ -485,10 +491,77 @@ __global__ void k_pcg_axpy_dot(int N, const double* __restrict__ dinv, double* u
 
 static int cg_grid(const tlfea_solver_s* s) { return s->cg_blocks; }
 
+static bool use_matrix_free(const tlfea_solver_s* s) {
+    const tlfea_element_s* el = s->el;
+    return s->op_mode == 0 && s->precond == 0 && el->material != TLFEA_MATERIAL_MOONEY_RIVLIN && el->eta_d == 0.0 &&
+           el->lambda_d == 0.0;
+}
+
+static MfArgs mf_args(tlfea_solver_s* s, const double* p, double* q, CgCtl* ctl) {
+    tlfea_element_s* el = s->el;
+    const Tiling& tl = el->tl;
+    MfArgs M;
+    memset(&M, 0, sizeof(M));
+    M.n_tiles = tl.n_tiles;
+    M.max_local = tl.max_local_pad;
+    M.node_off = tl.node_off;
+    M.pad_off = tl.pad_off;
+    M.pad_gid = tl.pad_gid;
+    M.pad_dst = tl.pad_dst;
+    M.pad_iend = tl.pad_iend;
+    M.inc = tl.inc;
+    M.lconn = tl.lconn;
+    M.grad = tl.grad64;
+    M.dv = tl.dv64;
+    M.sx = tl.sx;
+    M.sy = tl.sy;
+    M.sz = tl.sz;
+    M.p = p;
+    M.q = q;
+    M.partial = tl.partial64;
+    M.is_fixed = s->is_fixed;
+    M.tile_dot = s->mf_part;
+    M.lambda = el->lambda;
+    M.mu = el->mu;
+    M.ctl = ctl;
+    return M;
+}
+
+static size_t mf_smem(const tlfea_solver_s* s) {
+    const tlfea_element_s* el = s->el;
+    return (el->npe == 10) ? TileTmaLayout<double, 10>(el->tl.max_local_pad, true).total
+                           : TileTmaLayout<double, 4>(el->tl.max_local_pad, true).total;
+}
+
+// q = K_bc p matrix-free and p.q, alpha (the SpMV kernel's contract).
+static int launch_mf_apply(tlfea_solver_s* s, cudaStream_t st, const double* p, double* q, CgCtl* ctl) {
+    tlfea_element_s* el = s->el;
+    const MfArgs M = mf_args(s, p, q, ctl);
+    const size_t smem = mf_smem(s);
+    if (el->npe == 10)
+        k_mf_tile<10, 5><<<el->tl.n_tiles, TILE_ELEMS, smem, st>>>(M, el->d_err);
+    else
+        k_mf_tile<4, 1><<<el->tl.n_tiles, TILE_ELEMS, smem, st>>>(M, el->d_err);
+    if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+    const int nb = el->tl.n_bnodes;
+    const int cb = std::max(1, (nb + 255) / 256);
+    k_mf_combine_dot<<<cb, 256, 0, st>>>(nb, el->tl.bnode_gid, el->tl.bnode_off, M, s->mf_part + el->tl.n_tiles);
+    if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+    return TLFEA_OK;
+}
+
 static int launch_cg_iteration(tlfea_solver_s* s, cudaStream_t st) {
     tlfea_element_s* el = s->el;
     const int n = 3 * el->N;
     const int G = cg_grid(s);
+    if (use_matrix_free(s)) {
+        if (launch_mf_apply(s, st, s->p, s->q, s->ctl)) return TLFEA_CUDA_ERROR;
+        k_cg_axpy_dot<<<G, 256, 0, st>>>(n, s->u, s->r, s->p, s->q, s->cg_part, s->ctl, s->tol, s->max_iter);
+        if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+        k_cg_pupdate<<<G, 256, 0, st>>>(n, s->r, s->p, s->ctl);
+        if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+        return TLFEA_OK;
+    }
     k_cg_spmv_dot<<<G, 256, 0, st>>>(el->N, el->pat_off, el->pat_col, s->K, s->p, s->q, s->cg_part, s->ctl);
     if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
     if (s->precond) {
@@ -532,6 +605,7 @@ static int build_cg_graph(tlfea_solver_s* s, int iters) {
     }
     s->cg_graph_iters = iters;
     s->cg_graph_precond = s->precond;
+    s->cg_graph_mf = use_matrix_free(s) ? 1 : 0;
     return TLFEA_OK;
 }
 
@@ -561,6 +635,28 @@ int linear_static_prepare(tlfea_solver_s* s) {
     return TLFEA_OK;
 }
 
+// AssembleLinearStiffness (h = 1) at the given positions, then ApplyDirichletBCs to K
+// and f (is_fixed already marked).
+static int assemble_k(tlfea_solver_s* s, const double* x, const double* y, const double* z) {
+    tlfea_element_s* el = s->el;
+    cudaStream_t stream = el->stream;
+    const int N = el->N;
+    const bool mr = (el->material == TLFEA_MATERIAL_MOONEY_RIVLIN);
+    auto kern = (el->npe == 10) ? (mr ? k_stiffness_rows<10, 5, true> : k_stiffness_rows<10, 5, false>)
+                                : (mr ? k_stiffness_rows<4, 1, true> : k_stiffness_rows<4, 1, false>);
+    kern<<<(N + 127) / 128, 128, 0, stream>>>(N, el->E, el->d_conn, x, y, z, el->tl.elem_slot, el->tl.grad64,
+                                               el->tl.dv64, el->inc_off, el->inc_e, el->inc_a, el->pat_off,
+                                               el->pat_col, s->K, el->lambda, el->mu, el->eta_d, el->lambda_d, 1.0,
+                                               el->mu10, el->mu01, el->kappa);
+    TLFEA_CHECK_LAUNCH();
+    if (el->n_constraint > 0) {
+        k_apply_bcs<<<(N + 255) / 256, 256, 0, stream>>>(N, el->pat_off, el->pat_col, s->is_fixed, s->K, s->f);
+        TLFEA_CHECK_LAUNCH();
+    }
+    s->k_built = true;
+    return TLFEA_OK;
+}
+
 int linear_static_solve(tlfea_solver_s* s) {
     tlfea_element_s* el = s->el;
     if (!el->is_setup) {
@@ -571,26 +667,48 @@ int linear_static_solve(tlfea_solver_s* s) {
     if (st) return st;
     cudaStream_t stream = el->stream;
     const int N = el->N, n3 = 3 * N;
-    // AssembleLinearStiffness (h = 1)
-    const bool mr = (el->material == TLFEA_MATERIAL_MOONEY_RIVLIN);
-    auto kern = (el->npe == 10) ? (mr ? k_stiffness_rows<10, 5, true> : k_stiffness_rows<10, 5, false>)
-                                : (mr ? k_stiffness_rows<4, 1, true> : k_stiffness_rows<4, 1, false>);
-    kern<<<(N + 127) / 128, 128, 0, stream>>>(N, el->E, el->d_conn, el->x, el->y, el->z, el->tl.elem_slot,
-                                               el->tl.grad64, el->tl.dv64, el->inc_off, el->inc_e, el->inc_a,
-                                               el->pat_off, el->pat_col, s->K, el->lambda, el->mu, el->eta_d,
-                                               el->lambda_d, 1.0, el->mu10, el->mu01, el->kappa);
-    TLFEA_CHECK_LAUNCH();
+    // the right-hand side and the Dirichlet DOFs
     TLFEA_CUDA(cudaMemcpyAsync(s->f, el->f_ext, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
-    // ApplyDirichletBCs
+    TLFEA_CUDA(cudaMemsetAsync(s->is_fixed, 0, n3, stream));
     const int nf = el->n_constraint / 3;
     if (nf > 0) {
-        TLFEA_CUDA(cudaMemsetAsync(s->is_fixed, 0, n3, stream));
         k_mark_fixed<<<(nf + 255) / 256, 256, 0, stream>>>(nf, el->fixed, s->is_fixed);
         TLFEA_CHECK_LAUNCH();
-        k_apply_bcs<<<(N + 255) / 256, 256, 0, stream>>>(N, el->pat_off, el->pat_col, s->is_fixed, s->K, s->f);
-        TLFEA_CHECK_LAUNCH();
     }
-    s->k_built = true;
+    const bool mf = use_matrix_free(s);
+    if (mf) {
+        // matrix-free K p at these positions: the node record holds them; keep a copy so
+        // that K can still be assembled (Apply, RetrieveStiffness) after the update
+        k_zero_fixed<<<(n3 + 255) / 256, 256, 0, stream>>>(n3, s->is_fixed, s->f);
+        TLFEA_CHECK_LAUNCH();
+        if ((st = element_refresh_record(el, false))) return st;
+        el->stage_content = 3;  // this solve's positions, until they change
+        if (!s->xk && ((st = dalloc(&s->xk, (size_t)N)) || (st = dalloc(&s->yk, (size_t)N)) ||
+                       (st = dalloc(&s->zk, (size_t)N))))
+            return st;
+        TLFEA_CUDA(cudaMemcpyAsync(s->xk, el->x, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream));
+        TLFEA_CUDA(cudaMemcpyAsync(s->yk, el->y, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream));
+        TLFEA_CUDA(cudaMemcpyAsync(s->zk, el->z, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream));
+        TLFEA_CUDA(cudaMemsetAsync(s->q, 0, sizeof(double) * n3, stream));  // nodes of no element stay 0
+        const size_t need = (size_t)el->tl.n_tiles + std::max(1, (el->tl.n_bnodes + 255) / 256);
+        if (!s->mf_part && (st = dalloc(&s->mf_part, need))) return st;
+        const size_t smem = mf_smem(s);
+        if (smem > 227 * 1024) {
+            set_error("matrix-free stiffness: shared memory exceeds 227 KB (tile touches too many nodes)");
+            return TLFEA_UNSUPPORTED;
+        }
+        if (smem > 48 * 1024) {
+            if (el->npe == 10)
+                TLFEA_CUDA(cudaFuncSetAttribute(k_mf_tile<10, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            else
+                TLFEA_CUDA(cudaFuncSetAttribute(k_mf_tile<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        }
+        s->k_built = false;
+        s->mf_last = true;
+    } else {
+        if ((st = assemble_k(s, el->x, el->y, el->z))) return st;
+        s->mf_last = false;
+    }
     // SolveLinearSystemCG
     const int G = cg_grid(s);
     if (s->precond) {
@@ -609,7 +727,8 @@ int linear_static_solve(tlfea_solver_s* s) {
         TLFEA_CUDA(cudaMemcpyAsync(&h, s->ctl, sizeof(CgCtl), cudaMemcpyDeviceToHost, stream));
         TLFEA_CUDA(cudaStreamSynchronize(stream));
         if (h.done || launched >= s->max_iter) break;
-        if (!s->cg_graph || s->cg_graph_iters != chunk || s->cg_graph_precond != s->precond) {
+        if (!s->cg_graph || s->cg_graph_iters != chunk || s->cg_graph_precond != s->precond ||
+            s->cg_graph_mf != (mf ? 1 : 0)) {
             if ((st = build_cg_graph(s, chunk))) return st;
         }
         TLFEA_CUDA(cudaGraphLaunch(s->cg_graph, stream));
@@ -636,7 +755,7 @@ int linear_static_solve(tlfea_solver_s* s) {
 
 int linear_static_apply(tlfea_solver_s* s, const double* d_x, double* d_y) {
     tlfea_element_s* el = s->el;
-    if (!s->k_built) {
+    if (!s->k_built && !s->mf_last) {
         set_error("LinearStaticSolver::Solve has not assembled K yet");
         return TLFEA_NOT_SETUP;
     }
@@ -644,6 +763,18 @@ int linear_static_apply(tlfea_solver_s* s, const double* d_x, double* d_y) {
         int st = dalloc(&s->ctl_apply, 1);
         if (st) return st;
         TLFEA_CUDA(cudaMemsetAsync(s->ctl_apply, 0, sizeof(CgCtl), el->stream));
+    }
+    if (s->mf_last) {
+        // matrix-free, at the positions of the last solve (the node record is rebuilt
+        // from them and marked stale for the force kernels)
+        if (el->stage_content != 3 || el->positions_exposed) {
+            int st = element_stage_positions(el, s->xk, s->yk, s->zk);
+            if (st) return st;
+        }
+        if (launch_mf_apply(s, el->stream, d_x, d_y, s->ctl_apply)) return TLFEA_CUDA_ERROR;
+        TLFEA_LAUNCHED(2);
+        if (el->blocking) TLFEA_CUDA(cudaStreamSynchronize(el->stream));
+        return TLFEA_OK;
     }
     k_cg_spmv_dot<<<cg_grid(s), 256, 0, el->stream>>>(el->N, el->pat_off, el->pat_col, s->K, d_x, d_y, s->cg_part,
                                                       s->ctl_apply);
@@ -655,6 +786,12 @@ int linear_static_apply(tlfea_solver_s* s, const double* d_x, double* d_y) {
 int linear_static_retrieve_k(tlfea_solver_s* s, long long* nnz, int* offsets, int* columns, double* values) {
     tlfea_element_s* el = s->el;
     TLFEA_CUDA(cudaStreamSynchronize(el->stream));
+    if (!s->k_built && s->mf_last) {
+        // the last solve ran matrix-free: assemble K at its positions now
+        int st = assemble_k(s, s->xk, s->yk, s->zk);
+        if (st) return st;
+        TLFEA_CUDA(cudaStreamSynchronize(el->stream));
+    }
     if (!s->k_built) {
         if (nnz) *nnz = 0;
         return TLFEA_OK;
@@ -700,6 +837,10 @@ void linear_static_free(tlfea_solver_s* s) {
     dfree(s->cg_part);
     dfree(s->dinv);
     dfree(s->z);
+    dfree(s->mf_part);
+    dfree(s->xk);
+    dfree(s->yk);
+    dfree(s->zk);
 }
 
 }  // namespace tlfea

@@ -71,6 +71,11 @@ struct tlfea_solver_s {
     double* dinv = nullptr;     // block Jacobi: inverse diagonal blocks, 9 per node
     double* z = nullptr;        // block Jacobi: z = D^-1 r
     int cg_graph_precond = -1;  // preconditioner the captured graph was built for
+    int cg_graph_mf = -1;       // operator the captured graph was built for (1 = matrix-free)
+    int op_mode = 0;            // 0: matrix-free K p where it applies (SVK, no damping, no preconditioner), 1: assembled
+    bool mf_last = false;       // the last solve ran matrix-free: K is assembled on demand
+    double* mf_part = nullptr;  // matrix-free p.q partials: one per tile, then one per combine block
+    double *xk = nullptr, *yk = nullptr, *zk = nullptr;  // positions of the last matrix-free solve
     int cg_blocks = 0;
     cudaGraphExec_t cg_graph = nullptr;
     int cg_graph_iters = 0;

@@ -180,6 +180,12 @@ int tlfea_linear_static_set_preconditioner(tlfea_solver s, int kind) {
     return TLFEA_OK;
 }
 
+int tlfea_linear_static_set_operator(tlfea_solver s, int mode) {
+    if (!s || s->kind != KIND_LINEAR_STATIC || (mode != 0 && mode != 1)) return TLFEA_INVALID_ARG;
+    s->op_mode = mode;
+    return TLFEA_OK;
+}
+
 int tlfea_linear_static_apply(tlfea_solver s, const double* d_x, double* d_y) {
     if (!s || s->kind != KIND_LINEAR_STATIC || !d_x || !d_y) return TLFEA_INVALID_ARG;
     TLFEA_CUDA(cudaSetDevice(s->device));
