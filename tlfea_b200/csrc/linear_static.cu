@@ -771,6 +771,9 @@ int linear_static_apply(tlfea_solver_s* s, const double* d_x, double* d_y) {
             int st = element_stage_positions(el, s->xk, s->yk, s->zk);
             if (st) return st;
         }
+        // the product's kernels skip their work once the control block reads done
+        // (a p.q <= 0 would set it): start every product from a clear block
+        TLFEA_CUDA(cudaMemsetAsync(s->ctl_apply, 0, sizeof(CgCtl), el->stream));
         if (launch_mf_apply(s, el->stream, d_x, d_y, s->ctl_apply)) return TLFEA_CUDA_ERROR;
         TLFEA_LAUNCHED(2);
         if (el->blocking) TLFEA_CUDA(cudaStreamSynchronize(el->stream));
