@@ -261,8 +261,8 @@ int tlfea_solver_solve(tlfea_solver s);
  * Jacobi on the 3x3 node diagonal blocks of K (BCs applied).  The stop test
  * stays sqrt(r.r / r0.r0) < tol. */
 int tlfea_linear_static_set_preconditioner(tlfea_solver s, int kind);
-/* How the CG applies K (new).  0 (default) = matrix-free where it applies (SVK, no
- * damping, no preconditioner): K p from the elements' tangent at the current positions
+/* How the CG applies K (new).  0 (default) = matrix-free where it applies (TET10, SVK,
+ * no damping, no preconditioner): K p from the elements' tangent at the current positions
  * in each iteration, never assembled (K is assembled on demand, at the positions of the
  * last solve, for tlfea_linear_static_retrieve_k); otherwise, and with 1, the assembled
  * K of the reference (3x3 node blocks).  Both are the same operator: the solutions and

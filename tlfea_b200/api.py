@@ -474,7 +474,7 @@ class LinearStaticSolver(SolverBase):
         capi.call("tlfea_linear_static_set_preconditioner", self._h, {"none": 0, "block_jacobi": 1}[kind])
 
     def SetOperator(self, mode: str = "matrix-free"):
-        """New: "matrix-free" (default where it applies: SVK, no damping, no
+        """New: "matrix-free" (default where it applies: TET10, SVK, no damping, no
         preconditioner) or "assembled" (the reference's assembled K)."""
         capi.call("tlfea_linear_static_set_operator", self._h, {"matrix-free": 0, "assembled": 1}[mode])
 
