@@ -186,7 +186,8 @@ __device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int item, con
     // sum_a p_a (x) grad N_a keeps FP32 accuracy relative to the local variation
     const int g0 = noff + A.ln_gid[lb];
     const double r0 = p[3 * g0 + 0], r1 = p[3 * g0 + 1], r2 = p[3 * g0 + 2];
-    for (int ln = t; ln < nl; ln += TE) {
+#pragma unroll 4
+    for (int ln = t; ln < nl; ln += TE) {  // unrolled: several nodes' gathers in flight at once
         const int gid = noff + A.ln_gid[lb + ln];
         const int pslot = A.ln_pslot[lb + ln];
         dsts[ln] = (pslot < 0) ? gid : -(poff + pslot + 1);

@@ -94,7 +94,8 @@ __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_tile(MfArgs M, int* err) {
         bulk_g2s(smem_u32(iends), M.pad_iend + pb, np * sizeof(uint16_t), bar_rec);
     }
     const int nl = M.node_off[tile + 1] - M.node_off[tile];
-    for (int ln = t; ln < nl; ln += TE) {
+#pragma unroll 4
+    for (int ln = t; ln < nl; ln += TE) {  // unrolled: several nodes' gathers in flight at once
         const int g = M.pad_gid[pb + ln];
 #pragma unroll
         for (int d = 0; d < 3; ++d) ps[3 * ln + d] = M.is_fixed[3 * g + d] ? 0.0 : M.p[3 * g + d];
