@@ -55,10 +55,13 @@ WORKLOAD = ("configuration 2: cantilever 200x20x20 TET10, plain linear static CG
 CG_ITERS_CFG2 = 7071
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch from ncu captures:
 # the SpMV on the 120x16x16 beam moved 1.026 x its algorithmic bytes (the 200x20x20 K is
-# too large for a multi-pass capture; traffic scales with the blocks streamed); the FP32
-# tile force kernel on this workload moved 357.03 MB per launch.
+# too large for a multi-pass capture; traffic scales with the blocks streamed); on the
+# 160x16x16 beam the gradient-stream force kernel moved 1.118 (FP32) / 1.073 (FP64) x its
+# algorithmic bytes and the matrix-free product 1.073 x (the tile tables come on top;
+# both scale with the elements), so the 200x20x20 traffic is those ratios x its bytes.
 SPMV_TRAFFIC_RATIO = 1.026
-FORCE_FP32_TRAFFIC_BYTES = 357.03e6
+FORCE_TRAFFIC_RATIO = {"fp32": 1.118, "fp64": 1.073}
+MF_TRAFFIC_RATIO = 1.073
 
 
 def progress(msg):
@@ -1164,7 +1167,7 @@ def main():
     roofline = {"kernel": "k_mf_tile + k_mf_combine_dot", "bound": "hbm", "achieved": round(ach, 1), "peak": hbm,
                 "unit": "GB/s", "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": int(b_mf),
                 "format": "matrix-free SVK tangent from the FP64 gradient stream", "ms": round(ms_mf, 4),
-                "traffic": None}
+                "traffic": int(MF_TRAFFIC_RATIO * b_mf)}
     # fused element force, FP32 and FP64
     ef = {}
     f_by_prec = {}
@@ -1178,7 +1181,7 @@ def main():
         a = b / (ms_f / 1e3) / 1e9
         ef[prec] = {"kernel": "k_tile_force+k_combine", "bound": "hbm", "achieved": round(a, 1), "peak": hbm,
                     "unit": "GB/s", "frac": round(a / hbm, 4), "algorithmic_bytes": int(b), "ms": round(ms_f, 4),
-                    "traffic": int(FORCE_FP32_TRAFFIC_BYTES) if prec == "fp32" else None}
+                    "traffic": int(FORCE_TRAFFIC_RATIO[prec] * b)}
     # FP32 force error against the FP64 force at the same (deformed) positions
     ef["fp32"]["rel_error_vs_fp64"] = float(np.linalg.norm(f_by_prec["fp32"] - f_by_prec["fp64"]) /
                                             np.linalg.norm(f_by_prec["fp64"]))
