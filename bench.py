@@ -676,7 +676,7 @@ def config2_more_legs(args, T, cfg):
             dtf = time.perf_counter() - t0
             itf = max(1, s.GetStats()["inner_iters_total"])
             fixed_it[mode] = {"inner_iters": itf, "ms_per_inner_iteration": round(1e3 * dtf / itf, 4)}
-        s.SetMode("phased")
+        s.SetMode("auto")
         nes[prec]["fixed_60_iterations"] = fixed_it
         del s
     el.SetForcePrecision("fp64")
@@ -1131,7 +1131,7 @@ def main():
     step()
     ms_asm = time_stream(torch, stream, step, 1)
     asm_iters = solver.GetLastIterCount()
-    solver.SetOperator("matrix-free")
+    solver.SetOperator("auto")
     assembled = {"value": round(1e3 / ms_asm, 4), "unit": "solves/s", "ms_per_step": round(ms_asm, 3),
                  "cg_iters_per_solve": asm_iters,
                  "spmv": {"kernel": "k_cg_spmv_dot", "bound": "hbm", "achieved": round(ach_s, 1), "peak": hbm,

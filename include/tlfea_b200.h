@@ -261,12 +261,13 @@ int tlfea_solver_solve(tlfea_solver s);
  * Jacobi on the 3x3 node diagonal blocks of K (BCs applied).  The stop test
  * stays sqrt(r.r / r0.r0) < tol. */
 int tlfea_linear_static_set_preconditioner(tlfea_solver s, int kind);
-/* How the CG applies K (new).  0 (default) = matrix-free where it applies (TET10, SVK,
- * no damping, no preconditioner): K p from the elements' tangent at the current positions
+/* How the CG applies K (new).  2 = matrix-free where it applies (TET10, SVK, no
+ * damping, no preconditioner): K p from the elements' tangent at the current positions
  * in each iteration, never assembled (K is assembled on demand, at the positions of the
- * last solve, for tlfea_linear_static_retrieve_k); otherwise, and with 1, the assembled
- * K of the reference (3x3 node blocks).  Both are the same operator: the solutions and
- * iteration counts agree to rounding. */
+ * last solve, for tlfea_linear_static_retrieve_k); 1 = the assembled K of the reference
+ * (3x3 node blocks); 0 (default) = matrix-free where it applies from 100,000 elements,
+ * assembled otherwise.  Both are the same operator: the solutions and iteration counts
+ * agree to rounding. */
 int tlfea_linear_static_set_operator(tlfea_solver s, int mode);
 /* GetLastIterCount / GetLastResidual (LinearStaticSolver.cuh:68-72). */
 int tlfea_linear_static_last(tlfea_solver s, int* iters, double* rel_residual);
@@ -287,11 +288,12 @@ int tlfea_solver_get_stats(tlfea_solver s, tlfea_solve_stats* st);
  * positions the internal force was computed at, and the solve ends -- keeping
  * those positions -- once it is below rel_tol.  0 turns it off (default). */
 int tlfea_solver_set_stop_rule(tlfea_solver s, double rel_tol);
-/* New: launch mode of the Nesterov / AdamW solvers.  0 (default) = one kernel per
- * phase (velocity guess, forces, gradient, update, outer update) with the loop state
- * on the device, chunks of iterations replayed as CUDA graphs until the solve ends;
- * 1 = the whole Solve() in one persistent cooperative launch.  The iterations are the
- * same; with fixed iteration counts so are the trajectories, bit for bit. */
+/* New: launch mode of the Nesterov / AdamW solvers.  2 = one kernel per phase
+ * (velocity guess, forces, gradient, update, outer update) with the loop state on the
+ * device, chunks of iterations replayed as CUDA graphs until the solve ends; 1 = the
+ * whole Solve() in one persistent cooperative launch; 0 (default) = per-phase from
+ * 200,000 nodes, persistent below.  The iterations are the same; with fixed iteration
+ * counts so are the trajectories, bit for bit. */
 int tlfea_solver_set_mode(tlfea_solver s, int mode);
 
 /* New, no reference counterpart: n_steps implicit steps of a first-order solver

@@ -401,11 +401,12 @@ class _FirstOrder(SolverBase):
         (FP64, evaluated every inner iteration); 0 turns the rule off."""
         capi.call("tlfea_solver_set_stop_rule", self._h, float(rel_tol))
 
-    def SetMode(self, mode: str = "phased"):
-        """New: "phased" (default) -- one kernel per phase, the loop state on the
-        device, chunks of iterations replayed as CUDA graphs -- or "persistent" (the
-        whole Solve() in one cooperative launch)."""
-        capi.call("tlfea_solver_set_mode", self._h, {"phased": 0, "persistent": 1}[mode])
+    def SetMode(self, mode: str = "auto"):
+        """New: "phased" -- one kernel per phase, the loop state on the device, chunks of
+        iterations replayed as CUDA graphs -- or "persistent" (the whole Solve() in one
+        cooperative launch); "auto" (the default) takes the per-phase launches from
+        200,000 nodes."""
+        capi.call("tlfea_solver_set_mode", self._h, {"auto": 0, "persistent": 1, "phased": 2}[mode])
 
     def RunSteps(self, n_steps: int, f_var=None, amp: float = 1.0, omega: float = 0.0, phase: float = 0.0,
                  t0: float = 0.0):
@@ -473,10 +474,11 @@ class LinearStaticSolver(SolverBase):
         reference's unpreconditioned CG, the default)."""
         capi.call("tlfea_linear_static_set_preconditioner", self._h, {"none": 0, "block_jacobi": 1}[kind])
 
-    def SetOperator(self, mode: str = "matrix-free"):
-        """New: "matrix-free" (default where it applies: TET10, SVK, no damping, no
-        preconditioner) or "assembled" (the reference's assembled K)."""
-        capi.call("tlfea_linear_static_set_operator", self._h, {"matrix-free": 0, "assembled": 1}[mode])
+    def SetOperator(self, mode: str = "auto"):
+        """New: "matrix-free" (TET10, SVK, no damping, no preconditioner), "assembled"
+        (the reference's assembled K), or "auto" (the default: matrix-free from 100,000
+        elements where it applies)."""
+        capi.call("tlfea_linear_static_set_operator", self._h, {"auto": 0, "assembled": 1, "matrix-free": 2}[mode])
 
     def _last(self):
         it, res = C.c_int(), C.c_double()

@@ -1043,7 +1043,12 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     cudaStream_t stream = el->stream;
     const int n_steps = std::max(1, steps);
     st = TLFEA_OK;
-    if (s->fo_mode == 0) {
+    // per-phase launches by default from FO_PHASED_MIN_NODES nodes: below it the host
+    // round trip of each chunk outweighs the persistent kernel's latency (config 5's
+    // 88,641-node beam: 97 against 127 steps/s), above it the phases' occupancy wins
+    // (config 2's 674,081 nodes: 0.354 against 0.428 ms per Nesterov iteration)
+    constexpr int FO_PHASED_MIN_NODES = 200000;
+    if (s->fo_mode == 2 || (s->fo_mode == 0 && el->N >= FO_PHASED_MIN_NODES)) {
         // per-phase launches: each step's load, then its solve, then its statistics
         auto run_one = [&]() -> int {
 #define TLFEA_FO_PHASED(R_, NPE_, NQP_, AA)                                                              \

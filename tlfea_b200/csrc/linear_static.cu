@@ -491,13 +491,20 @@ __global__ void k_pcg_axpy_dot(int N, const double* __restrict__ dinv, double* u
 
 static int cg_grid(const tlfea_solver_s* s) { return s->cg_blocks; }
 
-// The matrix-free product where it applies and pays: SVK without damping and without
-// the preconditioner, on TET10 (on TET4 -- 12 values of K per element pair, few QPs --
-// the assembled SpMV measured faster: 7.5 against 5.7 solves/s at 200x20x20).
+// The matrix-free product where it applies -- SVK without damping, no preconditioner,
+// TET10 -- and, by default, where it pays: on TET4 (few QPs, small K blocks) the
+// assembled SpMV measured faster (7.5 against 5.7 solves/s at 200x20x20), and so it did
+// on meshes of a few thousand elements (12.7 against 17.4 solves/s on the 512-instance
+// batch's single-instance solves), while from about 10^5 elements the product's 2.2x
+// fewer bytes win (0.53 against 0.40 solves/s at 480,000 elements).
+constexpr int MF_MIN_ELEMENTS = 100000;
+
 static bool use_matrix_free(const tlfea_solver_s* s) {
     const tlfea_element_s* el = s->el;
-    return s->op_mode == 0 && s->precond == 0 && el->npe == 10 && el->material != TLFEA_MATERIAL_MOONEY_RIVLIN &&
-           el->eta_d == 0.0 && el->lambda_d == 0.0;
+    const bool applies = s->precond == 0 && el->npe == 10 && el->material != TLFEA_MATERIAL_MOONEY_RIVLIN &&
+                         el->eta_d == 0.0 && el->lambda_d == 0.0;
+    if (!applies || s->op_mode == 1) return false;
+    return s->op_mode == 2 || el->E >= MF_MIN_ELEMENTS;
 }
 
 static MfArgs mf_args(tlfea_solver_s* s, const double* p, double* q, CgCtl* ctl) {

@@ -47,7 +47,7 @@ struct tlfea_solver_s {
     unsigned char* node_fixed = nullptr;  // N, for the stop rule's free-DOF norm
     int max_blocks = 0;
     int* dstat = nullptr;    // device diagnostics (tlfea_solve_stats fields)
-    int fo_mode = 0;         // 0 = per-phase kernels and graph chunks, 1 = one persistent launch
+    int fo_mode = 0;         // 0 = by size (per-phase from FO_PHASED_MIN_NODES), 1 = persistent, 2 = per-phase
     void* fo_ctl = nullptr;  // per-phase mode: the device-side loop state
     cudaGraphExec_t fo_graph[2] = {nullptr, nullptr};  // per-phase mode: chunks of 8 and 32 slots
     std::vector<unsigned char> fo_graph_key;             // what the captured chunks bake in
@@ -72,7 +72,7 @@ struct tlfea_solver_s {
     double* z = nullptr;        // block Jacobi: z = D^-1 r
     int cg_graph_precond = -1;  // preconditioner the captured graph was built for
     int cg_graph_mf = -1;       // operator the captured graph was built for (1 = matrix-free)
-    int op_mode = 0;            // 0: matrix-free K p where it applies (SVK, no damping, no preconditioner), 1: assembled
+    int op_mode = 0;            // 0: by size (matrix-free from MF_MIN_ELEMENTS), 1: assembled, 2: matrix-free
     bool mf_last = false;       // the last solve ran matrix-free: K is assembled on demand
     double* mf_part = nullptr;  // matrix-free p.q partials: one per tile, then one per combine block
     double *xk = nullptr, *yk = nullptr, *zk = nullptr;  // positions of the last matrix-free solve

@@ -181,7 +181,7 @@ int tlfea_linear_static_set_preconditioner(tlfea_solver s, int kind) {
 }
 
 int tlfea_linear_static_set_operator(tlfea_solver s, int mode) {
-    if (!s || s->kind != KIND_LINEAR_STATIC || (mode != 0 && mode != 1)) return TLFEA_INVALID_ARG;
+    if (!s || s->kind != KIND_LINEAR_STATIC || mode < 0 || mode > 2) return TLFEA_INVALID_ARG;
     s->op_mode = mode;
     return TLFEA_OK;
 }
@@ -241,7 +241,7 @@ int tlfea_solver_set_stop_rule(tlfea_solver s, double rel_tol) {
 }
 
 int tlfea_solver_set_mode(tlfea_solver s, int mode) {
-    if (!s || (mode != 0 && mode != 1)) return TLFEA_INVALID_ARG;
+    if (!s || mode < 0 || mode > 2) return TLFEA_INVALID_ARG;
     if (s->kind == tlfea::KIND_LINEAR_STATIC) {
         tlfea::set_error("the launch mode applies to the Nesterov / AdamW solvers");
         return TLFEA_UNSUPPORTED;
