@@ -555,8 +555,18 @@ static int launch_mf_apply(tlfea_solver_s* s, cudaStream_t st, const double* p, 
     if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
     const int nb = el->tl.n_bnodes;
     const int cb = std::max(1, (nb + 255) / 256);
-    k_mf_combine_dot<<<cb, 256, 0, st>>>(nb, el->tl.bnode_gid, el->tl.bnode_off, M, s->mf_part + el->tl.n_tiles);
-    if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cb);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // overlaps the tile kernel's tail
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k_mf_combine_dot, nb, (const int*)el->tl.bnode_gid, (const int*)el->tl.bnode_off, M,
+                           s->mf_part + el->tl.n_tiles) != cudaSuccess)
+        return TLFEA_CUDA_ERROR;
     return TLFEA_OK;
 }
 

@@ -218,6 +218,8 @@ __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_tile(MfArgs M, int* err) {
     }
     dot = block_sum(dot, red_sh);
     if (t == 0) M.tile_dot[tile] = dot;
+    // outputs written: the combine (a programmatic dependent) may be scheduled
+    asm volatile("griddepcontrol.launch_dependents;");
 }
 
 // The nodes shared between tiles: their partials summed in tile order, then p.q folded
@@ -229,6 +231,8 @@ __global__ void __launch_bounds__(256) k_mf_combine_dot(int nb, const int* __res
     __shared__ bool am_last;
     constexpr int CAP = 384;  // staged partial values per warp (128 slots)
     __shared__ double buf[8][CAP];
+    // launched as a programmatic dependent of the tile kernel: wait for its results
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     CgCtl* ctl = M.ctl;
     if (ctl->done) return;
     // a warp owns 32 consecutive shared nodes, whose partial slots are one contiguous
