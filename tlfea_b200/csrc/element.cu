@@ -178,39 +178,28 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force(TileArgs<R> A) {
 // contiguous range [boff[b], boff[b+1]) and consecutive threads read
 // consecutive memory.
 template <typename R, bool ACCUM>
-__global__ void __launch_bounds__(256) k_combine(int nb, const int* __restrict__ bgid, const int* __restrict__ boff,
-                                                 const R* __restrict__ partial, R* f_out) {
+__global__ void k_combine(int nb, const int* __restrict__ bgid, const int* __restrict__ boff,
+                          const R* __restrict__ partial, R* f_out) {
     // launched as a programmatic dependent of the force kernel: its blocks may be
     // scheduled while the force kernel drains, and wait here until it has completed
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    // a warp owns 32 consecutive shared nodes, whose partial slots are one contiguous
-    // range: the warp stages that range with coalesced loads, then each lane sums its
-    // node's slots in slot (tile) order -- the same sums as slot-by-slot loads
-    constexpr int CAP = 384;  // staged values per warp (128 slots)
-    __shared__ R buf[8][CAP];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b0 = (blockIdx.x * 8 + w) * 32;
-    if (b0 >= nb) return;
-    const int b = b0 + lane, bend = min(b0 + 32, nb);
-    const int s0 = boff[b0], n = 3 * (boff[bend] - s0);
-    const bool staged = n <= CAP;
-    if (staged) {
-        for (int k = lane; k < n; k += 32) buf[w][k] = partial[3 * (size_t)s0 + k];
-        __syncwarp();
-    }
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
-    double s[3] = {0.0, 0.0, 0.0};  // node sums in FP64 (near equilibrium they cancel)
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;  // node sums in FP64 (near equilibrium they cancel)
     for (int k = boff[b]; k < boff[b + 1]; ++k) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) s[d] += staged ? buf[w][3 * (k - s0) + d] : partial[3 * (size_t)k + d];
+        s0 += partial[3 * k + 0];
+        s1 += partial[3 * k + 1];
+        s2 += partial[3 * k + 2];
     }
     const int g = bgid[b];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        if (ACCUM)
-            f_out[3 * g + d] += s[d];
-        else
-            f_out[3 * g + d] = s[d];
+    if (ACCUM) {
+        f_out[3 * g + 0] += s0;
+        f_out[3 * g + 1] += s1;
+        f_out[3 * g + 2] += s2;
+    } else {
+        f_out[3 * g + 0] = s0;
+        f_out[3 * g + 1] = s1;
+        f_out[3 * g + 2] = s2;
     }
 }
 
@@ -706,7 +695,7 @@ static int launch_combine(tlfea_element_s* h, const R* partial, R* f_out) {
     const int nb = h->tl.n_bnodes;
     if (nb == 0) return TLFEA_OK;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)((nb + 255) / 256));  // 8 warps of 32 nodes per block
+    cfg.gridDim = dim3((unsigned)((nb + 255) / 256));
     cfg.blockDim = dim3(256);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = h->stream;

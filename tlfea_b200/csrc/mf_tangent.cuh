@@ -229,39 +229,26 @@ __global__ void __launch_bounds__(256) k_mf_combine_dot(int nb, const int* __res
                                                         const int* __restrict__ boff, MfArgs M, double* part) {
     __shared__ double red[32];
     __shared__ bool am_last;
-    constexpr int CAP = 384;  // staged partial values per warp (128 slots)
-    __shared__ double buf[8][CAP];
     // launched as a programmatic dependent of the tile kernel: wait for its results
     asm volatile("griddepcontrol.wait;" ::: "memory");
     CgCtl* ctl = M.ctl;
     if (ctl->done) return;
-    // a warp owns 32 consecutive shared nodes, whose partial slots are one contiguous
-    // range: staged with coalesced loads, then summed per node in slot (tile) order
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b0 = (blockIdx.x * 8 + w) * 32, b = b0 + lane;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
     double dot = 0.0;
-    if (b0 < nb) {
-        const int bend = min(b0 + 32, nb);
-        const int s0 = boff[b0], n = 3 * (boff[bend] - s0);
-        const bool staged = n <= CAP;
-        if (staged) {
-            for (int k = lane; k < n; k += 32) buf[w][k] = M.partial[3 * (size_t)s0 + k];
-            __syncwarp();
+    if (b < nb) {
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int k = boff[b]; k < boff[b + 1]; ++k) {
+            s[0] += M.partial[3 * k + 0];
+            s[1] += M.partial[3 * k + 1];
+            s[2] += M.partial[3 * k + 2];
         }
-        if (b < nb) {
-            double s[3] = {0.0, 0.0, 0.0};
-            for (int k = boff[b]; k < boff[b + 1]; ++k) {
+        const int g = bgid[b];
 #pragma unroll
-                for (int d = 0; d < 3; ++d) s[d] += staged ? buf[w][3 * (k - s0) + d] : M.partial[3 * (size_t)k + d];
-            }
-            const int g = bgid[b];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const double pv = M.p[3 * g + d];
-                const double qv = M.is_fixed[3 * g + d] ? pv : s[d];
-                M.q[3 * g + d] = qv;
-                dot += pv * qv;
-            }
+        for (int d = 0; d < 3; ++d) {
+            const double pv = M.p[3 * g + d];
+            const double qv = M.is_fixed[3 * g + d] ? pv : s[d];
+            M.q[3 * g + d] = qv;
+            dot += pv * qv;
         }
     }
     const double bs = block_sum(dot, red);
