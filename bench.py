@@ -372,6 +372,55 @@ def kernels_only(args):
         print(json.dumps({"kernels_only": "batch", "cases": 64, "iterations": 10}))
         fm.destroy()
         return
+    if args.kernels_only == "mlp":
+        # the warm-start network's training step: 6-256-256-256-64, a batch of 512, 20 steps
+        net = T.WarmStartMLP((6, 256, 256, 256, 64), max_batch=512, seed=0)
+        g = torch.Generator(device="cuda").manual_seed(0)
+        xb = torch.randn(512, 6, device="cuda", generator=g)
+        tb = torch.randn(512, 64, device="cuda", generator=g)
+        torch.cuda.synchronize()
+        for _ in range(20):
+            net.TrainStep(xb.data_ptr(), tb.data_ptr(), 512)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernels_only": "mlp", "dims": [6, 256, 256, 256, 64], "batch": 512, "steps": 20}))
+        net.Destroy()
+        return
+    if args.kernels_only == "gemm":
+        # the MLP's tcgen05 product on its own at a size that fills the GPU:
+        # D[8192 x 8192] = A[8192 x 8192] B^T, BF16 operands, FP32 accumulation and output
+        n = args.gemm_size
+        g = torch.Generator(device="cuda").manual_seed(0)
+        A = torch.randn(n, n, device="cuda", generator=g).to(torch.bfloat16)
+        B = torch.randn(n, n, device="cuda", generator=g).to(torch.bfloat16)
+        D = torch.empty(n, n, device="cuda")
+        st = torch.cuda.current_stream()
+        flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+        def launch():
+            T.gemm_bf16_async(n, n, n, A.data_ptr(), n, B.data_ptr(), n, 0, D.data_ptr(), n, flag.data_ptr(),
+                              st.cuda_stream)
+
+        for _ in range(3):
+            launch()
+        # operands (2 x 128 MB at the default size) exceed L2, so back-to-back launches stream them
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(args.steps):
+            launch()
+        e1.record(st)
+        torch.cuda.synchronize()
+        if int(flag.item()) != 0:
+            raise RuntimeError("gemm: a bounded wait in the kernel ran out")
+        ref = (A[:256].float() @ B[:256].float().T)
+        err = float((D[:256, :256] - ref).abs().max() / ref.abs().max())
+        t = e0.elapsed_time(e1) * 1e-3 / args.steps
+        tf = 2.0 * n ** 3 / t / 1e12
+        pk = ROOT / "MEASURED_PEAKS.json"
+        peak = float(json.loads(pk.read_text())["bf16_tflops"]) if pk.exists() else 1590.0
+        print(json.dumps({"kernels_only": "gemm", "M": n, "N": n, "K": n, "ms": t * 1e3, "tflops": tf,
+                          "peak_tflops": peak, "frac": tf / peak if peak else None, "max_rel_err_256": err}))
+        return
     if args.kernels_only == "batch-uneven":
         # the batched CG of the uneven batch (general tiling): the first 64 seeded
         # cantilevers of the 512-instance batch, 10 iterations
@@ -1035,8 +1084,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-gpu-ref", action="store_true", help="skip the reference's own CUDA build leg")
     ap.add_argument("--kernel-reps", type=int, default=20)
+    ap.add_argument("--gemm-size", type=int, default=8192, help="M = N = K of --kernels-only gemm")
     ap.add_argument("--cg-iters", type=int, default=120, help="iteration cap of --kernels-only cg")
-    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg", "batch", "batch-uneven", "steps"], default=None,
+    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg", "batch", "batch-uneven", "steps", "mlp", "gemm"], default=None,
                     help="profiling case: set up, then launch only the named kernel a few times")
     ap.add_argument("--mesh", default=None, help="cells NXxNYxNZ (default 200x20x20)")
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")

@@ -456,9 +456,17 @@ int tlfea_dynbatch_retrieve_velocity(tlfea_dynbatch b, int seq, double* v);
 
 /* The MLP's tensor-core product on its own: d_d[M x N] (FP32, leading dim ldd)
  * = d_a[M x K] (BF16, lda) * d_b[N x K]^T (BF16, ldb) + d_bias[N] (or NULL).
- * N and K multiples of 16, lda and ldb multiples of 8. */
+ * N and K multiples of 16, lda and ldb multiples of 8 and >= K, operands
+ * 16-byte aligned.  Synchronises the stream and reports a product that did not
+ * complete as TLFEA_CUDA_ERROR. */
 int tlfea_mlp_gemm_bf16(int M, int N, int K, const void* d_a, int lda, const void* d_b, int ldb, const float* d_bias,
                         float* d_d, int ldd, void* stream);
+
+/* The same product, only enqueued on the stream (no host synchronisation):
+ * *d_err (a device int the caller zeroes) becomes non-zero if a bounded wait
+ * inside the kernel ran out. */
+int tlfea_mlp_gemm_bf16_async(int M, int N, int K, const void* d_a, int lda, const void* d_b, int ldb,
+                              const float* d_bias, float* d_d, int ldd, int* d_err, void* stream);
 
 #ifdef __cplusplus
 }

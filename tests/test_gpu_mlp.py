@@ -15,7 +15,8 @@ pytestmark = pytest.mark.gpu
 DIMS = [6, 256, 256, 256, 64]
 
 
-@pytest.mark.parametrize("M,N,K", [(128, 256, 256), (256, 64, 16), (300, 272, 80), (512, 256, 512), (128, 16, 16)])
+@pytest.mark.parametrize("M,N,K", [(128, 256, 256), (256, 64, 16), (300, 272, 80), (512, 256, 512), (128, 16, 16),
+                                   (1000, 528, 1040), (200, 48, 2048), (2048, 2048, 384), (4096, 1296, 320)])
 def test_gemm_bf16_matches_fp32_product_of_bf16_operands(M, N, K):
     import torch
 
@@ -27,11 +28,38 @@ def test_gemm_bf16_matches_fp32_product_of_bf16_operands(M, N, K):
     torch.cuda.synchronize()
     T.gemm_bf16(M, N, K, A.data_ptr(), K, B.data_ptr(), K, bias.data_ptr(), D.data_ptr(), N)
     ref = A.double() @ B.double().T + bias.double()
-    assert rel(D.cpu().numpy(), ref.cpu().numpy()) < 1e-6
+    # FP32 accumulation over K products inside the tensor core: the error bound
+    # grows linearly with K (measured 1.0e-6 at K = 1040, 2.1e-6 at K = 2048)
+    tol = 1e-6 * max(1.0, K / 512)
+    assert rel(D.cpu().numpy(), ref.cpu().numpy()) < tol
     D2 = torch.zeros(M, N, device="cuda")
     torch.cuda.synchronize()
     T.gemm_bf16(M, N, K, A.data_ptr(), K, B.data_ptr(), K, 0, D2.data_ptr(), N)
-    assert rel(D2.cpu().numpy(), (A.double() @ B.double().T).cpu().numpy()) < 1e-6
+    assert rel(D2.cpu().numpy(), (A.double() @ B.double().T).cpu().numpy()) < tol
+
+
+def test_gemm_bf16_async_matches_the_synchronous_call():
+    """The enqueue-only entry point gives the same product, bit for bit, and leaves
+    the error flag at zero; grouped tile order is exercised by a grid of several
+    row groups (M = 4480: 35 row tiles, groups of 16, 16 and 3)."""
+    import torch
+
+    M, N, K = 4480, 384, 256
+    g = torch.Generator(device="cpu").manual_seed(7)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16).cuda()
+    B = torch.randn(N, K, generator=g).to(torch.bfloat16).cuda()
+    D1 = torch.zeros(M, N, device="cuda")
+    D2 = torch.zeros(M, N, device="cuda")
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    T.gemm_bf16(M, N, K, A.data_ptr(), K, B.data_ptr(), K, 0, D1.data_ptr(), N)
+    st = torch.cuda.current_stream()
+    T.gemm_bf16_async(M, N, K, A.data_ptr(), K, B.data_ptr(), K, 0, D2.data_ptr(), N, flag.data_ptr(), st.cuda_stream)
+    torch.cuda.synchronize()
+    assert int(flag.item()) == 0
+    assert torch.equal(D1, D2)
+    ref = A.double() @ B.double().T
+    assert rel(D2.cpu().numpy(), ref.cpu().numpy()) < 1e-6
 
 
 def _data(B, seed=0):

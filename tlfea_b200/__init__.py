@@ -26,6 +26,7 @@ from .api import (
     BatchedDynamics,
     WarmStartMLP,
     gemm_bf16,
+    gemm_bf16_async,
     TYPE_3243,
     TYPE_3443,
     TYPE_T10,
@@ -38,6 +39,6 @@ __all__ = [
     "Quadrature", "mesh", "TLFEAError", "launch_count", "last_error", "FEASolver", "ElementBase",
     "GPU_FEAT10_Data", "GPU_FEAT4_Data", "SolverBase", "SyncedNesterovParams", "SyncedNesterovSolver",
     "SyncedAdamWParams", "SyncedAdamWNocoopParams", "SyncedAdamWSolver", "SyncedAdamWNocoopSolver",
-    "LinearStaticSolver", "LinearStaticSolverT10", "LinearStaticSolverT4", "BatchedLinearStaticSolver", "BatchedDynamics", "WarmStartMLP", "gemm_bf16", "TYPE_3243", "TYPE_3443", "TYPE_T10",
+    "LinearStaticSolver", "LinearStaticSolverT10", "LinearStaticSolverT4", "BatchedLinearStaticSolver", "BatchedDynamics", "WarmStartMLP", "gemm_bf16", "gemm_bf16_async", "TYPE_3243", "TYPE_3443", "TYPE_T10",
     "TYPE_T4", "MATERIAL_MODEL_SVK", "MATERIAL_MODEL_MOONEY_RIVLIN",
 ]

@@ -187,6 +187,7 @@ _SIGS = {
     "tlfea_mlp_train_step": [_P, _P, _P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _F],
     "tlfea_mlp_sync": [_P],
     "tlfea_mlp_gemm_bf16": [C.c_int, C.c_int, C.c_int, _P, C.c_int, _P, C.c_int, _P, _P, C.c_int, _P],
+    "tlfea_mlp_gemm_bf16_async": [C.c_int, C.c_int, C.c_int, _P, C.c_int, _P, C.c_int, _P, _P, C.c_int, _P, _P],
 }
 _RESTYPES = {"tlfea_last_error": C.c_char_p, "tlfea_launch_count": C.c_longlong, "tlfea_version": C.c_char_p}
 

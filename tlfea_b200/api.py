@@ -888,3 +888,11 @@ def gemm_bf16(M, N, K, d_a, lda, d_b, ldb, d_bias, d_d, ldd, stream=0):
     """The MLP's tcgen05 product on its own: D = A B^T (+ bias), BF16 in, FP32 out."""
     capi.call("tlfea_mlp_gemm_bf16", int(M), int(N), int(K), C.c_void_p(d_a), int(lda), C.c_void_p(d_b), int(ldb),
               C.c_void_p(d_bias) if d_bias else None, C.c_void_p(d_d), int(ldd), C.c_void_p(stream))
+
+
+def gemm_bf16_async(M, N, K, d_a, lda, d_b, ldb, d_bias, d_d, ldd, d_err, stream=0):
+    """gemm_bf16 only enqueued on `stream`; *d_err (device int32, zeroed by the
+    caller) turns non-zero if a bounded wait in the kernel ran out."""
+    capi.call("tlfea_mlp_gemm_bf16_async", int(M), int(N), int(K), C.c_void_p(d_a), int(lda), C.c_void_p(d_b),
+              int(ldb), C.c_void_p(d_bias) if d_bias else None, C.c_void_p(d_d), int(ldd), C.c_void_p(d_err),
+              C.c_void_p(stream))

@@ -2,15 +2,20 @@
 // GELU between layers) trained and evaluated on the GPU by this file's own
 // kernels.  New, no reference counterpart.
 //
-// Every matrix product is one tcgen05 kernel (k_gemm_bf16):
+// Every matrix product is one tcgen05 kernel (k_gemm_bf16<BN>):
 //     D[M x N] (FP32) = A[M x K] (BF16) * B[N x K]^T (BF16) (+ bias[N])
 // with both operands K-major (row-major with K contiguous).  A CTA owns a
-// 128-row x (<= 256)-column tile: K is staged 64 at a time in shared memory in
-// the canonical no-swizzle K-major layout (8-row x 16-byte core matrices, LBO =
-// 128 B between the two K halves of an MMA, SBO = 16 * kc bytes between 8-row
-// groups), one elected thread issues tcgen05.mma (kind::f16, BF16 in, FP32
-// accumulator in TMEM) and commits to an mbarrier, and the four warps read the
-// accumulator back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31).
+// 128-row x BN-column tile (BN = 64, 128 or 256, chosen per product so that
+// small products still spread over many SMs).  K streams through a ring of
+// GM_STAGES shared-memory stages, 64 elements (one 128-byte row) at a time:
+// one thread issues two tiled tensor copies per stage (A's 128 x 64 box and
+// B's BN x 64 box, 128-byte swizzle, rows past M / N and columns past K read
+// as zero), waits for the stage, issues four tcgen05.mma (kind::f16, BF16 in,
+// FP32 accumulator in TMEM) and commits them to the stage's "empty" barrier;
+// the stage is refilled as soon as the products that read it have finished,
+// so the copies of the next stages overlap the tensor-core work.  The four
+// warps then read the accumulator back with tcgen05.ld (warp w owns TMEM
+// lanes 32w..32w+31) and store D.
 //
 // Training keeps FP32 master weights and BF16 copies in both layouts
 // (W [N x Kp] for the forward product, W^T [Kp x N] for the input gradient),
@@ -18,6 +23,8 @@
 // product -- forward, input gradient, weight gradient -- is the same K-major
 // kernel.  The optimiser is AdamW.  Reductions (bias gradients, the loss) are
 // fixed-order, so a training run is deterministic.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -29,12 +36,18 @@
 
 namespace tlfea {
 
-constexpr int MLP_TM = 128;  // rows per CTA
-constexpr int MLP_KC = 64;   // K elements per shared-memory chunk
-constexpr int MLP_NT = 256;  // columns per CTA (TMEM columns, FP32)
-// shared memory requested per GEMM CTA: 16 KB A + 32 KB B chunk, padded so at
-// most two CTAs share an SM and their TMEM (2 x 256 columns) always fits
-constexpr size_t MLP_GEMM_SMEM = 100 * 1024;
+constexpr int MLP_TM = 128;    // rows per CTA (the MMA's M)
+constexpr int GM_BK = 64;      // K elements per stage: one 128-byte swizzle row
+constexpr int GM_STAGES = 4;   // shared-memory ring depth
+constexpr int GM_GROUP = 16;   // row tiles per group of the tile order
+
+template <int BN>
+struct GemmGeom {
+    static constexpr uint32_t A_BYTES = MLP_TM * GM_BK * 2;
+    static constexpr uint32_t B_BYTES = BN * GM_BK * 2;
+    static constexpr uint32_t STAGE = A_BYTES + B_BYTES;  // a multiple of 1024 (swizzle atoms stay aligned)
+    static constexpr size_t SMEM = 1024 + (size_t)GM_STAGES * STAGE;  // + slack to align the ring to 1024 B
+};
 
 struct GemmArgs {
     int M, N, K;
@@ -48,20 +61,18 @@ struct GemmArgs {
     int* err;
 };
 
-// Byte offset of (row r, 8-element K group k8) in a K-major no-swizzle tile
-// holding kc K-elements per row.
-__device__ __forceinline__ uint32_t kmajor_off(int r, int k8, int kc) {
-    return (uint32_t)(((r >> 3) * (kc >> 3) + k8) * 128 + (r & 7) * 16);
-}
-
-// Shared-memory matrix descriptor: start, leading and stride byte offsets (16-byte
-// units), descriptor version 1, no swizzle.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+// Shared-memory matrix descriptor of a K-major operand in the 128-byte swizzle
+// layout that the tensor copies write: rows of 128 bytes, 8-row groups 1024
+// bytes apart (stride byte offset), descriptor version 1, swizzle mode 2
+// (128 bytes).  The leading byte offset is unused for this layout.  A K step
+// of 16 elements inside the 128-byte row advances the start address by 32 B.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(1024 >> 4) << 32;
     d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
     return d;
 }
 
@@ -70,83 +81,121 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-__global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) unsigned long long mbar;
+// Tiled 2-D tensor copy global -> shared (box given by the tensor map), completion
+// counted on `bar`; x is the K coordinate (a multiple of 64 here, so 128-byte aligned).
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128) k_gemm_bf16(const __grid_constant__ CUtensorMap ta,
+                                                   const __grid_constant__ CUtensorMap tb, GemmArgs g) {
+    using G = GemmGeom<BN>;
+    extern __shared__ unsigned char gemm_smem[];
+    __shared__ __align__(8) unsigned long long bars[2 * GM_STAGES + 1];  // full[S], empty[S], done
     __shared__ uint32_t tmem_sh;
+    __shared__ int ok_sh;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int m0 = blockIdx.x * MLP_TM, n0 = blockIdx.y * MLP_NT;
-    const int nt = min(MLP_NT, g.N - n0);  // a multiple of 16 (checked by the host)
-    uint32_t ncols = 32;
-    while ((int)ncols < nt) ncols <<= 1;
-    unsigned char* sA = smem;
-    unsigned char* sB = smem + MLP_TM * MLP_KC * 2;
-    const uint32_t bar = smem_u32(&mbar);
+    // grouped tile order: consecutive CTAs walk GM_GROUP row tiles down one
+    // column tile before moving right, so the CTAs resident at one time share a
+    // few A row panels and B column panels in L2
+    const int mtiles = (g.M + MLP_TM - 1) / MLP_TM, ntiles = (g.N + BN - 1) / BN;
+    const int per_group = GM_GROUP * ntiles, grp = blockIdx.x / per_group;
+    const int first_m = grp * GM_GROUP, gm = min(mtiles - first_m, GM_GROUP);
+    const int in_grp = blockIdx.x - grp * per_group;
+    const int m0 = (first_m + in_grp % gm) * MLP_TM, n0 = (in_grp / gm) * BN;
+    const int nk = (g.K + GM_BK - 1) / GM_BK;
+    const uint32_t ring = (smem_u32(gemm_smem) + 1023u) & ~1023u;
+    const uint32_t bar0 = smem_u32(bars), done = bar0 + 16 * GM_STAGES;
+    auto full = [&](int s) { return bar0 + 8 * s; };
+    auto empty = [&](int s) { return bar0 + 8 * (GM_STAGES + s); };
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
-                     "r"(ncols)
+                     "n"(BN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (t == 0) {
-        mbar_init(bar, 1);
+        for (int i = 0; i < 2 * GM_STAGES + 1; ++i) mbar_init(bar0 + 8 * i, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_sh;
-    const uint32_t idesc = umma_idesc_bf16(MLP_TM, nt);
-    bool ok = true;
-    uint32_t phase = 0;
-    bool issued = false;
-    for (int k0 = 0; k0 < g.K; k0 += MLP_KC) {
-        const int kc = min(MLP_KC, g.K - k0);  // a multiple of 16
-        const int k8n = kc >> 3;
-        for (int i = t; i < MLP_TM * k8n; i += blockDim.x) {
-            const int r = i / k8n, k8 = i - r * k8n;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (m0 + r < g.M) v = *reinterpret_cast<const uint4*>(g.A + (size_t)(m0 + r) * g.lda + k0 + k8 * 8);
-            *reinterpret_cast<uint4*>(sA + kmajor_off(r, k8, kc)) = v;
-        }
-        for (int i = t; i < nt * k8n; i += blockDim.x) {
-            const int r = i / k8n, k8 = i - r * k8n;
-            const uint4 v = *reinterpret_cast<const uint4*>(g.B + (size_t)(n0 + r) * g.ldb + k0 + k8 * 8);
-            *reinterpret_cast<uint4*>(sB + kmajor_off(r, k8, kc)) = v;
-        }
-        // generic-proxy stores must be visible to the tensor core's async proxy
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (t == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-            const uint32_t sbo = (uint32_t)kc * 16;  // (kc / 8) core matrices of 128 B per 8-row group
-            for (int kk = 0; kk < kc; kk += 16) {
-                const uint64_t ad = umma_desc(a0 + (uint32_t)kk * 16, 128, sbo);
-                const uint64_t bd = umma_desc(b0 + (uint32_t)kk * 16, 128, sbo);
-                const uint32_t acc = (k0 > 0 || kk > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-                    : "memory");
+    if (warp == 0) {
+        if (lane == 0) {
+            // one thread: copies into the ring and tensor-core issue
+            constexpr uint32_t idesc = umma_idesc_bf16(MLP_TM, BN);
+            bool ok = true;
+            int loaded = 0, landed = 0;
+            auto load = [&](int k) {
+                const int s = k % GM_STAGES;
+                const uint32_t a = ring + s * G::STAGE;
+                mbar_expect_tx(full(s), G::STAGE);
+                tma_load_2d(a, &ta, k * GM_BK, m0, full(s));
+                tma_load_2d(a + G::A_BYTES, &tb, k * GM_BK, n0, full(s));
+            };
+            for (; loaded < nk && loaded < GM_STAGES; ++loaded) load(loaded);
+            for (int k = 0; k < nk; ++k) {
+                const int s = k % GM_STAGES;
+                if (!mbar_wait(full(s), (k / GM_STAGES) & 1)) {
+                    ok = false;
+                    break;
+                }
+                landed = k + 1;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a = ring + s * G::STAGE, b = a + G::A_BYTES;
+#pragma unroll
+                for (int kk = 0; kk < GM_BK / 16; ++kk) {
+                    const uint64_t ad = umma_desc_sw128(a + 32 * kk), bd = umma_desc_sw128(b + 32 * kk);
+                    const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                        "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                        : "memory");
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 empty(s))
+                             : "memory");
+                // refill the stage that the previous chunk's products read (they have
+                // had this chunk's issue time to finish; the tensor pipe keeps a queue)
+                if (k >= 1 && loaded < nk) {
+                    const int sp = (k - 1) % GM_STAGES;
+                    if (!mbar_wait(empty(sp), ((k - 1) / GM_STAGES) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    load(loaded++);
+                }
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+            // arrives once every product issued above has completed
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(done)
                          : "memory");
+            if (!ok) {
+                atomicExch(g.err, 5);
+                // copies still in flight land before the CTA's shared memory is released
+                for (int k = landed; k < loaded; ++k) mbar_wait(full(k % GM_STAGES), (k / GM_STAGES) & 1);
+            }
+            ok_sh = ok ? 1 : 0;
         }
-        issued = true;
-        if (!mbar_wait(bar, phase)) ok = false;
-        phase ^= 1u;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (!__syncthreads_and(ok)) {
-            ok = false;
-            break;
-        }
+        __syncwarp();
     }
+    const bool got = mbar_wait(done, 0);
+    const bool ok = __syncthreads_and(got) && ok_sh;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
-        const int row = warp * 32 + lane;
-        for (int c0 = 0; c0 < nt; c0 += 16) {
+        const int row = m0 + warp * 32 + lane;
+        const int ncols = min(BN, g.N - n0);
+        for (int c0 = 0; c0 < ncols; c0 += 16) {
             uint32_t v[16];
             const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
             asm volatile(
@@ -158,38 +207,107 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
                 : "r"(taddr)
                 : "memory");
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (m0 + row < g.M) {
-                float* d = g.D + (size_t)(m0 + row) * g.ldd + n0 + c0;
+            if (row < g.M) {
+                float* d = g.D + (size_t)row * g.ldd + n0 + c0;
+                const float* bias = g.bias ? g.bias + n0 + c0 : nullptr;
+                const int nc = min(16, ncols - c0);  // N is a multiple of 16, so nc is 16
 #pragma unroll
-                for (int i = 0; i < 16; ++i) d[i] = __uint_as_float(v[i]) + (g.bias ? g.bias[n0 + c0 + i] : 0.f);
+                for (int i = 0; i < 16; ++i)
+                    if (i < nc) d[i] = __uint_as_float(v[i]) + (bias ? bias[i] : 0.f);
             }
         }
-    } else {
-        if (t == 0) atomicExch(g.err, 5);
-        // a product still in flight finishes before its accumulator is released
-        if (issued) mbar_wait(bar, phase ^ 1u);
+    } else if (t == 0) {
+        atomicExch(g.err, 5);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(BN) : "memory");
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// Tensor map of a row-major BF16 operand [rows x k] with leading dimension ld
+// (elements): boxes of box_rows x 64, 128-byte swizzle, out-of-range elements
+// read as zero.
+static int operand_map(CUtensorMap* map, const __nv_bfloat16* base, int rows, int k, int ld, int box_rows) {
+    auto enc = tensor_map_encoder();
+    if (!enc) {
+        set_error("mlp gemm: cuTensorMapEncodeTiled is not available from the driver");
+        return TLFEA_CUDA_ERROR;
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)GM_BK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(base), dims, strides,
+                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("mlp gemm: tensor map encoding failed");
+        return TLFEA_INVALID_ARG;
+    }
+    return TLFEA_OK;
+}
+
+// Column-tile width: the widest of 256 / 128 / 64 whose grid still covers the SMs
+// (or 64 when even that does not).
+static int gemm_tile_n(int M, int N, int sms) {
+    const int mt = (M + MLP_TM - 1) / MLP_TM;
+    for (int bn : {256, 128})
+        if ((long long)mt * ((N + bn - 1) / bn) >= sms) return bn;
+    return 64;
+}
+
+template <int BN>
+static int gemm_launch_bn(const GemmArgs& g, const CUtensorMap& ta, const CUtensorMap& tb, cudaStream_t st) {
+    static bool configured = false;
+    if (!configured) {
+        TLFEA_CUDA(cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)GemmGeom<BN>::SMEM));
+        configured = true;
+    }
+    const unsigned tiles = (unsigned)(((g.M + MLP_TM - 1) / MLP_TM) * ((g.N + BN - 1) / BN));
+    k_gemm_bf16<BN><<<tiles, 128, GemmGeom<BN>::SMEM, st>>>(ta, tb, g);
+    TLFEA_CHECK_LAUNCH();
+    return TLFEA_OK;
 }
 
 static int gemm_launch(const GemmArgs& g, cudaStream_t st) {
-    if (g.M <= 0 || g.N <= 0 || g.K <= 0 || g.N % 16 || g.K % 16 || g.lda % 8 || g.ldb % 8 ||
-        (reinterpret_cast<uintptr_t>(g.A) & 15) || (reinterpret_cast<uintptr_t>(g.B) & 15)) {
-        set_error("mlp gemm: need N, K multiples of 16, leading dimensions multiples of 8, 16-byte aligned operands");
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0 || g.N % 16 || g.K % 16 || g.lda % 8 || g.ldb % 8 || g.lda < g.K ||
+        g.ldb < g.K || (reinterpret_cast<uintptr_t>(g.A) & 15) || (reinterpret_cast<uintptr_t>(g.B) & 15)) {
+        set_error("mlp gemm: need N, K multiples of 16, leading dimensions >= K and multiples of 8, 16-byte "
+                  "aligned operands");
         return TLFEA_INVALID_ARG;
     }
-    static bool configured = false;
-    if (!configured) {
-        TLFEA_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_GEMM_SMEM));
-        configured = true;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
     }
-    dim3 grid((g.M + MLP_TM - 1) / MLP_TM, (g.N + MLP_NT - 1) / MLP_NT);
-    k_gemm_bf16<<<grid, 128, MLP_GEMM_SMEM, st>>>(g);
-    TLFEA_CHECK_LAUNCH();
-    return TLFEA_OK;
+    const int bn = gemm_tile_n(g.M, g.N, sms);
+    CUtensorMap ta, tb;
+    int s = operand_map(&ta, g.A, g.M, g.K, g.lda, MLP_TM);
+    if (!s) s = operand_map(&tb, g.B, g.N, g.K, g.ldb, bn);
+    if (s) return s;
+    if (bn == 256) return gemm_launch_bn<256>(g, ta, tb, st);
+    if (bn == 128) return gemm_launch_bn<128>(g, ta, tb, st);
+    return gemm_launch_bn<64>(g, ta, tb, st);
 }
 
 // ------------------------------------------------------------- elementwise
@@ -454,6 +572,16 @@ int tlfea_mlp_gemm_bf16(int M, int N, int K, const void* d_a, int lda, const voi
     cudaStreamSynchronize(st);
     dfree(err);
     return s;
+}
+
+int tlfea_mlp_gemm_bf16_async(int M, int N, int K, const void* d_a, int lda, const void* d_b, int ldb,
+                              const float* d_bias, float* d_d, int ldd, int* d_err, void* stream) {
+    if (!d_err || !d_d) {
+        set_error("mlp gemm: null output or error flag");
+        return TLFEA_INVALID_ARG;
+    }
+    GemmArgs g{M, N, K, (const __nv_bfloat16*)d_a, lda, (const __nv_bfloat16*)d_b, ldb, d_bias, d_d, ldd, d_err};
+    return gemm_launch(g, (cudaStream_t)stream);
 }
 
 int tlfea_mlp_create(int n_layers, const int* dims, int max_batch, unsigned long long seed, tlfea_mlp* out) {
