@@ -521,7 +521,7 @@ static MfArgs mf_args(tlfea_solver_s* s, const double* p, double* q, CgCtl* ctl)
     M.pad_iend = tl.pad_iend;
     M.inc = tl.inc;
     M.lconn = tl.lconn;
-    M.grad = tl.grad64;
+    M.ji = tl.ji64;
     M.dv = tl.dv64;
     M.sx = tl.sx;
     M.sy = tl.sy;
@@ -533,14 +533,18 @@ static MfArgs mf_args(tlfea_solver_s* s, const double* p, double* q, CgCtl* ctl)
     M.tile_dot = s->mf_part;
     M.lambda = el->lambda;
     M.mu = el->mu;
+    M.qb = qp_bary(el);
     M.ctl = ctl;
     return M;
 }
 
+// The matrix-free product's tile kernel and its shared memory.
+using MfKernel = void (*)(MfArgs, int*);
+static MfKernel mf_kernel(const tlfea_solver_s* s) { return s->el->npe == 10 ? k_mf_geo<10, 5> : k_mf_geo<4, 1>; }
+
 static size_t mf_smem(const tlfea_solver_s* s) {
-    const tlfea_element_s* el = s->el;
-    return (el->npe == 10) ? TileTmaLayout<double, 10>(el->tl.max_local_pad, true).total
-                           : TileTmaLayout<double, 4>(el->tl.max_local_pad, true).total;
+    const int ml = s->el->tl.max_local_pad;
+    return (s->el->npe == 10) ? MfGeoLayout<10>(ml).total_mf : MfGeoLayout<4>(ml).total_mf;
 }
 
 // q = K_bc p matrix-free and p.q, alpha (the SpMV kernel's contract).
@@ -548,10 +552,7 @@ static int launch_mf_apply(tlfea_solver_s* s, cudaStream_t st, const double* p, 
     tlfea_element_s* el = s->el;
     const MfArgs M = mf_args(s, p, q, ctl);
     const size_t smem = mf_smem(s);
-    if (el->npe == 10)
-        k_mf_tile<10, 5><<<el->tl.n_tiles, TILE_ELEMS, smem, st>>>(M, el->d_err);
-    else
-        k_mf_tile<4, 1><<<el->tl.n_tiles, TILE_ELEMS, smem, st>>>(M, el->d_err);
+    mf_kernel(s)<<<el->tl.n_tiles, TILE_ELEMS, smem, st>>>(M, el->d_err);
     if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
     const int nb = el->tl.n_bnodes;
     const int cb = std::max(1, (nb + 255) / 256);
@@ -717,12 +718,9 @@ int linear_static_solve(tlfea_solver_s* s) {
             set_error("matrix-free stiffness: shared memory exceeds 227 KB (tile touches too many nodes)");
             return TLFEA_UNSUPPORTED;
         }
-        if (smem > 48 * 1024) {
-            if (el->npe == 10)
-                TLFEA_CUDA(cudaFuncSetAttribute(k_mf_tile<10, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            else
-                TLFEA_CUDA(cudaFuncSetAttribute(k_mf_tile<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        }
+        if (smem > 48 * 1024)
+            TLFEA_CUDA(cudaFuncSetAttribute((const void*)mf_kernel(s), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
         s->k_built = false;
         s->mf_last = true;
     } else {

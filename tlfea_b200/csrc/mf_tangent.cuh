@@ -9,9 +9,9 @@
 // eliminated as apply_bcs_kernel does (LinearStaticSolver.cu:284-306): their columns
 // are dropped (p is staged as zero there) and their rows of K_bc p are p itself.
 //
-// One tile per block: the gradient stream's QP slices by 1-D bulk copies (one stage,
-// read twice from shared memory), the tile's node positions, destinations and
-// incidence ends by bulk copies of the tile-ordered node record, p gathered per local
+// One tile per block: the compact geometry stream's QP slices by 1-D bulk copies
+// (two stages), the tile's node positions, destinations and incidence ends by bulk
+// copies of the tile-ordered node record, p and the fixed-DOF flags gathered per local
 // node; the element forces reduce per node in the tile's incidence order (no atomics)
 // and the tile's share of p.q over its interior nodes is written per tile, so the
 // combine kernel can fold the dot product deterministically.
@@ -31,7 +31,7 @@ struct MfArgs {
     const uint16_t* pad_iend;
     const uint16_t* inc;
     const uint16_t* lconn;
-    const double* grad;
+    const double* ji;  // compact geometry stream: J^-1 per QP
     const double* dv;
     const double* sx;
     const double* sy;
@@ -42,146 +42,73 @@ struct MfArgs {
     const unsigned char* is_fixed;  // 3N
     double* tile_dot;  // per tile: p.q over the tile's interior nodes
     double lambda, mu;
+    QpBary qb;
     CgCtl* ctl;
 };
 
-template <int NPE, int NQP>
-__global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_tile(MfArgs M, int* err) {
-    using G = TileTmaGeom<double, NPE>;
-    static_assert(G::STAGES == 1, "one stage, read twice");
-    constexpr int TE = TILE_ELEMS;
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ double red_sh[32];
-    if (M.ctl->done) return;  // uniform: written by the previous kernel
-    const int tile = blockIdx.x, t = threadIdx.x;
-    const int ML = M.max_local;
-    const TileTmaLayout<double, NPE> L(ML, true);  // the velocity region holds p
-    unsigned char* stage0 = smem;
-    const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + G::STAGE_BYTES);
-    const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
-    double* xs = reinterpret_cast<double*>(smem + L.pos);
-    double* ys = xs + ML;
-    double* zs = ys + ML;
-    int* dsts = reinterpret_cast<int*>(smem + L.dst);
-    uint16_t* iends = reinterpret_cast<uint16_t*>(smem + L.iend);
-    double* ps = reinterpret_cast<double*>(smem + L.vel);
-    double* fe = reinterpret_cast<double*>(smem);  // aliases the stage after the QP loop
-    const uint32_t bar0 = smem_u32(smem + L.bar), bar_rec = bar0 + 8;
-
-    auto issue = [&](int q) {  // thread 0 only
-        const uint32_t extra = (q == 0) ? G::LCONN_BYTES + G::INC_BYTES : 0;
-        mbar_expect_tx(bar0, G::STAGE_BYTES + extra);
-        bulk_g2s(smem_u32(stage0), M.grad + ((size_t)tile * NQP + q) * (NPE * 3) * TE, G::GRAD_BYTES, bar0);
-        bulk_g2s(smem_u32(stage0) + G::GRAD_BYTES, M.dv + ((size_t)tile * NQP + q) * TE, G::DV_BYTES, bar0);
-        if (q == 0) {
-            bulk_g2s(smem_u32(lcs), M.lconn + (size_t)tile * NPE * TE, G::LCONN_BYTES, bar0);
-            bulk_g2s(smem_u32(incs), M.inc + (size_t)tile * NPE * TE, G::INC_BYTES, bar0);
-        }
-    };
-    const int pb = M.pad_off[tile];
-    if (t == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar_rec, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue(0);
-        const int np = M.pad_off[tile + 1] - pb;
-        mbar_expect_tx(bar_rec, (uint32_t)np * (3 * sizeof(double) + sizeof(int) + sizeof(uint16_t)));
-        bulk_g2s(smem_u32(xs), M.sx + pb, np * sizeof(double), bar_rec);
-        bulk_g2s(smem_u32(ys), M.sy + pb, np * sizeof(double), bar_rec);
-        bulk_g2s(smem_u32(zs), M.sz + pb, np * sizeof(double), bar_rec);
-        bulk_g2s(smem_u32(dsts), M.pad_dst + pb, np * sizeof(int), bar_rec);
-        bulk_g2s(smem_u32(iends), M.pad_iend + pb, np * sizeof(uint16_t), bar_rec);
-    }
-    const int nl = M.node_off[tile + 1] - M.node_off[tile];
-#pragma unroll 4
-    for (int ln = t; ln < nl; ln += TE) {  // unrolled: several nodes' gathers in flight at once
-        const int g = M.pad_gid[pb + ln];
+// dP dV from F and the direction's Hp = dF (the SVK tangent along Hp):
+// E = (F^T F - I) / 2, dE = (Hp^T F + F^T Hp) / 2, S = lambda tr(E) I + 2 mu E,
+// dS likewise from dE, dP = Hp S + F dS.  E, dE, S and dS are symmetric: their six
+// upper entries are formed once (sym index k of (i, j): 0 00, 1 11, 2 22, 3 01, 4 02, 5 12).
+__device__ __forceinline__ void svk_tangent_dp(const double F[3][3], const double Hp[3][3], double lambda,
+                                               double mu, double dv, double dP[3][3]) {
+    constexpr int SI[6] = {0, 1, 2, 0, 0, 1}, SJ[6] = {0, 1, 2, 1, 2, 2};
+    double S[6], dS[6];
+    {
+        double E[6], dE[6];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) ps[3 * ln + d] = M.is_fixed[3 * g + d] ? 0.0 : M.p[3 * g + d];
-    }
-    __syncthreads();  // barriers initialised, p staged
-    if (!mbar_wait(bar_rec, 0)) atomicExch(err, 3);
-    auto lc = [&](int a) -> int { return lcs[a * TE + t]; };
-
-    double f[NPE][3];
+        for (int k = 0; k < 6; ++k) {
+            const int i = SI[k], j = SJ[k];
+            double e = 0.0, de = 0.0;
 #pragma unroll
-    for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = 0.0;
-#pragma unroll 1
-    for (int q = 0; q < NQP; ++q) {
-        if (!mbar_wait(bar0, q & 1)) atomicExch(err, 3);
-        const double* gs = reinterpret_cast<const double*>(stage0);
-        const double dv = reinterpret_cast<const double*>(stage0 + G::GRAD_BYTES)[t];
-        double F[3][3], Hp[3][3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) F[i][j] = Hp[i][j] = 0.0;
-#pragma unroll 2
-        for (int a = 0; a < NPE; ++a) {
-            const int l = lc(a);
-            const double xa[3] = {xs[l], ys[l], zs[l]};
-            const double pa[3] = {ps[3 * l + 0], ps[3 * l + 1], ps[3 * l + 2]};
-            const double ga[3] = {gs[grad_slot<double>(a, 0, t)], gs[grad_slot<double>(a, 1, t)],
-                                  gs[grad_slot<double>(a, 2, t)]};
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    F[i][j] += xa[i] * ga[j];
-                    Hp[i][j] += pa[i] * ga[j];
-                }
-        }
-        // E, S at F; dE, dS along dF = Hp; dP = Hp S + F dS (scaled by dV)
-        double S[3][3], dS[3][3];
-        {
-            double E[3][3], dE[3][3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    double e = 0.0, de = 0.0;
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        e += F[k][i] * F[k][j];
-                        de += Hp[k][i] * F[k][j] + F[k][i] * Hp[k][j];
-                    }
-                    E[i][j] = 0.5 * (e - (i == j ? 1.0 : 0.0));
-                    dE[i][j] = 0.5 * de;
-                }
-            const double trE = E[0][0] + E[1][1] + E[2][2], trdE = dE[0][0] + dE[1][1] + dE[2][2];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    S[i][j] = 2.0 * M.mu * E[i][j] + (i == j ? M.lambda * trE : 0.0);
-                    dS[i][j] = 2.0 * M.mu * dE[i][j] + (i == j ? M.lambda * trdE : 0.0);
-                }
-        }
-        double dP[3][3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                double v = 0.0;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) v += Hp[i][k] * S[k][j] + F[i][k] * dS[k][j];
-                dP[i][j] = v * dv;
+            for (int m = 0; m < 3; ++m) {
+                e += F[m][i] * F[m][j];
+                de += Hp[m][i] * F[m][j] + F[m][i] * Hp[m][j];
             }
-#pragma unroll
-        for (int a = 0; a < NPE; ++a) {
-            const double ga[3] = {gs[grad_slot<double>(a, 0, t)], gs[grad_slot<double>(a, 1, t)],
-                                  gs[grad_slot<double>(a, 2, t)]};
-#pragma unroll
-            for (int i = 0; i < 3; ++i) f[a][i] += dP[i][0] * ga[0] + dP[i][1] * ga[1] + dP[i][2] * ga[2];
+            E[k] = 0.5 * (e - (i == j ? 1.0 : 0.0));
+            dE[k] = 0.5 * de;
         }
-        if (q + 1 < NQP) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            if (t == 0) issue(q + 1);
+        const double trE = E[0] + E[1] + E[2], trdE = dE[0] + dE[1] + dE[2];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            S[k] = 2.0 * mu * E[k] + (k < 3 ? lambda * trE : 0.0);
+            dS[k] = 2.0 * mu * dE[k] + (k < 3 ? lambda * trdE : 0.0);
         }
     }
-    __syncthreads();  // every thread is done with the stage the force table reuses
+    auto sym = [](int i, int j) { return i == j ? i : (i + j == 1 ? 3 : (i + j == 2 ? 4 : 5)); };
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double v = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) v += Hp[i][k] * S[sym(k, j)] + F[i][k] * dS[sym(k, j)];
+            dP[i][j] = v * dv;
+        }
+}
+
+// The compact kernel's shared memory: the geometry kernel's layout (the velocity
+// region holds p) and a byte per local node with its three fixed-DOF flags.
+template <int NPE>
+struct MfGeoLayout : TileGeoLayout<double, NPE> {
+    size_t fmask, total_mf;
+    __host__ __device__ explicit MfGeoLayout(int max_local) : TileGeoLayout<double, NPE>(max_local, true) {
+        fmask = this->total;
+        total_mf = fmask + (((size_t)max_local + 15) & ~size_t(15));
+    }
+};
+
+// The tile's element forces f (this thread's element) reduced per node in the
+// incidence order: interior nodes write q (identity rows for eliminated DOFs) and
+// their share of p.q, shared nodes their partial slot; then the tile's p.q.  Called
+// by all threads after the stage region that fe aliases is free.
+template <int NPE>
+__device__ __forceinline__ void mf_tile_epilogue(const MfArgs& M, const double (&f)[NPE][3], double* fe,
+                                                 const uint16_t* incs, const uint16_t* iends, const int* dsts,
+                                                 const double* ps, const unsigned char* fmask, int tile, int nl,
+                                                 double* red_sh) {
+    constexpr int TE = TILE_ELEMS;
+    const int t = threadIdx.x;
 #pragma unroll
     for (int a = 0; a < NPE; ++a)
 #pragma unroll
@@ -203,7 +130,7 @@ __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_tile(MfArgs M, int* err) {
         if (dn >= 0) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                const bool fx = M.is_fixed[3 * dn + d];
+                const bool fx = (fmask[ln] >> d) & 1;  // staged with p
                 const double pv = fx ? M.p[3 * dn + d] : ps[3 * ln + d];
                 const double qv = fx ? pv : s[d];  // eliminated DOF: identity row
                 M.q[3 * dn + d] = qv;
@@ -220,6 +147,120 @@ __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_tile(MfArgs M, int* err) {
     if (t == 0) M.tile_dot[tile] = dot;
     // outputs written: the combine (a programmatic dependent) may be scheduled
     asm volatile("griddepcontrol.launch_dependents;");
+}
+
+// One tile per block on the compact geometry stream (J^-1 and dV per QP, 10 values
+// instead of the 3 NPE + 1 of the per-node gradients): F = (dx/dxi) J^-1 and
+// dF = (dp/dxi) J^-1 from the staged positions and p through the barycentric
+// structure of the shape functions, the nodal forces from Q = dP J^-T (tet_dx_dxi_at
+// / tet_scatter).  The 10-value slices fit a double-buffered ring (a slice is read
+// into registers, then its stage is refilled two QPs ahead), so each tile keeps a
+// copy in flight while it computes.
+template <int NPE, int NQP>
+__global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_geo(MfArgs M, int* err) {
+    using G = TileGeoGeom<double, NPE>;
+    constexpr int TE = TILE_ELEMS;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ double red_sh[32];
+    if (M.ctl->done) return;  // uniform: written by the previous kernel
+    const int tile = blockIdx.x, t = threadIdx.x;
+    const int ML = M.max_local;
+    const MfGeoLayout<NPE> L(ML);
+    unsigned char* stage0 = smem;
+    unsigned char* fmask = smem + L.fmask;
+    const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + L.lconn);
+    const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
+    double* xs = reinterpret_cast<double*>(smem + L.pos);
+    double* ys = xs + ML;
+    double* zs = ys + ML;
+    int* dsts = reinterpret_cast<int*>(smem + L.dst);
+    uint16_t* iends = reinterpret_cast<uint16_t*>(smem + L.iend);
+    double* ps = reinterpret_cast<double*>(smem + L.vel);
+    double* fe = reinterpret_cast<double*>(smem);  // aliases the stages after the QP loop
+    const uint32_t bar0 = smem_u32(smem + L.bar), bar_rec = bar0 + 16;
+
+    auto issue = [&](int q) {  // thread 0 only
+        const uint32_t bar = bar0 + 8 * (q & 1);
+        const uint32_t dst = smem_u32(stage0 + (size_t)(q & 1) * G::STAGE_BYTES);
+        const uint32_t extra = (q == 0) ? G::LCONN_BYTES + G::INC_BYTES : 0;
+        mbar_expect_tx(bar, G::STAGE_BYTES + extra);
+        bulk_g2s(dst, M.ji + ((size_t)tile * NQP + q) * 9 * TE, G::JI_BYTES, bar);
+        bulk_g2s(dst + G::JI_BYTES, M.dv + ((size_t)tile * NQP + q) * TE, G::DV_BYTES, bar);
+        if (q == 0) {
+            bulk_g2s(smem_u32(lcs), M.lconn + (size_t)tile * NPE * TE, G::LCONN_BYTES, bar);
+            bulk_g2s(smem_u32(incs), M.inc + (size_t)tile * NPE * TE, G::INC_BYTES, bar);
+        }
+    };
+    const int pb = M.pad_off[tile];
+    if (t == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        mbar_init(bar_rec, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(0);
+        if (NQP > 1) issue(1);
+        const int np = M.pad_off[tile + 1] - pb;
+        mbar_expect_tx(bar_rec, (uint32_t)np * (3 * sizeof(double) + sizeof(int) + sizeof(uint16_t)));
+        bulk_g2s(smem_u32(xs), M.sx + pb, np * sizeof(double), bar_rec);
+        bulk_g2s(smem_u32(ys), M.sy + pb, np * sizeof(double), bar_rec);
+        bulk_g2s(smem_u32(zs), M.sz + pb, np * sizeof(double), bar_rec);
+        bulk_g2s(smem_u32(dsts), M.pad_dst + pb, np * sizeof(int), bar_rec);
+        bulk_g2s(smem_u32(iends), M.pad_iend + pb, np * sizeof(uint16_t), bar_rec);
+    }
+    const int nl = M.node_off[tile + 1] - M.node_off[tile];
+#pragma unroll 4
+    for (int ln = t; ln < nl; ln += TE) {  // unrolled: several nodes' gathers in flight at once
+        const int g = M.pad_gid[pb + ln];
+        unsigned m = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const bool fx = M.is_fixed[3 * g + d];
+            m |= (unsigned)fx << d;
+            ps[3 * ln + d] = fx ? 0.0 : M.p[3 * g + d];
+        }
+        fmask[ln] = (unsigned char)m;
+    }
+    __syncthreads();  // barriers initialised, p and the fixed flags staged
+    if (!mbar_wait(bar_rec, 0)) atomicExch(err, 3);
+
+    int lc[NPE];
+    double f[NPE][3];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < NQP; ++q) {
+        if (!mbar_wait(bar0 + 8 * (q & 1), (q >> 1) & 1)) atomicExch(err, 3);
+        const unsigned char* st = stage0 + (size_t)(q & 1) * G::STAGE_BYTES;
+        const double* js = reinterpret_cast<const double*>(st);
+        if (q == 0) {
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
+        }
+        double ji[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) ji[m] = js[m * TE + t];
+        const double dv = reinterpret_cast<const double*>(st + G::JI_BYTES)[t];
+        if (q + 2 < NQP) {
+            // every thread's generic reads of this stage precede the bulk refill
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (t == 0) issue(q + 2);
+        }
+        const double Lq[4] = {M.qb.L[q][0], M.qb.L[q][1], M.qb.L[q][2], M.qb.L[q][3]};
+        double Gx[3][3], Gp[3][3], F[3][3], Hp[3][3];
+        tet_dx_dxi_at<double, NPE>(
+            [&](int a, int d) { return d == 0 ? xs[lc[a]] : (d == 1 ? ys[lc[a]] : zs[lc[a]]); }, Lq, Gx);
+        tet_dx_dxi_at<double, NPE>([&](int a, int d) { return ps[3 * lc[a] + d]; }, Lq, Gp);
+        mul_jinv(Gx, ji, F);
+        mul_jinv(Gp, ji, Hp);
+        double dP[3][3], Q[3][3];
+        svk_tangent_dp(F, Hp, M.lambda, M.mu, dv, dP);
+        mul_jinv_t(dP, ji, Q);
+        tet_scatter<double, NPE>(Q, Lq, [&](int a, int d, double v) { f[a][d] += v; });
+    }
+    __syncthreads();  // every thread is done with the stages the force table reuses
+    mf_tile_epilogue<NPE>(M, f, fe, incs, iends, dsts, ps, fmask, tile, nl, red_sh);
 }
 
 // The nodes shared between tiles: their partials summed in tile order, then p.q folded
