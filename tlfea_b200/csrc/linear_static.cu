@@ -530,6 +530,8 @@ static MfArgs mf_args(tlfea_solver_s* s, const double* p, double* q, CgCtl* ctl)
     M.q = q;
     M.partial = tl.partial64;
     M.is_fixed = s->is_fixed;
+    M.prec = s->mf_prec;
+    M.pfix = s->mf_pfix;
     M.tile_dot = s->mf_part;
     M.lambda = el->lambda;
     M.mu = el->mu;
@@ -552,17 +554,29 @@ static int launch_mf_apply(tlfea_solver_s* s, cudaStream_t st, const double* p, 
     tlfea_element_s* el = s->el;
     const MfArgs M = mf_args(s, p, q, ctl);
     const size_t smem = mf_smem(s);
-    mf_kernel(s)<<<el->tl.n_tiles, TILE_ELEMS, smem, st>>>(M, el->d_err);
+    const long long n_pad = el->tl.n_pad;
+    k_mf_gather<<<(unsigned)((n_pad + 255) / 256), 256, 0, st>>>(n_pad, el->tl.pad_gid, s->mf_pfix, p, s->mf_prec,
+                                                                  ctl);
     if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
+    // the tile kernel and the combine are programmatic dependents: each starts while its
+    // predecessor drains and waits (griddepcontrol.wait) before reading its results
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t tcfg = {};
+    tcfg.gridDim = dim3((unsigned)el->tl.n_tiles);
+    tcfg.blockDim = dim3(TILE_ELEMS);
+    tcfg.dynamicSmemBytes = smem;
+    tcfg.stream = st;
+    tcfg.attrs = attr;
+    tcfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&tcfg, mf_kernel(s), M, el->d_err) != cudaSuccess) return TLFEA_CUDA_ERROR;
     const int nb = el->tl.n_bnodes;
     const int cb = std::max(1, (nb + 255) / 256);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)cb);
     cfg.blockDim = dim3(256);
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // overlaps the tile kernel's tail
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     if (cudaLaunchKernelEx(&cfg, k_mf_combine_dot, nb, (const int*)el->tl.bnode_gid, (const int*)el->tl.bnode_off, M,
@@ -713,6 +727,12 @@ int linear_static_solve(tlfea_solver_s* s) {
         TLFEA_CUDA(cudaMemsetAsync(s->q, 0, sizeof(double) * n3, stream));  // nodes of no element stay 0
         const size_t need = (size_t)el->tl.n_tiles + std::max(1, (el->tl.n_bnodes + 255) / 256);
         if (!s->mf_part && (st = dalloc(&s->mf_part, need))) return st;
+        const long long n_pad = el->tl.n_pad;
+        if (!s->mf_prec && ((st = dalloc(&s->mf_prec, 3 * (size_t)n_pad)) || (st = dalloc(&s->mf_pfix, (size_t)n_pad))))
+            return st;
+        k_mf_fixbits<<<(unsigned)((n_pad + 255) / 256), 256, 0, stream>>>(n_pad, el->tl.pad_gid, s->is_fixed,
+                                                                           s->mf_pfix);
+        TLFEA_CHECK_LAUNCH();
         const size_t smem = mf_smem(s);
         if (smem > 227 * 1024) {
             set_error("matrix-free stiffness: shared memory exceeds 227 KB (tile touches too many nodes)");
@@ -750,7 +770,7 @@ int linear_static_solve(tlfea_solver_s* s) {
             if ((st = build_cg_graph(s, chunk))) return st;
         }
         TLFEA_CUDA(cudaGraphLaunch(s->cg_graph, stream));
-        TLFEA_LAUNCHED(3LL * chunk);
+        TLFEA_LAUNCHED((mf ? 5LL : 3LL) * chunk);  // matrix-free: gather, tiles, combine, axpy, direction
         launched += chunk;
         if (chunk < 64) chunk *= 2;
     }
@@ -793,7 +813,7 @@ int linear_static_apply(tlfea_solver_s* s, const double* d_x, double* d_y) {
         // (a p.q <= 0 would set it): start every product from a clear block
         TLFEA_CUDA(cudaMemsetAsync(s->ctl_apply, 0, sizeof(CgCtl), el->stream));
         if (launch_mf_apply(s, el->stream, d_x, d_y, s->ctl_apply)) return TLFEA_CUDA_ERROR;
-        TLFEA_LAUNCHED(2);
+        TLFEA_LAUNCHED(3);
         if (el->blocking) TLFEA_CUDA(cudaStreamSynchronize(el->stream));
         return TLFEA_OK;
     }
@@ -859,6 +879,8 @@ void linear_static_free(tlfea_solver_s* s) {
     dfree(s->dinv);
     dfree(s->z);
     dfree(s->mf_part);
+    dfree(s->mf_prec);
+    dfree(s->mf_pfix);
     dfree(s->xk);
     dfree(s->yk);
     dfree(s->zk);

@@ -10,9 +10,9 @@
 // are dropped (p is staged as zero there) and their rows of K_bc p are p itself.
 //
 // One tile per block: the compact geometry stream's QP slices by 1-D bulk copies
-// (two stages), the tile's node positions, destinations and incidence ends by bulk
-// copies of the tile-ordered node record, p and the fixed-DOF flags gathered per local
-// node; the element forces reduce per node in the tile's incidence order (no atomics)
+// (two stages), the tile's node positions, destinations, incidence ends, fixed-DOF
+// flags and p (gathered into the record's tile order by k_mf_gather) by bulk copies of
+// the tile-ordered node record; the element forces reduce per node in the tile's incidence order (no atomics)
 // and the tile's share of p.q over its interior nodes is written per tile, so the
 // combine kernel can fold the dot product deterministically.
 #pragma once
@@ -37,6 +37,8 @@ struct MfArgs {
     const double* sy;
     const double* sz;
     const double* p;
+    const double* prec;     // p in the node record's tile order (k_mf_gather), fixed DOFs zeroed
+    const uint16_t* pfix;   // per padded slot: its node's fixed-DOF flags (bits 0..2)
     double* q;
     double* partial;  // per partial slot of the nodes shared between tiles
     const unsigned char* is_fixed;  // 3N
@@ -88,15 +90,50 @@ __device__ __forceinline__ void svk_tangent_dp(const double F[3][3], const doubl
 }
 
 // The compact kernel's shared memory: the geometry kernel's layout (the velocity
-// region holds p) and a byte per local node with its three fixed-DOF flags.
+// region holds p) and per local node its fixed-DOF flags (16 bits).
 template <int NPE>
 struct MfGeoLayout : TileGeoLayout<double, NPE> {
     size_t fmask, total_mf;
     __host__ __device__ explicit MfGeoLayout(int max_local) : TileGeoLayout<double, NPE>(max_local, true) {
-        fmask = this->total;
-        total_mf = fmask + (((size_t)max_local + 15) & ~size_t(15));
+        fmask = (this->total + 15) & ~size_t(15);
+        total_mf = fmask + (((size_t)max_local * sizeof(uint16_t) + 15) & ~size_t(15));
     }
 };
+
+// Per padded slot of the node record, its node's fixed-DOF flags (padding: 0); once
+// per solve.
+__global__ void k_mf_fixbits(long long n_pad, const int* __restrict__ pad_gid,
+                             const unsigned char* __restrict__ is_fixed, uint16_t* __restrict__ pfix) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n_pad) return;
+    const int g = pad_gid[i];
+    unsigned m = 0;
+    if (g >= 0)
+        for (int d = 0; d < 3; ++d) m |= (unsigned)(is_fixed[3 * (size_t)g + d] != 0) << d;
+    pfix[i] = (uint16_t)m;
+}
+
+// p in the node record's tile order, per padded slot its node's three components with
+// the eliminated DOFs zeroed (their columns dropped from K p), padding 0: a streaming
+// gather over all slots, so the product's tiles bulk-copy p like the positions.
+__global__ void __launch_bounds__(256) k_mf_gather(long long n_pad, const int* __restrict__ pad_gid,
+                                                   const uint16_t* __restrict__ pfix, const double* __restrict__ p,
+                                                   double* __restrict__ prec, const CgCtl* __restrict__ ctl) {
+    // the tile kernel (a programmatic dependent) may start its own copies meanwhile
+    asm volatile("griddepcontrol.launch_dependents;");
+    if (ctl->done) return;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n_pad) return;
+    const int g = pad_gid[i];
+    const unsigned m = pfix[i];
+    double v[3] = {0.0, 0.0, 0.0};
+    if (g >= 0) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v[d] = ((m >> d) & 1) ? 0.0 : p[3 * (size_t)g + d];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) prec[3 * i + d] = v[d];
+}
 
 // The tile's element forces f (this thread's element) reduced per node in the
 // incidence order: interior nodes write q (identity rows for eliminated DOFs) and
@@ -105,7 +142,7 @@ struct MfGeoLayout : TileGeoLayout<double, NPE> {
 template <int NPE>
 __device__ __forceinline__ void mf_tile_epilogue(const MfArgs& M, const double (&f)[NPE][3], double* fe,
                                                  const uint16_t* incs, const uint16_t* iends, const int* dsts,
-                                                 const double* ps, const unsigned char* fmask, int tile, int nl,
+                                                 const double* ps, const uint16_t* fmask, int tile, int nl,
                                                  double* red_sh) {
     constexpr int TE = TILE_ELEMS;
     const int t = threadIdx.x;
@@ -130,7 +167,7 @@ __device__ __forceinline__ void mf_tile_epilogue(const MfArgs& M, const double (
         if (dn >= 0) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                const bool fx = (fmask[ln] >> d) & 1;  // staged with p
+                const bool fx = (fmask[ln] >> d) & 1;  // staged with the node record
                 const double pv = fx ? M.p[3 * dn + d] : ps[3 * ln + d];
                 const double qv = fx ? pv : s[d];  // eliminated DOF: identity row
                 M.q[3 * dn + d] = qv;
@@ -167,7 +204,7 @@ __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_geo(MfArgs M, int* err) {
     const int ML = M.max_local;
     const MfGeoLayout<NPE> L(ML);
     unsigned char* stage0 = smem;
-    unsigned char* fmask = smem + L.fmask;
+    uint16_t* fmask = reinterpret_cast<uint16_t*>(smem + L.fmask);
     const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + L.lconn);
     const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
     double* xs = reinterpret_cast<double*>(smem + L.pos);
@@ -201,27 +238,20 @@ __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_geo(MfArgs M, int* err) {
         issue(0);
         if (NQP > 1) issue(1);
         const int np = M.pad_off[tile + 1] - pb;
-        mbar_expect_tx(bar_rec, (uint32_t)np * (3 * sizeof(double) + sizeof(int) + sizeof(uint16_t)));
+        // positions, destinations, incidence ends, p (3 doubles) and fixed flags per slot
+        mbar_expect_tx(bar_rec, (uint32_t)np * (6 * sizeof(double) + sizeof(int) + 2 * sizeof(uint16_t)));
         bulk_g2s(smem_u32(xs), M.sx + pb, np * sizeof(double), bar_rec);
         bulk_g2s(smem_u32(ys), M.sy + pb, np * sizeof(double), bar_rec);
         bulk_g2s(smem_u32(zs), M.sz + pb, np * sizeof(double), bar_rec);
         bulk_g2s(smem_u32(dsts), M.pad_dst + pb, np * sizeof(int), bar_rec);
         bulk_g2s(smem_u32(iends), M.pad_iend + pb, np * sizeof(uint16_t), bar_rec);
+        bulk_g2s(smem_u32(fmask), M.pfix + pb, np * sizeof(uint16_t), bar_rec);
+        // p's tile-ordered copy comes from the gather kernel this one depends on
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        bulk_g2s(smem_u32(ps), M.prec + 3 * (size_t)pb, np * 3 * sizeof(double), bar_rec);
     }
     const int nl = M.node_off[tile + 1] - M.node_off[tile];
-#pragma unroll 4
-    for (int ln = t; ln < nl; ln += TE) {  // unrolled: several nodes' gathers in flight at once
-        const int g = M.pad_gid[pb + ln];
-        unsigned m = 0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const bool fx = M.is_fixed[3 * g + d];
-            m |= (unsigned)fx << d;
-            ps[3 * ln + d] = fx ? 0.0 : M.p[3 * g + d];
-        }
-        fmask[ln] = (unsigned char)m;
-    }
-    __syncthreads();  // barriers initialised, p and the fixed flags staged
+    __syncthreads();  // barriers initialised
     if (!mbar_wait(bar_rec, 0)) atomicExch(err, 3);
 
     int lc[NPE];

@@ -75,6 +75,8 @@ struct tlfea_solver_s {
     int op_mode = 0;            // 0: by size (matrix-free from MF_MIN_ELEMENTS), 1: assembled, 2: matrix-free
     bool mf_last = false;       // the last solve ran matrix-free: K is assembled on demand
     double* mf_part = nullptr;  // matrix-free p.q partials: one per tile, then one per combine block
+    double* mf_prec = nullptr;     // p in the node record's tile order (3 per padded slot)
+    uint16_t* mf_pfix = nullptr;   // fixed-DOF flags per padded slot
     double *xk = nullptr, *yk = nullptr, *zk = nullptr;  // positions of the last matrix-free solve
     int cg_blocks = 0;
     cudaGraphExec_t cg_graph = nullptr;
