@@ -523,9 +523,10 @@ static MfArgs mf_args(tlfea_solver_s* s, const double* p, double* q, CgCtl* ctl)
     M.lconn = tl.lconn;
     M.ji = tl.ji64;
     M.dv = tl.dv64;
-    M.sx = tl.sx;
-    M.sy = tl.sy;
-    M.sz = tl.sz;
+    M.tan = s->mf_tan;
+    M.x = s->xk;  // the last solve's positions
+    M.y = s->yk;
+    M.z = s->zk;
     M.p = p;
     M.q = q;
     M.partial = tl.partial64;
@@ -546,7 +547,7 @@ static MfKernel mf_kernel(const tlfea_solver_s* s) { return s->el->npe == 10 ? k
 
 static size_t mf_smem(const tlfea_solver_s* s) {
     const int ml = s->el->tl.max_local_pad;
-    return (s->el->npe == 10) ? MfGeoLayout<10>(ml).total_mf : MfGeoLayout<4>(ml).total_mf;
+    return (s->el->npe == 10) ? MfLayout<10>(ml).total : MfLayout<4>(ml).total;
 }
 
 // q = K_bc p matrix-free and p.q, alpha (the SpMV kernel's contract).
@@ -712,12 +713,10 @@ int linear_static_solve(tlfea_solver_s* s) {
     }
     const bool mf = use_matrix_free(s);
     if (mf) {
-        // matrix-free K p at these positions: the node record holds them; keep a copy so
-        // that K can still be assembled (Apply, RetrieveStiffness) after the update
+        // matrix-free K p at these positions: keep a copy (the products' tangent stream is
+        // formed from it, and K can still be assembled at them after the update)
         k_zero_fixed<<<(n3 + 255) / 256, 256, 0, stream>>>(n3, s->is_fixed, s->f);
         TLFEA_CHECK_LAUNCH();
-        if ((st = element_refresh_record(el, false))) return st;
-        el->stage_content = 3;  // this solve's positions, until they change
         if (!s->xk && ((st = dalloc(&s->xk, (size_t)N)) || (st = dalloc(&s->yk, (size_t)N)) ||
                        (st = dalloc(&s->zk, (size_t)N))))
             return st;
@@ -733,6 +732,17 @@ int linear_static_solve(tlfea_solver_s* s) {
         k_mf_fixbits<<<(unsigned)((n_pad + 255) / 256), 256, 0, stream>>>(n_pad, el->tl.pad_gid, s->is_fixed,
                                                                            s->mf_pfix);
         TLFEA_CHECK_LAUNCH();
+        // F and S at every element QP, once for the whole solve
+        const size_t ntan = (size_t)el->tl.n_tiles * el->nqp * MF_TAN * TILE_ELEMS;
+        if (!s->mf_tan && (st = dalloc(&s->mf_tan, ntan))) return st;
+        {
+            const MfArgs M = mf_args(s, s->p, s->q, s->ctl);
+            if (el->npe == 10)
+                k_mf_prep<10, 5><<<el->tl.n_tiles, TILE_ELEMS, 0, stream>>>(M);
+            else
+                k_mf_prep<4, 1><<<el->tl.n_tiles, TILE_ELEMS, 0, stream>>>(M);
+            TLFEA_CHECK_LAUNCH();
+        }
         const size_t smem = mf_smem(s);
         if (smem > 227 * 1024) {
             set_error("matrix-free stiffness: shared memory exceeds 227 KB (tile touches too many nodes)");
@@ -803,13 +813,8 @@ int linear_static_apply(tlfea_solver_s* s, const double* d_x, double* d_y) {
         TLFEA_CUDA(cudaMemsetAsync(s->ctl_apply, 0, sizeof(CgCtl), el->stream));
     }
     if (s->mf_last) {
-        // matrix-free, at the positions of the last solve (the node record is rebuilt
-        // from them and marked stale for the force kernels)
-        if (el->stage_content != 3 || el->positions_exposed) {
-            int st = element_stage_positions(el, s->xk, s->yk, s->zk);
-            if (st) return st;
-        }
-        // the product's kernels skip their work once the control block reads done
+        // matrix-free, at the positions of the last solve (its tangent stream); the
+        // product's kernels skip their work once the control block reads done
         // (a p.q <= 0 would set it): start every product from a clear block
         TLFEA_CUDA(cudaMemsetAsync(s->ctl_apply, 0, sizeof(CgCtl), el->stream));
         if (launch_mf_apply(s, el->stream, d_x, d_y, s->ctl_apply)) return TLFEA_CUDA_ERROR;
@@ -880,6 +885,7 @@ void linear_static_free(tlfea_solver_s* s) {
     dfree(s->z);
     dfree(s->mf_part);
     dfree(s->mf_prec);
+    dfree(s->mf_tan);
     dfree(s->mf_pfix);
     dfree(s->xk);
     dfree(s->yk);

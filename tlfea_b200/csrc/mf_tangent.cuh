@@ -9,12 +9,15 @@
 // eliminated as apply_bcs_kernel does (LinearStaticSolver.cu:284-306): their columns
 // are dropped (p is staged as zero there) and their rows of K_bc p are p itself.
 //
-// One tile per block: the compact geometry stream's QP slices by 1-D bulk copies
-// (two stages), the tile's node positions, destinations, incidence ends, fixed-DOF
-// flags and p (gathered into the record's tile order by k_mf_gather) by bulk copies of
-// the tile-ordered node record; the element forces reduce per node in the tile's incidence order (no atomics)
-// and the tile's share of p.q over its interior nodes is written per tile, so the
-// combine kernel can fold the dot product deterministically.
+// The positions do not change during a solve, so F and S at every QP are formed once
+// per solve (k_mf_prep) into a tangent stream beside the compact geometry stream
+// (J^-1, dV); each product then needs only dF = (dp/dxi) J^-1, dE, dS, dP and the
+// nodal forces Q dN/dxi (Q = dP J^-T).  One tile per block: the QP slices (J^-1, dV,
+// F, S) by 1-D bulk copies into two stages, the tile's destinations, incidence ends,
+// fixed-DOF flags and p (gathered into the node record's tile order by k_mf_gather)
+// by bulk copies; the element forces reduce per node in the tile's incidence order
+// (no atomics) and the tile's share of p.q over its interior nodes is written per
+// tile, so the combine kernel can fold the dot product deterministically.
 #pragma once
 
 #include "force_pipe.cuh"
@@ -33,9 +36,10 @@ struct MfArgs {
     const uint16_t* lconn;
     const double* ji;  // compact geometry stream: J^-1 per QP
     const double* dv;
-    const double* sx;
-    const double* sy;
-    const double* sz;
+    double* tan;       // per element and QP: F (9, row-major) and S (6, symmetric), tile/QP slices
+    const double* x;   // positions the tangent is formed at (node order)
+    const double* y;
+    const double* z;
     const double* p;
     const double* prec;     // p in the node record's tile order (k_mf_gather), fixed DOFs zeroed
     const uint16_t* pfix;   // per padded slot: its node's fixed-DOF flags (bits 0..2)
@@ -48,55 +52,92 @@ struct MfArgs {
     CgCtl* ctl;
 };
 
-// dP dV from F and the direction's Hp = dF (the SVK tangent along Hp):
-// E = (F^T F - I) / 2, dE = (Hp^T F + F^T Hp) / 2, S = lambda tr(E) I + 2 mu E,
-// dS likewise from dE, dP = Hp S + F dS.  E, dE, S and dS are symmetric: their six
-// upper entries are formed once (sym index k of (i, j): 0 00, 1 11, 2 22, 3 01, 4 02, 5 12).
-__device__ __forceinline__ void svk_tangent_dp(const double F[3][3], const double Hp[3][3], double lambda,
-                                               double mu, double dv, double dP[3][3]) {
+// Values per element and QP in the tangent stream: F (9) then S (6).
+constexpr int MF_TAN = 15;
+// Symmetric 3x3 storage: index k of (i, j), i <= j: 0 00, 1 11, 2 22, 3 01, 4 02, 5 12.
+__host__ __device__ constexpr int sym3(int i, int j) {
+    return i == j ? i : (i + j == 1 ? 3 : (i + j == 2 ? 4 : 5));
+}
+
+// S = lambda tr(E) I + 2 mu E with E = (F^T F - I) / 2 (six entries).
+__device__ __forceinline__ void svk_stress_sym(const double F[3][3], double lambda, double mu, double S[6]) {
     constexpr int SI[6] = {0, 1, 2, 0, 0, 1}, SJ[6] = {0, 1, 2, 1, 2, 2};
-    double S[6], dS[6];
+    double E[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const int i = SI[k], j = SJ[k];
+        double e = 0.0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) e += F[m][i] * F[m][j];
+        E[k] = 0.5 * (e - (i == j ? 1.0 : 0.0));
+    }
+    const double trE = E[0] + E[1] + E[2];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) S[k] = 2.0 * mu * E[k] + (k < 3 ? lambda * trE : 0.0);
+}
+
+// dP dV along dF = Hp at (F, S): dE = (Hp^T F + F^T Hp) / 2, dS = lambda tr(dE) I +
+// 2 mu dE, dP = Hp S + F dS (the SVK tangent).
+__device__ __forceinline__ void svk_tangent_dp(const double F[3][3], const double S[6], const double Hp[3][3],
+                                               double lambda, double mu, double dv, double dP[3][3]) {
+    constexpr int SI[6] = {0, 1, 2, 0, 0, 1}, SJ[6] = {0, 1, 2, 1, 2, 2};
+    double dS[6];
     {
-        double E[6], dE[6];
+        double dE[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             const int i = SI[k], j = SJ[k];
-            double e = 0.0, de = 0.0;
+            double de = 0.0;
 #pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                e += F[m][i] * F[m][j];
-                de += Hp[m][i] * F[m][j] + F[m][i] * Hp[m][j];
-            }
-            E[k] = 0.5 * (e - (i == j ? 1.0 : 0.0));
+            for (int m = 0; m < 3; ++m) de += Hp[m][i] * F[m][j] + F[m][i] * Hp[m][j];
             dE[k] = 0.5 * de;
         }
-        const double trE = E[0] + E[1] + E[2], trdE = dE[0] + dE[1] + dE[2];
+        const double trdE = dE[0] + dE[1] + dE[2];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            S[k] = 2.0 * mu * E[k] + (k < 3 ? lambda * trE : 0.0);
-            dS[k] = 2.0 * mu * dE[k] + (k < 3 ? lambda * trdE : 0.0);
-        }
+        for (int k = 0; k < 6; ++k) dS[k] = 2.0 * mu * dE[k] + (k < 3 ? lambda * trdE : 0.0);
     }
-    auto sym = [](int i, int j) { return i == j ? i : (i + j == 1 ? 3 : (i + j == 2 ? 4 : 5)); };
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             double v = 0.0;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) v += Hp[i][k] * S[sym(k, j)] + F[i][k] * dS[sym(k, j)];
+            for (int k = 0; k < 3; ++k) v += Hp[i][k] * S[sym3(k, j)] + F[i][k] * dS[sym3(k, j)];
             dP[i][j] = v * dv;
         }
 }
 
-// The compact kernel's shared memory: the geometry kernel's layout (the velocity
-// region holds p) and per local node its fixed-DOF flags (16 bits).
+// Bulk-copy sizes of the product's QP slices (J^-1, dV, F and S of a tile's elements).
 template <int NPE>
-struct MfGeoLayout : TileGeoLayout<double, NPE> {
-    size_t fmask, total_mf;
-    __host__ __device__ explicit MfGeoLayout(int max_local) : TileGeoLayout<double, NPE>(max_local, true) {
-        fmask = (this->total + 15) & ~size_t(15);
-        total_mf = fmask + (((size_t)max_local * sizeof(uint16_t) + 15) & ~size_t(15));
+struct MfGeom {
+    static constexpr uint32_t JI_BYTES = 9 * TILE_ELEMS * sizeof(double);
+    static constexpr uint32_t DV_BYTES = TILE_ELEMS * sizeof(double);
+    static constexpr uint32_t TAN_BYTES = MF_TAN * TILE_ELEMS * sizeof(double);
+    static constexpr uint32_t STAGE_BYTES = JI_BYTES + DV_BYTES + TAN_BYTES;
+    static constexpr uint32_t LCONN_BYTES = NPE * TILE_ELEMS * sizeof(uint16_t);
+    static constexpr uint32_t INC_BYTES = NPE * TILE_ELEMS * sizeof(uint16_t);
+    static constexpr uint32_t FE_BYTES = 3 * NPE * TILE_ELEMS * sizeof(double);
+    // the two stages, and after the QP loop the element forces of the reduction
+    static constexpr uint32_t REGION0 = ((2 * STAGE_BYTES > FE_BYTES ? 2 * STAGE_BYTES : FE_BYTES) + 15u) & ~15u;
+    static_assert(STAGE_BYTES % 16 == 0 && LCONN_BYTES % 16 == 0 && INC_BYTES % 16 == 0, "bulk sizes");
+};
+
+// The product's shared memory: [stages | element forces][lconn][incidence][destinations]
+// [incidence ends][p (3 per local node)][fixed flags][barriers: two stages, the record].
+template <int NPE>
+struct MfLayout {
+    size_t lconn, inc, dst, iend, pvals, fmask, bar, total;
+    __host__ __device__ explicit MfLayout(int max_local) {
+        using G = MfGeom<NPE>;
+        auto al = [](size_t v) { return (v + 15) & ~size_t(15); };
+        lconn = G::REGION0;
+        inc = lconn + G::LCONN_BYTES;
+        dst = inc + G::INC_BYTES;
+        iend = al(dst + (size_t)max_local * sizeof(int));
+        pvals = al(iend + (size_t)max_local * sizeof(uint16_t));
+        fmask = al(pvals + 3 * (size_t)max_local * sizeof(double));
+        bar = al(fmask + (size_t)max_local * sizeof(uint16_t));
+        total = bar + 3 * sizeof(unsigned long long);
     }
 };
 
@@ -186,33 +227,63 @@ __device__ __forceinline__ void mf_tile_epilogue(const MfArgs& M, const double (
     asm volatile("griddepcontrol.launch_dependents;");
 }
 
-// One tile per block on the compact geometry stream (J^-1 and dV per QP, 10 values
-// instead of the 3 NPE + 1 of the per-node gradients): F = (dx/dxi) J^-1 and
-// dF = (dp/dxi) J^-1 from the staged positions and p through the barycentric
-// structure of the shape functions, the nodal forces from Q = dP J^-T (tet_dx_dxi_at
-// / tet_scatter).  The 10-value slices fit a double-buffered ring (a slice is read
-// into registers, then its stage is refilled two QPs ahead), so each tile keeps a
-// copy in flight while it computes.
+// F and S of every element and QP at the given positions, into the tangent stream
+// (once per solve).  One tile per block, one element per thread: dx/dxi through the
+// barycentric structure, F = (dx/dxi) J^-1, S from E.  Padding element slots have a
+// zero J^-1 and dV, so they contribute nothing to a product.
+template <int NPE, int NQP>
+__global__ void __launch_bounds__(TILE_ELEMS) k_mf_prep(MfArgs M) {
+    constexpr int TE = TILE_ELEMS;
+    const int tile = blockIdx.x, t = threadIdx.x;
+    const int pb = M.pad_off[tile];
+    int gid[NPE];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) gid[a] = M.pad_gid[pb + M.lconn[((size_t)tile * NPE + a) * TE + t]];
+    auto x = [&](int a, int d) -> double {
+        const int g = gid[a];
+        if (g < 0) return 0.0;
+        return d == 0 ? M.x[g] : (d == 1 ? M.y[g] : M.z[g]);
+    };
+#pragma unroll 1
+    for (int q = 0; q < NQP; ++q) {
+        const size_t sl = (size_t)tile * NQP + q;
+        double ji[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) ji[m] = M.ji[(sl * 9 + m) * TE + t];
+        const double Lq[4] = {M.qb.L[q][0], M.qb.L[q][1], M.qb.L[q][2], M.qb.L[q][3]};
+        double Gx[3][3], F[3][3], S[6];
+        tet_dx_dxi_at<double, NPE>(x, Lq, Gx);
+        mul_jinv(Gx, ji, F);
+        svk_stress_sym(F, M.lambda, M.mu, S);
+        double* out = M.tan + sl * MF_TAN * TE + t;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) out[(3 * i + j) * TE] = F[i][j];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) out[(9 + k) * TE] = S[k];
+    }
+}
+
+// K_bc p for one tile per block (see the file comment).  The QP slices fill a
+// double-buffered ring: a slice is read into registers, then its stage is refilled two
+// QPs ahead, so each tile keeps a copy in flight while it computes.
 template <int NPE, int NQP>
 __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_geo(MfArgs M, int* err) {
-    using G = TileGeoGeom<double, NPE>;
+    using G = MfGeom<NPE>;
     constexpr int TE = TILE_ELEMS;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ double red_sh[32];
     if (M.ctl->done) return;  // uniform: written by the previous kernel
     const int tile = blockIdx.x, t = threadIdx.x;
-    const int ML = M.max_local;
-    const MfGeoLayout<NPE> L(ML);
+    const MfLayout<NPE> L(M.max_local);
     unsigned char* stage0 = smem;
-    uint16_t* fmask = reinterpret_cast<uint16_t*>(smem + L.fmask);
     const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + L.lconn);
     const uint16_t* incs = reinterpret_cast<const uint16_t*>(smem + L.inc);
-    double* xs = reinterpret_cast<double*>(smem + L.pos);
-    double* ys = xs + ML;
-    double* zs = ys + ML;
     int* dsts = reinterpret_cast<int*>(smem + L.dst);
     uint16_t* iends = reinterpret_cast<uint16_t*>(smem + L.iend);
-    double* ps = reinterpret_cast<double*>(smem + L.vel);
+    double* ps = reinterpret_cast<double*>(smem + L.pvals);
+    uint16_t* fmask = reinterpret_cast<uint16_t*>(smem + L.fmask);
     double* fe = reinterpret_cast<double*>(smem);  // aliases the stages after the QP loop
     const uint32_t bar0 = smem_u32(smem + L.bar), bar_rec = bar0 + 16;
 
@@ -220,9 +291,11 @@ __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_geo(MfArgs M, int* err) {
         const uint32_t bar = bar0 + 8 * (q & 1);
         const uint32_t dst = smem_u32(stage0 + (size_t)(q & 1) * G::STAGE_BYTES);
         const uint32_t extra = (q == 0) ? G::LCONN_BYTES + G::INC_BYTES : 0;
+        const size_t sl = (size_t)tile * NQP + q;
         mbar_expect_tx(bar, G::STAGE_BYTES + extra);
-        bulk_g2s(dst, M.ji + ((size_t)tile * NQP + q) * 9 * TE, G::JI_BYTES, bar);
-        bulk_g2s(dst + G::JI_BYTES, M.dv + ((size_t)tile * NQP + q) * TE, G::DV_BYTES, bar);
+        bulk_g2s(dst, M.ji + sl * 9 * TE, G::JI_BYTES, bar);
+        bulk_g2s(dst + G::JI_BYTES, M.dv + sl * TE, G::DV_BYTES, bar);
+        bulk_g2s(dst + G::JI_BYTES + G::DV_BYTES, M.tan + sl * MF_TAN * TE, G::TAN_BYTES, bar);
         if (q == 0) {
             bulk_g2s(smem_u32(lcs), M.lconn + (size_t)tile * NPE * TE, G::LCONN_BYTES, bar);
             bulk_g2s(smem_u32(incs), M.inc + (size_t)tile * NPE * TE, G::INC_BYTES, bar);
@@ -238,11 +311,8 @@ __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_geo(MfArgs M, int* err) {
         issue(0);
         if (NQP > 1) issue(1);
         const int np = M.pad_off[tile + 1] - pb;
-        // positions, destinations, incidence ends, p (3 doubles) and fixed flags per slot
-        mbar_expect_tx(bar_rec, (uint32_t)np * (6 * sizeof(double) + sizeof(int) + 2 * sizeof(uint16_t)));
-        bulk_g2s(smem_u32(xs), M.sx + pb, np * sizeof(double), bar_rec);
-        bulk_g2s(smem_u32(ys), M.sy + pb, np * sizeof(double), bar_rec);
-        bulk_g2s(smem_u32(zs), M.sz + pb, np * sizeof(double), bar_rec);
+        // destinations, incidence ends, fixed flags and p (3 doubles) per slot
+        mbar_expect_tx(bar_rec, (uint32_t)np * (sizeof(int) + 2 * sizeof(uint16_t) + 3 * sizeof(double)));
         bulk_g2s(smem_u32(dsts), M.pad_dst + pb, np * sizeof(int), bar_rec);
         bulk_g2s(smem_u32(iends), M.pad_iend + pb, np * sizeof(uint16_t), bar_rec);
         bulk_g2s(smem_u32(fmask), M.pfix + pb, np * sizeof(uint16_t), bar_rec);
@@ -254,23 +324,21 @@ __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_geo(MfArgs M, int* err) {
     __syncthreads();  // barriers initialised
     if (!mbar_wait(bar_rec, 0)) atomicExch(err, 3);
 
-    int lc[NPE];
     double f[NPE][3];
 #pragma unroll
     for (int a = 0; a < NPE; ++a) f[a][0] = f[a][1] = f[a][2] = 0.0;
 #pragma unroll 1
     for (int q = 0; q < NQP; ++q) {
         if (!mbar_wait(bar0 + 8 * (q & 1), (q >> 1) & 1)) atomicExch(err, 3);
-        const unsigned char* st = stage0 + (size_t)(q & 1) * G::STAGE_BYTES;
-        const double* js = reinterpret_cast<const double*>(st);
-        if (q == 0) {
+        const double* st = reinterpret_cast<const double*>(stage0 + (size_t)(q & 1) * G::STAGE_BYTES);
+        double ji[9], F[3][3], S[6];
 #pragma unroll
-            for (int a = 0; a < NPE; ++a) lc[a] = lcs[a * TE + t];
-        }
-        double ji[9];
+        for (int m = 0; m < 9; ++m) ji[m] = st[m * TE + t];
+        const double dv = st[9 * TE + t];
 #pragma unroll
-        for (int m = 0; m < 9; ++m) ji[m] = js[m * TE + t];
-        const double dv = reinterpret_cast<const double*>(st + G::JI_BYTES)[t];
+        for (int m = 0; m < 9; ++m) F[m / 3][m % 3] = st[(10 + m) * TE + t];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) S[k] = st[(19 + k) * TE + t];
         if (q + 2 < NQP) {
             // every thread's generic reads of this stage precede the bulk refill
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -278,14 +346,10 @@ __global__ void __launch_bounds__(TILE_ELEMS, 3) k_mf_geo(MfArgs M, int* err) {
             if (t == 0) issue(q + 2);
         }
         const double Lq[4] = {M.qb.L[q][0], M.qb.L[q][1], M.qb.L[q][2], M.qb.L[q][3]};
-        double Gx[3][3], Gp[3][3], F[3][3], Hp[3][3];
-        tet_dx_dxi_at<double, NPE>(
-            [&](int a, int d) { return d == 0 ? xs[lc[a]] : (d == 1 ? ys[lc[a]] : zs[lc[a]]); }, Lq, Gx);
-        tet_dx_dxi_at<double, NPE>([&](int a, int d) { return ps[3 * lc[a] + d]; }, Lq, Gp);
-        mul_jinv(Gx, ji, F);
+        double Gp[3][3], Hp[3][3], dP[3][3], Q[3][3];
+        tet_dx_dxi_at<double, NPE>([&](int a, int d) { return ps[3 * lcs[a * TE + t] + d]; }, Lq, Gp);
         mul_jinv(Gp, ji, Hp);
-        double dP[3][3], Q[3][3];
-        svk_tangent_dp(F, Hp, M.lambda, M.mu, dv, dP);
+        svk_tangent_dp(F, S, Hp, M.lambda, M.mu, dv, dP);
         mul_jinv_t(dP, ji, Q);
         tet_scatter<double, NPE>(Q, Lq, [&](int a, int d, double v) { f[a][d] += v; });
     }

@@ -77,6 +77,7 @@ struct tlfea_solver_s {
     double* mf_part = nullptr;  // matrix-free p.q partials: one per tile, then one per combine block
     double* mf_prec = nullptr;     // p in the node record's tile order (3 per padded slot)
     uint16_t* mf_pfix = nullptr;   // fixed-DOF flags per padded slot
+    double* mf_tan = nullptr;      // F and S per element QP at the last solve's positions
     double *xk = nullptr, *yk = nullptr, *zk = nullptr;  // positions of the last matrix-free solve
     int cg_blocks = 0;
     cudaGraphExec_t cg_graph = nullptr;
