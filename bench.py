@@ -17,7 +17,8 @@ The JSON line carries
   e2e       the same through the public API with host buffers: per step the
             external force and reference positions go host->device and the
             solved positions come back;
-  roofline  the dominant kernel of the step (the CG's matrix-free K p, k_mf_geo);
+  roofline  the dominant kernel of the step (the CG's matrix-free K p: gather,
+            k_mf_geo, combine);
   elem_force  the fused element-force kernel (FP32 and FP64) in GB/s of the
             algorithmic bytes E*(4*NPE + QP*NPE*3*s + QP*s) + N*6*s;
   gpu_reference the reference's own CUDA build (its unchanged sources compiled
@@ -61,7 +62,7 @@ CG_ITERS_CFG2 = 7071
 # both scale with the elements), so the 200x20x20 traffic is those ratios x its bytes.
 SPMV_TRAFFIC_RATIO = 1.026
 FORCE_TRAFFIC_RATIO = {"fp32": 1.118, "fp64": 1.073}
-MF_TRAFFIC_RATIO = 1.143
+MF_TRAFFIC_RATIO = 1.121
 
 
 def progress(msg):
@@ -171,18 +172,18 @@ def elem_force_bytes_compact(E, N, npe, nqp, s):
 
 
 def mf_apply_bytes(E, N, npe, nqp):
-    """Algorithmic bytes of one matrix-free K p: the FP64 compact geometry stream (J^-1
-    and dV, 10 values per QP), local connectivity and incidence (4 B per node slot), and
-    per node its position, p and q (FP64)."""
-    return E * (4 * npe + nqp * 10 * 8) + N * 3 * 8 * 3
+    """Algorithmic bytes of one matrix-free K p: per element and QP the FP64 compact
+    geometry (J^-1, dV) and the solve's tangent stream (F, S): 25 values; local
+    connectivity and incidence (4 B per node slot); per node p read and q written (FP64)."""
+    return E * (4 * npe + nqp * 25 * 8) + N * 3 * 8 * 2
 
 
 def mf_apply_flops(E, nqp):
-    """FP64 operations of one matrix-free K p per element and QP, counted from the
-    kernel's arithmetic: dx/dxi and dp/dxi (2 x 57), F and dF = G J^-1 (2 x 27 FMA),
-    symmetric E, dE, S, dS (66 + 24), dP (63), Q = dP J^-T (27 FMA), the nodal scatter (84);
+    """FP64 operations of one matrix-free K p, counted from the kernel's arithmetic per
+    element and QP: dp/dxi (57), dF = (dp/dxi) J^-1 (27 FMA), symmetric dE (42), dS (12),
+    dP = dF S + F dS scaled by dV (63), Q = dP J^-T (27 FMA), the nodal scatter (84);
     an FMA counts 2."""
-    per_qp_ops = 2 * 57 + 2 * 27 + 66 + 24 + 63 + 27 + 84
+    per_qp_ops = 57 + 27 + 42 + 12 + 63 + 27 + 84
     return E * nqp * per_qp_ops * 2
 
 
@@ -394,6 +395,27 @@ def kernels_only(args):
         torch.cuda.synchronize()
         print(json.dumps({"kernels_only": "mlp", "dims": [6, 256, 256, 256, 64], "batch": 512, "steps": 20}))
         net.Destroy()
+        return
+    if args.kernels_only == "nesterov":
+        # SyncedNesterov on the --mesh beam in per-phase launches: one warm-up solve,
+        # then 2 outer x 10 inner iterations at zero tolerances (FP64 element forces)
+        cfg = dict(CFG)
+        cfg["nx"], cfg["ny"], cfg["nz"] = (int(v) for v in (args.mesh or "200x20x20").split("x"))
+        x, y, z, conn, fixed, f = build_mesh(cfg)
+        el = setup_element(T, cfg, x, y, z, conn, fixed, f)
+        el.CalcMassMatrix()
+        el.CalcConstraintData()
+        el.ConvertToCSR_ConstraintJacT()
+        s = T.SyncedNesterovSolver(el, el.get_n_constraint())
+        s.Setup()
+        s.SetMode("phased")
+        for _ in range(2):
+            s.SetParameters(T.SyncedNesterovParams(1.0e-8, 1e14, 0.0, 0.0, 2, 10, 1.0e-3))
+            el.ResetPositions()
+            s.Solve()
+        torch.cuda.synchronize()
+        print(json.dumps({"kernels_only": "nesterov", "elements": int(conn.shape[0]), "nodes": int(len(x)),
+                          "inner_iters": s.GetStats()["inner_iters_total"]}))
         return
     if args.kernels_only == "gemm":
         # the MLP's tcgen05 product on its own at a size that fills the GPU:
@@ -1096,7 +1118,7 @@ def main():
     ap.add_argument("--kernel-reps", type=int, default=20)
     ap.add_argument("--gemm-size", type=int, default=8192, help="M = N = K of --kernels-only gemm")
     ap.add_argument("--cg-iters", type=int, default=120, help="iteration cap of --kernels-only cg")
-    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg", "batch", "batch-uneven", "steps", "mlp", "gemm"], default=None,
+    ap.add_argument("--kernels-only", choices=["force", "spmv", "cg", "batch", "batch-uneven", "steps", "mlp", "gemm", "nesterov"], default=None,
                     help="profiling case: set up, then launch only the named kernel a few times")
     ap.add_argument("--mesh", default=None, help="cells NXxNYxNZ (default 200x20x20)")
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")
@@ -1224,13 +1246,11 @@ def main():
     ms_mf = time_stream(torch, stream, lambda: solver.Apply(xin.data_ptr(), yout.data_ptr()), args.kernel_reps)
     b_mf = mf_apply_bytes(E, N, 10, 5)
     ach = b_mf / (ms_mf / 1e3) / 1e9
-    roofline = {"kernel": "k_mf_geo + k_mf_combine_dot", "bound": "hbm", "achieved": round(ach, 1), "peak": hbm,
+    roofline = {"kernel": "k_mf_gather + k_mf_geo + k_mf_combine_dot", "bound": "hbm", "achieved": round(ach, 1), "peak": hbm,
                 "unit": "GB/s", "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": int(b_mf),
-                "format": "matrix-free SVK tangent from the FP64 compact geometry stream (J^-1, dV per QP)",
+                "format": "matrix-free SVK tangent: per QP J^-1, dV and the solve's F, S (FP64), p per tile",
                 "ms": round(ms_mf, 4), "traffic": int(MF_TRAFFIC_RATIO * b_mf),
-                "fp64_tflops": round(mf_apply_flops(E, 5) / (ms_mf / 1e3) / 1e12, 2),
-                "note": "FP64-issue bound, not HBM-bound: the compact stream moves 2.5x fewer bytes than "
-                        "the per-node gradients, ncu shows DRAM 19% and the FP64 pipe 38% busy"}
+                "fp64_tflops": round(mf_apply_flops(E, 5) / (ms_mf / 1e3) / 1e12, 2)}
     # fused element force, FP32 and FP64
     ef = {}
     f_by_prec = {}
