@@ -755,8 +755,10 @@ def config2_more_legs(args, T, cfg):
             s.Solve()
             torch.cuda.synchronize()
             dtf = time.perf_counter() - t0
-            itf = max(1, s.GetStats()["inner_iters_total"])
-            fixed_it[mode] = {"inner_iters": itf, "ms_per_inner_iteration": round(1e3 * dtf / itf, 4)}
+            stf = s.GetStats()
+            itf = max(1, stf["inner_iters_total"])
+            fixed_it[mode] = {"inner_iters": itf, "ms_per_inner_iteration": round(1e3 * dtf / itf, 4),
+                              "gpu_ms_per_inner_iteration": round(stf["kernel_ms"] / itf, 4)}
         s.SetMode("auto")
         nes[prec]["fixed_60_iterations"] = fixed_it
         del s

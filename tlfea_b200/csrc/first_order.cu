@@ -803,15 +803,18 @@ template <typename R, int NPE, int NQP, bool DAMP, bool MR, bool MASS>
 static void fo_enqueue_slot(const tlfea_solver_s* s, const FOArgs& S, const TileArgs<R>& A, FOCtl* C,
                             cudaStream_t st) {
     const int gn = std::max(1, std::min(s->max_blocks, (S.N + FO_NODE_THREADS - 1) / FO_NODE_THREADS));
+    // the outer-step kernels do their work once per outer iteration and are no-ops in
+    // every inner slot: a small grid keeps the no-op launches short
+    const int go = std::min(gn, std::max(1, s->max_blocks / 8));  // two blocks per SM
     const size_t smem = tile_smem_bytes<R>(NPE, A.max_local, DAMP, MASS);
-    k_fo_outer_start<<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
+    k_fo_outer_start<<<go, FO_NODE_THREADS, 0, st>>>(S, C);
     k_fo_guess<R><<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
     k_fo_force<R, NPE, NQP, DAMP, MR, MASS><<<S.n_tiles, TILE_ELEMS, smem, st>>>(S, A, C);
     k_fo_grad<R, MASS><<<gn, FO_NODE_THREADS, 0, st>>>(S, A, C);
     if (S.kind == KIND_NESTEROV) k_fo_nesterov<<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
-    k_fo_outer_positions<R><<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
-    k_fo_outer_multipliers<<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
-    k_fo_final<R><<<gn, FO_NODE_THREADS, 0, st>>>(S, C);
+    k_fo_outer_positions<R><<<go, FO_NODE_THREADS, 0, st>>>(S, C);
+    k_fo_outer_multipliers<<<go, FO_NODE_THREADS, 0, st>>>(S, C);
+    k_fo_final<R><<<go, FO_NODE_THREADS, 0, st>>>(S, C);
 }
 
 // One Solve() in per-phase launches: the start kernel, then graph chunks of slots

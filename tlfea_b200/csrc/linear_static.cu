@@ -556,8 +556,9 @@ static int launch_mf_apply(tlfea_solver_s* s, cudaStream_t st, const double* p, 
     const MfArgs M = mf_args(s, p, q, ctl);
     const size_t smem = mf_smem(s);
     const long long n_pad = el->tl.n_pad;
-    k_mf_gather<<<(unsigned)((n_pad + 255) / 256), 256, 0, st>>>(n_pad, el->tl.pad_gid, s->mf_pfix, p, s->mf_prec,
-                                                                  ctl);
+    const long long per_block = 256LL * MF_GATHER_ILP;
+    k_mf_gather<<<(unsigned)((n_pad + per_block - 1) / per_block), 256, 0, st>>>(n_pad, el->tl.pad_gid, s->mf_pfix, p,
+                                                                                s->mf_prec, ctl);
     if (cudaGetLastError() != cudaSuccess) return TLFEA_CUDA_ERROR;
     // the tile kernel and the combine are programmatic dependents: each starts while its
     // predecessor drains and waits (griddepcontrol.wait) before reading its results

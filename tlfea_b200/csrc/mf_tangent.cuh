@@ -156,24 +156,39 @@ __global__ void k_mf_fixbits(long long n_pad, const int* __restrict__ pad_gid,
 
 // p in the node record's tile order, per padded slot its node's three components with
 // the eliminated DOFs zeroed (their columns dropped from K p), padding 0: a streaming
-// gather over all slots, so the product's tiles bulk-copy p like the positions.
+// gather over all slots, so the product's tiles bulk-copy p like the other record
+// arrays.  Each thread takes MF_GATHER_ILP slots (blockDim apart, so every load and
+// store stays coalesced across the warp) and issues all their loads before any use.
+constexpr int MF_GATHER_ILP = 4;
 __global__ void __launch_bounds__(256) k_mf_gather(long long n_pad, const int* __restrict__ pad_gid,
                                                    const uint16_t* __restrict__ pfix, const double* __restrict__ p,
                                                    double* __restrict__ prec, const CgCtl* __restrict__ ctl) {
     // the tile kernel (a programmatic dependent) may start its own copies meanwhile
     asm volatile("griddepcontrol.launch_dependents;");
     if (ctl->done) return;
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= n_pad) return;
-    const int g = pad_gid[i];
-    const unsigned m = pfix[i];
-    double v[3] = {0.0, 0.0, 0.0};
-    if (g >= 0) {
+    const long long base = (long long)blockIdx.x * blockDim.x * MF_GATHER_ILP + threadIdx.x;
+    int g[MF_GATHER_ILP];
+    unsigned m[MF_GATHER_ILP];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) v[d] = ((m >> d) & 1) ? 0.0 : p[3 * (size_t)g + d];
+    for (int j = 0; j < MF_GATHER_ILP; ++j) {
+        const long long i = base + (long long)j * blockDim.x;
+        g[j] = (i < n_pad) ? pad_gid[i] : -1;
+        m[j] = (i < n_pad) ? pfix[i] : 0u;
     }
+    double v[MF_GATHER_ILP][3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) prec[3 * i + d] = v[d];
+    for (int j = 0; j < MF_GATHER_ILP; ++j)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            v[j][d] = (g[j] >= 0 && !((m[j] >> d) & 1)) ? p[3 * (size_t)g[j] + d] : 0.0;
+#pragma unroll
+    for (int j = 0; j < MF_GATHER_ILP; ++j) {
+        const long long i = base + (long long)j * blockDim.x;
+        if (i < n_pad) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) prec[3 * i + d] = v[j][d];
+        }
+    }
 }
 
 // The tile's element forces f (this thread's element) reduced per node in the
