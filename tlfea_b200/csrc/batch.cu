@@ -180,12 +180,18 @@ __device__ __forceinline__ void linear_tile(const BatchArgs<R>& A, int item, con
     }
     const int lb = A.node_off[tile], nl = A.node_off[tile + 1] - lb;
     for (int k = t; k < NPE * TE; k += TE) incs[k] = A.inc[(size_t)tile * TE * NPE + k];
-    // p relative to the tile's first node, differenced in FP64: the gradients
+    // FP32: p relative to the tile's first node, differenced in FP64: the gradients
     // sum to zero over an element's nodes, so K p is unchanged, but the FP32
     // copy no longer carries the (large, cancelling) common part of p and H =
-    // sum_a p_a (x) grad N_a keeps FP32 accuracy relative to the local variation
-    const int g0 = noff + A.ln_gid[lb];
-    const double r0 = p[3 * g0 + 0], r1 = p[3 * g0 + 1], r2 = p[3 * g0 + 2];
+    // sum_a p_a (x) grad N_a keeps FP32 accuracy relative to the local variation.
+    // FP64 stages p as it is (no dependent loads before the gathers).
+    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+    if constexpr (sizeof(R) == 4) {
+        const int g0 = noff + A.ln_gid[lb];
+        r0 = p[3 * g0 + 0];
+        r1 = p[3 * g0 + 1];
+        r2 = p[3 * g0 + 2];
+    }
 #pragma unroll 4
     for (int ln = t; ln < nl; ln += TE) {  // unrolled: several nodes' gathers in flight at once
         const int gid = noff + A.ln_gid[lb + ln];
