@@ -661,8 +661,20 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
 
     const int lb = A.node_off[tile];
     const int nl = A.node_off[tile + 1] - lb;
+    if (MODE == TILE_FORCE && t == 0) {
+        // the tile's J^-1 and dV stream (every QP) into L2 while the node values are
+        // staged, so the per-QP loads below hit L2 instead of each waiting on DRAM
+        // (16-byte aligned, sizes multiples of 16 bytes)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.ji + (size_t)tile * NQP * 9 * TE),
+                     "r"((uint32_t)(NQP * 9 * TE * sizeof(R)))
+                     : "memory");
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.dv + (size_t)tile * NQP * TE),
+                     "r"((uint32_t)(NQP * TE * sizeof(R)))
+                     : "memory");
+    }
     if (MODE != TILE_FORCE_FROM_P) {
-        for (int ln = t; ln < nl; ln += TE) {
+#pragma unroll 4
+        for (int ln = t; ln < nl; ln += TE) {  // unrolled: several nodes' gathers in flight at once
             const int gid = A.ln_gid[lb + ln];
             stage_pos(A, gid, xs[ln], ys[ln], zs[ln]);
             if (DAMP) {

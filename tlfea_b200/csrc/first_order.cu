@@ -584,8 +584,11 @@ __global__ void __launch_bounds__(FO_NODE_THREADS) k_fo_guess(FOArgs S, const FO
 
 // P2: internal force, one tile per block (the fused tile routine), and the
 // constraint values at the new positions.
+// SVK without damping fits 3 blocks per SM in FP64 (168 registers) and 4 in FP32
+// (128); the damped and Mooney-Rivlin variants keep the registers they need.
 template <typename R, int NPE, int NQP, bool DAMP, bool MR, bool MASS>
-__global__ void __launch_bounds__(TILE_ELEMS) k_fo_force(FOArgs S, TileArgs<R> A, const FOCtl* C) {
+__global__ void __launch_bounds__(TILE_ELEMS, (DAMP || MR) ? 1 : (sizeof(R) == 4 ? 4 : 3))
+    k_fo_force(FOArgs S, TileArgs<R> A, const FOCtl* C) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (__ldcg(&C->mode) != FO_INNER) return;
     process_tile<R, NPE, NQP, TILE_FORCE, DAMP, MR, MASS>(A, blockIdx.x, smem);
