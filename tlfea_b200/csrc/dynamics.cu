@@ -153,9 +153,10 @@ __global__ void k_dyn_start(DynArgs D) {
     D.z[o] = D.zp[o] + D.dt * D.vg[b3 + 2];
 }
 
-// Element forces (and the element-wise mass term) of one tile of one sequence.
+// Element forces (and the element-wise mass term) of one tile of one sequence.  TET10
+// without damping: 3 blocks per SM (168 registers); the others keep what they need.
 template <int NPE, int NQP, bool DAMP>
-__global__ void __launch_bounds__(TILE_ELEMS) k_dyn_force(DynArgs D, TileArgs<double> A) {
+__global__ void __launch_bounds__(TILE_ELEMS, (DAMP || NPE != 10) ? 1 : 3) k_dyn_force(DynArgs D, TileArgs<double> A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int s = blockIdx.x % D.B, tile = blockIdx.x / D.B;
     const int st = D.done[s];
@@ -166,16 +167,10 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_dyn_force(DynArgs D, TileArgs<do
         return;
     }
     const size_t oN = (size_t)s * D.N, o3 = 3 * oN;
-    A.px = D.x + oN;
-    A.py = D.y + oN;
-    A.pz = D.z + oN;
-    A.v = D.vg + o3;
-    A.vp = D.vp + o3;
-    A.f_out = D.f + o3;
-    A.partial = D.partial + (size_t)s * 3 * D.n_pslots;
-    A.lambda = D.lam_s[s];
-    A.mu = D.mu_s[s];
-    process_tile<double, NPE, NQP, TILE_FORCE, DAMP, false, true>(A, tile, smem);
+    // this sequence's arrays and material; A itself stays the (unmodified) kernel parameter
+    const TileSeq<double> sq{D.x + oN, D.y + oN, D.z + oN, D.vg + o3, D.vp + o3, D.f + o3,
+                             D.partial + (size_t)s * 3 * D.n_pslots, D.lam_s[s], D.mu_s[s]};
+    process_tile<double, NPE, NQP, TILE_FORCE, DAMP, false, true, true>(A, tile, smem, &sq);
 }
 
 // Node force, gradient, ||g_free||^2 partials; the last block of a sequence folds them and

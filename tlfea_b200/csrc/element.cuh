@@ -523,7 +523,8 @@ __device__ __forceinline__ void mooney_rivlin_tangent_a(const double F[3][3], do
 // I + H, the cancellation-free form); with DAMP the Kelvin-Voigt term of the
 // velocity gradient Fd is added.
 template <typename R, bool DAMP, bool MR = false>
-__device__ __forceinline__ void tile_stress(const R H[3][3], const R Fd[3][3], const TileArgs<R>& A, R P[3][3]) {
+__device__ __forceinline__ void tile_stress(const R H[3][3], const R Fd[3][3], const TileArgs<R>& A, R P[3][3],
+                                            R lam, R mu) {
     if constexpr (MR) {
         // Mooney-Rivlin in FP64 whatever R is (FP32 mode: F = I + H formed in FP64)
         double F64[3][3], P64[3][3];
@@ -538,7 +539,7 @@ __device__ __forceinline__ void tile_stress(const R H[3][3], const R Fd[3][3], c
 #pragma unroll
             for (int j = 0; j < 3; ++j) P[i][j] = R(P64[i][j]);
     } else if constexpr (sizeof(R) == 8) {
-        svk_p_reference(H, A.lambda, A.mu, P);
+        svk_p_reference(H, lam, mu, P);
     } else {
         R Em[3][3];
 #pragma unroll
@@ -555,7 +556,7 @@ __device__ __forceinline__ void tile_stress(const R H[3][3], const R Fd[3][3], c
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
-            for (int j = 0; j < 3; ++j) Sm[i][j] = R(2) * A.mu * Em[i][j] + (i == j ? A.lambda * trE : R(0));
+            for (int j = 0; j < 3; ++j) Sm[i][j] = R(2) * mu * Em[i][j] + (i == j ? lam * trE : R(0));
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -624,7 +625,7 @@ __device__ __forceinline__ void mass_qp(const R (&wa)[NPE][3], const R Lq[4], R 
 
 template <typename R, int NPE, bool DAMP, bool FIRST, bool MR = false>
 __device__ __forceinline__ void compact_qp(const TileArgs<R>& A, const R (&xa)[NPE][3], const R (&va)[NPE][3],
-                                           const R ji[9], R dv, const R Lq[4], R (&f)[NPE][3]) {
+                                           const R ji[9], R dv, const R Lq[4], R (&f)[NPE][3], R lam, R mu) {
     R Gx[3][3], H[3][3], Fd[3][3], P[3][3], Q[3][3];
     tet_dx_dxi<R, NPE>(xa, Lq, Gx);
     mul_jinv(Gx, ji, H);
@@ -633,7 +634,7 @@ __device__ __forceinline__ void compact_qp(const TileArgs<R>& A, const R (&xa)[N
         tet_dx_dxi<R, NPE>(va, Lq, Gv);
         mul_jinv(Gv, ji, Fd);
     }
-    tile_stress<R, DAMP, MR>(H, Fd, A, P);
+    tile_stress<R, DAMP, MR>(H, Fd, A, P, lam, mu);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -645,12 +646,28 @@ __device__ __forceinline__ void compact_qp(const TileArgs<R>& A, const R (&xa)[N
         tet_scatter<R, NPE>(Q, Lq, [&](int a, int d, R v) { f[a][d] += v; });
 }
 
+// Per-sequence arrays and material of the batched dynamics (FP64): process_tile with
+// SEQ reads these instead of A's, so A itself stays an unmodified kernel parameter.
+template <typename R>
+struct TileSeq {
+    const double *px, *py, *pz;  // positions
+    const double *v, *vp;        // velocities (the mass term's v and v_prev; v also for damping)
+    R* f_out;
+    R* partial;
+    R lambda, mu;
+};
+
 // MASS (force mode only): the element-wise mass term M (v - v_prev) / dt of the
 // first-order solvers' gradient is added to the nodal forces (see mass_qp).
-template <typename R, int NPE, int NQP, int MODE, bool DAMP, bool MR = false, bool MASS = false>
-__device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, unsigned char* smem_raw) {
+template <typename R, int NPE, int NQP, int MODE, bool DAMP, bool MR = false, bool MASS = false, bool SEQ = false>
+__device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, unsigned char* smem_raw,
+                                             const TileSeq<R>* sq = nullptr) {
+    static_assert(!SEQ || (sizeof(R) == 8 && MODE == TILE_FORCE), "per-sequence override: FP64 forces only");
     constexpr int TE = TILE_ELEMS;
     const int t = threadIdx.x;
+    const R lam = SEQ ? sq->lambda : A.lambda, mu = SEQ ? sq->mu : A.mu;
+    const double* vsrc = SEQ ? sq->v : A.v;
+    const double* vpsrc = SEQ ? sq->vp : A.vp;
     // [x y z (FP64)][velocities (FP64, DAMP)][mass term (MASS)][element forces]
     double* xs = reinterpret_cast<double*>(smem_raw);
     double* ys = xs + A.max_local;
@@ -676,15 +693,21 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
 #pragma unroll 4
         for (int ln = t; ln < nl; ln += TE) {  // unrolled: several nodes' gathers in flight at once
             const int gid = A.ln_gid[lb + ln];
-            stage_pos(A, gid, xs[ln], ys[ln], zs[ln]);
+            if constexpr (SEQ) {
+                xs[ln] = sq->px[gid];
+                ys[ln] = sq->py[gid];
+                zs[ln] = sq->pz[gid];
+            } else {
+                stage_pos(A, gid, xs[ln], ys[ln], zs[ln]);
+            }
             if (DAMP) {
-                vs[3 * ln + 0] = A.v[3 * gid + 0];
-                vs[3 * ln + 1] = A.v[3 * gid + 1];
-                vs[3 * ln + 2] = A.v[3 * gid + 2];
+                vs[3 * ln + 0] = vsrc[3 * gid + 0];
+                vs[3 * ln + 1] = vsrc[3 * gid + 1];
+                vs[3 * ln + 2] = vsrc[3 * gid + 2];
             }
             if (MASS) {
 #pragma unroll
-                for (int d = 0; d < 3; ++d) ws[3 * ln + d] = R((A.v[3 * gid + d] - A.vp[3 * gid + d]) * A.mass_scale);
+                for (int d = 0; d < 3; ++d) ws[3 * ln + d] = R((vsrc[3 * gid + d] - vpsrc[3 * gid + d]) * A.mass_scale);
             }
         }
     }
@@ -714,7 +737,7 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
             element_nodes<R, NPE>(xs, ys, zs, lc, xa);
             if (DAMP) element_velocities<R, NPE>(vs, lc, va);
         }
-        compact_qp<R, NPE, DAMP, false, MR>(A, xa, va, ji, dv, Lq, f);
+        compact_qp<R, NPE, DAMP, false, MR>(A, xa, va, ji, dv, Lq, f, lam, mu);
         if constexpr (MASS) {
             R wa[NPE][3];
 #pragma unroll
@@ -767,7 +790,7 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
 #pragma unroll
                         for (int j = 0; j < 3; ++j) Fd[i][j] += va[a][i] * g[a][j];
             }
-            tile_stress<R, DAMP, MR>(H, Fd, A, P);
+            tile_stress<R, DAMP, MR>(H, Fd, A, P, lam, mu);
         }
 
         if constexpr (MODE == TILE_STORE_P) {
@@ -799,6 +822,8 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
     __syncthreads();
 
     const uint16_t* inc = A.inc + (size_t)tile * TE * NPE;
+    R* const f_out = SEQ ? sq->f_out : A.f_out;
+    R* const part = SEQ ? sq->partial : A.partial;
     for (int ln = t; ln < nl; ln += TE) {
         const int beg = ln ? A.ln_inc_end[lb + ln - 1] : 0;
         const int end = A.ln_inc_end[lb + ln];
@@ -814,18 +839,18 @@ __device__ __forceinline__ void process_tile(const TileArgs<R>& A, int tile, uns
         if (ps < 0) {
             const int gid = A.ln_gid[lb + ln];
             if (MODE == TILE_FORCE_FROM_P) {
-                A.f_out[3 * gid + 0] += s0;
-                A.f_out[3 * gid + 1] += s1;
-                A.f_out[3 * gid + 2] += s2;
+                f_out[3 * gid + 0] += s0;
+                f_out[3 * gid + 1] += s1;
+                f_out[3 * gid + 2] += s2;
             } else {
-                A.f_out[3 * gid + 0] = s0;
-                A.f_out[3 * gid + 1] = s1;
-                A.f_out[3 * gid + 2] = s2;
+                f_out[3 * gid + 0] = s0;
+                f_out[3 * gid + 1] = s1;
+                f_out[3 * gid + 2] = s2;
             }
         } else {
-            A.partial[3 * ps + 0] = s0;
-            A.partial[3 * ps + 1] = s1;
-            A.partial[3 * ps + 2] = s2;
+            part[3 * ps + 0] = s0;
+            part[3 * ps + 1] = s1;
+            part[3 * ps + 2] = s2;
         }
     }
     }  // MODE != TILE_STORE_P

@@ -584,10 +584,10 @@ __global__ void __launch_bounds__(FO_NODE_THREADS) k_fo_guess(FOArgs S, const FO
 
 // P2: internal force, one tile per block (the fused tile routine), and the
 // constraint values at the new positions.
-// SVK without damping fits 3 blocks per SM in FP64 (168 registers) and 4 in FP32
-// (128); the damped and Mooney-Rivlin variants keep the registers they need.
+// TET10 SVK without damping fits 3 blocks per SM in FP64 (168 registers) and 4 in
+// FP32 (128); the other variants keep the registers they need.
 template <typename R, int NPE, int NQP, bool DAMP, bool MR, bool MASS>
-__global__ void __launch_bounds__(TILE_ELEMS, (DAMP || MR) ? 1 : (sizeof(R) == 4 ? 4 : 3))
+__global__ void __launch_bounds__(TILE_ELEMS, (DAMP || MR || NPE != 10) ? 1 : (sizeof(R) == 4 ? 4 : 3))
     k_fo_force(FOArgs S, TileArgs<R> A, const FOCtl* C) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (__ldcg(&C->mode) != FO_INNER) return;

@@ -567,7 +567,8 @@ __global__ void __launch_bounds__(TILE_ELEMS, sizeof(R) == 4 ? 4 : 3) k_tile_for
                     H[i][j] = h2[i][j].x + h2[i][j].y;
                     Fd[i][j] = fd2[i][j].x + fd2[i][j].y;
                 }
-            tile_stress<float, DAMP, false>(H, Fd, reinterpret_cast<const TileArgs<float>&>(A), P);
+            tile_stress<float, DAMP, false>(H, Fd, reinterpret_cast<const TileArgs<float>&>(A), P, float(A.lambda),
+                                            float(A.mu));
             // f_a += (P dV) grad_a   (FEAT10DataFunc.cuh:417-449), two nodes per instruction
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
@@ -823,9 +824,9 @@ __global__ void __launch_bounds__(TILE_ELEMS) k_tile_force_geo(TileArgs<R> A, in
         // F (FP64) or H (FP32), the stress, f_a (+)= (dV P J^-T) dN_a/dxi
         // (FEAT10DataFunc.cuh:417-449 with gradN = J^-T dN/dxi)
         if (q == 0)
-            compact_qp<R, NPE, DAMP, true, MR>(A, xa, va, ji, dv, Lq, f);
+            compact_qp<R, NPE, DAMP, true, MR>(A, xa, va, ji, dv, Lq, f, A.lambda, A.mu);
         else
-            compact_qp<R, NPE, DAMP, false, MR>(A, xa, va, ji, dv, Lq, f);
+            compact_qp<R, NPE, DAMP, false, MR>(A, xa, va, ji, dv, Lq, f, A.lambda, A.mu);
     }
     __syncthreads();  // every thread is done with the stages the force table reuses
 #pragma unroll
