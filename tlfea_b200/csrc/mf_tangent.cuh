@@ -1,6 +1,6 @@
 // mf_tangent.cuh -- the LinearStaticSolver's K p without assembling K (new: the
 // reference assembles K, LinearStaticSolver.cu:196-263, and multiplies it with
-// cuSPARSE).  K is the SVK tangent at the current positions (the blocks of
+// cuSPARSE).  K is the SVK tangent at the solve's positions (the blocks of
 // compute_hessian_assemble_csr, FEAT10DataFunc.cuh:512-684 / SVK.cuh:41-67), so
 // K p = sum over elements and QPs of dP[dF] gradN_a dV with dF = sum_a p_a (x) gradN_a,
 // dP = dF S + F dS, S = lambda tr(E) I + 2 mu E, E = (F^T F - I) / 2,
