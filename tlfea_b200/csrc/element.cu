@@ -827,19 +827,6 @@ __global__ void k_stage_refresh(long long n, const int* __restrict__ gid, const 
     }
 }
 
-// The node record's values from the given FP64 positions (not the element's): the
-// matrix-free stiffness product at the positions of a past solve.  Tags the record as
-// holding them (content 3), which the force kernels treat as stale.
-int element_stage_positions(tlfea_element_s* h, const double* x, const double* y, const double* z) {
-    const long long n = h->tl.n_pad;
-    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
-    k_stage_refresh<<<blocks, 256, 0, h->stream>>>(n, h->tl.pad_gid, x, y, z, nullptr, nullptr, nullptr, 0, h->tl.sx,
-                                                   h->tl.sy, h->tl.sz);
-    TLFEA_CHECK_LAUNCH();
-    h->stage_content = 3;
-    return TLFEA_OK;
-}
-
 // Rebuild the tile-ordered node record for the precision about to be evaluated, after
 // a change of positions (or every time, once the positions' pointers are exposed).
 int element_refresh_record(tlfea_element_s* h, bool fp32) {

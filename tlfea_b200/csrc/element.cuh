@@ -899,8 +899,7 @@ struct tlfea_element_s {
     double* u64 = nullptr;  // interleaved x - X0 for the FP32 force (refreshed when positions change)
     bool u_dirty = true;
     // the tile-ordered node record (Tiling::sx/sy/sz): 0 = stale, 1 = FP64 positions,
-    // 2 = displacements x - X0 (FP32 mode), 3 = the positions of the last matrix-free
-    // linear solve; stale again whenever the positions change
+    // 2 = displacements x - X0 (FP32 mode); stale again whenever the positions change
     int stage_content = 0;
     // set once a caller has taken the positions' device pointers: it may write them at
     // any time, so the derived records are rebuilt before every evaluation
@@ -961,8 +960,6 @@ int element_force(tlfea_element_s* h, const double* d_v, bool fp32);
 int element_refresh_u64(tlfea_element_s* h);
 // Rebuild the tile-ordered node record (FP64 positions, or FP32 mode displacements) if stale.
 int element_refresh_record(tlfea_element_s* h, bool fp32);
-// The node record from given FP64 positions (marks it stale for the force kernels).
-int element_stage_positions(tlfea_element_s* h, const double* x, const double* y, const double* z);
 
 // Barycentric coordinates of the element's quadrature points.
 inline QpBary qp_bary(const tlfea_element_s* h) {
