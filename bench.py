@@ -360,9 +360,13 @@ def setup_element(T, cfg, x, y, z, conn, fixed, f):
 
 
 def kernels_only(args):
-    """Profiling case on the --mesh beam: the fused element force (2 x FP32 then
-    2 x FP64), the CG SpMV (assembly, a 5-iteration solve, then 3 applies), or
-    the benchmark solve capped at --cg-iters iterations."""
+    """A small profiling case per --kernels-only value: on the --mesh beam the fused
+    element force (force: 2 x FP32 then 2 x FP64), the CG operator (spmv: a 5-iteration
+    solve, then 3 applies), the benchmark solve capped at --cg-iters iterations (cg), or
+    SyncedNesterov in per-phase launches (nesterov); the batched CG (batch: shared mesh,
+    batch-uneven: uneven instances), the persistent first-order solver (steps), the
+    warm-start network's training step (mlp) or its BF16 product alone (gemm,
+    --gemm-size cubed)."""
     import torch
     import tlfea_b200 as T
 
@@ -378,6 +382,8 @@ def kernels_only(args):
         from tlfea_b200 import warmstart as W
 
         fm = W.FixedMeshCases(40, 8, 8, batch=64)
+        if args.batch_mode != "auto":
+            fm.solver.SetMode(args.batch_mode)
         fm.solve(W.sample_cases(64, seed=5), tol=1e-12, max_iter=10)
         torch.cuda.synchronize()
         print(json.dumps({"kernels_only": "batch", "cases": 64, "iterations": 10}))
@@ -490,6 +496,7 @@ def kernels_only(args):
         del s
     else:
         s = T.LinearStaticSolver(el, cfg["tol"], 5)
+        s.SetOperator(args.operator)
         s.Solve()
         xin = torch.randn(3 * len(x), dtype=torch.float64, device="cuda")
         yout = torch.empty_like(xin)
@@ -1118,6 +1125,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-gpu-ref", action="store_true", help="skip the reference's own CUDA build leg")
     ap.add_argument("--kernel-reps", type=int, default=20)
+    ap.add_argument("--operator", default="auto", choices=["auto", "assembled", "matrix-free"],
+                    help="K operator of --kernels-only spmv")
+    ap.add_argument("--batch-mode", default="auto", choices=["auto", "phased", "persistent"],
+                    help="launch mode of --kernels-only batch")
     ap.add_argument("--gemm-size", type=int, default=8192, help="M = N = K of --kernels-only gemm")
     ap.add_argument("--cg-iters", type=int, default=120, help="iteration cap of --kernels-only cg")
     ap.add_argument("--kernels-only", choices=["force", "spmv", "cg", "batch", "batch-uneven", "steps", "mlp", "gemm", "nesterov"], default=None,
