@@ -28,6 +28,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -275,11 +276,15 @@ static int gemm_tile_n(int M, int N, int sms) {
 
 template <int BN>
 static int gemm_launch_bn(const GemmArgs& g, const CUtensorMap& ta, const CUtensorMap& tb, cudaStream_t st) {
-    static bool configured = false;
-    if (!configured) {
+    // the shared-memory limit is a per-device attribute of the function: set it once per device
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    TLFEA_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(configured.load() & bit)) {
         TLFEA_CUDA(cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)GemmGeom<BN>::SMEM));
-        configured = true;
+        configured.fetch_or(bit);
     }
     const unsigned tiles = (unsigned)(((g.M + MLP_TM - 1) / MLP_TM) * ((g.N + BN - 1) / BN));
     k_gemm_bf16<BN><<<tiles, 128, GemmGeom<BN>::SMEM, st>>>(ta, tb, g);
