@@ -29,7 +29,8 @@ The JSON line carries
 --impl reference times the reference's own CUDA build on this workload (the
 reference has no CPU implementation of the path); where that build is absent it
 falls back to the CPU oracle port.
-Inputs are larger than L2 (K: 1.35 GB, gradient stream: 0.29 / 0.58 GB).
+Inputs are larger than L2 (the matrix-free product's streams: 0.53 GB; K: 1.35 GB;
+the force kernels' gradient streams: 0.29 / 0.58 GB).
 """
 from __future__ import annotations
 

@@ -161,3 +161,20 @@ def test_cpp_class_shim_builds_links_and_reports_no_device(tmp_path):
     r = subprocess.run([str(exe), str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], capture_output=True,
                        text=True, env={"CUDA_VISIBLE_DEVICES": ""})
     assert r.returncode == 3, r.stderr
+
+
+def test_bench_byte_and_flop_models_match_the_documented_configuration2_figures():
+    """The roofline's algorithmic bytes per unit (bench.py) at configuration 2
+    (480,000 TET10 elements, 674,081 nodes): the matrix-free product's 531.6 MB, the
+    fused force's 333.0 MB (FP32) / 646.8 MB (FP64), the compact stream's 131.4 MB /
+    243.6 MB."""
+    import bench as B
+
+    E, N = 480000, 674081
+    assert B.mf_apply_bytes(E, N, 10, 5) == 531555888
+    assert B.elem_force_bytes(E, N, 10, 5, 4) == 332977944
+    assert B.elem_force_bytes(E, N, 10, 5, 8) == 646755888
+    assert B.elem_force_bytes_compact(E, N, 10, 5, 4) == 131377944
+    assert B.elem_force_bytes_compact(E, N, 10, 5, 8) == 243555888
+    # the FP64 operation count behind the roofline's fp64_tflops: 312 per element and QP
+    assert B.mf_apply_flops(E, 5) == E * 5 * 312 * 2
