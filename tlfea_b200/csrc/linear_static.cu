@@ -492,11 +492,11 @@ __global__ void k_pcg_axpy_dot(int N, const double* __restrict__ dinv, double* u
 static int cg_grid(const tlfea_solver_s* s) { return s->cg_blocks; }
 
 // The matrix-free product where it applies -- SVK without damping, no preconditioner,
-// TET10 -- and, by default, where it pays: on TET4 (few QPs, small K blocks) the
-// assembled SpMV measured faster (7.5 against 5.7 solves/s at 200x20x20), and so it did
-// on meshes of a few thousand elements (12.7 against 17.4 solves/s on the 512-instance
-// batch's single-instance solves), while from about 10^5 elements the product's 2.7x
-// fewer bytes win (0.75 against 0.40 solves/s at 480,000 elements).
+// TET10 -- and, by default, where it pays: with the earlier per-node-gradient product the
+// assembled SpMV measured faster on TET4 (few QPs, small K blocks: 7.5 against 5.7
+// solves/s at 200x20x20) and on meshes of a few thousand elements (17.4 against 12.7
+// solves/s on the 512-instance batch's single-instance solves); from about 10^5 elements
+// the product wins (now 0.75 against 0.40 solves/s at 480,000 elements).
 constexpr int MF_MIN_ELEMENTS = 100000;
 
 static bool use_matrix_free(const tlfea_solver_s* s) {
