@@ -262,12 +262,13 @@ int tlfea_solver_solve(tlfea_solver s);
  * stays sqrt(r.r / r0.r0) < tol. */
 int tlfea_linear_static_set_preconditioner(tlfea_solver s, int kind);
 /* How the CG applies K (new).  2 = matrix-free where it applies (TET10, SVK, no
- * damping, no preconditioner): K p from the elements' tangent at the current positions
- * in each iteration, never assembled (K is assembled on demand, at the positions of the
- * last solve, for tlfea_linear_static_retrieve_k); 1 = the assembled K of the reference
- * (3x3 node blocks); 0 (default) = matrix-free where it applies from 100,000 elements,
- * assembled otherwise.  Both are the same operator: the solutions and iteration counts
- * agree to rounding. */
+ * damping, no preconditioner; elsewhere the assembled K): K p element by element in each
+ * iteration from the tangent at the solve's positions (F and S of every QP formed once per
+ * solve, 15 doubles per element and QP), never assembled (K is assembled on demand, at the
+ * positions of the last solve, for tlfea_linear_static_retrieve_k); 1 = the assembled K of
+ * the reference (3x3 node blocks); 0 (default) = matrix-free where it applies from 100,000
+ * elements, assembled otherwise.  Both are the same operator: the solutions and iteration
+ * counts agree to rounding. */
 int tlfea_linear_static_set_operator(tlfea_solver s, int mode);
 /* GetLastIterCount / GetLastResidual (LinearStaticSolver.cuh:68-72). */
 int tlfea_linear_static_last(tlfea_solver s, int* iters, double* rel_residual);

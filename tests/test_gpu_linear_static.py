@@ -174,7 +174,7 @@ def test_block_jacobi_pcg_matches_numpy_and_needs_fewer_iterations():
     el.Destroy()
 
 
-@pytest.mark.parametrize("order", [10, 4])
+@pytest.mark.parametrize("order", [10])  # the matrix-free operator is TET10's (TET4 keeps the assembled K)
 def test_matrix_free_operator_matches_the_assembled_stiffness(order):
     """The default matrix-free K p (the SVK tangent applied element by element in every
     CG iteration) against the assembled K of the reference: K x for random x with fixed
