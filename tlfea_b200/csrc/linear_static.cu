@@ -541,14 +541,12 @@ static MfArgs mf_args(tlfea_solver_s* s, const double* p, double* q, CgCtl* ctl)
     return M;
 }
 
-// The matrix-free product's tile kernel and its shared memory.
+// The matrix-free product's tile kernel and its shared memory (TET10: use_matrix_free
+// admits no other element type).
 using MfKernel = void (*)(MfArgs, int*);
-static MfKernel mf_kernel(const tlfea_solver_s* s) { return s->el->npe == 10 ? k_mf_geo<10, 5> : k_mf_geo<4, 1>; }
+static MfKernel mf_kernel(const tlfea_solver_s*) { return k_mf_geo<10, 5>; }
 
-static size_t mf_smem(const tlfea_solver_s* s) {
-    const int ml = s->el->tl.max_local_pad;
-    return (s->el->npe == 10) ? MfLayout<10>(ml).total : MfLayout<4>(ml).total;
-}
+static size_t mf_smem(const tlfea_solver_s* s) { return MfLayout<10>(s->el->tl.max_local_pad).total; }
 
 // q = K_bc p matrix-free and p.q, alpha (the SpMV kernel's contract).
 static int launch_mf_apply(tlfea_solver_s* s, cudaStream_t st, const double* p, double* q, CgCtl* ctl) {
@@ -738,10 +736,7 @@ int linear_static_solve(tlfea_solver_s* s) {
         if (!s->mf_tan && (st = dalloc(&s->mf_tan, ntan))) return st;
         {
             const MfArgs M = mf_args(s, s->p, s->q, s->ctl);
-            if (el->npe == 10)
-                k_mf_prep<10, 5><<<el->tl.n_tiles, TILE_ELEMS, 0, stream>>>(M);
-            else
-                k_mf_prep<4, 1><<<el->tl.n_tiles, TILE_ELEMS, 0, stream>>>(M);
+            k_mf_prep<10, 5><<<el->tl.n_tiles, TILE_ELEMS, 0, stream>>>(M);
             TLFEA_CHECK_LAUNCH();
         }
         const size_t smem = mf_smem(s);
