@@ -178,3 +178,23 @@ def test_bench_byte_and_flop_models_match_the_documented_configuration2_figures(
     assert B.elem_force_bytes_compact(E, N, 10, 5, 8) == 243555888
     # the FP64 operation count behind the roofline's fp64_tflops: 312 per element and QP
     assert B.mf_apply_flops(E, 5) == E * 5 * 312 * 2
+
+
+def test_warm_start_cases_and_features_span_their_ranges():
+    """The learned warm start's case sampler (E log-uniform, nu uniform, unit load
+    direction, uniform magnitude) and its network features (each in [-1, 1])."""
+    from tlfea_b200 import warmstart as W
+
+    c = W.sample_cases(4096, seed=3)
+    assert c.shape == (4096, 6)
+    r = W.CaseRanges()
+    assert r.E[0] <= c[:, 0].min() and c[:, 0].max() <= r.E[1]
+    assert r.nu[0] <= c[:, 1].min() and c[:, 1].max() <= r.nu[1]
+    assert np.allclose(np.linalg.norm(c[:, 2:5], axis=1), 1.0)
+    assert r.magnitude[0] <= c[:, 5].min() and c[:, 5].max() <= r.magnitude[1]
+    # log-uniform E: about half the cases below the geometric mean of the range
+    assert abs(np.mean(c[:, 0] < np.sqrt(r.E[0] * r.E[1])) - 0.5) < 0.05
+    f = W.features(c)
+    assert f.dtype == np.float32 and f.shape == (4096, 6)
+    assert f.min() >= -1.0 - 1e-6 and f.max() <= 1.0 + 1e-6
+    assert np.array_equal(W.sample_cases(16, seed=3), W.sample_cases(16, seed=3))
