@@ -1,7 +1,6 @@
 """GPU parity of the first-order solvers (SyncedNesterov, SyncedAdamW,
 SyncedAdamWNocoop) against the oracle restatements, on the cube fixture of
-examples/test_feat10_nesterov.cc and on BASELINE configuration 1 (10x2x2 TET10
-cantilever).  With a zero inner tolerance both sides run the same number of
+examples/test_feat10_nesterov.cc and on the 10x2x2 TET10 cantilever.  With a zero inner tolerance both sides run the same number of
 iterations, so trajectories compare at rel 1e-10 (FP64 mode)."""
 from pathlib import Path
 

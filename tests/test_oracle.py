@@ -17,7 +17,7 @@ LAM, MU = lame()
 
 @pytest.mark.parametrize("order", [10, 4])
 def test_box_mesh_counts_match_configs(order):
-    # BASELINE configurations: cells -> (nodes, elements); 10x2x2 T10 is 525 / 240.
+    # the benchmark meshes: cells -> (nodes, elements); 10x2x2 T10 is 525 / 240.
     for (nx, ny, nz) in [(10, 2, 2), (40, 8, 8), (100, 10, 10)]:
         nn, ne = M.box_counts(nx, ny, nz, order)
         x, y, z, conn = O.box_mesh(nx, ny, nz, order)

@@ -137,7 +137,7 @@ def write_vtk(path, x, y, z, conn):
 
 def cantilever_loads(x, y, z, total_force=(0.0, 0.0, -100.0), tol_frac=1e-9):
     """Fixed nodes at x = min(x) and the external force split equally over the
-    x = max(x) face nodes (BASELINE configuration 1 boundary conditions)."""
+    x = max(x) face nodes (the clamped-tip-loaded cantilever of the benchmark configurations)."""
     L = x.max() - x.min()
     tol = max(tol_frac * L, 1e-12)
     fixed = np.nonzero(np.abs(x - x.min()) < tol)[0].astype(np.int32)
