@@ -1,5 +1,6 @@
 // dynamics.cu -- implicit time steps for a batch of sequences on one mesh, each step
-// solved by the SyncedNesterov iteration (new: configuration 5's batched sequences).
+// solved by the SyncedNesterov iteration (new: e.g. 64 load sequences on the 100x10x10
+// TET10 cantilever advanced together).
 //
 // B sequences share one element object's mesh: its tiling and geometry stream, mass
 // pattern, fixed nodes, constraint targets and external load (gravity plus a device-side

@@ -1050,9 +1050,9 @@ int first_order_steps(tlfea_solver_s* s, int steps, const StepLoad* load, int* i
     const int n_steps = std::max(1, steps);
     st = TLFEA_OK;
     // per-phase launches by default from FO_PHASED_MIN_NODES nodes: below it the host
-    // round trip of each chunk outweighs the persistent kernel's latency (config 5's
-    // 88,641-node beam: 97 against 127 steps/s), above it the phases' occupancy wins
-    // (config 2's 674,081 nodes: 0.354 against 0.428 ms per Nesterov iteration)
+    // round trip of each chunk outweighs the persistent kernel's latency (the 100x10x10
+    // beam, 88,641 nodes: 97 against 127 steps/s), above it the phases' occupancy wins
+    // (the 200x20x20 beam, 674,081 nodes: 0.287 against 0.425 ms per Nesterov iteration)
     constexpr int FO_PHASED_MIN_NODES = 200000;
     if (s->fo_mode == 2 || (s->fo_mode == 0 && el->N >= FO_PHASED_MIN_NODES)) {
         // per-phase launches: each step's load, then its solve, then its statistics
